@@ -1,0 +1,130 @@
+/*
+ * opem_b200.h -- C ABI of the B200-native OpenParEM3D per-frequency solve stage.
+ *
+ * One library (libopem_b200.so), plain pointers and sizes, no C++ or torch
+ * types.  Every entry point returns an int status (OPEM_OK == 0, negative
+ * on error) and never exits the process.  Output buffers are owned by the
+ * caller.  One opem_context per host thread; a context owns one CUDA device
+ * and one stream.
+ *
+ * Reference seams replaced (paths inside the OpenParEM tree):
+ *   fem3D::solve                      src/OpenParEM3D/fem3D.cpp:712-799 (declared fem3D.hpp:167-168)
+ *   solveComplexLinearSystem          src/OpenParEM3D/solveComplexLinearSystem.c:100-209 (extern "C" at fem3D.cpp:24-25)
+ *   fem3D::build_A                    src/OpenParEM3D/fem3D.cpp:103-190
+ *   fem3D::buildHgrids / solveHfield  src/OpenParEM3D/fem3D.cpp:610-648, solveComplexLinearSystem.c:235-315
+ *   Mode::calculateSplits             src/OpenParEM3D/port.cpp:3524-3568
+ *   BoundaryDatabase::calculateS      src/OpenParEM3D/port.cpp:7499-7606
+ *   Result::forceReciprocal           src/OpenParEM3D/results.cpp:401-418
+ */
+#ifndef OPEM_B200_H
+#define OPEM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ----------------------------------------------------- */
+#define OPEM_OK                 0
+#define OPEM_ERR_ARG          (-1)   /* bad argument (null pointer, size, index)      */
+#define OPEM_ERR_CUDA         (-2)   /* a CUDA runtime call failed                     */
+#define OPEM_ERR_NOMEM        (-3)   /* device or host allocation failed               */
+#define OPEM_ERR_STATE        (-4)   /* call out of order (e.g. solve before assemble) */
+#define OPEM_ERR_MESH         (-5)   /* inconsistent mesh (boundary face not a mesh face, degenerate tet) */
+#define OPEM_ERR_NOT_CONVERGED (-6)  /* iteration limit reached; outputs hold the last iterate */
+#define OPEM_ERR_BREAKDOWN    (-7)   /* NaN/Inf or Krylov breakdown                    */
+#define OPEM_ERR_TIMEOUT      (-8)   /* device-side iteration/time budget exhausted    */
+#define OPEM_ERR_UNSUPPORTED  (-9)   /* order or feature not built                     */
+
+/* ---- boundary types (BoundaryDatabase attributes, src/OpenParEM3D/port.cpp:6885-7026) */
+#define OPEM_BDR_PEC        1   /* essential, E_t = 0 (fem3D.cpp:80-99)                      */
+#define OPEM_BDR_PMC        2   /* natural, nothing added                                    */
+#define OPEM_BDR_PORT       3   /* wave port; params[0] = port index                          */
+#define OPEM_BDR_IMPEDANCE  4   /* surface impedance; params = {sigma S/m, Rz m, mu_r}        */
+#define OPEM_BDR_RADIATION  5   /* 1st-order RBC; params[0] = wave impedance ohm (<=0: eta0)  */
+
+/* ---- precision modes ----------------------------------------------------- */
+#define OPEM_PREC_FP64      0   /* plain FP64 GMRES (the drop-in)                             */
+#define OPEM_PREC_MIXED     1   /* FP32 inner GMRES + polynomial/block-Jacobi, FP64 refinement */
+
+typedef struct opem_context_s* opem_context;
+typedef struct opem_problem_s* opem_problem;
+
+/* Solver options (solveComplexLinearSystem.c:131-141 defaults shown in brackets). */
+typedef struct {
+    double rtol;          /* relative residual tolerance [1e-10]                            */
+    int    maxits;        /* total inner iteration limit [5000]                              */
+    int    restart;       /* GMRES restart length m [150]                                    */
+    int    precision;     /* OPEM_PREC_FP64 or OPEM_PREC_MIXED                               */
+    int    poly_degree;   /* polynomial preconditioner degree (mixed mode), 0 = none [0]     */
+    int    force_reciprocal; /* S <- (S+S^T)/2 (results.cpp:401-418) [1]                      */
+    int    h_maxits;      /* iteration limit of the H projection CG [2000]                    */
+    double h_rtol;        /* tolerance of the H projection CG [1e-12]                         */
+} opem_solver_opts;
+
+typedef struct {
+    int    iterations;    /* inner iterations summed over driving sets                      */
+    int    outer;         /* refinement (outer) steps, mixed mode                            */
+    int    h_iterations;  /* CG iterations of the H projection                               */
+    int    converged;     /* 1 if every driving set met rtol                                  */
+    double rnorm;         /* worst final relative residual ||b-Ax||/||b|| (FP64)             */
+    double seconds;       /* device time of the whole call                                    */
+} opem_solve_stats;
+
+/* ---- context ----------------------------------------------------------- */
+int  opem_context_create(int device, opem_context* out);
+int  opem_context_destroy(opem_context ctx);
+/* Last error message of this context (static storage inside ctx). */
+const char* opem_context_last_error(opem_context ctx);
+void opem_default_opts(opem_solver_opts* opts);
+
+/* ---- problem setup (fem3D::build_fe_spaces, fem3D.cpp:65-78; mesh load OpenParEM3D.cpp:284-327)
+ * verts: nverts*3 doubles (m); tets: ntets*4 int64 (0-based vertex ids);
+ * tet_region: ntets int32 region index; bdr_tris: nbdr*3 int64; bdr_attr: nbdr int32 (>=1).
+ * order: Nedelec order p (ND_FECollection(p,3)); 1..3 are supported.          */
+int  opem_problem_create(opem_context ctx, int64_t nverts, const double* verts,
+                         int64_t ntets, const int64_t* tets, const int32_t* tet_region,
+                         int64_t nbdr, const int64_t* bdr_tris, const int32_t* bdr_attr,
+                         int order, opem_problem* out);
+int  opem_problem_destroy(opem_problem prob);
+/* Region materials (per-region PWConstCoefficients, OpenParEM3D.cpp:394-437): relative
+ * permittivity, loss tangent, conductivity (S/m), relative permeability.          */
+int  opem_problem_set_regions(opem_problem prob, int nregions, const double* eps_r,
+                              const double* tand, const double* sigma, const double* mu_r);
+int  opem_problem_set_boundary(opem_problem prob, int attr, int type, const double* params, int nparams);
+/* Analytic rectangular TE_mn port mode (the data load_modeMetrics reads, port.cpp:5302-5453).
+ * desc = {origin xyz, u-axis xyz, v-axis xyz, outward normal xyz, a, b, m, n,
+ *         voltage path start xyz, voltage path end xyz}  (22 doubles).          */
+int  opem_problem_set_port_te(opem_problem prob, int port, const double* desc);
+/* Builds DOF numbering, CSR pattern, vertex patches, and assembles the frequency-
+ * independent operators on the device.                                         */
+int  opem_problem_assemble(opem_problem prob);
+/* info[0]=ndofs, [1]=nnz, [2]=nports, [3]=npatches, [4]=max patch size, [5]=local dofs,
+ * [6]=device bytes held.                                                        */
+int  opem_problem_info(opem_problem prob, int64_t* info, int ninfo);
+
+/* ---- the per-frequency solve (fem3D::solve + calculateSplits + calculateS) ----
+ * S_out: nports*nports complex (interleaved re,im), row = portOut, col = portIn.
+ * Zo_out: nports complex (may be NULL).  stats may be NULL.                     */
+int  opem_solve_frequency(opem_problem prob, double freq, const opem_solver_opts* opts,
+                          double* S_out, double* Zo_out, opem_solve_stats* stats);
+/* A sweep: nfreq frequencies x all driving sets in one call (batched in mixed mode).
+ * S_out: nfreq*nports*nports complex.  stats: nfreq entries (may be NULL).      */
+int  opem_solve_sweep(opem_problem prob, int nfreq, const double* freqs, const opem_solver_opts* opts,
+                      double* S_out, opem_solve_stats* stats);
+/* E and H DOF vectors (ndofs complex each, interleaved) of the last single-frequency
+ * solve for driving set d (0-based).  Either pointer may be NULL.               */
+int  opem_get_fields(opem_problem prob, int d, double* e_out, double* h_out);
+
+/* ---- operator-level access (parity tests; fem3D::build_A / build_P / build_Q)
+ * which: 0=K(1/mu_r) 1=M(eps_r) 2=M(eps_r tand) 3=M(sigma) 4=M(1) 5=Q(1/mu_r)
+ * rowptr: ndofs+1 int64, cols: nnz int32, vals: nnz doubles. Any may be NULL.   */
+int  opem_get_operator(opem_problem prob, int which, int64_t* rowptr, int32_t* cols, double* vals);
+/* Complex A(freq) for driving set d (before Dirichlet handling), nnz complex.   */
+int  opem_get_system_matrix(opem_problem prob, double freq, int d, double* vals);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OPEM_B200_H */

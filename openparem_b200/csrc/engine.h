@@ -1,0 +1,140 @@
+// Host-side engine state shared by the .cu files (internal).
+#pragma once
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "opem_device.h"
+#include "opem_internal.h"
+
+namespace opem {
+
+#define OPEM_CUDA(call)                                                                   \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+struct CudaError : std::runtime_error {
+    explicit CudaError(const std::string& s) : std::runtime_error(s) {}
+};
+struct OpemError : std::runtime_error {
+    int code;
+    OpemError(int c, const std::string& s) : std::runtime_error(s), code(c) {}
+};
+
+// RAII device buffer
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    explicit DBuf(size_t n_) { alloc(n_); }
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    DBuf(DBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DBuf& operator=(DBuf&& o) noexcept { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; return *this; }
+    ~DBuf() { release(); }
+    void alloc(size_t n_) {
+        release();
+        n = n_;
+        if (n) {
+            cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+            if (e != cudaSuccess) { p = nullptr; n = 0; throw OpemError(OPEM_ERR_NOMEM, "cudaMalloc failed"); }
+        }
+    }
+    void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
+    void upload(const T* h, size_t cnt, cudaStream_t s) { OPEM_CUDA(cudaMemcpyAsync(p, h, cnt * sizeof(T), cudaMemcpyHostToDevice, s)); }
+    void upload(const std::vector<T>& v, cudaStream_t s) { if (v.size() > n) alloc(v.size()); if (!v.empty()) upload(v.data(), v.size(), s); }
+    void zero(cudaStream_t s) { if (n) OPEM_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s)); }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+struct Context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    double* pinned = nullptr;     // small host-mapped scratch for scalars
+    int sm_count = 148;
+};
+
+// A boundary group: every boundary triangle of one attribute that adds a
+// term to A (port ABC, impedance, radiation).
+struct BGroup {
+    int attr = 0, type = 0, port = -1;
+    double sigma = 0, Rz = 0, mu_r = 1, eta = 0;
+    std::vector<int32_t> faces;            // global face ids
+    int64_t nu = 0;                        // unique CSR slots
+    std::vector<int32_t> h_urow, h_ucol;   // row/col of each unique slot
+    DBuf<int32_t> uslot, urow, ucol;       // device
+    DBuf<double> R;                        // 5*nu: cc, eps, tand, sig, one
+    // boundary CSR over the group's rows (for the batched SpMV correction)
+    std::vector<int32_t> h_brow, h_bptr;
+    DBuf<int32_t> brow, bptr;
+};
+
+struct PortMode {
+    bool set = false;
+    double desc[26];
+};
+
+struct Problem {
+    Context* ctx = nullptr;
+    Topology topo;
+    int nregions = 0;
+    std::vector<double> eps_r, tand, sigma, mu_r;   // per region
+    struct Bdr { int type = 0; double params[3] = {0, 0, 0}; };
+    std::vector<std::pair<int, Bdr>> bdr;           // attr -> type
+    int nports = 0;
+    std::vector<PortMode> modes;
+    bool assembled = false;
+
+    // device mesh/operator data
+    DBuf<double> d_verts;
+    DBuf<int32_t> d_tets, d_region, d_elem_dofs;
+    DBuf<ElemGeo> d_geo;
+    DBuf<int32_t> d_rowptr, d_cols, d_d2e_ptr, d_d2e_elem;
+    DBuf<uint8_t> d_d2e_loc;
+    DBuf<double> d_ref;         // Kh(6) | Mh(6) | Qh, ld*ld each
+    DBuf<double> d_K, d_Meps, d_Mtand, d_Msig, d_M1, d_Q;
+    DBuf<float> f_K, f_Meps, f_Mtand, f_Msig;   // FP32 copies (mixed path)
+    bool has_tand = false, has_sig = false;
+    DBuf<double> d_elemcoef;    // per element: inv_mu, eps, eps*tand, sigma
+    std::vector<BGroup> groups;
+    // Dirichlet masks
+    std::vector<uint8_t> h_pec, h_portmask;
+    DBuf<uint8_t> d_pec, d_portmask;
+    std::vector<std::vector<int32_t>> port_dofs;   // all dofs on each port's faces
+    // port mode traces (frequency-independent shapes)
+    std::vector<std::vector<double>> et_trace;     // per port: n complex (only port dofs nonzero)
+    std::vector<std::vector<double>> nxe_trace;    // per port: trace of n x Et
+    DBuf<double> d_et, d_nxe;                      // nports * n complex
+    // vertex patches
+    DBuf<int32_t> d_patch_ptr, d_patch_dofs, d_d2p_ptr, d_d2p_idx;
+    DBuf<int64_t> d_patch_off;
+    int npatch = 0;
+    // last fields per driving set
+    std::vector<std::vector<double>> last_e, last_h;
+    int64_t device_bytes() const;
+};
+
+// ---- assembly (assemble.cu)
+void assemble_volume(Problem& P);
+void assemble_boundary(Problem& P);
+// A = K + vc.c_eps*Meps + ... plus boundary groups (FP64 complex, nnz)
+void form_system_matrix(Problem& P, const VolCoef& vc, const std::vector<BCoef>& bc, double2* A);
+// host: coefficients of A(freq) for driving set d
+void system_coefficients(const Problem& P, double freq, int d, VolCoef& vc, std::vector<BCoef>& bc);
+void port_gamma_Z_V(const Problem& P, int port, double freq, cd& gamma, cd& Z, cd& V);
+// overlaps <a, B_port b> for port k: out = conj(a)^T R_one b over the port's slots
+void port_overlap(Problem& P, int k, const double2* a, const double2* b, double2* out_dev);
+
+// ---- krylov / preconditioner (krylov.cu)
+struct SolveResult { int its = 0; int converged = 0; double relres = 0; int code = OPEM_OK; };
+SolveResult solve_plain_fp64(Problem& P, const double2* A, const uint8_t* dmask_dev, const double2* b,
+                             double2* x, const opem_solver_opts& o);
+SolveResult solve_mass_cg(Problem& P, const double2* b, double2* x, double rtol, int maxits);
+void spmv_real_complex(Problem& P, const double* vals, const double2* x, double2* y, double scale_re, double scale_im);
+void spmv_complex(Problem& P, const double2* A, const double2* x, double2* y, const uint8_t* zero_rows);
+
+}  // namespace opem

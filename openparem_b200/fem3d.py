@@ -1,0 +1,196 @@
+"""Host-side mirror of OpenParEM3D's per-frequency solve interface.
+
+``Fem3D`` plays the role of the reference's ``fem3D`` object for one mesh
+(src/OpenParEM3D/fem3D.hpp:70-192): ``build_fe_spaces``/``assemble`` set up
+the Nedelec space and operators, ``solve`` runs one frequency over every
+driving set (fem3D::solve + Mode::calculateSplits + BoundaryDatabase::calculateS),
+and ``fields`` returns the E and H DOF vectors.  Everything runs through the
+C ABI of libopem_b200.so on one CUDA device; errors raise ``OpemError``
+carrying the ABI status code, the way the reference returns a PetscErrorCode
+or ``true`` on failure.
+"""
+import ctypes as C
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import _lib
+from ._lib import SolverOpts, SolveStats
+
+
+class OpemError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{_lib.ERROR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def _dp(a):
+    return a.ctypes.data_as(_lib.DP)
+
+
+def _chk(ctx, rc, what):
+    if rc != _lib.OK:
+        msg = _lib.lib().opem_context_last_error(ctx).decode() if ctx else ""
+        raise OpemError(rc, f"{what}: {msg}")
+
+
+class Context:
+    """One CUDA device + stream (opem_context)."""
+
+    def __init__(self, device=0):
+        self.h = C.c_void_p()
+        rc = _lib.lib().opem_context_create(int(device), C.byref(self.h))
+        if rc != _lib.OK:
+            raise OpemError(rc, "opem_context_create")
+
+    def close(self):
+        if self.h:
+            _lib.lib().opem_context_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def default_opts(**kw):
+    o = SolverOpts()
+    _lib.lib().opem_default_opts(C.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise KeyError(k)
+        setattr(o, k, v)
+    return o
+
+
+def te_descriptor(mode):
+    """Pack a rectangular TE_mn mode dict into the ABI's 22 doubles."""
+    d = np.zeros(22)
+    d[0:3] = mode["origin"]; d[3:6] = mode["u"]; d[6:9] = mode["v"]; d[9:12] = mode["normal"]
+    d[12] = mode["a"]; d[13] = mode["b"]; d[14] = mode["m"]; d[15] = mode["n"]
+    d[16:19] = mode["vpath"][0]; d[19:22] = mode["vpath"][1]
+    return d
+
+
+_BTYPES = {"pec": _lib.BDR_PEC, "pmc": _lib.BDR_PMC, "port": _lib.BDR_PORT, "impedance": _lib.BDR_IMPEDANCE,
+           "radiation": _lib.BDR_RADIATION}
+
+
+class Fem3D:
+    """One mesh + materials + boundaries resident on the device."""
+
+    def __init__(self, prob, context=None, device=0):
+        self.ctx = context if context is not None else Context(device)
+        self.prob = prob
+        L = _lib.lib()
+        verts = np.ascontiguousarray(prob["verts"], dtype=np.float64)
+        tets = np.ascontiguousarray(prob["tets"], dtype=np.int64)
+        reg = np.ascontiguousarray(prob["tet_region"], dtype=np.int32)
+        tris = np.ascontiguousarray(prob["bdr_tris"], dtype=np.int64)
+        attr = np.ascontiguousarray(prob["bdr_attr"], dtype=np.int32)
+        self.h = C.c_void_p()
+        rc = L.opem_problem_create(self.ctx.h, len(verts), _dp(verts), len(tets), tets.ctypes.data_as(_lib.I64P),
+                                   reg.ctypes.data_as(_lib.I32P), len(tris), tris.ctypes.data_as(_lib.I64P),
+                                   attr.ctypes.data_as(_lib.I32P), int(prob["order"]), C.byref(self.h))
+        _chk(self.ctx.h, rc, "opem_problem_create")
+        er = np.ascontiguousarray(prob["eps_r"], dtype=np.float64)
+        td = np.ascontiguousarray(prob["tand"], dtype=np.float64)
+        sg = np.ascontiguousarray(prob["sigma"], dtype=np.float64)
+        mr = np.ascontiguousarray(prob["mu_r"], dtype=np.float64)
+        _chk(self.ctx.h, L.opem_problem_set_regions(self.h, len(er), _dp(er), _dp(td), _dp(sg), _dp(mr)), "set_regions")
+        for a, spec in prob["boundaries"].items():
+            t = _BTYPES[spec["type"]]
+            if spec["type"] == "port":
+                pr = np.array([float(spec["port"])])
+            elif spec["type"] == "impedance":
+                pr = np.array([spec["sigma"], spec.get("Rz", 0.0), spec.get("mu_r", 1.0)])
+            elif spec["type"] == "radiation":
+                pr = np.array([spec.get("wave_impedance", 0.0)])
+            else:
+                pr = np.zeros(0)
+            pr = np.ascontiguousarray(pr, dtype=np.float64)
+            _chk(self.ctx.h, L.opem_problem_set_boundary(self.h, int(a), t, _dp(pr) if len(pr) else None, len(pr)),
+                 "set_boundary")
+        for k, port in enumerate(prob["ports"]):
+            d = te_descriptor(port["mode"])
+            _chk(self.ctx.h, L.opem_problem_set_port_te(self.h, k, _dp(d)), "set_port_te")
+        self.nports = len(prob["ports"])
+        self._assembled = False
+
+    # fem3D::build_fe_spaces + build_A's frequency-independent part
+    def assemble(self):
+        _chk(self.ctx.h, _lib.lib().opem_problem_assemble(self.h), "opem_problem_assemble")
+        self._assembled = True
+        return self
+
+    def info(self):
+        a = np.zeros(7, dtype=np.int64)
+        _chk(self.ctx.h, _lib.lib().opem_problem_info(self.h, a.ctypes.data_as(_lib.I64P), 7), "info")
+        keys = ["ndofs", "nnz", "nports", "npatches", "max_patch", "local_dofs", "device_bytes"]
+        return dict(zip(keys, (int(v) for v in a)))
+
+    def solve(self, freq, opts=None, allow_not_converged=False):
+        """One frequency point over every driving set -> (S (N,N) complex, Zo, stats)."""
+        N = self.nports
+        S = np.zeros(2 * N * N)
+        Z = np.zeros(2 * N)
+        st = SolveStats()
+        o = opts if opts is not None else default_opts()
+        rc = _lib.lib().opem_solve_frequency(self.h, float(freq), C.byref(o), _dp(S), _dp(Z), C.byref(st))
+        if rc == _lib.ERR_NOT_CONVERGED and allow_not_converged:
+            rc = _lib.OK
+        _chk(self.ctx.h, rc, "opem_solve_frequency")
+        return (S[0::2] + 1j * S[1::2]).reshape(N, N), Z[0::2] + 1j * Z[1::2], st.as_dict()
+
+    def sweep(self, freqs, opts=None):
+        freqs = np.ascontiguousarray(freqs, dtype=np.float64)
+        N = self.nports
+        S = np.zeros(2 * N * N * len(freqs))
+        st = (SolveStats * len(freqs))()
+        o = opts if opts is not None else default_opts()
+        rc = _lib.lib().opem_solve_sweep(self.h, len(freqs), _dp(freqs), C.byref(o), _dp(S), st)
+        _chk(self.ctx.h, rc, "opem_solve_sweep")
+        return (S[0::2] + 1j * S[1::2]).reshape(len(freqs), N, N), [s.as_dict() for s in st]
+
+    def fields(self, d):
+        n = self.info()["ndofs"]
+        e = np.zeros(2 * n)
+        h = np.zeros(2 * n)
+        _chk(self.ctx.h, _lib.lib().opem_get_fields(self.h, int(d), _dp(e), _dp(h)), "opem_get_fields")
+        return e[0::2] + 1j * e[1::2], h[0::2] + 1j * h[1::2]
+
+    OPERATORS = {"K": 0, "M_eps": 1, "M_tand": 2, "M_sig": 3, "M1": 4, "Q_mu": 5}
+
+    def operator(self, name):
+        inf = self.info()
+        n, nnz = inf["ndofs"], inf["nnz"]
+        rp = np.zeros(n + 1, dtype=np.int64)
+        cols = np.zeros(nnz, dtype=np.int32)
+        vals = np.zeros(nnz)
+        _chk(self.ctx.h, _lib.lib().opem_get_operator(self.h, self.OPERATORS[name], rp.ctypes.data_as(_lib.I64P),
+                                                      cols.ctypes.data_as(_lib.I32P), _dp(vals)), "get_operator")
+        return sp.csr_matrix((vals, cols, rp), shape=(n, n))
+
+    def system_matrix(self, freq, d):
+        inf = self.info()
+        n, nnz = inf["ndofs"], inf["nnz"]
+        rp = np.zeros(n + 1, dtype=np.int64)
+        cols = np.zeros(nnz, dtype=np.int32)
+        _chk(self.ctx.h, _lib.lib().opem_get_operator(self.h, 0, rp.ctypes.data_as(_lib.I64P),
+                                                      cols.ctypes.data_as(_lib.I32P), None), "get_operator")
+        v = np.zeros(2 * nnz)
+        _chk(self.ctx.h, _lib.lib().opem_get_system_matrix(self.h, float(freq), int(d), _dp(v)), "system_matrix")
+        return sp.csr_matrix((v[0::2] + 1j * v[1::2], cols, rp), shape=(n, n))
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.lib().opem_problem_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
