@@ -124,6 +124,16 @@ int  opem_get_operator(opem_problem prob, int which, int64_t* rowptr, int32_t* c
 /* Complex A(freq) for driving set d (before Dirichlet handling), nnz complex.   */
 int  opem_get_system_matrix(opem_problem prob, double freq, int d, double* vals);
 
+/* ---- measurement support (no reference counterpart) -------------------------
+ * Kernel launches issued by this context so far.                                */
+int  opem_context_launches(opem_context ctx, int64_t* out);
+/* Times the hot kernels of the FP64 path in isolation on the context stream with
+ * CUDA events (A(freq) for driving set 0): reps launches each.  out receives
+ * nkern*3 doubles: {ms per launch, algorithmic bytes per launch, launches}, for
+ * kernels 0 = complex CSR SpMV, 1 = vertex-patch block apply, 2 = CGS2 step
+ * against 64 Krylov vectors (dot + update).                                     */
+int  opem_profile_kernels(opem_problem prob, double freq, int reps, double* out, int nout);
+
 #ifdef __cplusplus
 }
 #endif

@@ -59,6 +59,8 @@ SIGNATURES = [
     ("opem_get_fields", C.c_int, [P, C.c_int, DP, DP]),
     ("opem_get_operator", C.c_int, [P, C.c_int, I64P, I32P, DP]),
     ("opem_get_system_matrix", C.c_int, [P, C.c_double, C.c_int, DP]),
+    ("opem_context_launches", C.c_int, [P, I64P]),
+    ("opem_profile_kernels", C.c_int, [P, C.c_double, C.c_int, DP, C.c_int]),
 ]
 
 

@@ -24,7 +24,6 @@
 
 namespace opem {
 
-static const int FACES_H[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
 __constant__ int c_faces[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
 
 __global__ void geo_kernel(int64_t ne, const double* __restrict__ verts, const int32_t* __restrict__ tets,
@@ -148,7 +147,7 @@ static void launch_assemble(Problem& P, cudaStream_t s) {
     int grid = std::max(1, bpsm) * P.ctx->sm_count;
     kern<<<grid, 256, smem, s>>>(P.topo.n, P.d_rowptr.p, P.d_cols.p, P.d_d2e_ptr.p, P.d_d2e_elem.p, P.d_d2e_loc.p,
                                  P.d_elem_dofs.p, P.d_geo.p, P.d_elemcoef.p, P.d_ref.p, P.d_K.p, P.d_Meps.p,
-                                 P.has_tand ? P.d_Mtand.p : nullptr, P.has_sig ? P.d_Msig.p : nullptr, P.d_M1.p, P.d_Q.p);
+                                 P.has_tand ? P.d_Mtand.p : nullptr, P.has_sig ? P.d_Msig.p : nullptr, P.d_M1.p, P.d_Q.p); ++P.ctx->launches;
     OPEM_CUDA(cudaGetLastError());
 }
 
@@ -179,7 +178,7 @@ void assemble_volume(Problem& P) {
     P.d_ref.upload(ref, s);
     // element geometry and material coefficients
     P.d_geo.alloc(T.ne);
-    geo_kernel<<<(unsigned)((T.ne + 255) / 256), 256, 0, s>>>(T.ne, P.d_verts.p, P.d_tets.p, P.d_geo.p);
+    geo_kernel<<<(unsigned)((T.ne + 255) / 256), 256, 0, s>>>(T.ne, P.d_verts.p, P.d_tets.p, P.d_geo.p); ++P.ctx->launches;
     OPEM_CUDA(cudaGetLastError());
     std::vector<double> mat(4 * P.nregions);
     P.has_tand = P.has_sig = false;
@@ -191,7 +190,7 @@ void assemble_volume(Problem& P) {
     DBuf<double> d_mat;
     d_mat.upload(mat, s);
     P.d_elemcoef.alloc(4 * T.ne);
-    elem_coef_kernel<<<(unsigned)((T.ne + 255) / 256), 256, 0, s>>>(T.ne, P.d_region.p, d_mat.p, P.nregions, P.d_elemcoef.p);
+    elem_coef_kernel<<<(unsigned)((T.ne + 255) / 256), 256, 0, s>>>(T.ne, P.d_region.p, d_mat.p, P.nregions, P.d_elemcoef.p); ++P.ctx->launches;
     OPEM_CUDA(cudaGetLastError());
     size_t nnz = T.cols.size();
     P.d_K.alloc(nnz); P.d_Meps.alloc(nnz); P.d_M1.alloc(nnz); P.d_Q.alloc(nnz);
@@ -341,11 +340,11 @@ void assemble_boundary(Problem& P) {
         d_faces.upload(G.faces, s);
         DBuf<FaceGeo> d_fg(nf);
         face_geo_kernel<<<(nf + 127) / 128, 128, 0, s>>>(nf, d_faces.p, d_owner.p, d_lface.p, P.d_tets.p, P.d_verts.p,
-                                                         P.d_elemcoef.p, d_fg.p);
+                                                         P.d_elemcoef.p, d_fg.p); ++P.ctx->launches;
         OPEM_CUDA(cudaGetLastError());
         G.R.alloc(5 * G.nu);
         boundary_reduce_kernel<<<(unsigned)((G.nu + 127) / 128), 128, 0, s>>>(G.nu, ldf, d_uptr.p, d_uent.p, d_fg.p,
-                                                                             d_ftab.p, G.R.p);
+                                                                             d_ftab.p, G.R.p); ++P.ctx->launches;
         OPEM_CUDA(cudaGetLastError());
         OPEM_CUDA(cudaStreamSynchronize(s));
     }
@@ -381,7 +380,7 @@ void form_system_matrix(Problem& P, const VolCoef& vc, const std::vector<BCoef>&
     cudaStream_t s = P.ctx->stream;
     int64_t nnz = (int64_t)P.topo.cols.size();
     combine_kernel<<<P.ctx->sm_count * 8, 256, 0, s>>>(nnz, P.d_K.p, P.d_Meps.p, P.has_tand ? P.d_Mtand.p : nullptr,
-                                                       P.has_sig ? P.d_Msig.p : nullptr, vc, A);
+                                                       P.has_sig ? P.d_Msig.p : nullptr, vc, A); ++P.ctx->launches;
     OPEM_CUDA(cudaGetLastError());
     for (size_t g = 0; g < P.groups.size(); ++g) {
         BGroup& G = P.groups[g];
@@ -390,7 +389,7 @@ void form_system_matrix(Problem& P, const VolCoef& vc, const std::vector<BCoef>&
         if (c.c_cc.x == 0 && c.c_cc.y == 0 && c.c_eps.x == 0 && c.c_eps.y == 0 && c.c_tand.x == 0 && c.c_tand.y == 0 &&
             c.c_sig.x == 0 && c.c_sig.y == 0 && c.c_one.x == 0 && c.c_one.y == 0)
             continue;
-        boundary_add_kernel<<<(unsigned)((G.nu + 255) / 256), 256, 0, s>>>(G.nu, G.uslot.p, G.R.p, c, A);
+        boundary_add_kernel<<<(unsigned)((G.nu + 255) / 256), 256, 0, s>>>(G.nu, G.uslot.p, G.R.p, c, A); ++P.ctx->launches;
         OPEM_CUDA(cudaGetLastError());
     }
 }
@@ -423,7 +422,7 @@ __global__ void overlap_kernel(int64_t nu, const int32_t* __restrict__ urow, con
 void port_overlap(Problem& P, int k, const double2* a, const double2* b, double2* out_dev) {
     for (BGroup& G : P.groups) {
         if (G.type != OPEM_BDR_PORT || G.port != k || G.nu == 0) continue;
-        overlap_kernel<<<1, 256, 0, P.ctx->stream>>>(G.nu, G.urow.p, G.ucol.p, G.R.p + 4 * G.nu, a, b, out_dev);
+        overlap_kernel<<<1, 256, 0, P.ctx->stream>>>(G.nu, G.urow.p, G.ucol.p, G.R.p + 4 * G.nu, a, b, out_dev); ++P.ctx->launches;
         OPEM_CUDA(cudaGetLastError());
         return;
     }

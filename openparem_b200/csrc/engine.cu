@@ -306,12 +306,12 @@ static void solve_frequency_plain(Problem& P, double freq, const opem_solver_opt
         std::vector<BCoef> bc;
         system_coefficients(P, freq, d, vc, bc);
         form_system_matrix(P, vc, bc, A.p);
-        dmask_kernel<<<vg, 256, 0, s>>>(n, P.d_pec.p, P.d_portmask.p, d, dm.p);
+        dmask_kernel<<<vg, 256, 0, s>>>(n, P.d_pec.p, P.d_portmask.p, d, dm.p); ++P.ctx->launches;
         const double2* et = reinterpret_cast<const double2*>(P.d_et.p) + (size_t)d * n;
-        lift_kernel<<<vg, 256, 0, s>>>(n, et, P.d_pec.p, x0.p);
+        lift_kernel<<<vg, 256, 0, s>>>(n, et, P.d_pec.p, x0.p); ++P.ctx->launches;
         // b_F = -(A x0'')_F
         spmv_complex(P, A.p, x0.p, b.p, dm.p);
-        cscale_kernel<<<vg, 256, 0, s>>>(n, make_double2(-1, 0), b.p, b.p);
+        cscale_kernel<<<vg, 256, 0, s>>>(n, make_double2(-1, 0), b.p, b.p); ++P.ctx->launches;
         OPEM_CUDA(cudaGetLastError());
         SolveResult r = solve_plain_fp64(P, A.p, dm.p, b.p, x.p, o);
         out.st.iterations += r.its;
@@ -319,7 +319,7 @@ static void solve_frequency_plain(Problem& P, double freq, const opem_solver_opt
         if (!r.converged) out.st.converged = 0;
         if (r.code != OPEM_OK && r.code != OPEM_ERR_NOT_CONVERGED) throw OpemError(r.code, "E-field solve failed");
         // e = x_F + x0 on the driven port (identity rows keep x0 there)
-        add_kernel<<<vg, 256, 0, s>>>(n, et, x.p);
+        add_kernel<<<vg, 256, 0, s>>>(n, et, x.p); ++P.ctx->launches;
         // H: M1 h = (j / (w mu0)) Q_mu e
         spmv_real_complex(P, P.d_Q.p, x.p, bh.p, 0.0, 1.0 / (w * MU0));
         SolveResult rh = solve_mass_cg(P, bh.p, h.p, o.h_rtol, o.h_maxits);
@@ -724,6 +724,31 @@ int opem_get_system_matrix(opem_problem prob, double freq, int d, double* vals) 
         form_system_matrix(P, vc, bc, A.p);
         OPEM_CUDA(cudaStreamSynchronize(P.ctx->stream));
         OPEM_CUDA(cudaMemcpy(vals, A.p, nnz * sizeof(double2), cudaMemcpyDeviceToHost));
+    });
+}
+
+int opem_context_launches(opem_context ctx, int64_t* out) {
+    if (!ctx || !out) return OPEM_ERR_ARG;
+    *out = ctx->c.launches;
+    return OPEM_OK;
+}
+
+int opem_profile_kernels(opem_problem prob, double freq, int reps, double* out, int nout) {
+    if (!prob || !out || nout < 12 || reps <= 0 || !(freq > 0)) return OPEM_ERR_ARG;
+    Problem& P = prob->p;
+    if (!P.assembled) return OPEM_ERR_STATE;
+    return guarded(P.ctx, [&] {
+        OPEM_CUDA(cudaSetDevice(P.ctx->device));
+        const int64_t n = P.topo.n;
+        DBuf<double2> A(P.topo.cols.size());
+        DBuf<uint8_t> dm(n);
+        VolCoef vc;
+        std::vector<BCoef> bc;
+        system_coefficients(P, freq, 0, vc, bc);
+        form_system_matrix(P, vc, bc, A.p);
+        dmask_kernel<<<P.ctx->sm_count * 8, 256, 0, P.ctx->stream>>>(n, P.d_pec.p, P.d_portmask.p, 0, dm.p);
+        ++P.ctx->launches;
+        profile_fp64(P, A.p, dm.p, reps, out);
     });
 }
 

@@ -56,6 +56,7 @@ struct Context {
     std::string last_error;
     double* pinned = nullptr;     // small host-mapped scratch for scalars
     int sm_count = 148;
+    int64_t launches = 0;         // kernels this context has launched (bench accounting)
 };
 
 // A boundary group: every boundary triangle of one attribute that adds a
@@ -136,5 +137,6 @@ SolveResult solve_plain_fp64(Problem& P, const double2* A, const uint8_t* dmask_
 SolveResult solve_mass_cg(Problem& P, const double2* b, double2* x, double rtol, int maxits);
 void spmv_real_complex(Problem& P, const double* vals, const double2* x, double2* y, double scale_re, double scale_im);
 void spmv_complex(Problem& P, const double2* A, const double2* x, double2* y, const uint8_t* zero_rows);
+void profile_fp64(Problem& P, const double2* A, const uint8_t* dmask, int reps, double* out);
 
 }  // namespace opem

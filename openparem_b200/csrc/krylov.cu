@@ -85,6 +85,7 @@ void spmv_complex(Problem& P, const double2* A, const double2* x, double2* y, co
     if (tpr == 32) spmv_c64_kernel<32><<<grid, 256, 0, s>>>(n, P.d_rowptr.p, P.d_cols.p, A, x, y, zero_rows, one);
     else if (tpr == 16) spmv_c64_kernel<16><<<grid, 256, 0, s>>>(n, P.d_rowptr.p, P.d_cols.p, A, x, y, zero_rows, one);
     else spmv_c64_kernel<8><<<grid, 256, 0, s>>>(n, P.d_rowptr.p, P.d_cols.p, A, x, y, zero_rows, one);
+    ++P.ctx->launches;
     OPEM_CUDA(cudaGetLastError());
 }
 
@@ -97,6 +98,7 @@ static void spmv_complex_scaled(Problem& P, const double2* A, const double2* x, 
     if (tpr == 32) spmv_c64_kernel<32><<<grid, 256, 0, s>>>(n, P.d_rowptr.p, P.d_cols.p, A, x, y, zero_rows, scale);
     else if (tpr == 16) spmv_c64_kernel<16><<<grid, 256, 0, s>>>(n, P.d_rowptr.p, P.d_cols.p, A, x, y, zero_rows, scale);
     else spmv_c64_kernel<8><<<grid, 256, 0, s>>>(n, P.d_rowptr.p, P.d_cols.p, A, x, y, zero_rows, scale);
+    ++P.ctx->launches;
     OPEM_CUDA(cudaGetLastError());
 }
 
@@ -109,6 +111,7 @@ void spmv_real_complex(Problem& P, const double* vals, const double2* x, double2
     if (tpr == 32) spmv_rc64_kernel<32><<<grid, 256, 0, s>>>(n, P.d_rowptr.p, P.d_cols.p, vals, x, y, sc);
     else if (tpr == 16) spmv_rc64_kernel<16><<<grid, 256, 0, s>>>(n, P.d_rowptr.p, P.d_cols.p, vals, x, y, sc);
     else spmv_rc64_kernel<8><<<grid, 256, 0, s>>>(n, P.d_rowptr.p, P.d_cols.p, vals, x, y, sc);
+    ++P.ctx->launches;
     OPEM_CUDA(cudaGetLastError());
 }
 
@@ -507,15 +510,15 @@ static void dot_many(Problem& P, Red& R, const double2* V, int64_t ldv, int nvec
     cudaStream_t s = P.ctx->stream;
     int64_t n = P.topo.n;
     dim3 grid(RED_BLOCKS, nvec);
-    multidot_kernel<<<grid, 256, 0, s>>>(n, V, ldv, w, R.part.p);
-    finish_dot_kernel<<<nvec, 256, 0, s>>>(RED_BLOCKS, R.part.p, R.out.p, Hcol, accumulate);
+    multidot_kernel<<<grid, 256, 0, s>>>(n, V, ldv, w, R.part.p); ++P.ctx->launches;
+    finish_dot_kernel<<<nvec, 256, 0, s>>>(RED_BLOCKS, R.part.p, R.out.p, Hcol, accumulate); ++P.ctx->launches;
     OPEM_CUDA(cudaGetLastError());
 }
 
 static void nrm2_dev(Problem& P, Red& R, const double2* w, double2* sq_out) {
     cudaStream_t s = P.ctx->stream;
-    nrm2_partial_kernel<<<RED_BLOCKS, 256, 0, s>>>(P.topo.n, w, R.part.p);
-    finish_dot_kernel<<<1, 256, 0, s>>>(RED_BLOCKS, R.part.p, sq_out, nullptr, 0);
+    nrm2_partial_kernel<<<RED_BLOCKS, 256, 0, s>>>(P.topo.n, w, R.part.p); ++P.ctx->launches;
+    finish_dot_kernel<<<1, 256, 0, s>>>(RED_BLOCKS, R.part.p, sq_out, nullptr, 0); ++P.ctx->launches;
     OPEM_CUDA(cudaGetLastError());
 }
 
@@ -542,7 +545,7 @@ static void patch_setup(Problem& P, PatchPrec& pc, const double2* A, const uint8
     if (pc.status.n < 1) pc.status.alloc(1);
     pc.status.zero(s);
     patch_extract_kernel<<<P.npatch, 256, 0, s>>>(P.npatch, P.d_patch_ptr.p, P.d_patch_dofs.p, P.d_patch_off.p,
-                                                  P.d_rowptr.p, P.d_cols.p, A, dmask, pc.B.p);
+                                                  P.d_rowptr.p, P.d_cols.p, A, dmask, pc.B.p); ++P.ctx->launches;
     OPEM_CUDA(cudaGetLastError());
     int smax = 0;
     size_t smem = 0;
@@ -554,7 +557,7 @@ static void patch_setup(Problem& P, PatchPrec& pc, const double2* A, const uint8
     smem = (size_t)smax * smax * sizeof(double2);
     OPEM_CUDA(cudaFuncSetAttribute(patch_invert_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (T.max_patch > 512) throw OpemError(OPEM_ERR_UNSUPPORTED, "vertex patch larger than 512 dofs");
-    patch_invert_kernel<<<P.npatch, 256, smem, s>>>(P.npatch, P.d_patch_ptr.p, P.d_patch_off.p, pc.B.p, smax, pc.status.p);
+    patch_invert_kernel<<<P.npatch, 256, smem, s>>>(P.npatch, P.d_patch_ptr.p, P.d_patch_off.p, pc.B.p, smax, pc.status.p); ++P.ctx->launches;
     OPEM_CUDA(cudaGetLastError());
 }
 
@@ -562,8 +565,8 @@ static void patch_apply(Problem& P, PatchPrec& pc, const double2* r, double2* y,
     cudaStream_t s = P.ctx->stream;
     size_t smem = (size_t)P.topo.max_patch * sizeof(double2);
     patch_apply1_kernel<<<P.npatch, 128, smem, s>>>(P.npatch, P.d_patch_ptr.p, P.d_patch_dofs.p, P.d_patch_off.p, pc.B.p,
-                                                    r, pc.t.p);
-    patch_apply2_kernel<<<vgrid(P), 256, 0, s>>>(P.topo.n, P.d_d2p_ptr.p, P.d_d2p_idx.p, pc.t.p, dmask, y);
+                                                    r, pc.t.p); ++P.ctx->launches;
+    patch_apply2_kernel<<<vgrid(P), 256, 0, s>>>(P.topo.n, P.d_d2p_ptr.p, P.d_d2p_idx.p, pc.t.p, dmask, y); ++P.ctx->launches;
     OPEM_CUDA(cudaGetLastError());
 }
 
@@ -598,8 +601,8 @@ SolveResult solve_plain_fp64(Problem& P, const double2* A, const uint8_t* dmask,
         if (!std::isfinite(beta)) { res.code = OPEM_ERR_BREAKDOWN; break; }
         // V0 = r / beta
         nrm2_dev(P, R, w.p, scal.p);
-        normalize_kernel<<<vgrid(P), 256, 0, s>>>(n, scal.p, w.p, V.p, scal.p + 1);
-        set_g_kernel<<<1, 256, 0, s>>>(m + 1, g.p, scal.p + 1);
+        normalize_kernel<<<vgrid(P), 256, 0, s>>>(n, scal.p, w.p, V.p, scal.p + 1); ++P.ctx->launches;
+        set_g_kernel<<<1, 256, 0, s>>>(m + 1, g.p, scal.p + 1); ++P.ctx->launches;
         OPEM_CUDA(H.p ? cudaMemsetAsync(H.p, 0, H.bytes(), s) : cudaSuccess);
         int k = 0;
         for (int j = 0; j < m; ++j) {
@@ -609,11 +612,11 @@ SolveResult solve_plain_fp64(Problem& P, const double2* A, const uint8_t* dmask,
             double2* Hcol = H.p + (int64_t)j * (m + 1);
             for (int pass = 0; pass < 2; ++pass) {
                 dot_many(P, R, V.p, n, j + 1, w.p, Hcol, pass);
-                cgs_update_kernel<<<vgrid(P), 256, (j + 1) * sizeof(double2), s>>>(n, j + 1, V.p, n, R.out.p, w.p);
+                cgs_update_kernel<<<vgrid(P), 256, (j + 1) * sizeof(double2), s>>>(n, j + 1, V.p, n, R.out.p, w.p); ++P.ctx->launches;
             }
             nrm2_dev(P, R, w.p, scal.p + 2);
-            normalize_kernel<<<vgrid(P), 256, 0, s>>>(n, scal.p + 2, w.p, V.p + (int64_t)(j + 1) * n, scal.p + 3);
-            givens_kernel<<<1, 1, 0, s>>>(j, m + 1, H.p, cs.p, g.p, scal.p + 3, resid);
+            normalize_kernel<<<vgrid(P), 256, 0, s>>>(n, scal.p + 2, w.p, V.p + (int64_t)(j + 1) * n, scal.p + 3); ++P.ctx->launches;
+            givens_kernel<<<1, 1, 0, s>>>(j, m + 1, H.p, cs.p, g.p, scal.p + 3, resid); ++P.ctx->launches;
             OPEM_CUDA(cudaGetLastError());
             OPEM_CUDA(cudaStreamSynchronize(s));
             ++its;
@@ -624,13 +627,13 @@ SolveResult solve_plain_fp64(Problem& P, const double2* A, const uint8_t* dmask,
         }
         if (res.code != OPEM_OK) break;
         // x += P^-1 (V y)
-        backsolve_kernel<<<1, 1, 0, s>>>(k, m + 1, H.p, g.p, y.p);
-        combo_kernel<<<vgrid(P), 256, k * sizeof(double2), s>>>(n, k, V.p, n, y.p, w.p);
+        backsolve_kernel<<<1, 1, 0, s>>>(k, m + 1, H.p, g.p, y.p); ++P.ctx->launches;
+        combo_kernel<<<vgrid(P), 256, k * sizeof(double2), s>>>(n, k, V.p, n, y.p, w.p); ++P.ctx->launches;
         patch_apply(P, pc, w.p, z.p, dmask);
-        axpy_kernel<<<vgrid(P), 256, 0, s>>>(n, make_double2(1, 0), z.p, x);
+        axpy_kernel<<<vgrid(P), 256, 0, s>>>(n, make_double2(1, 0), z.p, x); ++P.ctx->launches;
         // true residual r = b - A x
         spmv_complex(P, A, x, z.p, dmask);
-        sub_kernel<<<vgrid(P), 256, 0, s>>>(n, b, z.p, w.p);
+        sub_kernel<<<vgrid(P), 256, 0, s>>>(n, b, z.p, w.p); ++P.ctx->launches;
         nrm2_dev(P, R, w.p, scal.p);
         beta = read_scalar(P, scal.p, true);
     }
@@ -679,13 +682,13 @@ SolveResult solve_mass_cg(Problem& P, const double2* b, double2* x, double rtol,
     DBuf<double> dinv(n);
     DBuf<double2> r(n), z(n), p(n), q(n), sc(8);
     Red R(4);
-    diag_inv_kernel<<<vgrid(P), 256, 0, s>>>(n, P.d_rowptr.p, P.d_cols.p, P.d_M1.p, dinv.p);
+    diag_inv_kernel<<<vgrid(P), 256, 0, s>>>(n, P.d_rowptr.p, P.d_cols.p, P.d_M1.p, dinv.p); ++P.ctx->launches;
     OPEM_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double2), s));
     OPEM_CUDA(cudaMemcpyAsync(r.p, b, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
     nrm2_dev(P, R, b, sc.p);
     double bnorm = read_scalar(P, sc.p, true);
     if (bnorm == 0) { res.converged = 1; return res; }
-    dscale_kernel<<<vgrid(P), 256, 0, s>>>(n, dinv.p, r.p, z.p);
+    dscale_kernel<<<vgrid(P), 256, 0, s>>>(n, dinv.p, r.p, z.p); ++P.ctx->launches;
     OPEM_CUDA(cudaMemcpyAsync(p.p, z.p, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
     dot_many(P, R, r.p, n, 1, z.p, nullptr, 0);   // rz = r^H z
     OPEM_CUDA(cudaMemcpyAsync(sc.p + 1, R.out.p, sizeof(double2), cudaMemcpyDeviceToDevice, s));
@@ -694,16 +697,16 @@ SolveResult solve_mass_cg(Problem& P, const double2* b, double2* x, double rtol,
     while (its < maxits) {
         spmv_real_complex(P, P.d_M1.p, p.p, q.p, 1.0, 0.0);
         dot_many(P, R, p.p, n, 1, q.p, nullptr, 0);   // p^H q
-        cg_update_kernel<<<vgrid(P), 256, 0, s>>>(n, sc.p + 1, R.out.p, p.p, q.p, x, r.p);
+        cg_update_kernel<<<vgrid(P), 256, 0, s>>>(n, sc.p + 1, R.out.p, p.p, q.p, x, r.p); ++P.ctx->launches;
         ++its;
         if (its % 10 == 0 || its >= maxits) {
             nrm2_dev(P, R, r.p, sc.p + 3);
             rn = read_scalar(P, sc.p + 3, true);
             if (rn / bnorm <= rtol || !std::isfinite(rn)) break;
         }
-        dscale_kernel<<<vgrid(P), 256, 0, s>>>(n, dinv.p, r.p, z.p);
+        dscale_kernel<<<vgrid(P), 256, 0, s>>>(n, dinv.p, r.p, z.p); ++P.ctx->launches;
         dot_many(P, R, r.p, n, 1, z.p, nullptr, 0);   // rz_new
-        cg_direction_kernel<<<vgrid(P), 256, 0, s>>>(n, R.out.p, sc.p + 1, z.p, p.p);
+        cg_direction_kernel<<<vgrid(P), 256, 0, s>>>(n, R.out.p, sc.p + 1, z.p, p.p); ++P.ctx->launches;
         OPEM_CUDA(cudaMemcpyAsync(sc.p + 1, R.out.p, sizeof(double2), cudaMemcpyDeviceToDevice, s));
     }
     OPEM_CUDA(cudaGetLastError());
@@ -712,6 +715,66 @@ SolveResult solve_mass_cg(Problem& P, const double2* b, double2* x, double rtol,
     res.converged = res.relres <= rtol;
     if (!std::isfinite(rn)) res.code = OPEM_ERR_BREAKDOWN;
     return res;
+}
+
+}  // namespace opem
+
+namespace opem {
+
+// Times the FP64-path kernels in isolation (CUDA events on the context stream).
+// out[3k+0] = ms per launch, out[3k+1] = algorithmic bytes per launch, out[3k+2] = launches.
+void profile_fp64(Problem& P, const double2* A, const uint8_t* dmask, int reps, double* out) {
+    cudaStream_t s = P.ctx->stream;
+    const int64_t n = P.topo.n, nnz = (int64_t)P.topo.cols.size();
+    const int nv = 64;
+    DBuf<double2> V((size_t)nv * n), w(n), z(n);
+    OPEM_CUDA(cudaMemsetAsync(V.p, 0, V.bytes(), s));
+    OPEM_CUDA(cudaMemsetAsync(w.p, 0, w.bytes(), s));
+    Red R(nv + 2);
+    PatchPrec pc;
+    patch_setup(P, pc, A, dmask);
+    cudaEvent_t e0, e1;
+    OPEM_CUDA(cudaEventCreate(&e0));
+    OPEM_CUDA(cudaEventCreate(&e1));
+    double patch_sq = 0, patch_len = 0;
+    for (size_t v = 0; v + 1 < P.topo.patch_ptr.size(); ++v) {
+        double sz = P.topo.patch_ptr[v + 1] - P.topo.patch_ptr[v];
+        patch_sq += sz * sz;
+        patch_len += sz;
+    }
+    auto timeit = [&](auto&& launch) {
+        for (int i = 0; i < 3; ++i) launch();
+        OPEM_CUDA(cudaEventRecord(e0, s));
+        for (int i = 0; i < reps; ++i) launch();
+        OPEM_CUDA(cudaEventRecord(e1, s));
+        OPEM_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        OPEM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        return (double)ms / reps;
+    };
+    size_t smem_p = (size_t)P.topo.max_patch * sizeof(double2);
+    out[0] = timeit([&] { spmv_complex(P, A, V.p, w.p, dmask); });
+    out[1] = (double)nnz * (16 + 4) + 4.0 * (n + 1) + n * (16.0 + 16.0 + 1.0);
+    out[3] = timeit([&] {
+        patch_apply1_kernel<<<P.npatch, 128, smem_p, s>>>(P.npatch, P.d_patch_ptr.p, P.d_patch_dofs.p, P.d_patch_off.p,
+                                                          pc.B.p, V.p, pc.t.p);
+        ++P.ctx->launches;
+    });
+    out[4] = patch_sq * 16 + patch_len * (4 + 16 + 16) + P.npatch * 12.0;
+    out[6] = timeit([&] {
+        multidot_kernel<<<dim3(RED_BLOCKS, nv), 256, 0, s>>>(n, V.p, n, w.p, R.part.p);
+        ++P.ctx->launches;
+    });
+    out[7] = (double)nv * n * 16 + n * 16.0;
+    out[9] = timeit([&] {
+        cgs_update_kernel<<<P.ctx->sm_count * 8, 256, nv * sizeof(double2), s>>>(n, nv, V.p, n, R.out.p, w.p);
+        ++P.ctx->launches;
+    });
+    out[10] = (double)nv * n * 16 + 2.0 * n * 16;
+    for (int k = 0; k < 4; ++k) out[3 * k + 2] = reps;
+    OPEM_CUDA(cudaGetLastError());
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
 }
 
 }  // namespace opem
