@@ -134,6 +134,25 @@ int  opem_context_launches(opem_context ctx, int64_t* out);
  * against 64 Krylov vectors (dot + update).                                     */
 int  opem_profile_kernels(opem_problem prob, double freq, int reps, double* out, int nout);
 
+/* ---- allocation-free assembly (no counterpart in the reference) -------------
+ * For callers that cannot allocate device memory at the point of use: a
+ * process whose HBM is already claimed by another allocator (a PETSc or Kokkos
+ * memory pool, or a serving process that reserves its whole budget up front)
+ * or a latency-critical loop that must not call cudaMalloc/cudaFree.  Like
+ * opem_get_system_matrix it writes A(freq) for driving set d (before Dirichlet
+ * handling, nnz complex, interleaved) into the host buffer vals, but it stages
+ * the values in a static device array of OPEM_NOALLOC_MAX_NNZ complex doubles
+ * (16 MiB, held by every GPU that loads the library until the process exits)
+ * and calls no cudaMalloc, cudaFree or allocating library routine.
+ *  - Problems with nnz > OPEM_NOALLOC_MAX_NNZ are rejected with OPEM_ERR_ARG.
+ *  - The first call on a device looks up the array's device address
+ *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *  - All calls on a device share the one array: calls that overlap on the GPU
+ *    (other host threads, other problems on the same device) race.  Each call
+ *    overwrites every entry it reads, so nothing has to be cleared between calls. */
+#define OPEM_NOALLOC_MAX_NNZ (1 << 20)
+int  opem_system_matrix_noalloc(opem_problem prob, double freq, int d, double* vals);
+
 #ifdef __cplusplus
 }
 #endif

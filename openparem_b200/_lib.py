@@ -14,6 +14,7 @@ ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_STATE, ERR_MESH = -1, -2, -3, -4, -5
 ERR_NOT_CONVERGED, ERR_BREAKDOWN, ERR_TIMEOUT, ERR_UNSUPPORTED = -6, -7, -8, -9
 BDR_PEC, BDR_PMC, BDR_PORT, BDR_IMPEDANCE, BDR_RADIATION = 1, 2, 3, 4, 5
 PREC_FP64, PREC_MIXED = 0, 1
+NOALLOC_MAX_NNZ = 1 << 20
 
 ERROR_NAMES = {ERR_ARG: "OPEM_ERR_ARG", ERR_CUDA: "OPEM_ERR_CUDA", ERR_NOMEM: "OPEM_ERR_NOMEM",
                ERR_STATE: "OPEM_ERR_STATE", ERR_MESH: "OPEM_ERR_MESH", ERR_NOT_CONVERGED: "OPEM_ERR_NOT_CONVERGED",
@@ -61,6 +62,7 @@ SIGNATURES = [
     ("opem_get_system_matrix", C.c_int, [P, C.c_double, C.c_int, DP]),
     ("opem_context_launches", C.c_int, [P, I64P]),
     ("opem_profile_kernels", C.c_int, [P, C.c_double, C.c_int, DP, C.c_int]),
+    ("opem_system_matrix_noalloc", C.c_int, [P, C.c_double, C.c_int, DP]),
 ]
 
 

@@ -394,6 +394,24 @@ void form_system_matrix(Problem& P, const VolCoef& vc, const std::vector<BCoef>&
     }
 }
 
+// Same kernels as form_system_matrix, coefficients from a plain array (no
+// host containers), for the allocation-free entry point.
+void form_system_matrix_n(Problem& P, const VolCoef& vc, const BCoef* bc, size_t nb, double2* A) {
+    cudaStream_t s = P.ctx->stream;
+    int64_t nnz = (int64_t)P.topo.cols.size();
+    combine_kernel<<<P.ctx->sm_count * 8, 256, 0, s>>>(nnz, P.d_K.p, P.d_Meps.p, P.has_tand ? P.d_Mtand.p : nullptr,
+                                                       P.has_sig ? P.d_Msig.p : nullptr, vc, A);
+    ++P.ctx->launches;
+    OPEM_CUDA(cudaGetLastError());
+    for (size_t g = 0; g < P.groups.size() && g < nb; ++g) {
+        BGroup& G = P.groups[g];
+        if (G.nu == 0) continue;
+        boundary_add_kernel<<<(unsigned)((G.nu + 255) / 256), 256, 0, s>>>(G.nu, G.uslot.p, G.R.p, bc[g], A);
+        ++P.ctx->launches;
+        OPEM_CUDA(cudaGetLastError());
+    }
+}
+
 // ---------------------------------------------------------------------------
 // port overlap: out = sum_u conj(a[row_u]) R_one[u] b[col_u]  (FP64)
 // Mode::calculateSplits / tangentialInnerProduct, src/OpenParEM3D/port.cpp:3463-3568

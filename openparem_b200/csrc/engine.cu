@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <mutex>
 
 #include "engine.h"
 
@@ -478,6 +479,71 @@ static void assemble_problem(Problem& P) {
     P.assembled = true;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free assembly of A(freq, d) (opem_system_matrix_noalloc).
+//
+// The device staging buffer for the assembled values is this file-scope
+// array instead of a cudaMalloc'd buffer.  Every GPU that loads the library
+// holds it (OPEM_NOALLOC_MAX_NNZ complex doubles = 16 MiB) until the process
+// exits.  In host code `g_noalloc_A` is only a host-side stand-in, not a device
+// address: the device address is obtained once per device with
+// cudaGetSymbolAddress and passed to the kernels.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) double2 g_noalloc_A[OPEM_NOALLOC_MAX_NNZ];
+
+static const int NOALLOC_MAX_DEVICES = 64;
+static double2* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+static std::mutex g_noalloc_mu;
+
+// Device address of g_noalloc_A on `device` (which must be current).
+static int noalloc_scratch(int device, double2** out, std::string& err) {
+    if (device < 0 || device >= NOALLOC_MAX_DEVICES) { err = "device index beyond the no-alloc set-up table"; return OPEM_ERR_ARG; }
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_A);
+        if (e != cudaSuccess || !ptr) { err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e); return OPEM_ERR_CUDA; }
+        g_noalloc_addr[device] = static_cast<double2*>(ptr);
+    }
+    *out = g_noalloc_addr[device];
+    return OPEM_OK;
+}
+
+// system_coefficients without host containers: the port terms only need gamma.
+static int coefficients_fixed(const Problem& P, double freq, int d, VolCoef& vc, BCoef* bc, int cap) {
+    if ((int)P.groups.size() > cap) return -1;
+    double w = 2 * M_PI * freq, k0 = w * std::sqrt(MU0 * EPS0), k02 = k0 * k0;
+    vc.c_eps = make_double2(-k02, 0);
+    vc.c_tand = make_double2(0, k02);
+    vc.c_sig = make_double2(0, w * MU0);
+    for (size_t g = 0; g < P.groups.size(); ++g) {
+        const BGroup& G = P.groups[g];
+        BCoef c;
+        std::memset(&c, 0, sizeof(c));
+        if (G.type == OPEM_BDR_PORT && G.port != d) {
+            const double* dd = P.modes[G.port].desc;
+            int r = port_region(P, G.port);
+            cd epsc = P.eps_r[r] * cd(1.0, -P.tand[r]) - cd(0.0, P.sigma[r] / (w * EPS0));
+            double kc2 = std::pow(dd[14] * M_PI / dd[12], 2) + std::pow(dd[15] * M_PI / dd[13], 2);
+            cd gamma = std::sqrt(cd(kc2, 0) - k02 * epsc * P.mu_r[r]);
+            if (gamma.real() < 0) gamma = -gamma;
+            cd ig = 1.0 / gamma;
+            cd ce = -k02 * ig, ct = cd(0, k02) * ig, cs = cd(0, w * MU0) * ig;
+            c.c_cc = make_double2(ig.real(), ig.imag());
+            c.c_eps = make_double2(ce.real(), ce.imag());
+            c.c_tand = make_double2(ct.real(), ct.imag());
+            c.c_sig = make_double2(cs.real(), cs.imag());
+        } else if (G.type == OPEM_BDR_IMPEDANCE) {
+            c.c_one = make_double2(0, w * MU0 / surface_resistance(freq, G.sigma, G.mu_r, G.Rz));
+        } else if (G.type == OPEM_BDR_RADIATION) {
+            double eta = G.eta > 0 ? G.eta : std::sqrt(MU0 / EPS0);
+            c.c_one = make_double2(0, w * MU0 / eta);
+        }
+        bc[g] = c;
+    }
+    return (int)P.groups.size();
+}
+
 }  // namespace opem
 
 // ===========================================================================
@@ -749,6 +815,41 @@ int opem_profile_kernels(opem_problem prob, double freq, int reps, double* out, 
         dmask_kernel<<<P.ctx->sm_count * 8, 256, 0, P.ctx->stream>>>(n, P.d_pec.p, P.d_portmask.p, 0, dm.p);
         ++P.ctx->launches;
         profile_fp64(P, A.p, dm.p, reps, out);
+    });
+}
+
+// No counterpart in the reference.  See include/opem_b200.h for the contract.
+int opem_system_matrix_noalloc(opem_problem prob, double freq, int d, double* vals) {
+    if (!prob || !vals || !(freq > 0)) return OPEM_ERR_ARG;
+    Problem& P = prob->p;
+    if (!P.assembled || d < 0 || d >= std::max(1, P.nports)) {
+        P.ctx->last_error = "opem_system_matrix_noalloc: problem not assembled or driving set out of range";
+        return OPEM_ERR_STATE;
+    }
+    const size_t nnz = P.topo.cols.size();
+    if (nnz > (size_t)OPEM_NOALLOC_MAX_NNZ) {
+        P.ctx->last_error = "opem_system_matrix_noalloc: nnz exceeds OPEM_NOALLOC_MAX_NNZ (1048576); "
+                            "use opem_get_system_matrix";
+        return OPEM_ERR_ARG;
+    }
+    const int CAP = 64;
+    BCoef bc[CAP];
+    VolCoef vc;
+    if (coefficients_fixed(P, freq, d, vc, bc, CAP) < 0) {
+        P.ctx->last_error = "opem_system_matrix_noalloc: more than 64 boundary groups";
+        return OPEM_ERR_ARG;
+    }
+    return guarded(P.ctx, [&] {
+        OPEM_CUDA(cudaSetDevice(P.ctx->device));
+        double2* scratch = nullptr;
+        std::string err;
+        int rc = noalloc_scratch(P.ctx->device, &scratch, err);
+        if (rc) throw OpemError(rc, err);
+        // combine_kernel writes every one of the nnz entries before the boundary
+        // kernels add to them, so nothing left by an earlier call is read.
+        form_system_matrix_n(P, vc, bc, (size_t)CAP, scratch);
+        OPEM_CUDA(cudaMemcpyAsync(vals, scratch, nnz * sizeof(double2), cudaMemcpyDeviceToHost, P.ctx->stream));
+        OPEM_CUDA(cudaStreamSynchronize(P.ctx->stream));
     });
 }
 

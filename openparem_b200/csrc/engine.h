@@ -124,6 +124,7 @@ void assemble_volume(Problem& P);
 void assemble_boundary(Problem& P);
 // A = K + vc.c_eps*Meps + ... plus boundary groups (FP64 complex, nnz)
 void form_system_matrix(Problem& P, const VolCoef& vc, const std::vector<BCoef>& bc, double2* A);
+void form_system_matrix_n(Problem& P, const VolCoef& vc, const BCoef* bc, size_t nb, double2* A);
 // host: coefficients of A(freq) for driving set d
 void system_coefficients(const Problem& P, double freq, int d, VolCoef& vc, std::vector<BCoef>& bc);
 void port_gamma_Z_V(const Problem& P, int port, double freq, cd& gamma, cd& Z, cd& V);
