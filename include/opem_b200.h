@@ -55,12 +55,13 @@ typedef struct opem_problem_s* opem_problem;
 typedef struct {
     double rtol;          /* relative residual tolerance [1e-10]                            */
     int    maxits;        /* total inner iteration limit [5000]                              */
-    int    restart;       /* GMRES restart length m [150]                                    */
+    int    restart;       /* GMRES restart length m, 2..2048 [100]                           */
     int    precision;     /* OPEM_PREC_FP64 or OPEM_PREC_MIXED                               */
     int    poly_degree;   /* polynomial preconditioner degree (mixed mode), 0 = none [0]     */
     int    force_reciprocal; /* S <- (S+S^T)/2 (results.cpp:401-418) [1]                      */
     int    h_maxits;      /* iteration limit of the H projection CG [2000]                    */
     double h_rtol;        /* tolerance of the H projection CG [1e-12]                         */
+    int    deflate;       /* harmonic Ritz vectors kept at each GMRES restart (GMRES-DR) [30] */
 } opem_solver_opts;
 
 typedef struct {

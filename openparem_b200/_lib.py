@@ -25,7 +25,7 @@ ERROR_NAMES = {ERR_ARG: "OPEM_ERR_ARG", ERR_CUDA: "OPEM_ERR_CUDA", ERR_NOMEM: "O
 class SolverOpts(C.Structure):
     _fields_ = [("rtol", C.c_double), ("maxits", C.c_int), ("restart", C.c_int), ("precision", C.c_int),
                 ("poly_degree", C.c_int), ("force_reciprocal", C.c_int), ("h_maxits", C.c_int),
-                ("h_rtol", C.c_double)]
+                ("h_rtol", C.c_double), ("deflate", C.c_int)]
 
 
 class SolveStats(C.Structure):

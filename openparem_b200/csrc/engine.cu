@@ -580,12 +580,13 @@ void opem_default_opts(opem_solver_opts* o) {
     if (!o) return;
     o->rtol = 1e-10;
     o->maxits = 5000;
-    o->restart = 150;
+    o->restart = 100;
     o->precision = OPEM_PREC_FP64;
     o->poly_degree = 0;
     o->force_reciprocal = 1;
     o->h_maxits = 2000;
     o->h_rtol = 1e-12;
+    o->deflate = 30;
 }
 
 int opem_context_create(int device, opem_context* out) {
@@ -710,7 +711,7 @@ int opem_problem_info(opem_problem prob, int64_t* info, int ninfo) {
 }
 
 static bool opts_ok(const opem_solver_opts* o) {
-    return o && o->rtol > 0 && o->maxits > 0 && o->restart >= 2 && o->restart <= 4096 && o->h_maxits > 0 && o->h_rtol > 0 &&
+    return o && o->rtol > 0 && o->maxits > 0 && o->restart >= 2 && o->restart <= 2048 && o->h_maxits > 0 && o->h_rtol > 0 && o->deflate >= 0 &&
            (o->precision == OPEM_PREC_FP64 || o->precision == OPEM_PREC_MIXED);
 }
 

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 
+#include "dense.h"
 #include "engine.h"
 
 namespace opem {
@@ -85,19 +86,6 @@ void spmv_complex(Problem& P, const double2* A, const double2* x, double2* y, co
     if (tpr == 32) spmv_c64_kernel<32><<<grid, 256, 0, s>>>(n, P.d_rowptr.p, P.d_cols.p, A, x, y, zero_rows, one);
     else if (tpr == 16) spmv_c64_kernel<16><<<grid, 256, 0, s>>>(n, P.d_rowptr.p, P.d_cols.p, A, x, y, zero_rows, one);
     else spmv_c64_kernel<8><<<grid, 256, 0, s>>>(n, P.d_rowptr.p, P.d_cols.p, A, x, y, zero_rows, one);
-    ++P.ctx->launches;
-    OPEM_CUDA(cudaGetLastError());
-}
-
-static void spmv_complex_scaled(Problem& P, const double2* A, const double2* x, double2* y, const uint8_t* zero_rows,
-                                double2 scale) {
-    int64_t n = P.topo.n;
-    int tpr = tpr_for(P);
-    unsigned grid = (unsigned)((n * tpr + 255) / 256);
-    cudaStream_t s = P.ctx->stream;
-    if (tpr == 32) spmv_c64_kernel<32><<<grid, 256, 0, s>>>(n, P.d_rowptr.p, P.d_cols.p, A, x, y, zero_rows, scale);
-    else if (tpr == 16) spmv_c64_kernel<16><<<grid, 256, 0, s>>>(n, P.d_rowptr.p, P.d_cols.p, A, x, y, zero_rows, scale);
-    else spmv_c64_kernel<8><<<grid, 256, 0, s>>>(n, P.d_rowptr.p, P.d_cols.p, A, x, y, zero_rows, scale);
     ++P.ctx->launches;
     OPEM_CUDA(cudaGetLastError());
 }
@@ -570,79 +558,241 @@ static void patch_apply(Problem& P, PatchPrec& pc, const double2* r, double2* y,
     OPEM_CUDA(cudaGetLastError());
 }
 
+// W[:, c] = sum_r V[:, r] Q[r, c]  (tall-skinny basis rotation for deflated restarts).
+// Q ((m+1) x (k+1), ~100 KB) is read through the read-only cache: every thread
+// reads the same entries, so they are L1 broadcasts.
+__global__ void basis_rotate_kernel(int64_t n, int nin, int nout, const double2* __restrict__ V, int64_t ldv,
+                                    const double2* __restrict__ Q, double2* __restrict__ W, int64_t ldw) {
+    constexpr int CH = 8;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        for (int c0 = 0; c0 < nout; c0 += CH) {
+            double re[CH], im[CH];
+#pragma unroll
+            for (int q = 0; q < CH; ++q) { re[q] = 0; im[q] = 0; }
+            for (int r = 0; r < nin; ++r) {
+                double2 v = V[(int64_t)r * ldv + k];
+#pragma unroll
+                for (int q = 0; q < CH; ++q) {
+                    if (c0 + q < nout) {
+                        double2 c = __ldg(&Q[(c0 + q) * nin + r]);
+                        re[q] += v.x * c.x - v.y * c.y;
+                        im[q] += v.x * c.y + v.y * c.x;
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < CH; ++q)
+                if (c0 + q < nout) W[(int64_t)(c0 + q) * ldw + k] = make_double2(re[q], im[q]);
+        }
+    }
+}
+
+namespace {
+// Incremental QR of the (m+1) x m least-squares matrix by Givens rotations.
+struct Rot { int i1, i2; double c; cd s; };
+struct LsqState {
+    int m = 0;
+    std::vector<cd> R;      // (m+1) x m column-major (rotated copy of H)
+    std::vector<cd> g;      // rotated right-hand side
+    std::vector<Rot> rots;
+    void reset(int m_, const std::vector<cd>& c) {
+        m = m_;
+        R.assign((size_t)(m + 1) * m, 0.0);
+        g = c;
+        rots.clear();
+    }
+    static void apply(const Rot& q, cd& a, cd& b) {
+        cd x = a, y = b;
+        a = q.c * x + q.s * y;
+        b = -std::conj(q.s) * x + q.c * y;
+    }
+    // add column j (entries 0..top) and eliminate its entries below the diagonal
+    double add_column(int j, const cd* col, int top) {
+        cd* rc = &R[(size_t)j * (m + 1)];
+        for (int i = 0; i <= top; ++i) rc[i] = col[i];
+        for (int i = top + 1; i <= m; ++i) rc[i] = 0.0;
+        for (const Rot& q : rots) apply(q, rc[q.i1], rc[q.i2]);
+        for (int r = j + 1; r <= top; ++r) {
+            if (rc[r] == 0.0) continue;
+            Rot q;
+            q.i1 = j; q.i2 = r;
+            double aa = std::abs(rc[j]), bb = std::abs(rc[r]);
+            if (aa == 0.0) { q.c = 0.0; q.s = std::conj(rc[r]) / bb; }
+            else { double rho = std::hypot(aa, bb); q.c = aa / rho; q.s = (rc[j] / aa) * std::conj(rc[r]) / rho; }
+            apply(q, rc[j], rc[r]);
+            rc[r] = 0.0;
+            apply(q, g[j], g[r]);
+            rots.push_back(q);
+        }
+        return std::abs(g[j + 1]);
+    }
+    // y = R[:k,:k]^-1 g[:k]
+    void solve(int k, std::vector<cd>& y) const {
+        y.assign(k, 0.0);
+        for (int i = k - 1; i >= 0; --i) {
+            cd s = g[i];
+            for (int c = i + 1; c < k; ++c) s -= R[i + (size_t)c * (m + 1)] * y[c];
+            y[i] = s / R[i + (size_t)i * (m + 1)];
+        }
+    }
+};
+}  // namespace
+
 // ---------------------------------------------------------------------------
-// GMRES(m), FP64, right preconditioned.  Solves the free block A_FF x_F = b_F;
-// rows/cols in dmask are identity and carry zero in every Krylov vector.
+// GMRES-DR(m, k), FP64, right preconditioned by vertex-patch block Jacobi.
+// Restarted GMRES (the reference's KSPGMRES) with deflated restarting: at
+// each restart the k harmonic Ritz vectors of smallest modulus are kept in
+// the basis (Morgan's GMRES-DR), so restarts do not throw away the slow
+// modes.  k = 0 gives plain GMRES(m).  Solves the free block A_FF x_F = b_F;
+// rows/cols in dmask are identity and every Krylov vector is zero there.
+// The device runs the Arnoldi steps (SpMV, block Jacobi, CGS2); the host keeps
+// the (m+1) x m Hessenberg least-squares problem and the per-restart
+// harmonic-Ritz eigenproblem in FP64.
 // ---------------------------------------------------------------------------
 SolveResult solve_plain_fp64(Problem& P, const double2* A, const uint8_t* dmask, const double2* b, double2* x,
                              const opem_solver_opts& o) {
     cudaStream_t s = P.ctx->stream;
     const int64_t n = P.topo.n;
     const int m = std::max(2, o.restart);
+    const int kd = std::max(0, std::min(o.deflate, m - 2));
     SolveResult res;
-    DBuf<double2> V((size_t)(m + 1) * n), w(n), z(n), H((size_t)(m + 1) * m), cs((size_t)2 * m + 2), g(m + 2),
-        y(m + 2), scal(8);
+    DBuf<double2> V((size_t)(m + 1) * n), w(n), z(n), H((size_t)(m + 1) * m), yd(m + 2), scal(8), Qd;
+    DBuf<double2> Wd;
+    if (kd > 0) { Wd.alloc((size_t)(kd + 1) * n); Qd.alloc((size_t)(m + 1) * (kd + 1)); }
     Red R(m + 2);
     PatchPrec pc;
     patch_setup(P, pc, A, dmask);
-    double* resid = P.ctx->pinned;
     OPEM_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double2), s));
-    // ||b||
     nrm2_dev(P, R, b, scal.p);
     double bnorm = read_scalar(P, scal.p, true);
     if (bnorm == 0.0) { res.converged = 1; return res; }
-    // r = b
     OPEM_CUDA(cudaMemcpyAsync(w.p, b, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+    std::vector<cd> Hh((size_t)(m + 1) * m, 0.0), c(m + 1, 0.0), y;
+    std::vector<double2> colbuf(m + 2);
+    LsqState L;
     double beta = bnorm;
-    int its = 0;
+    int start = 0, its = 0;
+    bool fresh = true;
     while (true) {
-        if (beta / bnorm <= o.rtol) { res.converged = 1; break; }
-        if (its >= o.maxits) break;
-        if (!std::isfinite(beta)) { res.code = OPEM_ERR_BREAKDOWN; break; }
-        // V0 = r / beta
-        nrm2_dev(P, R, w.p, scal.p);
-        normalize_kernel<<<vgrid(P), 256, 0, s>>>(n, scal.p, w.p, V.p, scal.p + 1); ++P.ctx->launches;
-        set_g_kernel<<<1, 256, 0, s>>>(m + 1, g.p, scal.p + 1); ++P.ctx->launches;
-        OPEM_CUDA(H.p ? cudaMemsetAsync(H.p, 0, H.bytes(), s) : cudaSuccess);
-        int k = 0;
-        for (int j = 0; j < m; ++j) {
+        if (fresh) {
+            // V0 = r / ||r||
+            nrm2_dev(P, R, w.p, scal.p);
+            normalize_kernel<<<vgrid(P), 256, 0, s>>>(n, scal.p, w.p, V.p, scal.p + 1);
+            ++P.ctx->launches;
+            std::fill(Hh.begin(), Hh.end(), 0.0);
+            std::fill(c.begin(), c.end(), 0.0);
+            c[0] = beta;
+            start = 0;
+        }
+        L.reset(m, c);
+        double est = 0;
+        for (int j = 0; j < start; ++j) est = L.add_column(j, &Hh[(size_t)j * (m + 1)], start);
+        int ncol = start;
+        for (int j = start; j < m; ++j) {
             double2* Vj = V.p + (int64_t)j * n;
             patch_apply(P, pc, Vj, z.p, dmask);
             spmv_complex(P, A, z.p, w.p, dmask);
             double2* Hcol = H.p + (int64_t)j * (m + 1);
             for (int pass = 0; pass < 2; ++pass) {
                 dot_many(P, R, V.p, n, j + 1, w.p, Hcol, pass);
-                cgs_update_kernel<<<vgrid(P), 256, (j + 1) * sizeof(double2), s>>>(n, j + 1, V.p, n, R.out.p, w.p); ++P.ctx->launches;
+                cgs_update_kernel<<<vgrid(P), 256, (j + 1) * sizeof(double2), s>>>(n, j + 1, V.p, n, R.out.p, w.p);
+                ++P.ctx->launches;
             }
             nrm2_dev(P, R, w.p, scal.p + 2);
-            normalize_kernel<<<vgrid(P), 256, 0, s>>>(n, scal.p + 2, w.p, V.p + (int64_t)(j + 1) * n, scal.p + 3); ++P.ctx->launches;
-            givens_kernel<<<1, 1, 0, s>>>(j, m + 1, H.p, cs.p, g.p, scal.p + 3, resid); ++P.ctx->launches;
+            normalize_kernel<<<vgrid(P), 256, 0, s>>>(n, scal.p + 2, w.p, V.p + (int64_t)(j + 1) * n, Hcol + j + 1);
+            ++P.ctx->launches;
             OPEM_CUDA(cudaGetLastError());
+            OPEM_CUDA(cudaMemcpyAsync(colbuf.data(), Hcol, (j + 2) * sizeof(double2), cudaMemcpyDeviceToHost, s));
             OPEM_CUDA(cudaStreamSynchronize(s));
+            for (int i = 0; i <= j + 1; ++i) Hh[i + (size_t)j * (m + 1)] = cd(colbuf[i].x, colbuf[i].y);
+            est = L.add_column(j, &Hh[(size_t)j * (m + 1)], j + 1);
             ++its;
-            k = j + 1;
-            double rr = *resid;
-            if (!std::isfinite(rr)) { res.code = OPEM_ERR_BREAKDOWN; break; }
-            if (rr / bnorm <= o.rtol || its >= o.maxits) break;
+            ncol = j + 1;
+            if (!std::isfinite(est)) { res.code = OPEM_ERR_BREAKDOWN; break; }
+            if (est / bnorm <= o.rtol || its >= o.maxits) break;
         }
         if (res.code != OPEM_OK) break;
-        // x += P^-1 (V y)
-        backsolve_kernel<<<1, 1, 0, s>>>(k, m + 1, H.p, g.p, y.p); ++P.ctx->launches;
-        combo_kernel<<<vgrid(P), 256, k * sizeof(double2), s>>>(n, k, V.p, n, y.p, w.p); ++P.ctx->launches;
+        // x += M^-1 (V y)
+        L.solve(ncol, y);
+        std::vector<double2> yh(ncol);
+        for (int i = 0; i < ncol; ++i) yh[i] = make_double2(y[i].real(), y[i].imag());
+        OPEM_CUDA(cudaMemcpyAsync(yd.p, yh.data(), ncol * sizeof(double2), cudaMemcpyHostToDevice, s));
+        combo_kernel<<<vgrid(P), 256, ncol * sizeof(double2), s>>>(n, ncol, V.p, n, yd.p, w.p);
+        ++P.ctx->launches;
         patch_apply(P, pc, w.p, z.p, dmask);
-        axpy_kernel<<<vgrid(P), 256, 0, s>>>(n, make_double2(1, 0), z.p, x); ++P.ctx->launches;
-        // true residual r = b - A x
+        axpy_kernel<<<vgrid(P), 256, 0, s>>>(n, make_double2(1, 0), z.p, x);
+        ++P.ctx->launches;
+        // true residual
         spmv_complex(P, A, x, z.p, dmask);
-        sub_kernel<<<vgrid(P), 256, 0, s>>>(n, b, z.p, w.p); ++P.ctx->launches;
+        sub_kernel<<<vgrid(P), 256, 0, s>>>(n, b, z.p, w.p);
+        ++P.ctx->launches;
         nrm2_dev(P, R, w.p, scal.p);
         beta = read_scalar(P, scal.p, true);
+        if (!std::isfinite(beta)) { res.code = OPEM_ERR_BREAKDOWN; break; }
+        if (beta / bnorm <= o.rtol) { res.converged = 1; break; }
+        if (its >= o.maxits) break;
+        fresh = true;
+        if (kd == 0 || ncol < m) continue;
+        // ---- deflated restart (harmonic Ritz vectors of the m x m problem)
+        std::vector<cd> rc(m + 1);
+        for (int i = 0; i <= m; ++i) {
+            cd t = c[i];
+            for (int j = 0; j < m; ++j) t -= Hh[i + (size_t)j * (m + 1)] * y[j];
+            rc[i] = t;
+        }
+        std::vector<cd> Hm((size_t)m * m), HmH((size_t)m * m), f(m, 0.0);
+        for (int j = 0; j < m; ++j)
+            for (int i = 0; i < m; ++i) {
+                Hm[i + (size_t)j * m] = Hh[i + (size_t)j * (m + 1)];
+                HmH[j + (size_t)i * m] = std::conj(Hh[i + (size_t)j * (m + 1)]);
+            }
+        f[m - 1] = 1.0;
+        if (!lu_solve(m, HmH, f)) continue;
+        double hm2 = std::norm(Hh[m + (size_t)(m - 1) * (m + 1)]);
+        for (int i = 0; i < m; ++i) Hm[i + (size_t)(m - 1) * m] += hm2 * f[i];
+        std::vector<cd> theta, gv;
+        if (!eig_smallest(m, Hm, kd, theta, gv)) continue;
+        std::vector<cd> Pm((size_t)(m + 1) * (kd + 1), 0.0);
+        for (int q = 0; q < kd; ++q)
+            for (int i = 0; i < m; ++i) Pm[i + (size_t)q * (m + 1)] = gv[i + (size_t)q * m];
+        for (int i = 0; i <= m; ++i) Pm[i + (size_t)kd * (m + 1)] = rc[i];
+        if (orthonormalise(m + 1, kd + 1, Pm) != kd + 1) continue;
+        // Hnew = Pm^H H Pm[:m, :kd] ; cnew = Pm^H rc
+        std::vector<cd> T1((size_t)(m + 1) * kd, 0.0);
+        for (int q = 0; q < kd; ++q)
+            for (int j = 0; j < m; ++j) {
+                cd pj = Pm[j + (size_t)q * (m + 1)];
+                if (pj == 0.0) continue;
+                for (int i = 0; i <= m; ++i) T1[i + (size_t)q * (m + 1)] += Hh[i + (size_t)j * (m + 1)] * pj;
+            }
+        std::vector<cd> Hn((size_t)(m + 1) * m, 0.0), cn(m + 1, 0.0);
+        for (int q = 0; q < kd; ++q)
+            for (int a = 0; a <= kd; ++a) {
+                cd t = 0;
+                for (int i = 0; i <= m; ++i) t += std::conj(Pm[i + (size_t)a * (m + 1)]) * T1[i + (size_t)q * (m + 1)];
+                Hn[a + (size_t)q * (m + 1)] = t;
+            }
+        for (int a = 0; a <= kd; ++a) {
+            cd t = 0;
+            for (int i = 0; i <= m; ++i) t += std::conj(Pm[i + (size_t)a * (m + 1)]) * rc[i];
+            cn[a] = t;
+        }
+        // device: V[:, :kd+1] = V Pm
+        std::vector<double2> Qh((size_t)(m + 1) * (kd + 1));
+        for (size_t t = 0; t < Qh.size(); ++t) Qh[t] = make_double2(Pm[t].real(), Pm[t].imag());
+        OPEM_CUDA(cudaMemcpyAsync(Qd.p, Qh.data(), Qh.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
+        basis_rotate_kernel<<<vgrid(P), 256, 0, s>>>(n, m + 1, kd + 1, V.p, n, Qd.p, Wd.p, n);
+        ++P.ctx->launches;
+        OPEM_CUDA(cudaMemcpyAsync(V.p, Wd.p, (size_t)(kd + 1) * n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+        OPEM_CUDA(cudaStreamSynchronize(s));
+        Hh = Hn;
+        c = cn;
+        start = kd;
+        fresh = false;
     }
     res.its = its;
     res.relres = beta / bnorm;
     if (!res.converged && res.code == OPEM_OK) res.code = OPEM_ERR_NOT_CONVERGED;
-    int st = 0;
-    OPEM_CUDA(cudaMemcpy(&st, pc.status.p, sizeof(int), cudaMemcpyDeviceToHost));
-    (void)st;
     return res;
 }
 

@@ -149,3 +149,15 @@ def test_errors_are_status_codes(ctx):
     with pytest.raises(OpemError) as ei:
         Fem3D(bad, context=ctx)
     assert ei.value.code == _lib.ERR_MESH
+
+
+def test_deflated_restart_cuts_iterations(ctx):
+    """GMRES-DR(m, k) vs plain GMRES(m): same S, fewer iterations on a mesh
+    where plain restarting stagnates."""
+    prob = meshgen.waveguide_problem(meshgen.WR_A, meshgen.WR_B, 50e-3, 8, 4, 20, 2, slab=(20e-3, 30e-3, 4.4, 0.02))
+    F = Fem3D(prob, context=ctx).assemble()
+    S0, _, st0 = F.solve(10e9, default_opts(restart=60, deflate=0, maxits=20000))
+    S1, _, st1 = F.solve(10e9, default_opts(restart=60, deflate=20, maxits=20000))
+    assert st0["converged"] == 1 and st1["converged"] == 1
+    assert np.abs(S0 - S1).max() <= 1e-7
+    assert st1["iterations"] < st0["iterations"]
