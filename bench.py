@@ -41,7 +41,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="plain", choices=["plain", "mixed"])
-    ap.add_argument("--restart", type=int, default=150)
+    ap.add_argument("--restart", type=int, default=100)
+    ap.add_argument("--deflate", type=int, default=30)
+    ap.add_argument("--mesh", default="24,12,60",
+                    help="hex grid nx,ny,nz of the same box/slab/ND2 problem (profiling runs use a smaller one)")
     ap.add_argument("--rtol", type=float, default=1e-10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -170,7 +173,8 @@ def config_dict(args):
     return {"workload": "WR90 guide 24x12x60 hex (103,680 tets), eps_r 4.4/tan_d 0.02 slab, ND2 "
                         "(681,312 DOF), 2 wave ports, 51-point 8-12 GHz sweep",
             "order": 2, "ndof": C2_NDOF, "nnz": 28969152, "driving_sets_per_step": 2, "mode": args.mode,
-            "gmres_restart": args.restart, "rtol": args.rtol, "precond": "vertex-patch block Jacobi",
+            "mesh": args.mesh, "gmres_restart": args.restart, "gmres_deflate": args.deflate, "rtol": args.rtol,
+            "krylov": "GMRES-DR (deflated restarting)", "precond": "vertex-patch block Jacobi",
             "l2": "operator arrays ~1 GB > 126 MB L2, no flush", "parallelism": f"replicas x{args.gpus}"}
 
 
@@ -182,11 +186,17 @@ def run_ours(args, rank, world, local_rank):
     import ctypes as C
     dev = local_rank
     torch.cuda.set_device(dev)
-    prob, freqs = meshgen.config2()
+    nx, ny, nz = (int(v) for v in args.mesh.split(","))
+    if (nx, ny, nz) == (24, 12, 60):
+        prob, freqs = meshgen.config2()
+    else:
+        prob = meshgen.waveguide_problem(meshgen.WR_A, meshgen.WR_B, 50e-3, nx, ny, nz, 2,
+                                         slab=(20e-3, 30e-3, 4.4, 0.02))
+        freqs = np.linspace(8e9, 12e9, 51)
     ctx = Context(dev)
     F = Fem3D(prob, context=ctx).assemble()
     info = F.info()
-    opts = default_opts(rtol=args.rtol, restart=args.restart, maxits=20000)
+    opts = default_opts(rtol=args.rtol, restart=args.restart, deflate=args.deflate, maxits=20000)
     # rank r takes frequencies r, r+world, ...
     my_freqs = freqs[rank::world]
 

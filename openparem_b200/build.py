@@ -24,7 +24,11 @@ def build(verbose=False, extra=()):
         deps = [src] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith(".h")]
         deps.append(os.path.join(HERE, "..", "include", "opem_b200.h"))
         if not os.path.exists(obj) or any(os.path.getmtime(d) > os.path.getmtime(obj) for d in deps):
-            cmd = [NVCC] + FLAGS + list(extra) + ["-x", "cu" if s.endswith(".cu") else "c++", "-c", src, "-o", obj]
+            fl = list(FLAGS)
+            if s == "dense.cpp":
+                # small dense complex LA: plain complex arithmetic, no C99 inf/NaN recovery
+                fl[fl.index("-fPIC,-fopenmp,-O3")] = "-fPIC,-fopenmp,-O3,-fcx-limited-range"
+            cmd = [NVCC] + fl + list(extra) + ["-x", "cu" if s.endswith(".cu") else "c++", "-c", src, "-o", obj]
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)

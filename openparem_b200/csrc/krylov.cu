@@ -144,6 +144,55 @@ __global__ void multidot_kernel(int64_t n, const double2* __restrict__ V, int64_
     if (threadIdx.x == 0) partial[(int64_t)blockIdx.y * gridDim.x + blockIdx.x] = make_double2(re, im);
 }
 
+// Tiled multi-dot: partial[i*gridDim.x + blockIdx.x] = sum over the block's
+// chunk of conj(V_i) w for all i < nvec.  w's chunk is read once per tile of
+// 8 vectors (L1 resident); every V_i is read exactly once.
+constexpr int MD_TILE = 8;
+__global__ void __launch_bounds__(256) multidot_tile_kernel(int64_t n, int nvec, const double2* __restrict__ V,
+                                                             int64_t ldv, const double2* __restrict__ w,
+                                                             double2* __restrict__ partial) {
+    __shared__ double red[2 * MD_TILE][8];
+    int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+    int64_t lo = blockIdx.x * chunk, hi = min(n, lo + chunk);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int i0 = 0; i0 < nvec; i0 += MD_TILE) {
+        double re[MD_TILE], im[MD_TILE];
+#pragma unroll
+        for (int q = 0; q < MD_TILE; ++q) { re[q] = 0; im[q] = 0; }
+        for (int64_t k = lo + threadIdx.x; k < hi; k += blockDim.x) {
+            double2 b = w[k];
+#pragma unroll
+            for (int q = 0; q < MD_TILE; ++q) {
+                if (i0 + q < nvec) {
+                    double2 a = V[(int64_t)(i0 + q) * ldv + k];
+                    re[q] += a.x * b.x + a.y * b.y;
+                    im[q] += a.x * b.y - a.y * b.x;
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < MD_TILE; ++q)
+            for (int o = 16; o > 0; o >>= 1) {
+                re[q] += __shfl_down_sync(0xffffffffu, re[q], o);
+                im[q] += __shfl_down_sync(0xffffffffu, im[q], o);
+            }
+        __syncthreads();
+        if (lane == 0)
+#pragma unroll
+            for (int q = 0; q < MD_TILE; ++q) { red[2 * q][wid] = re[q]; red[2 * q + 1][wid] = im[q]; }
+        __syncthreads();
+        if (threadIdx.x < 2 * MD_TILE) {
+            double acc = 0;
+            for (int u = 0; u < nw; ++u) acc += red[threadIdx.x][u];
+            int q = threadIdx.x >> 1;
+            if (i0 + q < nvec) {
+                double2* out = &partial[(int64_t)(i0 + q) * gridDim.x + blockIdx.x];
+                if (threadIdx.x & 1) out->y = acc; else out->x = acc;
+            }
+        }
+    }
+}
+
 // h[i] = sum_c partial[i][c]; optionally accumulate into Hcol[i]
 __global__ void finish_dot_kernel(int nparts, const double2* __restrict__ partial, double2* __restrict__ h,
                                   double2* __restrict__ Hcol, int accumulate) {
@@ -171,6 +220,7 @@ __global__ void cgs_update_kernel(int64_t n, int nvec, const double2* __restrict
     __syncthreads();
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         double2 acc = w[k];
+#pragma unroll 4
         for (int i = 0; i < nvec; ++i) {
             double2 v = V[(int64_t)i * ldv + k];
             double2 c = sh[i];
@@ -430,9 +480,13 @@ __global__ void patch_invert_kernel(int npatch, const int32_t* __restrict__ pptr
 }
 
 // phase 1: t[p0+a] = sum_b B_v[a][b] r[dofs[p0+b]]
-__global__ void patch_apply1_kernel(int npatch, const int32_t* __restrict__ pptr, const int32_t* __restrict__ pdofs,
-                                    const int64_t* __restrict__ poff, const double2* __restrict__ B,
-                                    const double2* __restrict__ r, double2* __restrict__ t) {
+// One CTA per patch; each warp keeps 4 block rows in flight (independent
+// 16-byte loads per lane) to hide DRAM latency; lanes stride the columns so
+// every row read is coalesced.
+__global__ void __launch_bounds__(256) patch_apply1_kernel(int npatch, const int32_t* __restrict__ pptr,
+                                                            const int32_t* __restrict__ pdofs,
+                                                            const int64_t* __restrict__ poff, const double2* __restrict__ B,
+                                                            const double2* __restrict__ r, double2* __restrict__ t) {
     extern __shared__ double2 rv[];
     int v = blockIdx.x;
     int32_t p0 = pptr[v];
@@ -440,19 +494,31 @@ __global__ void patch_apply1_kernel(int npatch, const int32_t* __restrict__ pptr
     for (int a = threadIdx.x; a < s; a += blockDim.x) rv[a] = r[pdofs[p0 + a]];
     __syncthreads();
     const double2* Bv = B + poff[v];
-    int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int a = w; a < s; a += nw) {
-        double re = 0, im = 0;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    constexpr int RW = 4;
+    for (int a0 = w * RW; a0 < s; a0 += nw * RW) {
+        double re[RW], im[RW];
+#pragma unroll
+        for (int q = 0; q < RW; ++q) { re[q] = 0; im[q] = 0; }
         for (int b = lane; b < s; b += 32) {
-            double2 m = Bv[(int64_t)a * s + b], x = rv[b];
-            re += m.x * x.x - m.y * x.y;
-            im += m.x * x.y + m.y * x.x;
+            double2 x = rv[b];
+#pragma unroll
+            for (int q = 0; q < RW; ++q) {
+                if (a0 + q < s) {
+                    double2 m = __ldcs(&Bv[(int64_t)(a0 + q) * s + b]);
+                    re[q] += m.x * x.x - m.y * x.y;
+                    im[q] += m.x * x.y + m.y * x.x;
+                }
+            }
         }
-        for (int o = 16; o > 0; o >>= 1) {
-            re += __shfl_down_sync(0xffffffffu, re, o);
-            im += __shfl_down_sync(0xffffffffu, im, o);
+#pragma unroll
+        for (int q = 0; q < RW; ++q) {
+            for (int o = 16; o > 0; o >>= 1) {
+                re[q] += __shfl_down_sync(0xffffffffu, re[q], o);
+                im[q] += __shfl_down_sync(0xffffffffu, im[q], o);
+            }
+            if (lane == 0 && a0 + q < s) t[p0 + a0 + q] = make_double2(re[q], im[q]);
         }
-        if (lane == 0) t[p0 + a] = make_double2(re, im);
     }
 }
 
@@ -493,13 +559,15 @@ struct Red {
     explicit Red(int nmax) : part((size_t)nmax * RED_BLOCKS), out(nmax + 4) {}
 };
 
+static int md_blocks(const Problem& P) { return std::min(RED_BLOCKS, 2 * P.ctx->sm_count); }
+
 static void dot_many(Problem& P, Red& R, const double2* V, int64_t ldv, int nvec, const double2* w, double2* Hcol,
                      int accumulate) {
     cudaStream_t s = P.ctx->stream;
     int64_t n = P.topo.n;
-    dim3 grid(RED_BLOCKS, nvec);
-    multidot_kernel<<<grid, 256, 0, s>>>(n, V, ldv, w, R.part.p); ++P.ctx->launches;
-    finish_dot_kernel<<<nvec, 256, 0, s>>>(RED_BLOCKS, R.part.p, R.out.p, Hcol, accumulate); ++P.ctx->launches;
+    const int nb = md_blocks(P);
+    multidot_tile_kernel<<<nb, 256, 0, s>>>(n, nvec, V, ldv, w, R.part.p); ++P.ctx->launches;
+    finish_dot_kernel<<<nvec, 256, 0, s>>>(nb, R.part.p, R.out.p, Hcol, accumulate); ++P.ctx->launches;
     OPEM_CUDA(cudaGetLastError());
 }
 
@@ -552,7 +620,7 @@ static void patch_setup(Problem& P, PatchPrec& pc, const double2* A, const uint8
 static void patch_apply(Problem& P, PatchPrec& pc, const double2* r, double2* y, const uint8_t* dmask) {
     cudaStream_t s = P.ctx->stream;
     size_t smem = (size_t)P.topo.max_patch * sizeof(double2);
-    patch_apply1_kernel<<<P.npatch, 128, smem, s>>>(P.npatch, P.d_patch_ptr.p, P.d_patch_dofs.p, P.d_patch_off.p, pc.B.p,
+    patch_apply1_kernel<<<P.npatch, 256, smem, s>>>(P.npatch, P.d_patch_ptr.p, P.d_patch_dofs.p, P.d_patch_off.p, pc.B.p,
                                                     r, pc.t.p); ++P.ctx->launches;
     patch_apply2_kernel<<<vgrid(P), 256, 0, s>>>(P.topo.n, P.d_d2p_ptr.p, P.d_d2p_idx.p, pc.t.p, dmask, y); ++P.ctx->launches;
     OPEM_CUDA(cudaGetLastError());
@@ -906,13 +974,13 @@ void profile_fp64(Problem& P, const double2* A, const uint8_t* dmask, int reps, 
     out[0] = timeit([&] { spmv_complex(P, A, V.p, w.p, dmask); });
     out[1] = (double)nnz * (16 + 4) + 4.0 * (n + 1) + n * (16.0 + 16.0 + 1.0);
     out[3] = timeit([&] {
-        patch_apply1_kernel<<<P.npatch, 128, smem_p, s>>>(P.npatch, P.d_patch_ptr.p, P.d_patch_dofs.p, P.d_patch_off.p,
+        patch_apply1_kernel<<<P.npatch, 256, smem_p, s>>>(P.npatch, P.d_patch_ptr.p, P.d_patch_dofs.p, P.d_patch_off.p,
                                                           pc.B.p, V.p, pc.t.p);
         ++P.ctx->launches;
     });
     out[4] = patch_sq * 16 + patch_len * (4 + 16 + 16) + P.npatch * 12.0;
     out[6] = timeit([&] {
-        multidot_kernel<<<dim3(RED_BLOCKS, nv), 256, 0, s>>>(n, V.p, n, w.p, R.part.p);
+        multidot_tile_kernel<<<md_blocks(P), 256, 0, s>>>(n, nv, V.p, n, w.p, R.part.p);
         ++P.ctx->launches;
     });
     out[7] = (double)nv * n * 16 + n * 16.0;
