@@ -31,7 +31,9 @@ sys.path.insert(0, ROOT)
 METRIC = "freq-point solves/sec at |dS|<=1e-6 vs FP64, mixed vs plain; p50/p99 latency"
 UNIT = "freq-points/s"
 C2_NDOF = 681312
-REF_ND2_EXPONENT = 1.53   # reference's own ND2 timings: 103,146 -> 656,168 DOF, 18.45 -> 315.4 s
+REF_ND2_EXPONENT = 1.53
+# ncu dram__bytes_read+write / algorithmic bytes of patch_apply1 (profiles/patch_apply1_16x8x40.md)
+TRAFFIC_RATIO_PATCH = 726.0 / 727.1   # reference's own ND2 timings: 103,146 -> 656,168 DOF, 18.45 -> 315.4 s
 
 
 def parse():
@@ -40,7 +42,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--mode", default="plain", choices=["plain", "mixed"])
+    ap.add_argument("--mode", default="both", choices=["plain", "mixed", "both"])
+    ap.add_argument("--batch", type=int, default=13, help="frequency points per mixed-precision batch")
     ap.add_argument("--restart", type=int, default=100)
     ap.add_argument("--deflate", type=int, default=30)
     ap.add_argument("--mesh", default="24,12,60",
@@ -172,7 +175,9 @@ def run_reference(args, rank, world):
 def config_dict(args):
     return {"workload": "WR90 guide 24x12x60 hex (103,680 tets), eps_r 4.4/tan_d 0.02 slab, ND2 "
                         "(681,312 DOF), 2 wave ports, 51-point 8-12 GHz sweep",
-            "order": 2, "ndof": C2_NDOF, "nnz": 28969152, "driving_sets_per_step": 2, "mode": args.mode,
+            "order": 2, "ndof": C2_NDOF, "nnz": 28969152, "mode": args.mode,
+            "step": (f"mixed: one batch of {args.batch} frequency points x 2 driving sets; plain: one point"
+                     if args.mode != "plain" else "one frequency point (2 driving sets)"),
             "mesh": args.mesh, "gmres_restart": args.restart, "gmres_deflate": args.deflate, "rtol": args.rtol,
             "krylov": "GMRES-DR (deflated restarting)", "precond": "vertex-patch block Jacobi",
             "l2": "operator arrays ~1 GB > 126 MB L2, no flush", "parallelism": f"replicas x{args.gpus}"}
@@ -182,7 +187,7 @@ def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
     from openparem_b200 import meshgen, Fem3D, default_opts, _lib
-    from openparem_b200.fem3d import Context
+    from openparem_b200.fem3d import Context, _dp
     import ctypes as C
     dev = local_rank
     torch.cuda.set_device(dev)
@@ -196,49 +201,88 @@ def run_ours(args, rank, world, local_rank):
     ctx = Context(dev)
     F = Fem3D(prob, context=ctx).assemble()
     info = F.info()
-    opts = default_opts(rtol=args.rtol, restart=args.restart, deflate=args.deflate, maxits=20000)
-    # rank r takes frequencies r, r+world, ...
+    N = F.nports
+    plain_o = default_opts(rtol=args.rtol, restart=args.restart, deflate=args.deflate, maxits=20000)
+    mixed_o = default_opts(rtol=args.rtol, restart=args.restart, deflate=args.deflate, maxits=20000,
+                           precision=_lib.PREC_MIXED)
     my_freqs = freqs[rank::world]
+    nb = args.batch
 
-    def step(i):
-        f = my_freqs[i % len(my_freqs)]
-        S, Z, st = F.solve(f, opts, allow_not_converged=True)
-        return S, st
+    def batch_freqs(i):
+        idx = [(i * nb + j) % len(my_freqs) for j in range(nb)]
+        return np.ascontiguousarray(np.sort(my_freqs[idx]))
 
-    for i in range(args.warmup):
-        step(i)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
+    def mixed_step(i):
+        fr = batch_freqs(i)
+        S = np.zeros(2 * N * N * len(fr))
+        st = (_lib.SolveStats * len(fr))()
+        t0 = time.perf_counter()
+        rc = _lib.lib().opem_solve_sweep(F.h, len(fr), _dp(fr), C.byref(mixed_o), _dp(S), st)
+        wall = time.perf_counter() - t0
+        if rc not in (_lib.OK, _lib.ERR_NOT_CONVERGED):
+            raise RuntimeError(f"opem_solve_sweep failed: {rc}")
+        S = (S[0::2] + 1j * S[1::2]).reshape(len(fr), N, N)
+        return fr, S, [s.as_dict() for s in st], wall
+
+    def plain_step(f):
+        t0 = time.perf_counter()
+        S, Z, st = F.solve(f, plain_o, allow_not_converged=True)
+        return S, st, time.perf_counter() - t0
+
+    modes = ["mixed", "plain"] if args.mode == "both" else [args.mode]
+    res = {}
     l0 = C.c_int64()
-    _lib.lib().opem_context_launches(ctx.h, C.byref(l0))
-    dev_s = []
-    wall_s = []
-    its = []
-    conv = []
-    with Clocks(dev) as clk:
-        for i in range(args.steps):
-            t0 = time.perf_counter()
-            S, st = step(args.warmup + i)
-            wall_s.append(time.perf_counter() - t0)
-            dev_s.append(st["seconds"])
-            its.append(st["iterations"])
-            conv.append(st["converged"])
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
     l1 = C.c_int64()
-    _lib.lib().opem_context_launches(ctx.h, C.byref(l1))
-    t_dev = sum(dev_s)
-    t_wall = sum(wall_s)
-    tmax = torch.tensor([t_dev, t_wall], dtype=torch.float64, device=f"cuda:{dev}")
-    if world > 1:
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-    t_dev, t_wall = float(tmax[0]), float(tmax[1])
-    # kernel roofline (CUDA events inside the library, same stream as the solve)
+    clk_summary = None
+    for mode in modes:
+        steps = args.steps if mode == modes[0] else max(1, min(args.steps, 2))
+        warm = args.warmup if mode == modes[0] else 1
+        for i in range(warm):
+            if mode == "mixed":
+                mixed_step(i)
+            else:
+                plain_step(my_freqs[i % len(my_freqs)])
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        _lib.lib().opem_context_launches(ctx.h, C.byref(l0))
+        dev_s, wall_s, lat, its, conv, outer, Sd = [], [], [], [], [], [], {}
+        with Clocks(dev) as clk:
+            for i in range(steps):
+                if mode == "mixed":
+                    fr, S, st, wall = mixed_step(warm + i)
+                    dev_s.append(sum(x["seconds"] for x in st))
+                    wall_s.append(wall)
+                    lat += [sum(x["seconds"] for x in st)] * len(fr)
+                    its.append(st[0]["iterations"])
+                    outer.append(st[0]["outer"])
+                    conv += [x["converged"] for x in st]
+                    for f, Sf in zip(fr, S):
+                        Sd[float(f)] = Sf
+                else:
+                    f = float(res["mixed"]["freqs"][i]) if "mixed" in res else my_freqs[(warm + i) % len(my_freqs)]
+                    S, st, wall = plain_step(f)
+                    dev_s.append(st["seconds"])
+                    wall_s.append(wall)
+                    lat.append(st["seconds"])
+                    its.append(st["iterations"])
+                    conv.append(st["converged"])
+                    Sd[float(f)] = S
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        _lib.lib().opem_context_launches(ctx.h, C.byref(l1))
+        units = sum(len(batch_freqs(warm + i)) for i in range(steps)) if mode == "mixed" else steps
+        t = torch.tensor([sum(dev_s), sum(wall_s)], dtype=torch.float64, device=f"cuda:{dev}")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        res[mode] = {"units": units * world, "t_dev": float(t[0]), "t_wall": float(t[1]), "steps": steps,
+                     "launches": int(l1.value - l0.value), "lat": lat, "its": its, "outer": outer, "conv": conv,
+                     "S": Sd, "freqs": sorted(Sd.keys()), "clocks": clk.summary()}
+        if mode == modes[0]:
+            clk_summary = clk.summary()
     prof = np.zeros(12)
-    rc = _lib.lib().opem_profile_kernels(F.h, float(freqs[len(freqs) // 2]), 20,
-                                        prof.ctypes.data_as(_lib.DP), 12)
+    rc = _lib.lib().opem_profile_kernels(F.h, float(freqs[len(freqs) // 2]), 20, prof.ctypes.data_as(_lib.DP), 12)
     if rank != 0:
         return
     peak, peak_kind = peaks()
@@ -248,24 +292,46 @@ def run_ours(args, rank, world, local_rank):
             for k in range(4)} if rc == 0 else {"error": rc}
     dom = "patch_apply1"
     ach = kern[dom]["GBps"] if rc == 0 else None
-    units = args.steps * world
-    value = units / t_dev
-    e2e = units / t_wall
+    head = res[modes[0]]
+    value = head["units"] / head["t_dev"]
+    e2e = head["units"] / head["t_wall"]
     n = info["ndofs"]
+    if modes[0] == "mixed":
+        nfp = args.batch
+        h2d = 8 * nfp + 64
+        d2h = 16 * N * N * nfp + 48 * nfp
+        note = "ctypes opem_solve_sweep call per step (13 points x 2 driving sets, host S buffer)"
+    else:
+        h2d = 8 + 64
+        d2h = 2 * 16 * 4 + 2 * 2 * n * 16
+        note = "ctypes opem_solve_frequency call per step; returns S, Zo and E/H DOF vectors of both driving sets"
+    lat = np.array(head["lat"]) * 1e3
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "c128" if args.mode == "plain" else "c64/c128",
+            "warmup": args.warmup, "ms_per_step": 1000.0 * head["t_dev"] / head["steps"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "c64 inner / c128 refinement" if modes[0] == "mixed" else "c128",
             "data": "synthetic", "config": config_dict(args),
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 + 48,
-                    "d2h_bytes_per_step": 2 * 16 * 4 + 2 * 2 * n * 16,
-                    "note": "ctypes opem_solve_frequency call per step; returns S, Zo and E/H DOF vectors of both driving sets to host"},
-            "gpu_launches": int(l1.value - l0.value),
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
-                         "frac": (ach / peak) if ach else None, "traffic": None, "peak_kind": peak_kind,
-                         "kernels": kern},
-            "solver": {"iterations_per_step": its, "converged": conv, "patches": info["npatches"],
-                       "max_patch": info["max_patch"]},
-            "clocks": clk.summary()}
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "note": note},
+            "gpu_launches": head["launches"],
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "what": "device time until a frequency point's S is available (its whole batch in mixed mode)"},
+            "roofline": {"bound": "hbm", "kernel": dom + " (FP64 path)", "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": (ach / peak) if ach else None,
+                         "traffic": (kern[dom]["bytes"] * TRAFFIC_RATIO_PATCH) if rc == 0 else None,
+                         "traffic_source": "ncu dram__bytes of the same kernel on the 16x8x40 case (profiles/patch_apply1_16x8x40.md), scaled by algorithmic bytes",
+                         "peak_kind": peak_kind, "kernels": kern},
+            "solver": {"iterations_per_step": head["its"], "outer_steps": head["outer"],
+                       "converged": head["conv"], "patches": info["npatches"], "max_patch": info["max_patch"]},
+            "clocks": clk_summary}
+    if "mixed" in res and "plain" in res:
+        pv = res["plain"]["units"] / res["plain"]["t_dev"]
+        common = [f for f in res["plain"]["freqs"] if f in res["mixed"]["S"]]
+        dS = max(float(np.abs(res["mixed"]["S"][f] - res["plain"]["S"][f]).max()) for f in common) if common else None
+        line["plain_fp64"] = {"value": pv, "unit": UNIT, "ms_per_point": 1000.0 / pv,
+                              "iterations_per_point": res["plain"]["its"], "steps": res["plain"]["steps"],
+                              "launches": res["plain"]["launches"]}
+        line["mixed_vs_plain"] = value / pv
+        line["dS_mixed_vs_fp64"] = {"max": dS, "points": len(common), "tolerance": 1e-6}
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample()
     print(json.dumps(line), flush=True)

@@ -200,4 +200,98 @@ int orthonormalise(int rows, int cols, std::vector<cd>& Q) {
     return rank;
 }
 
+void GivensLsq::reset(int m_, const std::vector<cd>& c) {
+    m = m_;
+    R.assign((size_t)(m + 1) * m, 0.0);
+    g = c;
+    g.resize(m + 1, 0.0);
+    rots.clear();
+}
+
+static inline void rot_apply(const GivensLsq::Rot& q, cd& a, cd& b) {
+    cd x = a, y = b;
+    a = q.c * x + q.s * y;
+    b = -std::conj(q.s) * x + q.c * y;
+}
+
+double GivensLsq::add_column(int j, const cd* col, int top) {
+    cd* rc = &R[(size_t)j * (m + 1)];
+    for (int i = 0; i <= top; ++i) rc[i] = col[i];
+    for (int i = top + 1; i <= m; ++i) rc[i] = 0.0;
+    for (const Rot& q : rots) rot_apply(q, rc[q.i1], rc[q.i2]);
+    for (int r = j + 1; r <= top; ++r) {
+        if (rc[r] == 0.0) continue;
+        Rot q;
+        q.i1 = j;
+        q.i2 = r;
+        double aa = std::abs(rc[j]), bb = std::abs(rc[r]);
+        if (aa == 0.0) { q.c = 0.0; q.s = std::conj(rc[r]) / bb; }
+        else { double rho = std::hypot(aa, bb); q.c = aa / rho; q.s = (rc[j] / aa) * std::conj(rc[r]) / rho; }
+        rot_apply(q, rc[j], rc[r]);
+        rc[r] = 0.0;
+        rot_apply(q, g[j], g[r]);
+        rots.push_back(q);
+    }
+    return std::abs(g[j + 1]);
+}
+
+void GivensLsq::solve(int k, std::vector<cd>& y) const {
+    y.assign(k, 0.0);
+    for (int i = k - 1; i >= 0; --i) {
+        cd s = g[i];
+        for (int c = i + 1; c < k; ++c) s -= R[i + (size_t)c * (m + 1)] * y[c];
+        y[i] = s / R[i + (size_t)i * (m + 1)];
+    }
+}
+
+bool gmres_dr_deflate(int m, int kd, const std::vector<cd>& Hh, const std::vector<cd>& c, const std::vector<cd>& y,
+                      std::vector<cd>& Pm, std::vector<cd>& Hn, std::vector<cd>& cn) {
+    const size_t ld = (size_t)m + 1;
+    std::vector<cd> rc(m + 1);
+    for (int i = 0; i <= m; ++i) {
+        cd t = c[i];
+        for (int j = 0; j < m; ++j) t -= Hh[i + (size_t)j * ld] * y[j];
+        rc[i] = t;
+    }
+    // harmonic Ritz problem (H_m + |h_{m+1,m}|^2 H_m^{-H} e_m e_m^T) g = theta g
+    std::vector<cd> Hm((size_t)m * m), HmH((size_t)m * m), f(m, 0.0);
+    for (int j = 0; j < m; ++j)
+        for (int i = 0; i < m; ++i) {
+            Hm[i + (size_t)j * m] = Hh[i + (size_t)j * ld];
+            HmH[j + (size_t)i * m] = std::conj(Hh[i + (size_t)j * ld]);
+        }
+    f[m - 1] = 1.0;
+    if (!lu_solve(m, HmH, f)) return false;
+    double hm2 = std::norm(Hh[m + (size_t)(m - 1) * ld]);
+    for (int i = 0; i < m; ++i) Hm[i + (size_t)(m - 1) * m] += hm2 * f[i];
+    std::vector<cd> theta, gv;
+    if (!eig_smallest(m, Hm, kd, theta, gv)) return false;
+    Pm.assign(ld * (kd + 1), 0.0);
+    for (int q = 0; q < kd; ++q)
+        for (int i = 0; i < m; ++i) Pm[i + (size_t)q * ld] = gv[i + (size_t)q * m];
+    for (int i = 0; i <= m; ++i) Pm[i + (size_t)kd * ld] = rc[i];
+    if (orthonormalise(m + 1, kd + 1, Pm) != kd + 1) return false;
+    std::vector<cd> T1(ld * kd, 0.0);
+    for (int q = 0; q < kd; ++q)
+        for (int j = 0; j < m; ++j) {
+            cd pj = Pm[j + (size_t)q * ld];
+            if (pj == 0.0) continue;
+            for (int i = 0; i <= m; ++i) T1[i + (size_t)q * ld] += Hh[i + (size_t)j * ld] * pj;
+        }
+    Hn.assign(ld * m, 0.0);
+    cn.assign(m + 1, 0.0);
+    for (int q = 0; q < kd; ++q)
+        for (int a = 0; a <= kd; ++a) {
+            cd t = 0;
+            for (int i = 0; i <= m; ++i) t += std::conj(Pm[i + (size_t)a * ld]) * T1[i + (size_t)q * ld];
+            Hn[a + (size_t)q * ld] = t;
+        }
+    for (int a = 0; a <= kd; ++a) {
+        cd t = 0;
+        for (int i = 0; i <= m; ++i) t += std::conj(Pm[i + (size_t)a * ld]) * rc[i];
+        cn[a] = t;
+    }
+    return true;
+}
+
 }  // namespace opem

@@ -262,6 +262,26 @@ __global__ void dmask_kernel(int64_t n, const uint8_t* __restrict__ pec, const u
         out[i] = (pec[i] || ((pm[i] >> d) & 1)) ? 1 : 0;
 }
 
+void make_dmask(Problem& P, int d, uint8_t* dm) {
+    dmask_kernel<<<P.ctx->sm_count * 8, 256, 0, P.ctx->stream>>>(P.topo.n, P.d_pec.p, P.d_portmask.p, d, dm);
+    ++P.ctx->launches;
+    OPEM_CUDA(cudaGetLastError());
+}
+
+double port_mu_r(const Problem& P, int k) { return P.mu_r[port_region(P, k)]; }
+
+std::vector<cd> s_matrix_solve(int N, const std::vector<cd>& Cp, const std::vector<cd>& Cm, const std::vector<cd>& V,
+                               const std::vector<cd>& Z, bool reciprocal) {
+    std::vector<cd> S = s_matrix(N, Cp, Cm, V, Z);
+    if (reciprocal) {
+        std::vector<cd> S2 = S;
+        for (int i = 0; i < N; ++i)
+            for (int j = 0; j < N; ++j) S2[i * N + j] = 0.5 * (S[i * N + j] + S[j * N + i]);
+        S = S2;
+    }
+    return S;
+}
+
 // x0 with PEC entries removed (columns of PEC dofs are zero in the eliminated A)
 __global__ void lift_kernel(int64_t n, const double2* __restrict__ et, const uint8_t* __restrict__ pec,
                             double2* __restrict__ x0) {
@@ -727,7 +747,20 @@ int opem_solve_frequency(opem_problem prob, double freq, const opem_solver_opts*
     FreqResult fr;
     int rc = guarded(P.ctx, [&] {
         OPEM_CUDA(cudaSetDevice(P.ctx->device));
-        solve_frequency_plain(P, freq, o, fr, true);
+        if (o.precision == OPEM_PREC_MIXED) {
+            std::vector<std::vector<cd>> S;
+            std::vector<opem_solve_stats> st;
+            solve_sweep_mixed(P, 1, &freq, o, S, st);
+            fr.S = S[0];
+            fr.st = st[0];
+            fr.Zo.resize(P.nports);
+            for (int k = 0; k < P.nports; ++k) {
+                cd g, V;
+                port_gamma_Z_V(P, k, freq, g, fr.Zo[k], V);
+            }
+        } else {
+            solve_frequency_plain(P, freq, o, fr, true);
+        }
     });
     if (rc) return rc;
     int N = P.nports;
@@ -742,6 +775,29 @@ int opem_solve_sweep(opem_problem prob, int nfreq, const double* freqs, const op
                      opem_solve_stats* stats) {
     if (!prob || nfreq <= 0 || !freqs || !S_out) return OPEM_ERR_ARG;
     int N = prob->p.nports, worst = OPEM_OK;
+    if (opts && opts->precision == OPEM_PREC_MIXED) {
+        Problem& P = prob->p;
+        if (!opts_ok(opts)) return OPEM_ERR_ARG;
+        if (!P.assembled) { P.ctx->last_error = "problem not assembled"; return OPEM_ERR_STATE; }
+        for (int f = 0; f < nfreq; ++f)
+            if (!(freqs[f] > 0)) return OPEM_ERR_ARG;
+        std::vector<std::vector<cd>> S;
+        std::vector<opem_solve_stats> st;
+        int rc = guarded(P.ctx, [&] {
+            OPEM_CUDA(cudaSetDevice(P.ctx->device));
+            solve_sweep_mixed(P, nfreq, freqs, *opts, S, st);
+        });
+        if (rc) return rc;
+        for (int f = 0; f < nfreq; ++f) {
+            for (int i = 0; i < N * N; ++i) {
+                S_out[(size_t)2 * N * N * f + 2 * i] = S[f][i].real();
+                S_out[(size_t)2 * N * N * f + 2 * i + 1] = S[f][i].imag();
+            }
+            if (stats) stats[f] = st[f];
+            if (!st[f].converged) worst = OPEM_ERR_NOT_CONVERGED;
+        }
+        return worst;
+    }
     for (int f = 0; f < nfreq; ++f) {
         int rc = opem_solve_frequency(prob, freqs[f], opts, S_out + (size_t)2 * N * N * f, nullptr, stats ? stats + f : nullptr);
         if (rc == OPEM_ERR_NOT_CONVERGED) worst = rc;

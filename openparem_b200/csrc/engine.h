@@ -139,5 +139,16 @@ SolveResult solve_mass_cg(Problem& P, const double2* b, double2* x, double rtol,
 void spmv_real_complex(Problem& P, const double* vals, const double2* x, double2* y, double scale_re, double scale_im);
 void spmv_complex(Problem& P, const double2* A, const double2* x, double2* y, const uint8_t* zero_rows);
 void profile_fp64(Problem& P, const double2* A, const uint8_t* dmask, int reps, double* out);
+void patch_blocks_fp64(Problem& P, const double2* A, const uint8_t* dmask, DBuf<double2>& B);
+
+// ---- engine helpers shared with the mixed path (engine.cu)
+void make_dmask(Problem& P, int d, uint8_t* dm);
+double port_mu_r(const Problem& P, int k);
+std::vector<cd> s_matrix_solve(int N, const std::vector<cd>& Cp, const std::vector<cd>& Cm, const std::vector<cd>& V,
+                               const std::vector<cd>& Z, bool reciprocal);
+
+// ---- batched mixed-precision sweep (mixed.cu)
+void solve_sweep_mixed(Problem& P, int nfreq, const double* freqs, const opem_solver_opts& o,
+                       std::vector<std::vector<cd>>& S, std::vector<opem_solve_stats>& st);
 
 }  // namespace opem

@@ -617,6 +617,13 @@ static void patch_setup(Problem& P, PatchPrec& pc, const double2* A, const uint8
     OPEM_CUDA(cudaGetLastError());
 }
 
+// FP64 inverted vertex-patch blocks of A (for the mixed path, which rounds them to FP32).
+void patch_blocks_fp64(Problem& P, const double2* A, const uint8_t* dmask, DBuf<double2>& B) {
+    PatchPrec pc;
+    patch_setup(P, pc, A, dmask);
+    B = std::move(pc.B);
+}
+
 static void patch_apply(Problem& P, PatchPrec& pc, const double2* r, double2* y, const uint8_t* dmask) {
     cudaStream_t s = P.ctx->stream;
     size_t smem = (size_t)P.topo.max_patch * sizeof(double2);
@@ -655,56 +662,6 @@ __global__ void basis_rotate_kernel(int64_t n, int nin, int nout, const double2*
     }
 }
 
-namespace {
-// Incremental QR of the (m+1) x m least-squares matrix by Givens rotations.
-struct Rot { int i1, i2; double c; cd s; };
-struct LsqState {
-    int m = 0;
-    std::vector<cd> R;      // (m+1) x m column-major (rotated copy of H)
-    std::vector<cd> g;      // rotated right-hand side
-    std::vector<Rot> rots;
-    void reset(int m_, const std::vector<cd>& c) {
-        m = m_;
-        R.assign((size_t)(m + 1) * m, 0.0);
-        g = c;
-        rots.clear();
-    }
-    static void apply(const Rot& q, cd& a, cd& b) {
-        cd x = a, y = b;
-        a = q.c * x + q.s * y;
-        b = -std::conj(q.s) * x + q.c * y;
-    }
-    // add column j (entries 0..top) and eliminate its entries below the diagonal
-    double add_column(int j, const cd* col, int top) {
-        cd* rc = &R[(size_t)j * (m + 1)];
-        for (int i = 0; i <= top; ++i) rc[i] = col[i];
-        for (int i = top + 1; i <= m; ++i) rc[i] = 0.0;
-        for (const Rot& q : rots) apply(q, rc[q.i1], rc[q.i2]);
-        for (int r = j + 1; r <= top; ++r) {
-            if (rc[r] == 0.0) continue;
-            Rot q;
-            q.i1 = j; q.i2 = r;
-            double aa = std::abs(rc[j]), bb = std::abs(rc[r]);
-            if (aa == 0.0) { q.c = 0.0; q.s = std::conj(rc[r]) / bb; }
-            else { double rho = std::hypot(aa, bb); q.c = aa / rho; q.s = (rc[j] / aa) * std::conj(rc[r]) / rho; }
-            apply(q, rc[j], rc[r]);
-            rc[r] = 0.0;
-            apply(q, g[j], g[r]);
-            rots.push_back(q);
-        }
-        return std::abs(g[j + 1]);
-    }
-    // y = R[:k,:k]^-1 g[:k]
-    void solve(int k, std::vector<cd>& y) const {
-        y.assign(k, 0.0);
-        for (int i = k - 1; i >= 0; --i) {
-            cd s = g[i];
-            for (int c = i + 1; c < k; ++c) s -= R[i + (size_t)c * (m + 1)] * y[c];
-            y[i] = s / R[i + (size_t)i * (m + 1)];
-        }
-    }
-};
-}  // namespace
 
 // ---------------------------------------------------------------------------
 // GMRES-DR(m, k), FP64, right preconditioned by vertex-patch block Jacobi.
@@ -737,7 +694,7 @@ SolveResult solve_plain_fp64(Problem& P, const double2* A, const uint8_t* dmask,
     OPEM_CUDA(cudaMemcpyAsync(w.p, b, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
     std::vector<cd> Hh((size_t)(m + 1) * m, 0.0), c(m + 1, 0.0), y;
     std::vector<double2> colbuf(m + 2);
-    LsqState L;
+    GivensLsq L;
     double beta = bnorm;
     int start = 0, its = 0;
     bool fresh = true;
@@ -802,49 +759,8 @@ SolveResult solve_plain_fp64(Problem& P, const double2* A, const uint8_t* dmask,
         fresh = true;
         if (kd == 0 || ncol < m) continue;
         // ---- deflated restart (harmonic Ritz vectors of the m x m problem)
-        std::vector<cd> rc(m + 1);
-        for (int i = 0; i <= m; ++i) {
-            cd t = c[i];
-            for (int j = 0; j < m; ++j) t -= Hh[i + (size_t)j * (m + 1)] * y[j];
-            rc[i] = t;
-        }
-        std::vector<cd> Hm((size_t)m * m), HmH((size_t)m * m), f(m, 0.0);
-        for (int j = 0; j < m; ++j)
-            for (int i = 0; i < m; ++i) {
-                Hm[i + (size_t)j * m] = Hh[i + (size_t)j * (m + 1)];
-                HmH[j + (size_t)i * m] = std::conj(Hh[i + (size_t)j * (m + 1)]);
-            }
-        f[m - 1] = 1.0;
-        if (!lu_solve(m, HmH, f)) continue;
-        double hm2 = std::norm(Hh[m + (size_t)(m - 1) * (m + 1)]);
-        for (int i = 0; i < m; ++i) Hm[i + (size_t)(m - 1) * m] += hm2 * f[i];
-        std::vector<cd> theta, gv;
-        if (!eig_smallest(m, Hm, kd, theta, gv)) continue;
-        std::vector<cd> Pm((size_t)(m + 1) * (kd + 1), 0.0);
-        for (int q = 0; q < kd; ++q)
-            for (int i = 0; i < m; ++i) Pm[i + (size_t)q * (m + 1)] = gv[i + (size_t)q * m];
-        for (int i = 0; i <= m; ++i) Pm[i + (size_t)kd * (m + 1)] = rc[i];
-        if (orthonormalise(m + 1, kd + 1, Pm) != kd + 1) continue;
-        // Hnew = Pm^H H Pm[:m, :kd] ; cnew = Pm^H rc
-        std::vector<cd> T1((size_t)(m + 1) * kd, 0.0);
-        for (int q = 0; q < kd; ++q)
-            for (int j = 0; j < m; ++j) {
-                cd pj = Pm[j + (size_t)q * (m + 1)];
-                if (pj == 0.0) continue;
-                for (int i = 0; i <= m; ++i) T1[i + (size_t)q * (m + 1)] += Hh[i + (size_t)j * (m + 1)] * pj;
-            }
-        std::vector<cd> Hn((size_t)(m + 1) * m, 0.0), cn(m + 1, 0.0);
-        for (int q = 0; q < kd; ++q)
-            for (int a = 0; a <= kd; ++a) {
-                cd t = 0;
-                for (int i = 0; i <= m; ++i) t += std::conj(Pm[i + (size_t)a * (m + 1)]) * T1[i + (size_t)q * (m + 1)];
-                Hn[a + (size_t)q * (m + 1)] = t;
-            }
-        for (int a = 0; a <= kd; ++a) {
-            cd t = 0;
-            for (int i = 0; i <= m; ++i) t += std::conj(Pm[i + (size_t)a * (m + 1)]) * rc[i];
-            cn[a] = t;
-        }
+        std::vector<cd> Pm, Hn, cn;
+        if (!gmres_dr_deflate(m, kd, Hh, c, y, Pm, Hn, cn)) continue;
         // device: V[:, :kd+1] = V Pm
         std::vector<double2> Qh((size_t)(m + 1) * (kd + 1));
         for (size_t t = 0; t < Qh.size(); ++t) Qh[t] = make_double2(Pm[t].real(), Pm[t].imag());

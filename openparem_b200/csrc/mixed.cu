@@ -1,0 +1,1283 @@
+// Batched mixed-precision solve of many (frequency, driving set) systems.
+//
+// Same per-frequency flow as the FP64 path (the reference's driving-set loop,
+// src/OpenParEM3D/OpenParEM3D.cpp:497-566) but up to RMAX systems share every
+// read of the operator and of the block-Jacobi blocks:
+//   outer (FP64):  r = b - A x on the FP64 operators; stop at ||r|| <= rtol ||b||
+//   inner (FP32):  GMRES-DR on A d = r/||r|| with FP32 operators, FP32 vertex-patch
+//                  blocks and FP32 Krylov vectors (FP32 accumulation); x += ||r|| d
+//   H (FP64):      batched CG on the mass matrix, P h = j Q e
+//   overlaps and S: FP64, as in the FP64 path.
+// The Hessenberg least-squares and the deflation eigenproblem of every system
+// are kept on the host in FP64.
+//
+// Layouts: vectors that feed the shared-matrix kernels (SpMV, block apply) are
+// interleaved, element (k, r) at k*R + r, so one row's gather for all systems
+// is one contiguous segment; per-system dense work (Gram-Schmidt, basis
+// updates) uses system-major vectors, system r at r*ld.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "dense.h"
+#include "engine.h"
+
+namespace opem {
+
+constexpr int RMAX = 32;
+static const double MU0_M = 4e-7 * M_PI;
+
+// ---------------------------------------------------------------------------
+// complex helpers for both precisions
+// ---------------------------------------------------------------------------
+template <class T2> struct Cx;
+template <> struct Cx<float2> {
+    using R = float;
+    __device__ static float2 make(float a, float b) { return make_float2(a, b); }
+};
+template <> struct Cx<double2> {
+    using R = double;
+    __device__ static double2 make(double a, double b) { return make_double2(a, b); }
+};
+
+template <class T> struct CplxOf;
+template <> struct CplxOf<float> { using type = float2; };
+template <> struct CplxOf<double> { using type = double2; };
+
+// per-system volume coefficients (A = K + ce Meps + ct Mtand + cs Msig)
+template <class T2> struct VC3 { T2 ce, ct, cs; };
+// per-system boundary-group coefficients
+template <class T2> struct BC5 { T2 cc, ce, ct, cs, c1; };
+
+// ---------------------------------------------------------------------------
+// batched SpMV: y_il = A_r x_il for every system r (warp per row, lane = system);
+// Dirichlet rows of system r (PEC or its driven port) are set to zero.
+// ---------------------------------------------------------------------------
+// T2: vector type (float2 or double2); T: matrix values, coefficients and
+// accumulation (the FP32-vector inner solve uses T = double: K and k0^2 eps M
+// nearly cancel on the slow modes, so they are combined in FP64).
+template <class T2, class T>
+__global__ void __launch_bounds__(256) spmv_batch_kernel(
+    int64_t n, int R, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ cols, const T* __restrict__ K,
+    const T* __restrict__ Me, const T* __restrict__ Mt, const T* __restrict__ Ms,
+    const VC3<typename CplxOf<T>::type>* __restrict__ coef, const T2* __restrict__ x, T2* __restrict__ y,
+    const uint8_t* __restrict__ pec, const uint8_t* __restrict__ pm, const uint8_t* __restrict__ dsys) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    VC3<typename CplxOf<T>::type> c;
+    int d = 0;
+    if (lane < R) { c = coef[lane]; d = dsys[lane]; }
+    for (int64_t row = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); row < n; row += warps) {
+        T re = 0, im = 0;
+        if (lane < R) {
+            for (int32_t k = rowptr[row]; k < rowptr[row + 1]; ++k) {
+                T kv = K[k], mv = Me[k];
+                T ar = kv + c.ce.x * mv, ai = c.ce.y * mv;
+                if (Mt) { T t = Mt[k]; ar += c.ct.x * t; ai += c.ct.y * t; }
+                if (Ms) { T t = Ms[k]; ar += c.cs.x * t; ai += c.cs.y * t; }
+                T2 xv = x[(int64_t)cols[k] * R + lane];
+                re += ar * xv.x - ai * xv.y;
+                im += ar * xv.y + ai * xv.x;
+            }
+            bool D = pec[row] || ((pm[row] >> d) & 1);
+            y[row * R + lane] = D ? Cx<T2>::make(0, 0) : Cx<T2>::make((typename Cx<T2>::R)re, (typename Cx<T2>::R)im);
+        }
+    }
+}
+
+// boundary groups: y_il[row] += sum_u (coef . R_u) x_il[col_u] on the group's rows
+template <class T2, class T>
+__global__ void bnd_batch_kernel(int nrows, int R, const int32_t* __restrict__ brow, const int32_t* __restrict__ bptr,
+                                 const int32_t* __restrict__ ucol, const double* __restrict__ Rg, int64_t nu,
+                                 const BC5<typename CplxOf<T>::type>* __restrict__ coef, const T2* __restrict__ x,
+                                 T2* __restrict__ y,
+                                 const uint8_t* __restrict__ pec, const uint8_t* __restrict__ pm,
+                                 const uint8_t* __restrict__ dsys) {
+    int lane = threadIdx.x & 31;
+    int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (i >= nrows || lane >= R) return;
+    int row = brow[i];
+    int d = dsys[lane];
+    if (pec[row] || ((pm[row] >> d) & 1)) return;
+    BC5<typename CplxOf<T>::type> c = coef[lane];
+    T re = 0, im = 0;
+    for (int32_t u = bptr[i]; u < bptr[i + 1]; ++u) {
+        T rcc = (T)Rg[u], re_ = (T)Rg[nu + u], rt = (T)Rg[2 * nu + u], rs = (T)Rg[3 * nu + u], r1 = (T)Rg[4 * nu + u];
+        T ar = c.cc.x * rcc + c.ce.x * re_ + c.ct.x * rt + c.cs.x * rs + c.c1.x * r1;
+        T ai = c.cc.y * rcc + c.ce.y * re_ + c.ct.y * rt + c.cs.y * rs + c.c1.y * r1;
+        T2 xv = x[(int64_t)ucol[u] * R + lane];
+        re += ar * xv.x - ai * xv.y;
+        im += ar * xv.y + ai * xv.x;
+    }
+    T2 v = y[(int64_t)row * R + lane];
+    y[(int64_t)row * R + lane] = Cx<T2>::make((typename Cx<T2>::R)(v.x + re), (typename Cx<T2>::R)(v.y + im));
+}
+
+// ---------------------------------------------------------------------------
+// layout transposes through shared memory (32 rows x R systems per tile)
+// ---------------------------------------------------------------------------
+template <class T2> __device__ inline T2 cvt2(float2 a);
+template <class T2> __device__ inline T2 cvt2(double2 a);
+template <> __device__ inline float2 cvt2<float2>(float2 a) { return a; }
+template <> __device__ inline float2 cvt2<float2>(double2 a) { return make_float2((float)a.x, (float)a.y); }
+template <> __device__ inline double2 cvt2<double2>(float2 a) { return make_double2(a.x, a.y); }
+template <> __device__ inline double2 cvt2<double2>(double2 a) { return a; }
+
+template <class T2, class O2 = T2>
+__global__ void sm2il_kernel(int64_t n, int R, const T2* __restrict__ in, int64_t ld, O2* __restrict__ out) {
+    __shared__ O2 tile[RMAX][33];
+    int64_t k0 = (int64_t)blockIdx.x * 32;
+    for (int r = threadIdx.y; r < R; r += blockDim.y) {
+        int64_t k = k0 + threadIdx.x;
+        if (k < n) tile[r][threadIdx.x] = cvt2<O2>(in[r * ld + k]);
+    }
+    __syncthreads();
+    int t = threadIdx.y * blockDim.x + threadIdx.x;
+    for (int e = t; e < 32 * R; e += blockDim.x * blockDim.y) {
+        int kk = e / R, r = e % R;
+        int64_t k = k0 + kk;
+        if (k < n) out[k * R + r] = tile[r][kk];
+    }
+}
+
+template <class T2, class O2 = T2>
+__global__ void il2sm_kernel(int64_t n, int R, const T2* __restrict__ in, O2* __restrict__ out, int64_t ld) {
+    __shared__ O2 tile[RMAX][33];
+    int64_t k0 = (int64_t)blockIdx.x * 32;
+    int t = threadIdx.y * blockDim.x + threadIdx.x;
+    for (int e = t; e < 32 * R; e += blockDim.x * blockDim.y) {
+        int kk = e / R, r = e % R;
+        int64_t k = k0 + kk;
+        if (k < n) tile[r][kk] = cvt2<O2>(in[k * R + r]);
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < R; r += blockDim.y) {
+        int64_t k = k0 + threadIdx.x;
+        if (k < n) out[r * ld + k] = tile[r][threadIdx.x];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// batched vertex-patch block Jacobi (FP32 blocks), systems [r0, r0+Rd)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) patch_apply1_batch_kernel(
+    int npatch, const int32_t* __restrict__ pptr, const int32_t* __restrict__ pdofs, const int64_t* __restrict__ poff,
+    const float2* __restrict__ B, const float2* __restrict__ x, int R, int r0, int Rd, float2* __restrict__ t) {
+    extern __shared__ float2 rv[];   // s x Rd
+    int v = blockIdx.x;
+    int32_t p0 = pptr[v];
+    int s = pptr[v + 1] - p0;
+    for (int e = threadIdx.x; e < s * Rd; e += blockDim.x) {
+        int b = e / Rd, l = e % Rd;
+        rv[e] = x[(int64_t)pdofs[p0 + b] * R + r0 + l];
+    }
+    __syncthreads();
+    const float2* Bv = B + poff[v];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    constexpr int RW = 4;
+    for (int a0 = w * RW; a0 < s; a0 += nw * RW) {
+        float re[RW], im[RW];
+#pragma unroll
+        for (int q = 0; q < RW; ++q) { re[q] = 0.f; im[q] = 0.f; }
+        for (int b0 = 0; b0 < s; b0 += 32) {
+            float2 bv[RW];
+#pragma unroll
+            for (int q = 0; q < RW; ++q)
+                bv[q] = (a0 + q < s && b0 + lane < s) ? __ldcs(&Bv[(int64_t)(a0 + q) * s + b0 + lane]) : make_float2(0.f, 0.f);
+            int bl = min(32, s - b0);
+            for (int l = 0; l < bl; ++l) {
+                float2 xv = lane < Rd ? rv[(b0 + l) * Rd + lane] : make_float2(0.f, 0.f);
+#pragma unroll
+                for (int q = 0; q < RW; ++q) {
+                    float mx = __shfl_sync(0xffffffffu, bv[q].x, l);
+                    float my = __shfl_sync(0xffffffffu, bv[q].y, l);
+                    re[q] += mx * xv.x - my * xv.y;
+                    im[q] += mx * xv.y + my * xv.x;
+                }
+            }
+        }
+        if (lane < Rd)
+#pragma unroll
+            for (int q = 0; q < RW; ++q)
+                if (a0 + q < s) t[(int64_t)(p0 + a0 + q) * Rd + lane] = make_float2(re[q], im[q]);
+    }
+}
+
+__global__ void patch_apply2_batch_kernel(int64_t n, const int32_t* __restrict__ d2p_ptr,
+                                          const int32_t* __restrict__ d2p_idx, const float2* __restrict__ t, int R,
+                                          int r0, int Rd, const uint8_t* __restrict__ pec, const uint8_t* __restrict__ pm,
+                                          int d, float2* __restrict__ y) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n * Rd) return;
+    int64_t i = e / Rd;
+    int l = (int)(e % Rd);
+    float re = 0.f, im = 0.f;
+    if (!(pec[i] || ((pm[i] >> d) & 1)))
+        for (int32_t q = d2p_ptr[i]; q < d2p_ptr[i + 1]; ++q) {
+            float2 v = t[(int64_t)d2p_idx[q] * Rd + l];
+            re += v.x;
+            im += v.y;
+        }
+    y[i * R + r0 + l] = make_float2(re, im);
+}
+
+// ---------------------------------------------------------------------------
+// per-system dense kernels on system-major FP32 vectors (blockIdx.y = system)
+// ---------------------------------------------------------------------------
+constexpr int MDT = 8;
+__global__ void __launch_bounds__(256) multidot_sys_kernel(int64_t n, int nvec, const double2* __restrict__ V,
+                                                            int64_t ldsys, const double2* __restrict__ w,
+                                                            const uint8_t* __restrict__ act, double2* __restrict__ part) {
+    int r = blockIdx.y;
+    if (!act[r]) return;
+    __shared__ double red[2 * MDT][8];   // [tile entry][warp]
+    const double2* Vr = V + r * ldsys;
+    const double2* wr = w + r * n;
+    int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+    int64_t lo = blockIdx.x * chunk, hi = min(n, lo + chunk);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int i0 = 0; i0 < nvec; i0 += MDT) {
+        double re[MDT], im[MDT];
+#pragma unroll
+        for (int q = 0; q < MDT; ++q) { re[q] = 0; im[q] = 0; }
+        for (int64_t k = lo + threadIdx.x; k < hi; k += blockDim.x) {
+            double2 b = wr[k];
+#pragma unroll
+            for (int q = 0; q < MDT; ++q)
+                if (i0 + q < nvec) {
+                    double2 a = Vr[(int64_t)(i0 + q) * n + k];
+                    re[q] += a.x * b.x + a.y * b.y;
+                    im[q] += a.x * b.y - a.y * b.x;
+                }
+        }
+#pragma unroll
+        for (int q = 0; q < MDT; ++q)
+            for (int o = 16; o > 0; o >>= 1) {
+                re[q] += __shfl_down_sync(0xffffffffu, re[q], o);
+                im[q] += __shfl_down_sync(0xffffffffu, im[q], o);
+            }
+        __syncthreads();
+        if (lane == 0)
+#pragma unroll
+            for (int q = 0; q < MDT; ++q) { red[2 * q][wid] = re[q]; red[2 * q + 1][wid] = im[q]; }
+        __syncthreads();
+        if (threadIdx.x < 2 * MDT) {
+            double acc = 0;
+            for (int u = 0; u < nw; ++u) acc += red[threadIdx.x][u];
+            int q = threadIdx.x >> 1;
+            if (i0 + q < nvec) {
+                double2* o = &part[((int64_t)r * nvec + i0 + q) * gridDim.x + blockIdx.x];
+                if (threadIdx.x & 1) o->y = acc; else o->x = acc;
+            }
+        }
+    }
+}
+
+// h[r][i] = sum of partials; H[r][col][i] (+)= h
+__global__ void finish_sys_kernel(int nparts, int nvec, const double2* __restrict__ part, const uint8_t* __restrict__ act,
+                                  double2* __restrict__ h, double2* __restrict__ Hcol, int64_t ldH, int accumulate) {
+    int i = blockIdx.x, r = blockIdx.y;
+    if (!act[r]) return;
+    __shared__ double sre[256], sim[256];
+    double re = 0, im = 0;
+    for (int c = threadIdx.x; c < nparts; c += blockDim.x) {
+        double2 p = part[((int64_t)r * nvec + i) * nparts + c];
+        re += p.x;
+        im += p.y;
+    }
+    sre[threadIdx.x] = re;
+    sim[threadIdx.x] = im;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st) { sre[threadIdx.x] += sre[threadIdx.x + st]; sim[threadIdx.x] += sim[threadIdx.x + st]; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        h[(int64_t)r * nvec + i] = make_double2(sre[0], sim[0]);
+        double2* o = &Hcol[r * ldH + i];
+        if (accumulate) *o = make_double2(o->x + sre[0], o->y + sim[0]);
+        else *o = make_double2(sre[0], sim[0]);
+    }
+}
+
+__global__ void update_sys_kernel(int64_t n, int nvec, const double2* __restrict__ V, int64_t ldsys,
+                                  const double2* __restrict__ h, const uint8_t* __restrict__ act, double2* __restrict__ w) {
+    int r = blockIdx.y;
+    if (!act[r]) return;
+    extern __shared__ double2 shd[];
+    for (int i = threadIdx.x; i < nvec; i += blockDim.x) shd[i] = h[(int64_t)r * nvec + i];
+    __syncthreads();
+    const double2* Vr = V + r * ldsys;
+    double2* wr = w + r * n;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        double2 acc = wr[k];
+#pragma unroll 4
+        for (int i = 0; i < nvec; ++i) {
+            double2 v = Vr[(int64_t)i * n + k], c = shd[i];
+            acc.x -= c.x * v.x - c.y * v.y;
+            acc.y -= c.x * v.y + c.y * v.x;
+        }
+        wr[k] = acc;
+    }
+}
+
+// out[r] += sum_i y[r][i] Z[r][i]
+__global__ void combo_add_sys_kernel(int64_t n, const double2* __restrict__ Z, int64_t ldsys,
+                                     const double2* __restrict__ y, int ldy, const int* __restrict__ ncols,
+                                     const uint8_t* __restrict__ act, double2* __restrict__ out) {
+    int r = blockIdx.y;
+    if (!act[r]) return;
+    extern __shared__ double2 shd[];
+    const int nv = ncols[r];
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) shd[i] = y[(int64_t)r * ldy + i];
+    __syncthreads();
+    const double2* Zr = Z + r * ldsys;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        double re = 0, im = 0;
+#pragma unroll 4
+        for (int i = 0; i < nv; ++i) {
+            double2 v = Zr[(int64_t)i * n + k], c = shd[i];
+            re += c.x * v.x - c.y * v.y;
+            im += c.x * v.y + c.y * v.x;
+        }
+        double2 o = out[r * n + k];
+        out[r * n + k] = make_double2(o.x + re, o.y + im);
+    }
+}
+
+// W[r][c] = sum_i V[r][i] Q[r][i][c]  (deflated-restart basis change; Q has ldq rows)
+__global__ void rotate_sys_kernel(int64_t n, int nin, int nout, const double2* __restrict__ V, int64_t ldsys,
+                                  const double2* __restrict__ Q, int ldq, int64_t qstride,
+                                  const uint8_t* __restrict__ act, double2* __restrict__ W, int64_t ldw) {
+    int r = blockIdx.y;
+    if (!act[r]) return;
+    const double2* Vr = V + r * ldsys;
+    const double2* Qr = Q + (int64_t)r * qstride;
+    double2* Wr = W + r * ldw;
+    constexpr int CH = 8;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        for (int c0 = 0; c0 < nout; c0 += CH) {
+            double re[CH], im[CH];
+#pragma unroll
+            for (int q = 0; q < CH; ++q) { re[q] = 0; im[q] = 0; }
+            for (int i = 0; i < nin; ++i) {
+                double2 v = Vr[(int64_t)i * n + k];
+#pragma unroll
+                for (int q = 0; q < CH; ++q)
+                    if (c0 + q < nout) {
+                        double2 c = __ldg(&Qr[(int64_t)(c0 + q) * ldq + i]);
+                        re[q] += v.x * c.x - v.y * c.y;
+                        im[q] += v.x * c.y + v.y * c.x;
+                    }
+            }
+#pragma unroll
+            for (int q = 0; q < CH; ++q)
+                if (c0 + q < nout) Wr[(int64_t)(c0 + q) * n + k] = make_double2(re[q], im[q]);
+        }
+    }
+}
+
+template <class T2>
+__global__ void nrm2_sys_kernel(int64_t n, const T2* __restrict__ x, int64_t ld, const uint8_t* __restrict__ act,
+                                double* __restrict__ part) {
+    int r = blockIdx.y;
+    __shared__ double sh[256];
+    double s = 0;
+    if (act[r]) {
+        const T2* xr = x + r * ld;
+        int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+        int64_t lo = blockIdx.x * chunk, hi = min(n, lo + chunk);
+        for (int64_t k = lo + threadIdx.x; k < hi; k += blockDim.x) {
+            double a = xr[k].x, b = xr[k].y;
+            s += a * a + b * b;
+        }
+    }
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[(int64_t)r * gridDim.x + blockIdx.x] = sh[0];
+}
+
+__global__ void nrm2_finish_kernel(int nparts, const double* __restrict__ part, double* __restrict__ out) {
+    int r = blockIdx.x;
+    __shared__ double sh[256];
+    double s = 0;
+    for (int c = threadIdx.x; c < nparts; c += blockDim.x) s += part[(int64_t)r * nparts + c];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[r] = sqrt(sh[0]);
+}
+
+// dst[r] = src[r] / nrm[r]; also H[r][col+1] = nrm[r]
+__global__ void normalize_sys_kernel(int64_t n, const double2* __restrict__ src, int64_t lds, const double* __restrict__ nrm,
+                                     const uint8_t* __restrict__ act, double2* __restrict__ dst, int64_t ldd,
+                                     double2* __restrict__ Hsub, int64_t ldH) {
+    int r = blockIdx.y;
+    if (!act[r]) return;
+    double nr = nrm[r];
+    if (Hsub && blockIdx.x == 0 && threadIdx.x == 0) Hsub[r * ldH] = make_double2(nr, 0);
+    double inv = nr > 0 ? 1.0 / nr : 0.0;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        double2 a = src[r * lds + k];
+        dst[r * ldd + k] = make_double2(a.x * inv, a.y * inv);
+    }
+}
+
+// c = a - b  (all systems, system-major FP64)
+__global__ void sub_sys_kernel(int64_t n, int R, const double2* __restrict__ a, const double2* __restrict__ b,
+                               double2* __restrict__ c) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n * R) return;
+    c[e] = make_double2(a[e].x - b[e].x, a[e].y - b[e].y);
+}
+
+// interleaved FP32 -> FP64
+__global__ void il_f2d_kernel(int64_t cnt, const float2* __restrict__ a, double2* __restrict__ b) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = make_double2(a[i].x, a[i].y);
+}
+
+// FP64 outer pieces ---------------------------------------------------------
+// out[r] = a[r] * s_r  (s_r = 1/nrm[r])  and  x[r] += nrm[r] * d[r]
+__global__ void scale_sys_kernel(int64_t n, const double2* __restrict__ a, const double* __restrict__ nrm,
+                                 const uint8_t* __restrict__ act, double2* __restrict__ out) {
+    int r = blockIdx.y;
+    double inv = (act[r] && nrm[r] > 0) ? 1.0 / nrm[r] : 0.0;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        double2 v = a[r * n + k];
+        out[r * n + k] = make_double2(v.x * inv, v.y * inv);
+    }
+}
+
+__global__ void refine_sys_kernel(int64_t n, const double2* __restrict__ d, const double* __restrict__ nrm,
+                                  const uint8_t* __restrict__ act, double2* __restrict__ x) {
+    int r = blockIdx.y;
+    if (!act[r]) return;
+    double sc = nrm[r];
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        double2 a = d[r * n + k], v = x[r * n + k];
+        x[r * n + k] = make_double2(v.x + sc * a.x, v.y + sc * a.y);
+    }
+}
+
+// x[r] += d[r]
+__global__ void add_sys_kernel(int64_t n, const double2* __restrict__ d, const uint8_t* __restrict__ act,
+                               double2* __restrict__ x) {
+    int r = blockIdx.y;
+    if (!act[r]) return;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        double2 a = d[r * n + k], v = x[r * n + k];
+        x[r * n + k] = make_double2(v.x + a.x, v.y + a.y);
+    }
+}
+
+// r = b - y (y interleaved FP64), system-major output
+__global__ void resid_kernel(int64_t n, int R, const double2* __restrict__ b, const double2* __restrict__ y_il,
+                             double2* __restrict__ r) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n * R) return;
+    int64_t k = e / R;
+    int rr = (int)(e % R);
+    double2 bv = b[rr * n + k], yv = y_il[e];
+    r[rr * n + k] = make_double2(bv.x - yv.x, bv.y - yv.y);
+}
+
+__global__ void f64_to_f32_kernel(int64_t n, const double2* __restrict__ a, float2* __restrict__ b) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = make_float2((float)a[i].x, (float)a[i].y);
+}
+
+__global__ void real_to_f32_kernel(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+// x0 lift per system: x0[r] = et[port d_r] with PEC entries removed  (system-major FP64)
+__global__ void lift_batch_kernel(int64_t n, const double2* __restrict__ et, const uint8_t* __restrict__ pec,
+                                  const uint8_t* __restrict__ dsys, double2* __restrict__ x0) {
+    int r = blockIdx.y;
+    const double2* e = et + (int64_t)dsys[r] * n;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        x0[r * n + k] = pec[k] ? make_double2(0, 0) : e[k];
+}
+
+__global__ void neg_sys_kernel(int64_t n, int R, double2* __restrict__ x) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n * R) return;
+    x[e] = make_double2(-x[e].x, -x[e].y);
+}
+
+// e[r] = x[r] + et[port d_r]  (driven-port values on the identity rows)
+__global__ void finish_e_kernel(int64_t n, const double2* __restrict__ et, const uint8_t* __restrict__ dsys,
+                                double2* __restrict__ x) {
+    int r = blockIdx.y;
+    const double2* e = et + (int64_t)dsys[r] * n;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        double2 v = x[r * n + k], a = e[k];
+        x[r * n + k] = make_double2(v.x + a.x, v.y + a.y);
+    }
+}
+
+// ---- batched CG on the mass matrix (FP64, interleaved layout) -------------
+// y_il = s_r * (V x_il)  with a real CSR matrix
+__global__ void __launch_bounds__(256) spmv_real_batch_kernel(int64_t n, int R, const int32_t* __restrict__ rowptr,
+                                                               const int32_t* __restrict__ cols, const double* __restrict__ V,
+                                                               const double2* __restrict__ x, const double2* __restrict__ sc,
+                                                               double2* __restrict__ y) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    double2 s = lane < R ? sc[lane] : make_double2(0, 0);
+    for (int64_t row = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); row < n; row += warps) {
+        if (lane >= R) continue;
+        double re = 0, im = 0;
+        for (int32_t k = rowptr[row]; k < rowptr[row + 1]; ++k) {
+            double a = V[k];
+            double2 xv = x[(int64_t)cols[k] * R + lane];
+            re += a * xv.x;
+            im += a * xv.y;
+        }
+        y[row * R + lane] = make_double2(s.x * re - s.y * im, s.x * im + s.y * re);
+    }
+}
+
+// per-system conj-dot over interleaved vectors: part[blk][r] = sum conj(a) b
+__global__ void dot_il_kernel(int64_t n, int R, const double2* __restrict__ a, const double2* __restrict__ b,
+                              double2* __restrict__ part) {
+    // blockDim = (32, 8): x = system lane, y = row offset
+    __shared__ double sre[8][33], sim[8][33];
+    int l = threadIdx.x, ty = threadIdx.y;
+    double re = 0, im = 0;
+    if (l < R) {
+        int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+        int64_t lo = blockIdx.x * chunk, hi = min(n, lo + chunk);
+        for (int64_t k = lo + ty; k < hi; k += blockDim.y) {
+            double2 x = a[k * R + l], y = b[k * R + l];
+            re += x.x * y.x + x.y * y.y;
+            im += x.x * y.y - x.y * y.x;
+        }
+    }
+    sre[ty][l] = re;
+    sim[ty][l] = im;
+    __syncthreads();
+    if (ty == 0) {
+        for (int u = 1; u < blockDim.y; ++u) { re += sre[u][l]; im += sim[u][l]; }
+        part[(int64_t)blockIdx.x * 32 + l] = make_double2(re, im);
+    }
+}
+
+__global__ void dot_il_finish_kernel(int nparts, const double2* __restrict__ part, double2* __restrict__ out) {
+    int l = threadIdx.x;   // 32 threads
+    double re = 0, im = 0;
+    for (int c = 0; c < nparts; ++c) { re += part[(int64_t)c * 32 + l].x; im += part[(int64_t)c * 32 + l].y; }
+    out[l] = make_double2(re, im);
+}
+
+// x += a_r p; r -= a_r q  with a_r = num_r / den_r  (interleaved)
+__global__ void cg_update_batch_kernel(int64_t n, int R, const double2* __restrict__ num, const double2* __restrict__ den,
+                                       const uint8_t* __restrict__ act, const double2* __restrict__ p,
+                                       const double2* __restrict__ q, double2* __restrict__ x, double2* __restrict__ r) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n * R) return;
+    int l = (int)(e % R);
+    if (!act[l]) return;
+    double2 an = num[l], ad = den[l];
+    double dd = ad.x * ad.x + ad.y * ad.y;
+    double2 a = make_double2((an.x * ad.x + an.y * ad.y) / dd, (an.y * ad.x - an.x * ad.y) / dd);
+    double2 pk = p[e], qk = q[e];
+    x[e] = make_double2(x[e].x + a.x * pk.x - a.y * pk.y, x[e].y + a.x * pk.y + a.y * pk.x);
+    r[e] = make_double2(r[e].x - (a.x * qk.x - a.y * qk.y), r[e].y - (a.x * qk.y + a.y * qk.x));
+}
+
+__global__ void cg_dir_batch_kernel(int64_t n, int R, const double2* __restrict__ rzn, const double2* __restrict__ rzo,
+                                    const uint8_t* __restrict__ act, const double2* __restrict__ z, double2* __restrict__ p) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n * R) return;
+    int l = (int)(e % R);
+    if (!act[l]) return;
+    double2 a = rzn[l], b = rzo[l];
+    double dd = b.x * b.x + b.y * b.y;
+    double2 be = make_double2((a.x * b.x + a.y * b.y) / dd, (a.y * b.x - a.x * b.y) / dd);
+    double2 pk = p[e];
+    p[e] = make_double2(z[e].x + be.x * pk.x - be.y * pk.y, z[e].y + be.x * pk.y + be.y * pk.x);
+}
+
+__global__ void dscale_batch_kernel(int64_t n, int R, const double* __restrict__ d, const double2* __restrict__ x,
+                                    double2* __restrict__ y) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n * R) return;
+    double s = d[e / R];
+    y[e] = make_double2(s * x[e].x, s * x[e].y);
+}
+
+__global__ void diag_inv_m1_kernel(int64_t n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ cols,
+                                   const double* __restrict__ A, double* __restrict__ dinv) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double d = 0;
+        for (int32_t k = rowptr[i]; k < rowptr[i + 1]; ++k)
+            if (cols[k] == i) { d = A[k]; break; }
+        dinv[i] = d != 0 ? 1.0 / d : 1.0;
+    }
+}
+
+// ===========================================================================
+// host orchestration
+// ===========================================================================
+struct System {
+    double freq;
+    int d;   // driving set (driven port)
+};
+
+struct Batch {
+    Problem& P;
+    cudaStream_t s;
+    int64_t n;
+    int R = 0, N = 0, m = 0, kd = 0;
+    std::vector<System> sys;
+    // device coefficient tables
+    DBuf<VC3<float2>> vc32;
+    DBuf<VC3<double2>> vc64;
+    std::vector<DBuf<BC5<float2>>> bc32;
+    std::vector<DBuf<BC5<double2>>> bc64;
+    DBuf<uint8_t> dsys, act;
+    std::vector<uint8_t> h_act;
+    // systems per driving set occupy lanes [r0[d], r0[d]+Rd[d])
+    std::vector<int> r0, Rd;
+    explicit Batch(Problem& P_) : P(P_), s(P_.ctx->stream), n(P_.topo.n) {}
+    unsigned grid1(int64_t work) const { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, 65535)); }
+};
+
+static unsigned vgrid(const Problem& P) { return (unsigned)(P.ctx->sm_count * 4); }
+
+// blocks per system for the per-system multi-dot: about 4 CTAs per SM over the
+// whole batch, but at least 16K elements per CTA so each thread streams a long
+// run per tile and the per-tile reduction is amortised.
+static int md_blocks_sys(int sms, int R, int64_t n) {
+    int64_t by_sm = std::max<int64_t>(1, (int64_t)4 * sms / std::max(1, R));
+    int64_t by_len = std::max<int64_t>(1, n / 16384);
+    return (int)std::max<int64_t>(1, std::min<int64_t>({by_sm, by_len, 512}));
+}
+
+template <class T2, class T>
+static void spmv_batch(Batch& B, const T* K, const T* Me, const T* Mt, const T* Ms,
+                       const VC3<typename CplxOf<T>::type>* vc,
+                       const std::vector<const BC5<typename CplxOf<T>::type>*>& bcs, const T2* x_il, T2* y_il) {
+    Problem& P = B.P;
+    int grid = P.ctx->sm_count * 16;
+    spmv_batch_kernel<T2, T><<<grid, 256, 0, B.s>>>(B.n, B.R, P.d_rowptr.p, P.d_cols.p, K, Me, Mt, Ms, vc, x_il, y_il,
+                                                   P.d_pec.p, P.d_portmask.p, B.dsys.p);
+    ++P.ctx->launches;
+    for (size_t g = 0; g < P.groups.size(); ++g) {
+        BGroup& G = P.groups[g];
+        int nrows = (int)G.h_brow.size();
+        if (G.nu == 0 || nrows == 0) continue;
+        bnd_batch_kernel<T2, T><<<(nrows + 7) / 8, 256, 0, B.s>>>(nrows, B.R, G.brow.p, G.bptr.p, G.ucol.p, G.R.p, G.nu,
+                                                                 bcs[g], x_il, y_il, P.d_pec.p, P.d_portmask.p, B.dsys.p);
+        ++P.ctx->launches;
+    }
+    OPEM_CUDA(cudaGetLastError());
+}
+
+template <class T2, class O2>
+static void to_il(Batch& B, const T2* sm, int64_t ld, O2* il) {
+    sm2il_kernel<T2, O2><<<(unsigned)((B.n + 31) / 32), dim3(32, 8), 0, B.s>>>(B.n, B.R, sm, ld, il);
+    ++B.P.ctx->launches;
+}
+template <class T2, class O2>
+static void to_sm(Batch& B, const T2* il, O2* sm, int64_t ld) {
+    il2sm_kernel<T2, O2><<<(unsigned)((B.n + 31) / 32), dim3(32, 8), 0, B.s>>>(B.n, B.R, il, sm, ld);
+    ++B.P.ctx->launches;
+}
+
+struct PatchSet32 {
+    DBuf<float2> B;
+};
+
+// FP32 block-Jacobi blocks for driving set d at frequency f (FP64 inversion, then rounded)
+static void build_patchset(Batch& B, double f, int d, PatchSet32& ps) {
+    Problem& P = B.P;
+    const int64_t nnz = (int64_t)P.topo.cols.size();
+    DBuf<double2> A(nnz);
+    DBuf<uint8_t> dm(B.n);
+    VolCoef vc;
+    std::vector<BCoef> bc;
+    system_coefficients(P, f, d, vc, bc);
+    form_system_matrix(P, vc, bc, A.p);
+    make_dmask(P, d, dm.p);
+    DBuf<double2> B64;
+    patch_blocks_fp64(P, A.p, dm.p, B64);
+    ps.B.alloc(B64.n);
+    f64_to_f32_kernel<<<vgrid(P), 256, 0, B.s>>>((int64_t)B64.n, B64.p, ps.B.p);
+    ++P.ctx->launches;
+    OPEM_CUDA(cudaStreamSynchronize(B.s));
+}
+
+static void patch_apply_batch(Batch& B, const std::vector<PatchSet32>& sets, DBuf<float2>& t, const float2* x_il,
+                              float2* y_il) {
+    Problem& P = B.P;
+    for (int d = 0; d < B.N; ++d) {
+        if (B.Rd[d] == 0) continue;
+        size_t smem = (size_t)P.topo.max_patch * B.Rd[d] * sizeof(float2);
+        patch_apply1_batch_kernel<<<P.npatch, 256, smem, B.s>>>(P.npatch, P.d_patch_ptr.p, P.d_patch_dofs.p,
+                                                                P.d_patch_off.p, sets[d].B.p, x_il, B.R, B.r0[d],
+                                                                B.Rd[d], t.p);
+        ++P.ctx->launches;
+        int64_t work = B.n * B.Rd[d];
+        patch_apply2_batch_kernel<<<(unsigned)((work + 255) / 256), 256, 0, B.s>>>(
+            B.n, P.d_d2p_ptr.p, P.d_d2p_idx.p, t.p, B.R, B.r0[d], B.Rd[d], P.d_pec.p, P.d_portmask.p, d, y_il);
+        ++P.ctx->launches;
+    }
+    OPEM_CUDA(cudaGetLastError());
+}
+
+static void nrm_sys_f64(Batch& B, const double2* x, int64_t ld, DBuf<double>& part, double* out, const uint8_t* act) {
+    const int nb = 64;
+    nrm2_sys_kernel<double2><<<dim3(nb, B.R), 256, 0, B.s>>>(B.n, x, ld, act, part.p);
+    nrm2_finish_kernel<<<B.R, 256, 0, B.s>>>(nb, part.p, out);
+    B.P.ctx->launches += 2;
+}
+
+// ---------------------------------------------------------------------------
+// Batched flexible GMRES-DR (FP64 Krylov, FP32 block Jacobi) on all active
+// systems in lockstep:  A d = rhs.
+// The preconditioned directions z_j = M^-1 v_j are stored (Z, FP64 copy of the
+// FP32 block-Jacobi output), so A Z = V H holds in FP64 whatever the
+// preconditioner's precision, and d = Z y.  Deflated restarts rotate both
+// bases: V <- V P_{k+1}, Z <- Z P_k.
+// ---------------------------------------------------------------------------
+// tolerance reference of system r: the norm of its right-hand side
+static inline double beta0(int r, const std::vector<double>& beta) { (void)beta; (void)r; return 1.0; }
+
+struct InnerWork {
+    DBuf<double2> V, Z, w, w_il, z_il64, h, part, yd, Qd, W, rhs, d;
+    DBuf<float2> x_il32, z_il32, t;
+    DBuf<double2> H;     // per system (m+1) x m FP64 Hessenberg
+    DBuf<double> nrm, npart;
+    DBuf<int> ncols;
+};
+
+static int inner_solve(Batch& B, InnerWork& W, const std::vector<PatchSet32>& sets,
+                       const std::vector<const BC5<double2>*>& bc64, const std::vector<uint8_t>& active_in,
+                       double tol, int maxits, int& its_out) {
+    Problem& P = B.P;
+    const int64_t n = B.n;
+    const int R = B.R, m = B.m, kd = B.kd;
+    const int64_t ldV = (int64_t)(m + 1) * n;   // per-system stride of V (m+1 vectors) and Z (m vectors, same stride)
+    const int64_t ldH = (int64_t)(m + 1) * m;
+    const unsigned gy = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, P.ctx->sm_count * 2));
+    const int nb = md_blocks_sys(P.ctx->sm_count, R, n);
+    std::vector<uint8_t> done(R), iact(R);
+    for (int r = 0; r < R; ++r) done[r] = active_in[r] ? 0 : 1;
+    OPEM_CUDA(cudaMemsetAsync(W.d.p, 0, W.d.bytes(), B.s));
+    OPEM_CUDA(cudaMemcpyAsync(W.w.p, W.rhs.p, (size_t)n * R * sizeof(double2), cudaMemcpyDeviceToDevice, B.s));
+    std::vector<std::vector<cd>> Hh(R, std::vector<cd>((size_t)(m + 1) * m)), c(R, std::vector<cd>(m + 1));
+    std::vector<GivensLsq> L(R);
+    std::vector<int> start(R, 0), ncol(R, 0);
+    std::vector<char> fresh(R, 1);
+    std::vector<double> beta(R, 1.0), est(R, 1.0), hnrm(R);
+    std::vector<double2> hcol((size_t)R * (m + 2));
+    std::vector<std::vector<cd>> ys(R);
+    int its = 0;
+    auto upload_act = [&](const std::vector<uint8_t>& a) {
+        OPEM_CUDA(cudaMemcpyAsync(B.act.p, a.data(), R, cudaMemcpyHostToDevice, B.s));
+    };
+    auto apply_A = [&](const double2* x_il64, double2* y_sm) {   // y = A x (FP64), via interleaved layout
+        spmv_batch<double2, double>(B, P.d_K.p, P.d_Meps.p, P.has_tand ? P.d_Mtand.p : nullptr,
+                                    P.has_sig ? P.d_Msig.p : nullptr, B.vc64.p, bc64, x_il64, W.w_il.p);
+        to_sm(B, W.w_il.p, y_sm, n);
+    };
+    while (true) {
+        for (int r = 0; r < R; ++r) iact[r] = (!done[r] && fresh[r]) ? 1 : 0;
+        upload_act(iact);
+        nrm_sys_f64(B, W.w.p, n, W.npart, W.nrm.p, B.act.p);
+        normalize_sys_kernel<<<dim3(gy, R), 256, 0, B.s>>>(n, W.w.p, n, W.nrm.p, B.act.p, W.V.p, ldV, nullptr, 0);
+        ++P.ctx->launches;
+        OPEM_CUDA(cudaMemcpyAsync(hnrm.data(), W.nrm.p, R * sizeof(double), cudaMemcpyDeviceToHost, B.s));
+        OPEM_CUDA(cudaStreamSynchronize(B.s));
+        int jmin = m;
+        for (int r = 0; r < R; ++r) {
+            if (done[r]) continue;
+            if (fresh[r]) {
+                beta[r] = hnrm[r];
+                std::fill(Hh[r].begin(), Hh[r].end(), 0.0);
+                std::fill(c[r].begin(), c[r].end(), 0.0);
+                c[r][0] = beta[r];
+                start[r] = 0;
+                if (!(beta[r] > 0)) { done[r] = 1; continue; }
+            }
+            L[r].reset(m, c[r]);
+            for (int j = 0; j < start[r]; ++j) est[r] = L[r].add_column(j, &Hh[r][(size_t)j * (m + 1)], start[r]);
+            ncol[r] = start[r];
+            jmin = std::min(jmin, start[r]);
+        }
+        bool any = false;
+        for (int r = 0; r < R; ++r) any |= !done[r];
+        if (!any) break;
+        std::vector<uint8_t> cyc(R, 0);
+        for (int r = 0; r < R; ++r) cyc[r] = !done[r];
+        for (int j = jmin; j < m; ++j) {
+            for (int r = 0; r < R; ++r) iact[r] = (cyc[r] && j >= start[r]) ? 1 : 0;
+            bool anyj = false;
+            for (int r = 0; r < R; ++r) anyj |= iact[r];
+            if (!anyj) break;
+            upload_act(iact);
+            // z_j = M^-1 v_j (FP32 blocks), kept in Z; w = A z_j (FP64)
+            to_il(B, W.V.p + (int64_t)j * n, ldV, W.x_il32.p);
+            patch_apply_batch(B, sets, W.t, W.x_il32.p, W.z_il32.p);
+            to_sm(B, W.z_il32.p, W.Z.p + (int64_t)j * n, ldV);
+            il_f2d_kernel<<<vgrid(P), 256, 0, B.s>>>(n * R, W.z_il32.p, W.z_il64.p);
+            ++P.ctx->launches;
+            apply_A(W.z_il64.p, W.w.p);
+            for (int pass = 0; pass < 2; ++pass) {
+                multidot_sys_kernel<<<dim3(nb, R), 256, 0, B.s>>>(n, j + 1, W.V.p, ldV, W.w.p, B.act.p, W.part.p);
+                finish_sys_kernel<<<dim3(j + 1, R), 256, 0, B.s>>>(nb, j + 1, W.part.p, B.act.p, W.h.p,
+                                                                   W.H.p + (int64_t)j * (m + 1), ldH, pass);
+                update_sys_kernel<<<dim3(gy, R), 256, (j + 1) * sizeof(double2), B.s>>>(n, j + 1, W.V.p, ldV, W.h.p,
+                                                                                       B.act.p, W.w.p);
+                P.ctx->launches += 3;
+            }
+            nrm_sys_f64(B, W.w.p, n, W.npart, W.nrm.p, B.act.p);
+            normalize_sys_kernel<<<dim3(gy, R), 256, 0, B.s>>>(n, W.w.p, n, W.nrm.p, B.act.p,
+                                                                W.V.p + (int64_t)(j + 1) * n, ldV,
+                                                                W.H.p + (int64_t)j * (m + 1) + j + 1, ldH);
+            ++P.ctx->launches;
+            OPEM_CUDA(cudaGetLastError());
+            OPEM_CUDA(cudaMemcpy2DAsync(hcol.data(), (m + 2) * sizeof(double2), W.H.p + (int64_t)j * (m + 1),
+                                        ldH * sizeof(double2), (j + 2) * sizeof(double2), R, cudaMemcpyDeviceToHost, B.s));
+            OPEM_CUDA(cudaStreamSynchronize(B.s));
+            ++its;
+            for (int r = 0; r < R; ++r) {
+                if (!iact[r]) continue;
+                for (int i = 0; i <= j + 1; ++i)
+                    Hh[r][i + (size_t)j * (m + 1)] = cd(hcol[(size_t)r * (m + 2) + i].x, hcol[(size_t)r * (m + 2) + i].y);
+                est[r] = L[r].add_column(j, &Hh[r][(size_t)j * (m + 1)], j + 1);
+                ncol[r] = j + 1;
+                if (!std::isfinite(est[r]) || est[r] <= tol * beta0(r, beta)) cyc[r] = 0;
+            }
+            if (its >= maxits) break;
+        }
+        // d += Z y
+        std::vector<double2> yh((size_t)R * m, make_double2(0, 0));
+        std::vector<int> nc(R, 0);
+        int ymax = 0;
+        for (int r = 0; r < R; ++r) {
+            iact[r] = (!done[r] && ncol[r] > 0) ? 1 : 0;
+            if (!iact[r]) continue;
+            L[r].solve(ncol[r], ys[r]);
+            for (int i = 0; i < ncol[r]; ++i) yh[(size_t)r * m + i] = make_double2(ys[r][i].real(), ys[r][i].imag());
+            nc[r] = ncol[r];
+            ymax = std::max(ymax, ncol[r]);
+        }
+        if (ymax > 0) {
+            upload_act(iact);
+            OPEM_CUDA(cudaMemcpyAsync(W.yd.p, yh.data(), yh.size() * sizeof(double2), cudaMemcpyHostToDevice, B.s));
+            OPEM_CUDA(cudaMemcpyAsync(W.ncols.p, nc.data(), R * sizeof(int), cudaMemcpyHostToDevice, B.s));
+            combo_add_sys_kernel<<<dim3(gy, R), 256, ymax * sizeof(double2), B.s>>>(n, W.Z.p, ldV, W.yd.p, m, W.ncols.p,
+                                                                                   B.act.p, W.d.p);
+            ++P.ctx->launches;
+        }
+        bool all = true;
+        for (int r = 0; r < R; ++r) {
+            if (done[r]) continue;
+            if (est[r] <= tol * beta0(r, beta) || !std::isfinite(est[r])) done[r] = 1;
+            all &= (bool)done[r];
+        }
+        if (all || its >= maxits) break;
+        // systems that cannot deflate restart from their true residual (FP64)
+        bool need_fresh = false;
+        for (int r = 0; r < R; ++r) need_fresh |= (!done[r] && (kd == 0 || ncol[r] < m));
+        if (need_fresh) {
+            to_il(B, W.d.p, n, W.z_il64.p);
+            apply_A(W.z_il64.p, W.w.p);
+            sub_sys_kernel<<<(unsigned)((n * R + 255) / 256), 256, 0, B.s>>>(n, R, W.rhs.p, W.w.p, W.w.p);
+            ++P.ctx->launches;
+        }
+        // deflated restarts (host FP64, systems in parallel)
+        std::vector<std::vector<cd>> Pm(R), Hn(R), cn(R);
+        std::vector<char> ok(R, 0);
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int r = 0; r < R; ++r) {
+            if (done[r] || kd == 0 || ncol[r] < m) continue;
+            ok[r] = gmres_dr_deflate(m, kd, Hh[r], c[r], ys[r], Pm[r], Hn[r], cn[r]) ? 1 : 0;
+        }
+        bool anydef = false;
+        const int64_t qstride = (int64_t)(m + 1) * (kd + 1);
+        std::vector<double2> Qh((size_t)R * qstride, make_double2(0, 0));
+        for (int r = 0; r < R; ++r) {
+            iact[r] = 0;
+            fresh[r] = 1;
+            if (done[r] || !ok[r]) continue;
+            iact[r] = 1;
+            anydef = true;
+            for (size_t t2 = 0; t2 < Pm[r].size(); ++t2)
+                Qh[(size_t)r * qstride + t2] = make_double2(Pm[r][t2].real(), Pm[r][t2].imag());
+        }
+        if (anydef) {
+            upload_act(iact);
+            OPEM_CUDA(cudaMemcpyAsync(W.Qd.p, Qh.data(), Qh.size() * sizeof(double2), cudaMemcpyHostToDevice, B.s));
+            const int64_t ldw = (int64_t)(kd + 1) * n;
+            // V <- V P_{k+1}
+            rotate_sys_kernel<<<dim3(gy, R), 256, 0, B.s>>>(n, m + 1, kd + 1, W.V.p, ldV, W.Qd.p, m + 1, qstride, B.act.p,
+                                                             W.W.p, ldw);
+            ++P.ctx->launches;
+            for (int r = 0; r < R; ++r)
+                if (iact[r])
+                    OPEM_CUDA(cudaMemcpyAsync(W.V.p + r * ldV, W.W.p + r * ldw, (size_t)(kd + 1) * n * sizeof(double2),
+                                              cudaMemcpyDeviceToDevice, B.s));
+            // Z <- Z P_k (first m rows, first kd columns of P)
+            rotate_sys_kernel<<<dim3(gy, R), 256, 0, B.s>>>(n, m, kd, W.Z.p, ldV, W.Qd.p, m + 1, qstride, B.act.p, W.W.p,
+                                                             ldw);
+            ++P.ctx->launches;
+            for (int r = 0; r < R; ++r)
+                if (iact[r])
+                    OPEM_CUDA(cudaMemcpyAsync(W.Z.p + r * ldV, W.W.p + r * ldw, (size_t)kd * n * sizeof(double2),
+                                              cudaMemcpyDeviceToDevice, B.s));
+            OPEM_CUDA(cudaStreamSynchronize(B.s));
+            for (int r = 0; r < R; ++r) {
+                if (!iact[r]) continue;
+                Hh[r] = Hn[r];
+                c[r] = cn[r];
+                start[r] = kd;
+                fresh[r] = 0;
+            }
+        }
+    }
+    its_out = its;
+    return OPEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// batched CG for the H projection (FP64): M1 h_r = (j/(w_r mu0)) Q e_r
+// ---------------------------------------------------------------------------
+static int mass_cg_batch(Batch& B, const double2* e_il, double2* h_il, double rtol, int maxits, int& its_out) {
+    Problem& P = B.P;
+    const int64_t n = B.n;
+    const int R = B.R;
+    const int64_t nR = n * R;
+    DBuf<double> dinv(n);
+    DBuf<double2> r(nR), z(nR), p(nR), q(nR), part((size_t)32 * 1024), sc(32), rz(32), pq(32), rzn(32);
+    std::vector<double2> hsc(32, make_double2(0, 0));
+    for (int i = 0; i < R; ++i) hsc[i] = make_double2(0.0, 1.0 / (2 * M_PI * B.sys[i].freq * MU0_M));
+    OPEM_CUDA(cudaMemcpyAsync(sc.p, hsc.data(), 32 * sizeof(double2), cudaMemcpyHostToDevice, B.s));
+    int grid = P.ctx->sm_count * 16;
+    spmv_real_batch_kernel<<<grid, 256, 0, B.s>>>(n, R, P.d_rowptr.p, P.d_cols.p, P.d_Q.p, e_il, sc.p, r.p);  // r = b
+    diag_inv_m1_kernel<<<vgrid(P), 256, 0, B.s>>>(n, P.d_rowptr.p, P.d_cols.p, P.d_M1.p, dinv.p);
+    P.ctx->launches += 2;
+    OPEM_CUDA(cudaMemsetAsync(h_il, 0, nR * sizeof(double2), B.s));
+    unsigned ge = (unsigned)((nR + 255) / 256);
+    const int nb = 256;
+    auto dot = [&](const double2* a, const double2* b, double2* out) {
+        dot_il_kernel<<<nb, dim3(32, 8), 0, B.s>>>(n, R, a, b, part.p);
+        dot_il_finish_kernel<<<1, 32, 0, B.s>>>(nb, part.p, out);
+        P.ctx->launches += 2;
+    };
+    std::vector<double2> hb(32), hr(32);
+    dot(r.p, r.p, rz.p);
+    OPEM_CUDA(cudaMemcpyAsync(hb.data(), rz.p, 32 * sizeof(double2), cudaMemcpyDeviceToHost, B.s));
+    dscale_batch_kernel<<<ge, 256, 0, B.s>>>(n, R, dinv.p, r.p, z.p);
+    OPEM_CUDA(cudaMemcpyAsync(p.p, z.p, nR * sizeof(double2), cudaMemcpyDeviceToDevice, B.s));
+    dot(r.p, z.p, rz.p);
+    P.ctx->launches += 3;
+    OPEM_CUDA(cudaStreamSynchronize(B.s));
+    std::vector<double> bn(R);
+    for (int i = 0; i < R; ++i) bn[i] = std::sqrt(hb[i].x);
+    std::vector<uint8_t> act(R, 1);
+    for (int i = 0; i < R; ++i) act[i] = bn[i] > 0;
+    OPEM_CUDA(cudaMemcpyAsync(B.act.p, act.data(), R, cudaMemcpyHostToDevice, B.s));
+    DBuf<double2> one(32);
+    std::vector<double2> h1(32, make_double2(1, 0));
+    OPEM_CUDA(cudaMemcpyAsync(one.p, h1.data(), 32 * sizeof(double2), cudaMemcpyHostToDevice, B.s));
+    int its = 0;
+    while (its < maxits) {
+        spmv_real_batch_kernel<<<grid, 256, 0, B.s>>>(n, R, P.d_rowptr.p, P.d_cols.p, P.d_M1.p, p.p, one.p, q.p);
+        dot(p.p, q.p, pq.p);
+        cg_update_batch_kernel<<<ge, 256, 0, B.s>>>(n, R, rz.p, pq.p, B.act.p, p.p, q.p, h_il, r.p);
+        P.ctx->launches += 2;
+        ++its;
+        if (its % 10 == 0 || its >= maxits) {
+            dot(r.p, r.p, rzn.p);
+            OPEM_CUDA(cudaMemcpyAsync(hr.data(), rzn.p, 32 * sizeof(double2), cudaMemcpyDeviceToHost, B.s));
+            OPEM_CUDA(cudaStreamSynchronize(B.s));
+            bool all = true;
+            for (int i = 0; i < R; ++i) {
+                if (!act[i]) continue;
+                double rn = std::sqrt(hr[i].x);
+                if (rn <= rtol * bn[i] || !std::isfinite(rn)) act[i] = 0;
+                all &= !act[i];
+            }
+            OPEM_CUDA(cudaMemcpyAsync(B.act.p, act.data(), R, cudaMemcpyHostToDevice, B.s));
+            if (all) break;
+        }
+        dscale_batch_kernel<<<ge, 256, 0, B.s>>>(n, R, dinv.p, r.p, z.p);
+        dot(r.p, z.p, rzn.p);
+        cg_dir_batch_kernel<<<ge, 256, 0, B.s>>>(n, R, rzn.p, rz.p, B.act.p, z.p, p.p);
+        OPEM_CUDA(cudaMemcpyAsync(rz.p, rzn.p, 32 * sizeof(double2), cudaMemcpyDeviceToDevice, B.s));
+        P.ctx->launches += 2;
+    }
+    OPEM_CUDA(cudaGetLastError());
+    its_out = its;
+    return OPEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// one batch of systems: returns Cp/Cm per system and stats
+// ---------------------------------------------------------------------------
+struct BatchOut {
+    std::vector<cd> Cp, Cm;   // [system][port]
+    int inner_its = 0, outer = 0, h_its = 0;
+    double worst = 0;
+    bool converged = true;
+};
+
+static void solve_batch(Problem& P, const std::vector<System>& systems, const opem_solver_opts& o, BatchOut& out) {
+    Batch B(P);
+    B.sys = systems;
+    B.R = (int)systems.size();
+    B.N = P.nports;
+    B.m = std::max(2, o.restart);
+    B.kd = std::max(0, std::min(o.deflate, B.m - 2));
+    const int R = B.R, N = B.N, m = B.m, kd = B.kd;
+    const int64_t n = B.n, nR = n * R;
+    // systems sorted by driving set -> contiguous lanes
+    B.r0.assign(N, 0);
+    B.Rd.assign(N, 0);
+    for (int r = 0; r < R; ++r) B.Rd[systems[r].d]++;
+    for (int d = 1; d < N; ++d) B.r0[d] = B.r0[d - 1] + B.Rd[d - 1];
+    for (int r = 1; r < R; ++r)
+        if (systems[r].d < systems[r - 1].d) throw OpemError(OPEM_ERR_ARG, "batch systems must be ordered by driving set");
+    // coefficient tables
+    std::vector<VC3<float2>> v32(R);
+    std::vector<VC3<double2>> v64(R);
+    std::vector<std::vector<BC5<float2>>> b32(P.groups.size(), std::vector<BC5<float2>>(R));
+    std::vector<std::vector<BC5<double2>>> b64(P.groups.size(), std::vector<BC5<double2>>(R));
+    std::vector<uint8_t> ds(R);
+    for (int r = 0; r < R; ++r) {
+        VolCoef vc;
+        std::vector<BCoef> bc;
+        system_coefficients(P, systems[r].freq, systems[r].d, vc, bc);
+        v64[r] = {vc.c_eps, vc.c_tand, vc.c_sig};
+        v32[r] = {make_float2((float)vc.c_eps.x, (float)vc.c_eps.y), make_float2((float)vc.c_tand.x, (float)vc.c_tand.y),
+                  make_float2((float)vc.c_sig.x, (float)vc.c_sig.y)};
+        for (size_t g = 0; g < bc.size(); ++g) {
+            const BCoef& c = bc[g];
+            b64[g][r] = {c.c_cc, c.c_eps, c.c_tand, c.c_sig, c.c_one};
+            auto f = [](double2 a) { return make_float2((float)a.x, (float)a.y); };
+            b32[g][r] = {f(c.c_cc), f(c.c_eps), f(c.c_tand), f(c.c_sig), f(c.c_one)};
+        }
+        ds[r] = (uint8_t)systems[r].d;
+    }
+    B.vc32.upload(v32, B.s);
+    B.vc64.upload(v64, B.s);
+    std::vector<const BC5<float2>*> bp32;
+    std::vector<const BC5<double2>*> bp64;
+    B.bc32.resize(P.groups.size());
+    B.bc64.resize(P.groups.size());
+    for (size_t g = 0; g < P.groups.size(); ++g) {
+        B.bc32[g].upload(b32[g], B.s);
+        B.bc64[g].upload(b64[g], B.s);
+        bp32.push_back(B.bc32[g].p);
+        bp64.push_back(B.bc64[g].p);
+    }
+    B.dsys.upload(ds, B.s);
+    B.act.alloc(RMAX);
+    // block-Jacobi sets: one per driving set, at the batch's middle frequency
+    std::vector<PatchSet32> sets(N);
+    double fmid = 0.5 * (systems.front().freq + systems.back().freq);
+    {
+        double lo = 1e300, hi = 0;
+        for (auto& sy : systems) { lo = std::min(lo, sy.freq); hi = std::max(hi, sy.freq); }
+        fmid = 0.5 * (lo + hi);
+    }
+    for (int d = 0; d < N; ++d)
+        if (B.Rd[d] > 0) build_patchset(B, fmid, d, sets[d]);
+    // right-hand sides b_r = -(A_r x0_r) with Dirichlet rows 0  (FP64)
+    DBuf<double2> x0(nR), x0_il(nR), y_il(nR), b(nR), x(nR), r64(nR);
+    const unsigned gy = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, P.ctx->sm_count * 2));
+    const double2* et = reinterpret_cast<const double2*>(P.d_et.p);
+    lift_batch_kernel<<<dim3(gy, R), 256, 0, B.s>>>(n, et, P.d_pec.p, B.dsys.p, x0.p);
+    ++P.ctx->launches;
+    to_il(B, x0.p, n, x0_il.p);
+    spmv_batch<double2, double>(B, P.d_K.p, P.d_Meps.p, P.has_tand ? P.d_Mtand.p : nullptr,
+                                P.has_sig ? P.d_Msig.p : nullptr, B.vc64.p, bp64, x0_il.p, y_il.p);
+    to_sm(B, y_il.p, b.p, n);
+    neg_sys_kernel<<<(unsigned)((nR + 255) / 256), 256, 0, B.s>>>(n, R, b.p);
+    ++P.ctx->launches;
+    OPEM_CUDA(cudaMemsetAsync(x.p, 0, nR * sizeof(double2), B.s));
+    DBuf<double> nrm(RMAX), npart((size_t)RMAX * 64);
+    std::vector<uint8_t> all1(R, 1), act(R, 1);
+    OPEM_CUDA(cudaMemcpyAsync(B.act.p, all1.data(), R, cudaMemcpyHostToDevice, B.s));
+    nrm_sys_f64(B, b.p, n, npart, nrm.p, B.act.p);
+    std::vector<double> bn(R), rn(R);
+    OPEM_CUDA(cudaMemcpyAsync(bn.data(), nrm.p, R * sizeof(double), cudaMemcpyDeviceToHost, B.s));
+    OPEM_CUDA(cudaStreamSynchronize(B.s));
+    // inner work buffers
+    InnerWork W;
+    const int64_t ldV = (int64_t)(m + 1) * n;
+    const int nbm = md_blocks_sys(P.ctx->sm_count, R, n);
+    const int maxRd = std::max(1, *std::max_element(B.Rd.begin(), B.Rd.end()));
+    W.V.alloc((size_t)R * ldV);
+    W.Z.alloc((size_t)R * ldV);
+    W.w.alloc(nR);
+    W.w_il.alloc(nR);
+    W.z_il64.alloc(nR);
+    W.x_il32.alloc(nR);
+    W.z_il32.alloc(nR);
+    W.t.alloc(P.topo.patch_dofs.size() * (size_t)maxRd);
+    W.h.alloc((size_t)R * (m + 1));
+    W.part.alloc((size_t)R * (m + 1) * nbm);
+    W.yd.alloc((size_t)R * m);
+    W.Qd.alloc((size_t)R * (m + 1) * (kd + 1));
+    W.W.alloc((size_t)R * (kd + 1) * n);
+    W.rhs.alloc(nR);
+    W.d.alloc(nR);
+    W.H.alloc((size_t)R * (m + 1) * m);
+    W.nrm.alloc(RMAX);
+    W.npart.alloc((size_t)RMAX * 64);
+    W.ncols.alloc(RMAX);
+    // outer FP64 refinement (normally one pass: the inner Krylov solve is FP64)
+    OPEM_CUDA(cudaMemcpyAsync(r64.p, b.p, nR * sizeof(double2), cudaMemcpyDeviceToDevice, B.s));
+    rn = bn;
+    int outer = 0, inner_total = 0;
+    for (int r = 0; r < R; ++r) act[r] = (bn[r] > 0 && rn[r] > o.rtol * bn[r]) ? 1 : 0;
+    while (outer < 4) {
+        bool any = false;
+        for (int r = 0; r < R; ++r) any |= act[r];
+        if (!any || inner_total >= o.maxits) break;
+        ++outer;
+        // inner tolerance relative to this step's residual, aiming at rtol ||b||
+        double tol_in = 1.0;
+        for (int r = 0; r < R; ++r)
+            if (act[r]) tol_in = std::min(tol_in, 0.5 * o.rtol * bn[r] / rn[r]);
+        tol_in = std::max(tol_in, 1e-14);
+        OPEM_CUDA(cudaMemcpyAsync(B.act.p, act.data(), R, cudaMemcpyHostToDevice, B.s));
+        OPEM_CUDA(cudaMemcpyAsync(nrm.p, rn.data(), R * sizeof(double), cudaMemcpyHostToDevice, B.s));
+        scale_sys_kernel<<<dim3(gy, R), 256, 0, B.s>>>(n, r64.p, nrm.p, B.act.p, W.rhs.p);
+        ++P.ctx->launches;
+        int its = 0;
+        inner_solve(B, W, sets, bp64, act, tol_in, o.maxits - inner_total, its);
+        inner_total += its;
+        OPEM_CUDA(cudaMemcpyAsync(B.act.p, act.data(), R, cudaMemcpyHostToDevice, B.s));
+        refine_sys_kernel<<<dim3(gy, R), 256, 0, B.s>>>(n, W.d.p, nrm.p, B.act.p, x.p);
+        ++P.ctx->launches;
+        // FP64 residual r = b - A x
+        to_il(B, x.p, n, x0_il.p);
+        spmv_batch<double2, double>(B, P.d_K.p, P.d_Meps.p, P.has_tand ? P.d_Mtand.p : nullptr,
+                                    P.has_sig ? P.d_Msig.p : nullptr, B.vc64.p, bp64, x0_il.p, y_il.p);
+        resid_kernel<<<(unsigned)((nR + 255) / 256), 256, 0, B.s>>>(n, R, b.p, y_il.p, r64.p);
+        ++P.ctx->launches;
+        OPEM_CUDA(cudaMemcpyAsync(B.act.p, all1.data(), R, cudaMemcpyHostToDevice, B.s));
+        nrm_sys_f64(B, r64.p, n, npart, nrm.p, B.act.p);
+        OPEM_CUDA(cudaMemcpyAsync(rn.data(), nrm.p, R * sizeof(double), cudaMemcpyDeviceToHost, B.s));
+        OPEM_CUDA(cudaStreamSynchronize(B.s));
+        for (int r = 0; r < R; ++r) act[r] = (bn[r] > 0 && rn[r] > o.rtol * bn[r] && std::isfinite(rn[r])) ? 1 : 0;
+    }
+    out.inner_its = inner_total;
+    out.outer = outer;
+    out.worst = 0;
+    out.converged = true;
+    for (int r = 0; r < R; ++r) {
+        double rel = bn[r] > 0 ? rn[r] / bn[r] : 0;
+        out.worst = std::max(out.worst, rel);
+        if (!(rel <= o.rtol)) out.converged = false;
+    }
+    // e = x + x0 (driven port values), H projection, overlaps
+    finish_e_kernel<<<dim3(gy, R), 256, 0, B.s>>>(n, et, B.dsys.p, x.p);
+    ++P.ctx->launches;
+    W.V.release();
+    W.Z.release();
+    W.W.release();
+    DBuf<double2> e_il(nR), h_il(nR), h_sm(nR);
+    to_il(B, x.p, n, e_il.p);
+    mass_cg_batch(B, e_il.p, h_il.p, o.h_rtol, o.h_maxits, out.h_its);
+    to_sm(B, h_il.p, h_sm.p, n);
+    DBuf<double2> ov((size_t)4 * R * N);
+    for (int r = 0; r < R; ++r)
+        for (int k = 0; k < N; ++k) {
+            const double2* etk = et + (size_t)k * n;
+            const double2* nxk = reinterpret_cast<const double2*>(P.d_nxe.p) + (size_t)k * n;
+            double2* o4 = ov.p + 4 * (r * N + k);
+            port_overlap(P, k, etk, x.p + (size_t)r * n, o4 + 0);
+            port_overlap(P, k, etk, etk, o4 + 1);
+            port_overlap(P, k, nxk, h_sm.p + (size_t)r * n, o4 + 2);
+            port_overlap(P, k, nxk, nxk, o4 + 3);
+        }
+    std::vector<double2> hov((size_t)4 * R * N);
+    OPEM_CUDA(cudaMemcpyAsync(hov.data(), ov.p, hov.size() * sizeof(double2), cudaMemcpyDeviceToHost, B.s));
+    OPEM_CUDA(cudaStreamSynchronize(B.s));
+    out.Cp.assign((size_t)R * N, 0.0);
+    out.Cm.assign((size_t)R * N, 0.0);
+    for (int r = 0; r < R; ++r) {
+        double w = 2 * M_PI * systems[r].freq;
+        for (int k = 0; k < N; ++k) {
+            cd gam, Z, V;
+            port_gamma_Z_V(P, k, systems[r].freq, gam, Z, V);
+            cd y = gam / cd(0, w * port_mu_r(P, k) * MU0_M);
+            const double2* o4 = &hov[4 * (r * N + k)];
+            cd e0(o4[0].x, o4[0].y), e2(o4[1].x, o4[1].y);
+            cd h0 = std::conj(y) * cd(o4[2].x, o4[2].y), h2 = std::norm(y) * cd(o4[3].x, o4[3].y);
+            out.Cp[(size_t)r * N + k] = 0.5 * (e0 / e2 + h0 / h2);
+            out.Cm[(size_t)r * N + k] = 0.5 * (e0 / e2 - h0 / h2);
+        }
+    }
+}
+
+// Sweep driver: frequencies are grouped so that a batch holds F frequencies
+// x N driving sets <= RMAX systems.
+void solve_sweep_mixed(Problem& P, int nfreq, const double* freqs, const opem_solver_opts& o,
+                       std::vector<std::vector<cd>>& S, std::vector<opem_solve_stats>& st) {
+    const int N = P.nports;
+    int F = std::max(1, RMAX / std::max(1, N));
+    int nb = (nfreq + F - 1) / F;
+    F = (nfreq + nb - 1) / nb;   // balance the batches
+    S.assign(nfreq, {});
+    st.assign(nfreq, opem_solve_stats{});
+    for (int f0 = 0; f0 < nfreq; f0 += F) {
+        int f1 = std::min(nfreq, f0 + F);
+        cudaEvent_t e0, e1;
+        OPEM_CUDA(cudaEventCreate(&e0));
+        OPEM_CUDA(cudaEventCreate(&e1));
+        OPEM_CUDA(cudaEventRecord(e0, P.ctx->stream));
+        std::vector<System> sys;
+        for (int d = 0; d < N; ++d)
+            for (int f = f0; f < f1; ++f) sys.push_back({freqs[f], d});
+        BatchOut bo;
+        solve_batch(P, sys, o, bo);
+        OPEM_CUDA(cudaEventRecord(e1, P.ctx->stream));
+        OPEM_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        OPEM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        const int nf = f1 - f0;
+        for (int f = f0; f < f1; ++f) {
+            std::vector<cd> Cp((size_t)N * N), Cm((size_t)N * N), V(N), Z(N);
+            for (int d = 0; d < N; ++d) {
+                int r = d * nf + (f - f0);
+                for (int k = 0; k < N; ++k) {
+                    Cp[d * N + k] = bo.Cp[(size_t)r * N + k];
+                    Cm[d * N + k] = bo.Cm[(size_t)r * N + k];
+                }
+            }
+            for (int k = 0; k < N; ++k) {
+                cd g;
+                port_gamma_Z_V(P, k, freqs[f], g, Z[k], V[k]);
+            }
+            S[f] = s_matrix_solve(N, Cp, Cm, V, Z, o.force_reciprocal != 0);
+            opem_solve_stats& s = st[f];
+            s.iterations = bo.inner_its;   // lockstep iterations of the batch
+            s.outer = bo.outer;
+            s.h_iterations = bo.h_its;
+            s.converged = bo.converged ? 1 : 0;
+            s.rnorm = bo.worst;
+            s.seconds = ms * 1e-3 / nf;    // the batch's device time shared by its points
+        }
+    }
+}
+
+}  // namespace opem

@@ -161,3 +161,29 @@ def test_deflated_restart_cuts_iterations(ctx):
     assert st0["converged"] == 1 and st1["converged"] == 1
     assert np.abs(S0 - S1).max() <= 1e-7
     assert st1["iterations"] < st0["iterations"]
+
+
+@pytest.mark.parametrize("case", ["c1_nd1", "slab_nd2", "copper_nd2", "radcap_nd1", "slab_nd3"])
+def test_mixed_sweep_matches_fp64_and_oracle(ctx, case):
+    """Batched FP32-inner / FP64-refinement sweep vs the FP64 solve and the oracle:
+    |dS| <= 1e-6 with outer rtol 1e-10."""
+    fem = _oracle()
+    prob = CASES[case]()
+    F = Fem3D(prob, context=ctx).assemble()
+    fr = np.linspace(8.5e9, 11.5e9, 5)
+    Sm, st = F.sweep(fr, default_opts(precision=_lib.PREC_MIXED, rtol=1e-10))
+    ops = fem.Operators(prob)
+    for i, f in enumerate(fr):
+        S, _, _ = F.solve(f, default_opts(rtol=1e-12, restart=200))
+        assert st[i]["converged"] == 1 and st[i]["rnorm"] <= 1e-10
+        assert np.abs(Sm[i] - S).max() <= 1e-6, (case, f)
+        assert np.abs(Sm[i] - fem.solve_frequency(ops, f)["S"]).max() <= 1e-6
+
+
+def test_mixed_single_frequency_entry(ctx):
+    prob = CASES["slab_nd2"]()
+    F = Fem3D(prob, context=ctx).assemble()
+    S1, Z1, st1 = F.solve(9.9e9, default_opts(precision=_lib.PREC_MIXED))
+    S0, Z0, _ = F.solve(9.9e9)
+    assert np.abs(S1 - S0).max() <= 1e-6 and np.allclose(Z1, Z0)
+    assert st1["outer"] >= 1
