@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="both", choices=["plain", "mixed", "both"])
     ap.add_argument("--batch", type=int, default=13, help="frequency points per mixed-precision batch")
+    ap.add_argument("--poly", type=int, default=8, help="GMRES-polynomial preconditioner degree of the batched path")
     ap.add_argument("--restart", type=int, default=100)
     ap.add_argument("--deflate", type=int, default=30)
     ap.add_argument("--mesh", default="24,12,60",
@@ -179,7 +180,9 @@ def config_dict(args):
             "step": (f"mixed: one batch of {args.batch} frequency points x 2 driving sets; plain: one point"
                      if args.mode != "plain" else "one frequency point (2 driving sets)"),
             "mesh": args.mesh, "gmres_restart": args.restart, "gmres_deflate": args.deflate, "rtol": args.rtol,
-            "krylov": "GMRES-DR (deflated restarting)", "precond": "vertex-patch block Jacobi",
+            "krylov": "GMRES-DR (deflated restarting); batched path: flexible GMRES-DR",
+            "precond": "vertex-patch block Jacobi (FP64 plain; FP32 blocks + GMRES polynomial in the batched path)",
+            "poly_degree": args.poly,
             "l2": "operator arrays ~1 GB > 126 MB L2, no flush", "parallelism": f"replicas x{args.gpus}"}
 
 
@@ -204,7 +207,7 @@ def run_ours(args, rank, world, local_rank):
     N = F.nports
     plain_o = default_opts(rtol=args.rtol, restart=args.restart, deflate=args.deflate, maxits=20000)
     mixed_o = default_opts(rtol=args.rtol, restart=args.restart, deflate=args.deflate, maxits=20000,
-                           precision=_lib.PREC_MIXED)
+                           precision=_lib.PREC_MIXED, poly_degree=args.poly)
     my_freqs = freqs[rank::world]
     nb = args.batch
 

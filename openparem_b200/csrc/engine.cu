@@ -731,7 +731,7 @@ int opem_problem_info(opem_problem prob, int64_t* info, int ninfo) {
 }
 
 static bool opts_ok(const opem_solver_opts* o) {
-    return o && o->rtol > 0 && o->maxits > 0 && o->restart >= 2 && o->restart <= 2048 && o->h_maxits > 0 && o->h_rtol > 0 && o->deflate >= 0 &&
+    return o && o->rtol > 0 && o->maxits > 0 && o->restart >= 2 && o->restart <= 2048 && o->h_maxits > 0 && o->h_rtol > 0 && o->deflate >= 0 && o->poly_degree >= 0 && o->poly_degree <= 32 &&
            (o->precision == OPEM_PREC_FP64 || o->precision == OPEM_PREC_MIXED);
 }
 

@@ -160,46 +160,62 @@ __global__ void il2sm_kernel(int64_t n, int R, const T2* __restrict__ in, O2* __
 // ---------------------------------------------------------------------------
 // batched vertex-patch block Jacobi (FP32 blocks), systems [r0, r0+Rd)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) patch_apply1_batch_kernel(
+// One CTA (4 warps) per patch.  Each warp owns 32 block rows (lane = row) and
+// streams 32x32 tiles of the block through shared memory (coalesced global
+// reads, padded to avoid bank conflicts); each lane accumulates its row for up
+// to RC systems in registers while the system inputs are broadcast from shared
+// memory.  Lanes map to rows, not to systems, so no lane idles when a driving
+// set has fewer than 32 systems.
+constexpr int PA_RC = 16;
+__global__ void __launch_bounds__(128) patch_apply1_batch_kernel(
     int npatch, const int32_t* __restrict__ pptr, const int32_t* __restrict__ pdofs, const int64_t* __restrict__ poff,
     const float2* __restrict__ B, const float2* __restrict__ x, int R, int r0, int Rd, float2* __restrict__ t) {
-    extern __shared__ float2 rv[];   // s x Rd
-    int v = blockIdx.x;
-    int32_t p0 = pptr[v];
-    int s = pptr[v + 1] - p0;
+    extern __shared__ float2 smem[];
+    float2* rv = smem;                                 // s x Rd inputs
+    const int v = blockIdx.x;
+    const int32_t p0 = pptr[v];
+    const int s = pptr[v + 1] - p0;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    float2* tile = smem + (size_t)s * Rd + (size_t)w * 32 * 33;   // per-warp 32 x 33 tile
     for (int e = threadIdx.x; e < s * Rd; e += blockDim.x) {
         int b = e / Rd, l = e % Rd;
         rv[e] = x[(int64_t)pdofs[p0 + b] * R + r0 + l];
     }
     __syncthreads();
     const float2* Bv = B + poff[v];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    constexpr int RW = 4;
-    for (int a0 = w * RW; a0 < s; a0 += nw * RW) {
-        float re[RW], im[RW];
+    for (int a0 = w * 32; a0 < s; a0 += nw * 32) {
+        const int a = a0 + lane;
+        for (int c0 = 0; c0 < Rd; c0 += PA_RC) {
+            const int nc = min(PA_RC, Rd - c0);
+            float re[PA_RC], im[PA_RC];
 #pragma unroll
-        for (int q = 0; q < RW; ++q) { re[q] = 0.f; im[q] = 0.f; }
-        for (int b0 = 0; b0 < s; b0 += 32) {
-            float2 bv[RW];
+            for (int q = 0; q < PA_RC; ++q) { re[q] = 0.f; im[q] = 0.f; }
+            for (int b0 = 0; b0 < s; b0 += 32) {
+                // stage rows a0..a0+31, columns b0..b0+31 (lane = column)
+                __syncwarp();
+                for (int rr = 0; rr < 32; ++rr) {
+                    float2 val = make_float2(0.f, 0.f);
+                    if (a0 + rr < s && b0 + lane < s) val = __ldcs(&Bv[(int64_t)(a0 + rr) * s + b0 + lane]);
+                    tile[rr * 33 + lane] = val;
+                }
+                __syncwarp();
+                const int bl = min(32, s - b0);
+                for (int l = 0; l < bl; ++l) {
+                    float2 m = tile[lane * 33 + l];
+                    const float2* xr = rv + (size_t)(b0 + l) * Rd + c0;
 #pragma unroll
-            for (int q = 0; q < RW; ++q)
-                bv[q] = (a0 + q < s && b0 + lane < s) ? __ldcs(&Bv[(int64_t)(a0 + q) * s + b0 + lane]) : make_float2(0.f, 0.f);
-            int bl = min(32, s - b0);
-            for (int l = 0; l < bl; ++l) {
-                float2 xv = lane < Rd ? rv[(b0 + l) * Rd + lane] : make_float2(0.f, 0.f);
-#pragma unroll
-                for (int q = 0; q < RW; ++q) {
-                    float mx = __shfl_sync(0xffffffffu, bv[q].x, l);
-                    float my = __shfl_sync(0xffffffffu, bv[q].y, l);
-                    re[q] += mx * xv.x - my * xv.y;
-                    im[q] += mx * xv.y + my * xv.x;
+                    for (int q = 0; q < PA_RC; ++q) {
+                        if (q < nc) {
+                            float2 xv = xr[q];
+                            re[q] += m.x * xv.x - m.y * xv.y;
+                            im[q] += m.x * xv.y + m.y * xv.x;
+                        }
+                    }
                 }
             }
+            if (a < s)
+                for (int q = 0; q < nc; ++q) t[(int64_t)(p0 + a) * Rd + c0 + q] = make_float2(re[q], im[q]);
         }
-        if (lane < Rd)
-#pragma unroll
-            for (int q = 0; q < RW; ++q)
-                if (a0 + q < s) t[(int64_t)(p0 + a0 + q) * Rd + lane] = make_float2(re[q], im[q]);
     }
 }
 
@@ -436,6 +452,25 @@ __global__ void sub_sys_kernel(int64_t n, int R, const double2* __restrict__ a, 
     int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (e >= n * R) return;
     c[e] = make_double2(a[e].x - b[e].x, a[e].y - b[e].y);
+}
+
+// polynomial preconditioner steps on interleaved FP32 vectors, c[r] = 1/theta_i of system r:
+//   y += c u   (first = 1: y = c u)      and      u -= c t
+__global__ void poly_acc_kernel(int64_t cnt, int R, const float2* __restrict__ c, const float2* __restrict__ u,
+                                float2* __restrict__ y, int first) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < cnt; e += (int64_t)gridDim.x * blockDim.x) {
+        float2 cc = c[e % R], uu = u[e];
+        float2 p = make_float2(cc.x * uu.x - cc.y * uu.y, cc.x * uu.y + cc.y * uu.x);
+        if (first) y[e] = p;
+        else y[e] = make_float2(y[e].x + p.x, y[e].y + p.y);
+    }
+}
+__global__ void poly_sub_kernel(int64_t cnt, int R, const float2* __restrict__ c, const float2* __restrict__ t,
+                                float2* __restrict__ u) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < cnt; e += (int64_t)gridDim.x * blockDim.x) {
+        float2 cc = c[e % R], tt = t[e];
+        u[e] = make_float2(u[e].x - (cc.x * tt.x - cc.y * tt.y), u[e].y - (cc.x * tt.y + cc.y * tt.x));
+    }
 }
 
 // interleaved FP32 -> FP64
@@ -723,8 +758,10 @@ static void patch_apply_batch(Batch& B, const std::vector<PatchSet32>& sets, DBu
     Problem& P = B.P;
     for (int d = 0; d < B.N; ++d) {
         if (B.Rd[d] == 0) continue;
-        size_t smem = (size_t)P.topo.max_patch * B.Rd[d] * sizeof(float2);
-        patch_apply1_batch_kernel<<<P.npatch, 256, smem, B.s>>>(P.npatch, P.d_patch_ptr.p, P.d_patch_dofs.p,
+        size_t smem = ((size_t)P.topo.max_patch * B.Rd[d] + 4 * 32 * 33) * sizeof(float2);
+        if (smem > 48 * 1024)
+            OPEM_CUDA(cudaFuncSetAttribute(patch_apply1_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        patch_apply1_batch_kernel<<<P.npatch, 128, smem, B.s>>>(P.npatch, P.d_patch_ptr.p, P.d_patch_dofs.p,
                                                                 P.d_patch_off.p, sets[d].B.p, x_il, B.R, B.r0[d],
                                                                 B.Rd[d], t.p);
         ++P.ctx->launches;
@@ -757,14 +794,38 @@ static inline double beta0(int r, const std::vector<double>& beta) { (void)beta;
 struct InnerWork {
     DBuf<double2> V, Z, w, w_il, z_il64, h, part, yd, Qd, W, rhs, d;
     DBuf<float2> x_il32, z_il32, t;
+    DBuf<float2> pu, py, pt, pt2, pc;   // polynomial preconditioner work (interleaved FP32) and 1/theta table
     DBuf<double2> H;     // per system (m+1) x m FP64 Hessenberg
     DBuf<double> nrm, npart;
     DBuf<int> ncols;
 };
 
+// Leja ordering of polynomial roots (largest first, then maximising the product of distances)
+static std::vector<cd> leja(std::vector<cd> th) {
+    std::vector<cd> out;
+    if (th.empty()) return out;
+    size_t i0 = 0;
+    for (size_t i = 1; i < th.size(); ++i)
+        if (std::abs(th[i]) > std::abs(th[i0])) i0 = i;
+    out.push_back(th[i0]);
+    th.erase(th.begin() + i0);
+    while (!th.empty()) {
+        size_t best = 0;
+        double bv = -1;
+        for (size_t i = 0; i < th.size(); ++i) {
+            double lp = 0;
+            for (const cd& o : out) lp += std::log(std::abs(th[i] - o) + 1e-300);
+            if (lp > bv) { bv = lp; best = i; }
+        }
+        out.push_back(th[best]);
+        th.erase(th.begin() + best);
+    }
+    return out;
+}
+
 static int inner_solve(Batch& B, InnerWork& W, const std::vector<PatchSet32>& sets,
                        const std::vector<const BC5<double2>*>& bc64, const std::vector<uint8_t>& active_in,
-                       double tol, int maxits, int& its_out) {
+                       double tol, int maxits, int poly_deg, int& its_out) {
     Problem& P = B.P;
     const int64_t n = B.n;
     const int R = B.R, m = B.m, kd = B.kd;
@@ -784,6 +845,7 @@ static int inner_solve(Batch& B, InnerWork& W, const std::vector<PatchSet32>& se
     std::vector<double2> hcol((size_t)R * (m + 2));
     std::vector<std::vector<cd>> ys(R);
     int its = 0;
+    int npoly = 0;   // degree of the polynomial preconditioner in use (0: block Jacobi alone)
     auto upload_act = [&](const std::vector<uint8_t>& a) {
         OPEM_CUDA(cudaMemcpyAsync(B.act.p, a.data(), R, cudaMemcpyHostToDevice, B.s));
     };
@@ -827,9 +889,29 @@ static int inner_solve(Batch& B, InnerWork& W, const std::vector<PatchSet32>& se
             for (int r = 0; r < R; ++r) anyj |= iact[r];
             if (!anyj) break;
             upload_act(iact);
-            // z_j = M^-1 v_j (FP32 blocks), kept in Z; w = A z_j (FP64)
+            // z_j = P v_j, kept in Z (P = M^-1 for the first steps, then M^-1 q(A M^-1)
+            // with the GMRES polynomial q of each system, all in FP32); w = A z_j (FP64)
             to_il(B, W.V.p + (int64_t)j * n, ldV, W.x_il32.p);
-            patch_apply_batch(B, sets, W.t, W.x_il32.p, W.z_il32.p);
+            if (npoly > 0) {
+                const int64_t cnt = n * R;
+                const unsigned gp = (unsigned)std::min<int64_t>((cnt + 255) / 256, P.ctx->sm_count * 16);
+                // y = q(A M^-1) v with Leja-ordered roots: y += u/theta_i ; u -= (A M^-1 u)/theta_i
+                OPEM_CUDA(cudaMemcpyAsync(W.pu.p, W.x_il32.p, cnt * sizeof(float2), cudaMemcpyDeviceToDevice, B.s));
+                for (int i = 0; i < npoly; ++i) {
+                    poly_acc_kernel<<<gp, 256, 0, B.s>>>(cnt, R, W.pc.p + (size_t)i * R, W.pu.p, W.py.p, i == 0);
+                    ++P.ctx->launches;
+                    if (i + 1 < npoly) {
+                        patch_apply_batch(B, sets, W.t, W.pu.p, W.pt.p);
+                        spmv_batch<float2, double>(B, P.d_K.p, P.d_Meps.p, P.has_tand ? P.d_Mtand.p : nullptr,
+                                                   P.has_sig ? P.d_Msig.p : nullptr, B.vc64.p, bc64, W.pt.p, W.pt2.p);
+                        poly_sub_kernel<<<gp, 256, 0, B.s>>>(cnt, R, W.pc.p + (size_t)i * R, W.pt2.p, W.pu.p);
+                        ++P.ctx->launches;
+                    }
+                }
+                patch_apply_batch(B, sets, W.t, W.py.p, W.z_il32.p);
+            } else {
+                patch_apply_batch(B, sets, W.t, W.x_il32.p, W.z_il32.p);
+            }
             to_sm(B, W.z_il32.p, W.Z.p + (int64_t)j * n, ldV);
             il_f2d_kernel<<<vgrid(P), 256, 0, B.s>>>(n * R, W.z_il32.p, W.z_il64.p);
             ++P.ctx->launches;
@@ -859,6 +941,40 @@ static int inner_solve(Batch& B, InnerWork& W, const std::vector<PatchSet32>& se
                 est[r] = L[r].add_column(j, &Hh[r][(size_t)j * (m + 1)], j + 1);
                 ncol[r] = j + 1;
                 if (!std::isfinite(est[r]) || est[r] <= tol * beta0(r, beta)) cyc[r] = 0;
+            }
+            if (poly_deg > 1 && npoly == 0 && j + 1 == poly_deg) {
+                // harmonic Ritz values of the first poly_deg steps of every system -> GMRES polynomial roots
+                const int dg = poly_deg;
+                std::vector<float2> hc((size_t)dg * R, make_float2(0.f, 0.f));
+                bool okall = true;
+                for (int r = 0; r < R; ++r) {
+                    if (done[r]) continue;
+                    std::vector<cd> Hd((size_t)dg * dg), HdH((size_t)dg * dg), f(dg, 0.0);
+                    for (int b2 = 0; b2 < dg; ++b2)
+                        for (int a2 = 0; a2 < dg; ++a2) {
+                            Hd[a2 + (size_t)b2 * dg] = Hh[r][a2 + (size_t)b2 * (m + 1)];
+                            HdH[b2 + (size_t)a2 * dg] = std::conj(Hh[r][a2 + (size_t)b2 * (m + 1)]);
+                        }
+                    f[dg - 1] = 1.0;
+                    std::vector<cd> th, gv;
+                    if (!lu_solve(dg, HdH, f)) { okall = false; break; }
+                    double h2 = std::norm(Hh[r][dg + (size_t)(dg - 1) * (m + 1)]);
+                    for (int a2 = 0; a2 < dg; ++a2) Hd[a2 + (size_t)(dg - 1) * dg] += h2 * f[a2];
+                    if (!eig_smallest(dg, Hd, dg, th, gv)) { okall = false; break; }
+                    double tmax = 0;
+                    for (auto& t3 : th) tmax = std::max(tmax, std::abs(t3));
+                    for (auto& t3 : th)
+                        if (!(std::abs(t3) > 1e-6 * tmax)) okall = false;
+                    th = leja(th);
+                    for (int i = 0; i < dg; ++i) {
+                        cd ci = 1.0 / th[i];
+                        hc[(size_t)i * R + r] = make_float2((float)ci.real(), (float)ci.imag());
+                    }
+                }
+                if (okall) {
+                    OPEM_CUDA(cudaMemcpyAsync(W.pc.p, hc.data(), hc.size() * sizeof(float2), cudaMemcpyHostToDevice, B.s));
+                    npoly = dg;
+                }
             }
             if (its >= maxits) break;
         }
@@ -1140,6 +1256,13 @@ static void solve_batch(Problem& P, const std::vector<System>& systems, const op
     W.nrm.alloc(RMAX);
     W.npart.alloc((size_t)RMAX * 64);
     W.ncols.alloc(RMAX);
+    if (o.poly_degree > 1) {
+        W.pu.alloc(nR);
+        W.py.alloc(nR);
+        W.pt.alloc(nR);
+        W.pt2.alloc(nR);
+        W.pc.alloc((size_t)o.poly_degree * R);
+    }
     // outer FP64 refinement (normally one pass: the inner Krylov solve is FP64)
     OPEM_CUDA(cudaMemcpyAsync(r64.p, b.p, nR * sizeof(double2), cudaMemcpyDeviceToDevice, B.s));
     rn = bn;
@@ -1160,7 +1283,7 @@ static void solve_batch(Problem& P, const std::vector<System>& systems, const op
         scale_sys_kernel<<<dim3(gy, R), 256, 0, B.s>>>(n, r64.p, nrm.p, B.act.p, W.rhs.p);
         ++P.ctx->launches;
         int its = 0;
-        inner_solve(B, W, sets, bp64, act, tol_in, o.maxits - inner_total, its);
+        inner_solve(B, W, sets, bp64, act, tol_in, o.maxits - inner_total, o.poly_degree, its);
         inner_total += its;
         OPEM_CUDA(cudaMemcpyAsync(B.act.p, act.data(), R, cudaMemcpyHostToDevice, B.s));
         refine_sys_kernel<<<dim3(gy, R), 256, 0, B.s>>>(n, W.d.p, nrm.p, B.act.p, x.p);
