@@ -39,7 +39,7 @@ TRAFFIC_RATIO_PATCH = 726.0 / 727.1   # reference's own ND2 timings: 103,146 -> 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="both", choices=["plain", "mixed", "both"])
@@ -208,7 +208,8 @@ def run_ours(args, rank, world, local_rank):
     plain_o = default_opts(rtol=args.rtol, restart=args.restart, deflate=args.deflate, maxits=20000)
     mixed_o = default_opts(rtol=args.rtol, restart=args.restart, deflate=args.deflate, maxits=20000,
                            precision=_lib.PREC_MIXED, poly_degree=args.poly)
-    my_freqs = freqs[rank::world]
+    from openparem_b200.replicas import partition, max_over_ranks
+    my_freqs = partition(freqs, rank, world)
     nb = args.batch
 
     def batch_freqs(i):
@@ -276,9 +277,7 @@ def run_ours(args, rank, world, local_rank):
             dist.barrier()
         _lib.lib().opem_context_launches(ctx.h, C.byref(l1))
         units = sum(len(batch_freqs(warm + i)) for i in range(steps)) if mode == "mixed" else steps
-        t = torch.tensor([sum(dev_s), sum(wall_s)], dtype=torch.float64, device=f"cuda:{dev}")
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t = max_over_ranks([sum(dev_s), sum(wall_s)], dist if world > 1 else None, device=f"cuda:{dev}")
         res[mode] = {"units": units * world, "t_dev": float(t[0]), "t_wall": float(t[1]), "steps": steps,
                      "launches": int(l1.value - l0.value), "lat": lat, "its": its, "outer": outer, "conv": conv,
                      "S": Sd, "freqs": sorted(Sd.keys()), "clocks": clk.summary()}

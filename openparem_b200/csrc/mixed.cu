@@ -1356,6 +1356,19 @@ void solve_sweep_mixed(Problem& P, int nfreq, const double* freqs, const opem_so
                        std::vector<std::vector<cd>>& S, std::vector<opem_solve_stats>& st) {
     const int N = P.nports;
     int F = std::max(1, RMAX / std::max(1, N));
+    // Keep a batch's per-system Krylov storage (V and Z, FP64, (m+1) vectors each,
+    // plus the rotation buffer and vectors) within half of the free device memory.
+    {
+        size_t freeb = 0, totb = 0;
+        OPEM_CUDA(cudaMemGetInfo(&freeb, &totb));
+        const int m = std::max(2, o.restart), kd = std::max(0, std::min(o.deflate, m - 2));
+        const double per_sys = (double)P.topo.n * sizeof(double2) * (2.0 * (m + 1) + (kd + 1) + 16) +
+                               (double)P.topo.patch_dofs.size() * sizeof(float2);
+        const double fixed = (double)P.topo.patch_off.back() * (sizeof(float2) * N + sizeof(double2));
+        int Fm = (int)std::floor((0.5 * (double)freeb - fixed) / (per_sys * std::max(1, N)));
+        if (Fm < 1) throw OpemError(OPEM_ERR_NOMEM, "not enough device memory for one batched frequency point");
+        F = std::min(F, Fm);
+    }
     int nb = (nfreq + F - 1) / F;
     F = (nfreq + nb - 1) / nb;   // balance the batches
     S.assign(nfreq, {});
