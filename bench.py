@@ -77,14 +77,26 @@ def cpu_sample(npoints=None, cores=None):
     workload with the reference's own ND2 growth exponent (1.53, from its
     published 103k -> 656k DOF timings)."""
     import multiprocessing as mp
-    cores = cores or min(8, os.cpu_count() or 1)
+    cores = cores or min(16, os.cpu_count() or 1)
     npoints = npoints or cores
     freqs = np.linspace(8e9, 12e9, 51)[:npoints]
     ctx = mp.get_context("spawn")
-    t0 = time.perf_counter()
-    with ctx.Pool(cores) as pool:
-        res = pool.map(_cpu_point, [(6, 3, 15, f) for f in freqs])
-    wall = time.perf_counter() - t0
+    # one BLAS thread per worker process: several multi-threaded OpenBLAS
+    # instances on the same cores livelock
+    saved = {k: os.environ.get(k) for k in ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "MKL_NUM_THREADS")}
+    for k in saved:
+        os.environ[k] = "1"
+    try:
+        t0 = time.perf_counter()
+        with ctx.Pool(cores) as pool:
+            res = pool.map(_cpu_point, [(6, 3, 15, f) for f in freqs])
+        wall = time.perf_counter() - t0
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
     per_point = float(np.mean([r[0] for r in res]))
     n_s = res[0][1]
     scaled = per_point * (C2_NDOF / n_s) ** REF_ND2_EXPONENT
