@@ -1373,15 +1373,23 @@ void solve_sweep_mixed(Problem& P, int nfreq, const double* freqs, const opem_so
     F = (nfreq + nb - 1) / nb;   // balance the batches
     S.assign(nfreq, {});
     st.assign(nfreq, opem_solve_stats{});
-    for (int f0 = 0; f0 < nfreq; f0 += F) {
+    // batches are contiguous in frequency and span at most 15% of their centre
+    // frequency, since a batch shares one block-Jacobi set per driving set
+    std::vector<int> order(nfreq);
+    for (int i = 0; i < nfreq; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return freqs[a] < freqs[b]; });
+    std::vector<double> fs(nfreq);
+    for (int i = 0; i < nfreq; ++i) fs[i] = freqs[order[i]];
+    for (int f0 = 0; f0 < nfreq;) {
         int f1 = std::min(nfreq, f0 + F);
+        while (f1 - f0 > 1 && (fs[f1 - 1] - fs[f0]) > 0.15 * 0.5 * (fs[f1 - 1] + fs[f0])) --f1;
         cudaEvent_t e0, e1;
         OPEM_CUDA(cudaEventCreate(&e0));
         OPEM_CUDA(cudaEventCreate(&e1));
         OPEM_CUDA(cudaEventRecord(e0, P.ctx->stream));
         std::vector<System> sys;
         for (int d = 0; d < N; ++d)
-            for (int f = f0; f < f1; ++f) sys.push_back({freqs[f], d});
+            for (int f = f0; f < f1; ++f) sys.push_back({fs[f], d});
         BatchOut bo;
         solve_batch(P, sys, o, bo);
         OPEM_CUDA(cudaEventRecord(e1, P.ctx->stream));
@@ -1402,10 +1410,10 @@ void solve_sweep_mixed(Problem& P, int nfreq, const double* freqs, const opem_so
             }
             for (int k = 0; k < N; ++k) {
                 cd g;
-                port_gamma_Z_V(P, k, freqs[f], g, Z[k], V[k]);
+                port_gamma_Z_V(P, k, fs[f], g, Z[k], V[k]);
             }
-            S[f] = s_matrix_solve(N, Cp, Cm, V, Z, o.force_reciprocal != 0);
-            opem_solve_stats& s = st[f];
+            S[order[f]] = s_matrix_solve(N, Cp, Cm, V, Z, o.force_reciprocal != 0);
+            opem_solve_stats& s = st[order[f]];
             s.iterations = bo.inner_its;   // lockstep iterations of the batch
             s.outer = bo.outer;
             s.h_iterations = bo.h_its;
@@ -1413,6 +1421,7 @@ void solve_sweep_mixed(Problem& P, int nfreq, const double* freqs, const opem_so
             s.rnorm = bo.worst;
             s.seconds = ms * 1e-3 / nf;    // the batch's device time shared by its points
         }
+        f0 = f1;
     }
 }
 
