@@ -333,7 +333,7 @@ def run_ours(args, rank, world, local_rank):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * head["t_dev"] / head["steps"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "c64 inner / c128 refinement" if modes[0] == "mixed" else "c128",
+            "dtype": "c128 Krylov+SpMV, c64 block-Jacobi+polynomial" if modes[0] == "mixed" else "c128",
             "data": "synthetic", "config": config_dict(args),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "note": e2e_note},
             "gpu_launches": head["launches"],
