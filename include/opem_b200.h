@@ -130,10 +130,15 @@ int  opem_get_system_matrix(opem_problem prob, double freq, int d, double* vals)
 int  opem_context_launches(opem_context ctx, int64_t* out);
 /* Times the hot kernels of the FP64 path in isolation on the context stream with
  * CUDA events (A(freq) for driving set 0): reps launches each.  out receives
- * nkern*3 doubles: {ms per launch, algorithmic bytes per launch, launches}, for
- * kernels 0 = complex CSR SpMV, 1 = vertex-patch block apply, 2 = CGS2 step
- * against 64 Krylov vectors (dot + update).                                     */
+ * 12 doubles: {ms per launch, algorithmic bytes per launch, launches}, for
+ * kernels 0 = complex CSR SpMV, 1 = vertex-patch block apply, 2 = Gram-Schmidt
+ * dot products against 64 Krylov vectors, 3 = the matching vector update.       */
 int  opem_profile_kernels(opem_problem prob, double freq, int reps, double* out, int nout);
+/* The same for the batched sweep solver's kernels, nsys (1..32) systems near
+ * freq on driving set 0; out receives 15 doubles, kernels 0 = FP32 block apply
+ * for nsys systems, 1 = batched SpMV with FP32 operators and vectors, 2 = FP64
+ * operators and FP32 vectors, 3 = FP64 operators and vectors, 4 = patch sum.     */
+int  opem_profile_batch_kernels(opem_problem prob, double freq, int nsys, int reps, double* out, int nout);
 
 /* ---- allocation-free assembly (no counterpart in the reference) -------------
  * For callers that cannot allocate device memory at the point of use: a

@@ -62,6 +62,7 @@ SIGNATURES = [
     ("opem_get_system_matrix", C.c_int, [P, C.c_double, C.c_int, DP]),
     ("opem_context_launches", C.c_int, [P, I64P]),
     ("opem_profile_kernels", C.c_int, [P, C.c_double, C.c_int, DP, C.c_int]),
+    ("opem_profile_batch_kernels", C.c_int, [P, C.c_double, C.c_int, C.c_int, DP, C.c_int]),
     ("opem_system_matrix_noalloc", C.c_int, [P, C.c_double, C.c_int, DP]),
 ]
 

@@ -875,6 +875,16 @@ int opem_profile_kernels(opem_problem prob, double freq, int reps, double* out, 
     });
 }
 
+int opem_profile_batch_kernels(opem_problem prob, double freq, int nsys, int reps, double* out, int nout) {
+    if (!prob || !out || nout < 15 || reps <= 0 || !(freq > 0) || nsys < 1 || nsys > 32) return OPEM_ERR_ARG;
+    Problem& P = prob->p;
+    if (!P.assembled) return OPEM_ERR_STATE;
+    return guarded(P.ctx, [&] {
+        OPEM_CUDA(cudaSetDevice(P.ctx->device));
+        profile_batch(P, freq, nsys, reps, out);
+    });
+}
+
 // No counterpart in the reference.  See include/opem_b200.h for the contract.
 int opem_system_matrix_noalloc(opem_problem prob, double freq, int d, double* vals) {
     if (!prob || !vals || !(freq > 0)) return OPEM_ERR_ARG;

@@ -17,6 +17,7 @@
 // updates) uses system-major vectors, system r at r*ld.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "dense.h"
@@ -50,37 +51,104 @@ template <class T2> struct VC3 { T2 ce, ct, cs; };
 template <class T2> struct BC5 { T2 cc, ce, ct, cs, c1; };
 
 // ---------------------------------------------------------------------------
-// batched SpMV: y_il = A_r x_il for every system r (warp per row, lane = system);
-// Dirichlet rows of system r (PEC or its driven port) are set to zero.
+// batched SpMV: y_il = A_r x_il for every system r; Dirichlet rows of system r
+// (PEC or its driven port) are set to zero.
 // ---------------------------------------------------------------------------
 // T2: vector type (float2 or double2); T: matrix values, coefficients and
-// accumulation (the FP32-vector inner solve uses T = double: K and k0^2 eps M
-// nearly cancel on the slow modes, so they are combined in FP64).
-template <class T2, class T>
+// accumulation.  A group of W lanes owns one row (W = 16: two rows per warp
+// when R <= 16; W = 32 otherwise), lane = system.  The row's nonzeros are
+// staged SPMV_CH at a time in shared memory (column index and the real
+// operator values, coalesced loads), then every lane gathers its system's
+// entries of x for 8 nonzeros at once and accumulates the products with each
+// real operator separately (K x, Meps x, Mtand x, Msig x); the system's
+// coefficients are applied once per row.
+constexpr int SPMV_CH = 32;
+template <class T> struct SpmvStage;
+template <> struct SpmvStage<float> {
+    float4 v[SPMV_CH];   // K, Meps, Mtand, Msig
+    int col[SPMV_CH];
+};
+template <> struct SpmvStage<double> {
+    double2 km[SPMV_CH];   // K, Meps
+    double2 ts[SPMV_CH];   // Mtand, Msig
+    int col[SPMV_CH];
+};
+
+template <class T2, class T, bool HT, bool HS, int W>
 __global__ void __launch_bounds__(256) spmv_batch_kernel(
     int64_t n, int R, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ cols, const T* __restrict__ K,
     const T* __restrict__ Me, const T* __restrict__ Mt, const T* __restrict__ Ms,
     const VC3<typename CplxOf<T>::type>* __restrict__ coef, const T2* __restrict__ x, T2* __restrict__ y,
     const uint8_t* __restrict__ pec, const uint8_t* __restrict__ pm, const uint8_t* __restrict__ dsys) {
-    const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    VC3<typename CplxOf<T>::type> c;
+    constexpr int SUB = 32 / W;   // rows per warp
+    __shared__ SpmvStage<T> stage[8][SUB];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int sub = lane / W, sl = lane - sub * W;
+    SpmvStage<T>& st = stage[wid][sub];
+    const bool act = sl < R;
+    VC3<typename CplxOf<T>::type> c{};
     int d = 0;
-    if (lane < R) { c = coef[lane]; d = dsys[lane]; }
-    for (int64_t row = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); row < n; row += warps) {
-        T re = 0, im = 0;
-        if (lane < R) {
-            for (int32_t k = rowptr[row]; k < rowptr[row + 1]; ++k) {
-                T kv = K[k], mv = Me[k];
-                T ar = kv + c.ce.x * mv, ai = c.ce.y * mv;
-                if (Mt) { T t = Mt[k]; ar += c.ct.x * t; ai += c.ct.y * t; }
-                if (Ms) { T t = Ms[k]; ar += c.cs.x * t; ai += c.cs.y * t; }
-                T2 xv = x[(int64_t)cols[k] * R + lane];
-                re += ar * xv.x - ai * xv.y;
-                im += ar * xv.y + ai * xv.x;
+    if (act) { c = coef[sl]; d = dsys[sl]; }
+    const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t rb = (blockIdx.x * (int64_t)(blockDim.x >> 5) + wid) * SUB; rb < n; rb += nwarps * SUB) {
+        const int64_t row = rb + sub;
+        const bool rv = row < n;
+        const int32_t ks = rv ? rowptr[row] : 0;
+        const int len = rv ? rowptr[row + 1] - ks : 0;
+        int maxlen = len;
+        if (SUB == 2) maxlen = max(len, __shfl_xor_sync(0xffffffffu, len, 16));
+        T kr = 0, ki = 0, mr = 0, mi = 0, tr = 0, ti = 0, sr = 0, si = 0;
+        for (int c0 = 0; c0 < maxlen; c0 += SPMV_CH) {
+#pragma unroll
+            for (int w = 0; w < SPMV_CH / W; ++w) {
+                const int e = w * W + sl;
+                if (c0 + e < len) {
+                    const int32_t k = ks + c0 + e;
+                    st.col[e] = __ldg(cols + k);
+                    if constexpr (sizeof(T) == 4) {
+                        st.v[e] = make_float4(__ldg(K + k), __ldg(Me + k), HT ? __ldg(Mt + k) : 0.f,
+                                              HS ? __ldg(Ms + k) : 0.f);
+                    } else {
+                        st.km[e] = make_double2(__ldg(K + k), __ldg(Me + k));
+                        if (HT || HS) st.ts[e] = make_double2(HT ? __ldg(Mt + k) : 0.0, HS ? __ldg(Ms + k) : 0.0);
+                    }
+                }
             }
-            bool D = pec[row] || ((pm[row] >> d) & 1);
-            y[row * R + lane] = D ? Cx<T2>::make(0, 0) : Cx<T2>::make((typename Cx<T2>::R)re, (typename Cx<T2>::R)im);
+            __syncwarp();
+            const int cnt = min(SPMV_CH, len - c0);
+            if (act)
+                for (int j0 = 0; j0 < cnt; j0 += 8) {
+                    T2 xv[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+                        if (j0 + u < cnt) xv[u] = x[(int64_t)st.col[j0 + u] * R + sl];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+                        if (j0 + u < cnt) {
+                            const T xr = (T)xv[u].x, xi = (T)xv[u].y;
+                            T kv, mv, tv = 0, sv = 0;
+                            if constexpr (sizeof(T) == 4) {
+                                const float4 q = st.v[j0 + u];
+                                kv = q.x; mv = q.y; tv = q.z; sv = q.w;
+                            } else {
+                                const double2 q = st.km[j0 + u];
+                                kv = q.x; mv = q.y;
+                                if (HT || HS) { const double2 q2 = st.ts[j0 + u]; tv = q2.x; sv = q2.y; }
+                            }
+                            kr = fma(kv, xr, kr); ki = fma(kv, xi, ki);
+                            mr = fma(mv, xr, mr); mi = fma(mv, xi, mi);
+                            if (HT) { tr = fma(tv, xr, tr); ti = fma(tv, xi, ti); }
+                            if (HS) { sr = fma(sv, xr, sr); si = fma(sv, xi, si); }
+                        }
+                }
+            __syncwarp();
+        }
+        if (act && rv) {
+            T re = kr + c.ce.x * mr - c.ce.y * mi, im = ki + c.ce.x * mi + c.ce.y * mr;
+            if (HT) { re += c.ct.x * tr - c.ct.y * ti; im += c.ct.x * ti + c.ct.y * tr; }
+            if (HS) { re += c.cs.x * sr - c.cs.y * si; im += c.cs.x * si + c.cs.y * sr; }
+            const bool D = pec[row] || ((pm[row] >> d) & 1);
+            y[row * R + sl] = D ? Cx<T2>::make(0, 0) : Cx<T2>::make((typename Cx<T2>::R)re, (typename Cx<T2>::R)im);
         }
     }
 }
@@ -160,62 +228,200 @@ __global__ void il2sm_kernel(int64_t n, int R, const T2* __restrict__ in, O2* __
 // ---------------------------------------------------------------------------
 // batched vertex-patch block Jacobi (FP32 blocks), systems [r0, r0+Rd)
 // ---------------------------------------------------------------------------
-// One CTA (4 warps) per patch.  Each warp owns 32 block rows (lane = row) and
-// streams 32x32 tiles of the block through shared memory (coalesced global
-// reads, padded to avoid bank conflicts); each lane accumulates its row for up
-// to RC systems in registers while the system inputs are broadcast from shared
-// memory.  Lanes map to rows, not to systems, so no lane idles when a driving
-// set has fewer than 32 systems.
-constexpr int PA_RC = 16;
-__global__ void __launch_bounds__(128) patch_apply1_batch_kernel(
-    int npatch, const int32_t* __restrict__ pptr, const int32_t* __restrict__ pdofs, const int64_t* __restrict__ poff,
-    const float2* __restrict__ B, const float2* __restrict__ x, int R, int r0, int Rd, float2* __restrict__ t) {
-    extern __shared__ float2 smem[];
-    float2* rv = smem;                                 // s x Rd inputs
+// ---- bulk-copy (TMA) and mbarrier helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16) completing on bar
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait for phase `parity` of bar; false if it did not complete within the poll limit
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    for (int it = 0; it < (1 << 22); ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// The FP32 blocks are stored column-major per patch (element (a, b) at
+// off32[v] + b*s + a; off32[v] a multiple of 16 elements).  One CTA per patch.
+// The block streams through shared memory in panels of PA_PW columns (each
+// panel is contiguous in HBM) with bulk copies (TMA) into a PA_NS-stage ring
+// whose stages complete on mbarriers; thread 0 refills a stage as soon as the
+// CTA has consumed it.  The driving set's systems are split into G =
+// ceil(Rd / RC) groups of at most RC systems, the block rows into SA =
+// ceil(s / TR) slots of TR rows (slot j holds rows j, j + SA, ...).  Work item
+// i = (g, j), g = i / SA, j = i % SA, accumulates its TR rows of T = B X for the
+// RC systems of group g in registers, one item per thread (the launch has at
+// least SA * G threads).  The inputs X[b][group] are staged once per patch in
+// shared memory and read by all threads of a warp at the same address
+// (broadcast), 16 bytes at a time, each value feeding TR complex multiply-adds.
+// A stage that does not complete within the poll limit sets *err and the CTA
+// stops after waiting (again bounded) for its copies in flight.
+constexpr int PA_NS = 4;   // ring stages
+constexpr int PA_PW = 8;   // block columns per stage (even: keeps every panel 16-byte aligned)
+// bulk copy of block panel p (columns p*PA_PW ..) into ring stage p % PA_NS; the
+// size is rounded up to 16 bytes, so it may read 8 bytes past the block (the
+// FP32 block array ends with slack)
+__device__ __forceinline__ void pa_issue(int p, int s, int smax, const float2* Bv, float2* ring, uint64_t* bar) {
+    const int b0 = p * PA_PW, pw = min(PA_PW, s - b0);
+    const uint32_t bytes = (uint32_t)(((int64_t)pw * s * 8 + 15) & ~15ll);
+    uint64_t* bb = &bar[p % PA_NS];
+    mbar_expect_tx(bb, bytes);
+    bulk_g2s(ring + (size_t)(p % PA_NS) * PA_PW * smax, Bv + (int64_t)b0 * s, bytes, bb);
+}
+
+template <int RC, int TR>
+__global__ void __launch_bounds__(512, 1) patch_apply1_batch_kernel(
+    int npatch, int smax, const int32_t* __restrict__ pptr, const int32_t* __restrict__ pdofs,
+    const int64_t* __restrict__ off32, const float2* __restrict__ B, const float2* __restrict__ x, int R, int r0, int Rd,
+    float2* __restrict__ t, int* __restrict__ err) {
+    constexpr int RCP = (RC + 1) & ~1;   // group stride in shared memory (16-byte aligned groups)
+    constexpr int NV = RCP / 2;          // float4 loads per input row and group
+    __shared__ __align__(8) uint64_t bar[PA_NS];
+    extern __shared__ float4 smem4[];
     const int v = blockIdx.x;
     const int32_t p0 = pptr[v];
     const int s = pptr[v + 1] - p0;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    float2* tile = smem + (size_t)s * Rd + (size_t)w * 32 * 33;   // per-warp 32 x 33 tile
-    for (int e = threadIdx.x; e < s * Rd; e += blockDim.x) {
-        int b = e / Rd, l = e % Rd;
-        rv[e] = x[(int64_t)pdofs[p0 + b] * R + r0 + l];
+    const int G = (Rd + RC - 1) / RC;
+    const int RP = G * RCP;
+    float2* ring = reinterpret_cast<float2*>(smem4);          // PA_NS x (PA_PW * smax)
+    float2* xs = ring + (size_t)PA_NS * PA_PW * smax;           // s x RP
+    const float2* __restrict__ Bv = B + off32[v];
+    const int npanel = (s + PA_PW - 1) / PA_PW;
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < PA_NS; ++k) mbar_init(&bar[k], 1);
+        mbar_init_fence();
     }
     __syncthreads();
-    const float2* Bv = B + poff[v];
-    for (int a0 = w * 32; a0 < s; a0 += nw * 32) {
-        const int a = a0 + lane;
-        for (int c0 = 0; c0 < Rd; c0 += PA_RC) {
-            const int nc = min(PA_RC, Rd - c0);
-            float re[PA_RC], im[PA_RC];
+    if (threadIdx.x == 0)
+        for (int p = 0; p < min(PA_NS, npanel); ++p) pa_issue(p, s, smax, Bv, ring, bar);
+    // stage X (s rows x G groups) while the first panels are in flight
+    const int tot = s * RP;
+    for (int e0 = threadIdx.x; e0 < tot; e0 += 4 * blockDim.x) {
+        int64_t src[4];
 #pragma unroll
-            for (int q = 0; q < PA_RC; ++q) { re[q] = 0.f; im[q] = 0.f; }
-            for (int b0 = 0; b0 < s; b0 += 32) {
-                // stage rows a0..a0+31, columns b0..b0+31 (lane = column)
-                __syncwarp();
-                for (int rr = 0; rr < 32; ++rr) {
-                    float2 val = make_float2(0.f, 0.f);
-                    if (a0 + rr < s && b0 + lane < s) val = __ldcs(&Bv[(int64_t)(a0 + rr) * s + b0 + lane]);
-                    tile[rr * 33 + lane] = val;
-                }
-                __syncwarp();
-                const int bl = min(32, s - b0);
-                for (int l = 0; l < bl; ++l) {
-                    float2 m = tile[lane * 33 + l];
-                    const float2* xr = rv + (size_t)(b0 + l) * Rd + c0;
+        for (int u = 0; u < 4; ++u) {
+            const int e = e0 + u * blockDim.x;
+            src[u] = -1;
+            if (e < tot) {
+                const int b = e / RP, c = e - b * RP, g = c / RCP, q = c - g * RCP, l = g * RC + q;
+                if (q < RC && l < Rd) src[u] = (int64_t)pdofs[p0 + b] * R + r0 + l;
+            }
+        }
+        float2 val[4];
 #pragma unroll
-                    for (int q = 0; q < PA_RC; ++q) {
-                        if (q < nc) {
-                            float2 xv = xr[q];
-                            re[q] += m.x * xv.x - m.y * xv.y;
-                            im[q] += m.x * xv.y + m.y * xv.x;
+        for (int u = 0; u < 4; ++u) val[u] = src[u] >= 0 ? x[src[u]] : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (e0 + u * blockDim.x < tot) xs[e0 + u * blockDim.x] = val[u];
+    }
+    __syncthreads();
+    const int SA = (s + TR - 1) / TR;
+    const int i = threadIdx.x;
+    const bool work = i < SA * G;
+    const int g = work ? i / SA : 0, j = work ? i - g * SA : 0;
+    const float4* __restrict__ xg = reinterpret_cast<const float4*>(xs + g * RCP);
+    const int xstride = RP / 2;   // float4 per input row
+    float re[TR][RC], im[TR][RC];
+    int row[TR];
+#pragma unroll
+    for (int r = 0; r < TR; ++r) {
+        row[r] = min(j + r * SA, s - 1);   // rows past the block repeat the last row (not stored)
+#pragma unroll
+        for (int q = 0; q < RC; ++q) { re[r][q] = 0.f; im[r][q] = 0.f; }
+    }
+    bool ok = true;
+    int p = 0;
+    for (; p < npanel; ++p) {
+        if (!mbar_wait(&bar[p % PA_NS], (uint32_t)((p / PA_NS) & 1))) { ok = false; break; }
+        const int b0 = p * PA_PW, pw = min(PA_PW, s - b0);
+        const float2* panel = ring + (size_t)(p % PA_NS) * PA_PW * smax;
+        if (work) {
+#pragma unroll
+            for (int bb = 0; bb < PA_PW; ++bb) {
+                if (bb < pw) {
+                    float2 m[TR];
+#pragma unroll
+                    for (int r = 0; r < TR; ++r) m[r] = panel[bb * s + row[r]];
+                    const float4* xr = xg + (b0 + bb) * xstride;
+#pragma unroll
+                    for (int h = 0; h < NV; ++h) {
+                        const float4 xv = xr[h];
+#pragma unroll
+                        for (int r = 0; r < TR; ++r) {
+                            re[r][2 * h] = fmaf(m[r].x, xv.x, fmaf(-m[r].y, xv.y, re[r][2 * h]));
+                            im[r][2 * h] = fmaf(m[r].x, xv.y, fmaf(m[r].y, xv.x, im[r][2 * h]));
+                            if (2 * h + 1 < RC) {
+                                re[r][2 * h + 1] = fmaf(m[r].x, xv.z, fmaf(-m[r].y, xv.w, re[r][2 * h + 1]));
+                                im[r][2 * h + 1] = fmaf(m[r].x, xv.w, fmaf(m[r].y, xv.z, im[r][2 * h + 1]));
+                            }
                         }
                     }
                 }
             }
-            if (a < s)
-                for (int q = 0; q < nc; ++q) t[(int64_t)(p0 + a) * Rd + c0 + q] = make_float2(re[q], im[q]);
         }
+        __syncthreads();   // every thread is done with this stage
+        if (threadIdx.x == 0 && p + PA_NS < npanel) pa_issue(p + PA_NS, s, smax, Bv, ring, bar);
+    }
+    if (!ok) {
+        // a stage never completed: flag it and drain the copies this CTA issued (bounded)
+        if (threadIdx.x == 0) {
+            atomicExch(err, 1);
+            for (int q = p; q < min(npanel, p + PA_NS); ++q) mbar_wait(&bar[q % PA_NS], (uint32_t)((q / PA_NS) & 1));
+        }
+        return;
+    }
+    if (work) {
+        const int nc = min(RC, Rd - g * RC);
+#pragma unroll
+        for (int r = 0; r < TR; ++r) {
+            const int a = j + r * SA;
+            if (a < s) {
+                float2* out = t + (int64_t)(p0 + a) * Rd + g * RC;
+#pragma unroll
+                for (int q = 0; q < RC; ++q)
+                    if (q < nc) out[q] = make_float2(re[r][q], im[r][q]);
+            }
+        }
+    }
+}
+
+// systems per group for a driving set of Rd systems: at most 8, groups balanced
+static inline int patch_rc(int Rd) {
+    const int G = (Rd + 7) / 8;
+    return (Rd + G - 1) / G;
+}
+
+// FP64 row-major blocks -> FP32 column-major blocks at off32 (one CTA per patch)
+__global__ void blocks_to_f32_colmajor_kernel(int npatch, const int32_t* __restrict__ pptr,
+                                              const int64_t* __restrict__ poff, const int64_t* __restrict__ off32,
+                                              const double2* __restrict__ in, float2* __restrict__ out) {
+    const int v = blockIdx.x;
+    const int s = pptr[v + 1] - pptr[v];
+    const double2* src = in + poff[v];
+    float2* dst = out + off32[v];
+    for (int e = threadIdx.x; e < s * s; e += blockDim.x) {
+        const int a = e / s, b = e - a * s;
+        double2 val = src[e];
+        dst[b * s + a] = make_float2((float)val.x, (float)val.y);
     }
 }
 
@@ -681,6 +887,7 @@ struct Batch {
     std::vector<DBuf<BC5<float2>>> bc32;
     std::vector<DBuf<BC5<double2>>> bc64;
     DBuf<uint8_t> dsys, act;
+    DBuf<int> err;   // set by a kernel whose bounded wait ran out
     std::vector<uint8_t> h_act;
     // systems per driving set occupy lanes [r0[d], r0[d]+Rd[d])
     std::vector<int> r0, Rd;
@@ -704,9 +911,24 @@ static void spmv_batch(Batch& B, const T* K, const T* Me, const T* Mt, const T* 
                        const VC3<typename CplxOf<T>::type>* vc,
                        const std::vector<const BC5<typename CplxOf<T>::type>*>& bcs, const T2* x_il, T2* y_il) {
     Problem& P = B.P;
-    int grid = P.ctx->sm_count * 16;
-    spmv_batch_kernel<T2, T><<<grid, 256, 0, B.s>>>(B.n, B.R, P.d_rowptr.p, P.d_cols.p, K, Me, Mt, Ms, vc, x_il, y_il,
-                                                   P.d_pec.p, P.d_portmask.p, B.dsys.p);
+    const int grid = P.ctx->sm_count * 16;
+    const int32_t* rp = P.d_rowptr.p;
+    const int32_t* cl = P.d_cols.p;
+#define OPEM_SPMV_LAUNCH(HT_, HS_, W_)                                                                            \
+    spmv_batch_kernel<T2, T, HT_, HS_, W_><<<grid, 256, 0, B.s>>>(B.n, B.R, rp, cl, K, Me, Mt, Ms, vc, x_il, y_il, \
+                                                                  P.d_pec.p, P.d_portmask.p, B.dsys.p)
+    if (B.R <= 16) {
+        if (Mt && Ms) OPEM_SPMV_LAUNCH(true, true, 16);
+        else if (Mt) OPEM_SPMV_LAUNCH(true, false, 16);
+        else if (Ms) OPEM_SPMV_LAUNCH(false, true, 16);
+        else OPEM_SPMV_LAUNCH(false, false, 16);
+    } else {
+        if (Mt && Ms) OPEM_SPMV_LAUNCH(true, true, 32);
+        else if (Mt) OPEM_SPMV_LAUNCH(true, false, 32);
+        else if (Ms) OPEM_SPMV_LAUNCH(false, true, 32);
+        else OPEM_SPMV_LAUNCH(false, false, 32);
+    }
+#undef OPEM_SPMV_LAUNCH
     ++P.ctx->launches;
     for (size_t g = 0; g < P.groups.size(); ++g) {
         BGroup& G = P.groups[g];
@@ -730,9 +952,25 @@ static void to_sm(Batch& B, const T2* il, O2* sm, int64_t ld) {
     ++B.P.ctx->launches;
 }
 
+// FP32 block-Jacobi blocks of one driving set: column-major, block v at off32[v]
+// (a multiple of 16 elements, so every block and every even column starts
+// 16-byte aligned for the bulk copies), 16 elements of slack at the end.
 struct PatchSet32 {
     DBuf<float2> B;
+    DBuf<int64_t> off32;
 };
+
+static std::vector<int64_t> block_offsets32(const Topology& T) {
+    std::vector<int64_t> off(T.patch_ptr.size() - 1);
+    int64_t o = 0;
+    for (size_t v = 0; v + 1 < T.patch_ptr.size(); ++v) {
+        off[v] = o;
+        const int64_t sz = (int64_t)(T.patch_ptr[v + 1] - T.patch_ptr[v]);
+        o += (sz * sz + 15) / 16 * 16;
+    }
+    off.push_back(o + 16);   // total elements incl. slack
+    return off;
+}
 
 // FP32 block-Jacobi blocks for driving set d at frequency f (FP64 inversion, then rounded)
 static void build_patchset(Batch& B, double f, int d, PatchSet32& ps) {
@@ -747,10 +985,63 @@ static void build_patchset(Batch& B, double f, int d, PatchSet32& ps) {
     make_dmask(P, d, dm.p);
     DBuf<double2> B64;
     patch_blocks_fp64(P, A.p, dm.p, B64);
-    ps.B.alloc(B64.n);
-    f64_to_f32_kernel<<<vgrid(P), 256, 0, B.s>>>((int64_t)B64.n, B64.p, ps.B.p);
+    std::vector<int64_t> off = block_offsets32(P.topo);
+    ps.B.alloc((size_t)off.back());
+    OPEM_CUDA(cudaMemsetAsync(ps.B.p, 0, ps.B.bytes(), B.s));
+    off.pop_back();
+    ps.off32.upload(off, B.s);
+    blocks_to_f32_colmajor_kernel<<<P.npatch, 256, 0, B.s>>>(P.npatch, P.d_patch_ptr.p, P.d_patch_off.p, ps.off32.p,
+                                                            B64.p, ps.B.p);
     ++P.ctx->launches;
     OPEM_CUDA(cudaStreamSynchronize(B.s));
+}
+
+template <int RC, int TR>
+static void launch_patch_apply1(Problem& P, cudaStream_t s, const PatchSet32& ps, const float2* x_il, int R, int r0,
+                                int Rd, float2* t, int* err) {
+    const int G = (Rd + RC - 1) / RC;
+    const int RCP = (RC + 1) & ~1;
+    const int smax = P.topo.max_patch;
+    const size_t smem = ((size_t)PA_NS * PA_PW * smax + (size_t)smax * G * RCP) * sizeof(float2);
+    if (smem > 48 * 1024)
+        OPEM_CUDA(cudaFuncSetAttribute(patch_apply1_batch_kernel<RC, TR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    const int items = (smax + TR - 1) / TR * G;
+    const int threads = std::max(32, (items + 31) / 32 * 32);
+    if (threads > 512) throw OpemError(OPEM_ERR_UNSUPPORTED, "vertex patch too large for the batched block apply");
+    patch_apply1_batch_kernel<RC, TR><<<P.npatch, threads, smem, s>>>(P.npatch, smax, P.d_patch_ptr.p,
+                                                                      P.d_patch_dofs.p, ps.off32.p, ps.B.p, x_il, R,
+                                                                      r0, Rd, t, err);
+    ++P.ctx->launches;
+}
+
+
+template <int TR>
+static void patch_apply1_batch_tr(Problem& P, cudaStream_t s, const PatchSet32& ps, const float2* x_il, int R, int r0,
+                                  int Rd, float2* t, int* err) {
+    switch (patch_rc(Rd)) {
+        case 1: launch_patch_apply1<1, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
+        case 2: launch_patch_apply1<2, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
+        case 3: launch_patch_apply1<3, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
+        case 4: launch_patch_apply1<4, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
+        case 5: launch_patch_apply1<5, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
+        case 6: launch_patch_apply1<6, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
+        case 7: launch_patch_apply1<7, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
+        default: launch_patch_apply1<8, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
+    }
+}
+
+// t = blocks (x restricted to the patches) for systems [r0, r0+Rd) of x_il (R systems)
+static void patch_apply1_batch(Problem& P, cudaStream_t s, const PatchSet32& ps, const float2* x_il, int R, int r0,
+                               int Rd, float2* t, int* err) {
+    int tr = 1;   // rows per thread: 1 unless the patch needs more than 512 threads
+    const int G = (Rd + patch_rc(Rd) - 1) / patch_rc(Rd);
+    while (tr < 4 && (P.topo.max_patch + tr - 1) / tr * G > 512) tr *= 2;   // one work item per thread
+    switch (tr) {
+        case 1: patch_apply1_batch_tr<1>(P, s, ps, x_il, R, r0, Rd, t, err); break;
+        case 4: patch_apply1_batch_tr<4>(P, s, ps, x_il, R, r0, Rd, t, err); break;
+        default: patch_apply1_batch_tr<2>(P, s, ps, x_il, R, r0, Rd, t, err); break;
+    }
 }
 
 static void patch_apply_batch(Batch& B, const std::vector<PatchSet32>& sets, DBuf<float2>& t, const float2* x_il,
@@ -758,13 +1049,7 @@ static void patch_apply_batch(Batch& B, const std::vector<PatchSet32>& sets, DBu
     Problem& P = B.P;
     for (int d = 0; d < B.N; ++d) {
         if (B.Rd[d] == 0) continue;
-        size_t smem = ((size_t)P.topo.max_patch * B.Rd[d] + 4 * 32 * 33) * sizeof(float2);
-        if (smem > 48 * 1024)
-            OPEM_CUDA(cudaFuncSetAttribute(patch_apply1_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        patch_apply1_batch_kernel<<<P.npatch, 128, smem, B.s>>>(P.npatch, P.d_patch_ptr.p, P.d_patch_dofs.p,
-                                                                P.d_patch_off.p, sets[d].B.p, x_il, B.R, B.r0[d],
-                                                                B.Rd[d], t.p);
-        ++P.ctx->launches;
+        patch_apply1_batch(P, B.s, sets[d], x_il, B.R, B.r0[d], B.Rd[d], t.p, B.err.p);
         int64_t work = B.n * B.Rd[d];
         patch_apply2_batch_kernel<<<(unsigned)((work + 255) / 256), 256, 0, B.s>>>(
             B.n, P.d_d2p_ptr.p, P.d_d2p_idx.p, t.p, B.R, B.r0[d], B.Rd[d], P.d_pec.p, P.d_portmask.p, d, y_il);
@@ -823,8 +1108,26 @@ static std::vector<cd> leja(std::vector<cd> th) {
     return out;
 }
 
+// FP32 copies of the real volume operators (matrix products inside the FP32
+// polynomial preconditioner; the Arnoldi products stay FP64)
+static void ensure_f32_operators(Problem& P, cudaStream_t s) {
+    if (P.f_K.p) return;
+    const int64_t nnz = (int64_t)P.topo.cols.size();
+    const unsigned g = (unsigned)(P.ctx->sm_count * 4);
+    auto cvt = [&](const DBuf<double>& a, DBuf<float>& b) {
+        b.alloc(nnz);
+        real_to_f32_kernel<<<g, 256, 0, s>>>(nnz, a.p, b.p);
+        ++P.ctx->launches;
+    };
+    cvt(P.d_K, P.f_K);
+    cvt(P.d_Meps, P.f_Meps);
+    if (P.has_tand) cvt(P.d_Mtand, P.f_Mtand);
+    if (P.has_sig) cvt(P.d_Msig, P.f_Msig);
+    OPEM_CUDA(cudaGetLastError());
+}
+
 static int inner_solve(Batch& B, InnerWork& W, const std::vector<PatchSet32>& sets,
-                       const std::vector<const BC5<double2>*>& bc64, const std::vector<uint8_t>& active_in,
+                       const std::vector<const BC5<double2>*>& bc64, const std::vector<const BC5<float2>*>& bc32, const std::vector<uint8_t>& active_in,
                        double tol, int maxits, int poly_deg, int& its_out) {
     Problem& P = B.P;
     const int64_t n = B.n;
@@ -902,8 +1205,8 @@ static int inner_solve(Batch& B, InnerWork& W, const std::vector<PatchSet32>& se
                     ++P.ctx->launches;
                     if (i + 1 < npoly) {
                         patch_apply_batch(B, sets, W.t, W.pu.p, W.pt.p);
-                        spmv_batch<float2, double>(B, P.d_K.p, P.d_Meps.p, P.has_tand ? P.d_Mtand.p : nullptr,
-                                                   P.has_sig ? P.d_Msig.p : nullptr, B.vc64.p, bc64, W.pt.p, W.pt2.p);
+                        spmv_batch<float2, float>(B, P.f_K.p, P.f_Meps.p, P.has_tand ? P.f_Mtand.p : nullptr,
+                                                  P.has_sig ? P.f_Msig.p : nullptr, B.vc32.p, bc32, W.pt.p, W.pt2.p);
                         poly_sub_kernel<<<gp, 256, 0, B.s>>>(cnt, R, W.pc.p + (size_t)i * R, W.pt2.p, W.pu.p);
                         ++P.ctx->launches;
                     }
@@ -1151,23 +1454,11 @@ struct BatchOut {
     bool converged = true;
 };
 
-static void solve_batch(Problem& P, const std::vector<System>& systems, const opem_solver_opts& o, BatchOut& out) {
-    Batch B(P);
-    B.sys = systems;
-    B.R = (int)systems.size();
-    B.N = P.nports;
-    B.m = std::max(2, o.restart);
-    B.kd = std::max(0, std::min(o.deflate, B.m - 2));
-    const int R = B.R, N = B.N, m = B.m, kd = B.kd;
-    const int64_t n = B.n, nR = n * R;
-    // systems sorted by driving set -> contiguous lanes
-    B.r0.assign(N, 0);
-    B.Rd.assign(N, 0);
-    for (int r = 0; r < R; ++r) B.Rd[systems[r].d]++;
-    for (int d = 1; d < N; ++d) B.r0[d] = B.r0[d - 1] + B.Rd[d - 1];
-    for (int r = 1; r < R; ++r)
-        if (systems[r].d < systems[r - 1].d) throw OpemError(OPEM_ERR_ARG, "batch systems must be ordered by driving set");
-    // coefficient tables
+// Coefficient tables of the batch's systems (FP64 and FP32 copies), device pointers in bp32/bp64.
+static void setup_coefficients(Batch& B, const std::vector<System>& systems, std::vector<const BC5<float2>*>& bp32,
+                               std::vector<const BC5<double2>*>& bp64) {
+    Problem& P = B.P;
+    const int R = B.R;
     std::vector<VC3<float2>> v32(R);
     std::vector<VC3<double2>> v64(R);
     std::vector<std::vector<BC5<float2>>> b32(P.groups.size(), std::vector<BC5<float2>>(R));
@@ -1190,8 +1481,8 @@ static void solve_batch(Problem& P, const std::vector<System>& systems, const op
     }
     B.vc32.upload(v32, B.s);
     B.vc64.upload(v64, B.s);
-    std::vector<const BC5<float2>*> bp32;
-    std::vector<const BC5<double2>*> bp64;
+    bp32.clear();
+    bp64.clear();
     B.bc32.resize(P.groups.size());
     B.bc64.resize(P.groups.size());
     for (size_t g = 0; g < P.groups.size(); ++g) {
@@ -1202,6 +1493,37 @@ static void solve_batch(Problem& P, const std::vector<System>& systems, const op
     }
     B.dsys.upload(ds, B.s);
     B.act.alloc(RMAX);
+    B.err.alloc(1);
+    B.err.zero(B.s);
+}
+
+// raises if a kernel of the batch flagged a bounded wait that ran out
+static void check_batch_err(Batch& B) {
+    int e = 0;
+    OPEM_CUDA(cudaMemcpyAsync(&e, B.err.p, sizeof(int), cudaMemcpyDeviceToHost, B.s));
+    OPEM_CUDA(cudaStreamSynchronize(B.s));
+    if (e) throw OpemError(OPEM_ERR_TIMEOUT, "batched block apply: a bulk-copy stage did not complete");
+}
+
+static void solve_batch(Problem& P, const std::vector<System>& systems, const opem_solver_opts& o, BatchOut& out) {
+    Batch B(P);
+    B.sys = systems;
+    B.R = (int)systems.size();
+    B.N = P.nports;
+    B.m = std::max(2, o.restart);
+    B.kd = std::max(0, std::min(o.deflate, B.m - 2));
+    const int R = B.R, N = B.N, m = B.m, kd = B.kd;
+    const int64_t n = B.n, nR = n * R;
+    // systems sorted by driving set -> contiguous lanes
+    B.r0.assign(N, 0);
+    B.Rd.assign(N, 0);
+    for (int r = 0; r < R; ++r) B.Rd[systems[r].d]++;
+    for (int d = 1; d < N; ++d) B.r0[d] = B.r0[d - 1] + B.Rd[d - 1];
+    for (int r = 1; r < R; ++r)
+        if (systems[r].d < systems[r - 1].d) throw OpemError(OPEM_ERR_ARG, "batch systems must be ordered by driving set");
+    std::vector<const BC5<float2>*> bp32;
+    std::vector<const BC5<double2>*> bp64;
+    setup_coefficients(B, systems, bp32, bp64);
     // block-Jacobi sets: one per driving set, at the batch's middle frequency
     std::vector<PatchSet32> sets(N);
     double fmid = 0.5 * (systems.front().freq + systems.back().freq);
@@ -1283,7 +1605,8 @@ static void solve_batch(Problem& P, const std::vector<System>& systems, const op
         scale_sys_kernel<<<dim3(gy, R), 256, 0, B.s>>>(n, r64.p, nrm.p, B.act.p, W.rhs.p);
         ++P.ctx->launches;
         int its = 0;
-        inner_solve(B, W, sets, bp64, act, tol_in, o.maxits - inner_total, o.poly_degree, its);
+        inner_solve(B, W, sets, bp64, bp32, act, tol_in, o.maxits - inner_total, o.poly_degree, its);
+        check_batch_err(B);
         inner_total += its;
         OPEM_CUDA(cudaMemcpyAsync(B.act.p, act.data(), R, cudaMemcpyHostToDevice, B.s));
         refine_sys_kernel<<<dim3(gy, R), 256, 0, B.s>>>(n, W.d.p, nrm.p, B.act.p, x.p);
@@ -1356,6 +1679,7 @@ void solve_sweep_mixed(Problem& P, int nfreq, const double* freqs, const opem_so
                        std::vector<std::vector<cd>>& S, std::vector<opem_solve_stats>& st) {
     const int N = P.nports;
     int F = std::max(1, RMAX / std::max(1, N));
+    if (o.poly_degree > 1) ensure_f32_operators(P, P.ctx->stream);
     // Keep a batch's per-system Krylov storage (V and Z, FP64, (m+1) vectors each,
     // plus the rotation buffer and vectors) within half of the free device memory.
     {
@@ -1423,6 +1747,82 @@ void solve_sweep_mixed(Problem& P, int nfreq, const double* freqs, const opem_so
         }
         f0 = f1;
     }
+}
+
+
+// Times the batched-path kernels in isolation (CUDA events on the context
+// stream): R systems near frequency f on driving set 0.  out[3k+0] = ms per
+// launch, out[3k+1] = algorithmic bytes per launch, out[3k+2] = launches for
+//   k = 0  FP32 block apply (patch_apply1_batch_kernel, one driving set of R systems)
+//   k = 1  batched SpMV, FP32 operators and vectors (polynomial products)
+//   k = 2  batched SpMV, FP64 operators, FP32 vectors
+//   k = 3  batched SpMV, FP64 operators and vectors (Arnoldi products)
+//   k = 4  patch sum of the block apply (patch_apply2_batch_kernel)
+// The SpMV entries include the boundary-group kernels of the same product.
+void profile_batch(Problem& P, double f, int R, int reps, double* out) {
+    if (R < 1 || R > RMAX) throw OpemError(OPEM_ERR_ARG, "profile_batch: 1 <= nsys <= 32");
+    Batch B(P);
+    B.R = R;
+    B.N = std::max(1, P.nports);
+    B.r0.assign(B.N, 0);
+    B.Rd.assign(B.N, 0);
+    B.Rd[0] = R;
+    std::vector<System> systems(R);
+    for (int r = 0; r < R; ++r) systems[r] = {f * (1.0 + 0.002 * r), 0};
+    B.sys = systems;
+    std::vector<const BC5<float2>*> bp32;
+    std::vector<const BC5<double2>*> bp64;
+    setup_coefficients(B, systems, bp32, bp64);
+    ensure_f32_operators(P, B.s);
+    PatchSet32 set;
+    build_patchset(B, f, 0, set);
+    const int64_t n = B.n, nR = n * R, nnz = (int64_t)P.topo.cols.size();
+    const int64_t sum_s = (int64_t)P.topo.patch_dofs.size();
+    const double sum_s2 = (double)P.topo.patch_off.back();
+    DBuf<float2> x32(nR), y32(nR), t((size_t)sum_s * R);
+    DBuf<double2> x64(nR), y64(nR);
+    OPEM_CUDA(cudaMemsetAsync(x32.p, 0x3c, x32.bytes(), B.s));   // finite, nonzero inputs
+    OPEM_CUDA(cudaMemsetAsync(x64.p, 0x3c, x64.bytes(), B.s));
+    OPEM_CUDA(cudaMemsetAsync(t.p, 0, t.bytes(), B.s));
+    cudaEvent_t e0, e1;
+    OPEM_CUDA(cudaEventCreate(&e0));
+    OPEM_CUDA(cudaEventCreate(&e1));
+    auto timeit = [&](auto&& launch) {
+        for (int i = 0; i < 3; ++i) launch();
+        OPEM_CUDA(cudaEventRecord(e0, B.s));
+        for (int i = 0; i < reps; ++i) launch();
+        OPEM_CUDA(cudaEventRecord(e1, B.s));
+        OPEM_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        OPEM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        return (double)ms / reps;
+    };
+    const double nops = 2.0 + (P.has_tand ? 1 : 0) + (P.has_sig ? 1 : 0);
+    const double csr = (double)nnz * 4 + 4.0 * (n + 1) + 2.0 * n;   // cols, rowptr, masks
+    out[0] = timeit([&] { patch_apply1_batch(P, B.s, set, x32.p, R, 0, R, t.p, B.err.p); });
+    check_batch_err(B);
+    out[1] = sum_s2 * 8 + (double)sum_s * (4 + 2.0 * R * 8) + P.npatch * 12.0;
+    const double* Mt = P.has_tand ? P.d_Mtand.p : nullptr;
+    const double* Ms = P.has_sig ? P.d_Msig.p : nullptr;
+    out[3] = timeit([&] {
+        spmv_batch<float2, float>(B, P.f_K.p, P.f_Meps.p, P.has_tand ? P.f_Mtand.p : nullptr,
+                                  P.has_sig ? P.f_Msig.p : nullptr, B.vc32.p, bp32, x32.p, y32.p);
+    });
+    out[4] = csr + nnz * 4.0 * nops + 2.0 * nR * 8;
+    out[6] = timeit([&] { spmv_batch<float2, double>(B, P.d_K.p, P.d_Meps.p, Mt, Ms, B.vc64.p, bp64, x32.p, y32.p); });
+    out[7] = csr + nnz * 8.0 * nops + 2.0 * nR * 8;
+    out[9] = timeit([&] { spmv_batch<double2, double>(B, P.d_K.p, P.d_Meps.p, Mt, Ms, B.vc64.p, bp64, x64.p, y64.p); });
+    out[10] = csr + nnz * 8.0 * nops + 2.0 * nR * 16;
+    out[12] = timeit([&] {
+        patch_apply2_batch_kernel<<<(unsigned)((nR + 255) / 256), 256, 0, B.s>>>(
+            n, P.d_d2p_ptr.p, P.d_d2p_idx.p, t.p, R, 0, R, P.d_pec.p, P.d_portmask.p, 0, y32.p);
+        ++P.ctx->launches;
+    });
+    out[13] = (double)sum_s * (R * 8 + 4) + 4.0 * (n + 1) + 2.0 * n + nR * 8.0;
+    for (int k = 0; k < 5; ++k) out[3 * k + 2] = reps;
+    OPEM_CUDA(cudaGetLastError());
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
 }
 
 }  // namespace opem
