@@ -33,7 +33,14 @@ UNIT = "freq-points/s"
 C2_NDOF = 681312
 REF_ND2_EXPONENT = 1.53
 # ncu dram__bytes_read+write / algorithmic bytes of patch_apply1 (profiles/patch_apply1_16x8x40.md)
-TRAFFIC_RATIO_PATCH = 726.0 / 727.1   # reference's own ND2 timings: 103,146 -> 656,168 DOF, 18.45 -> 315.4 s
+TRAFFIC_RATIO_PATCH = 726.0 / 727.1
+# the same for patch_apply1_batch_kernel, 13 systems (profiles/patch_apply1_batch_16x8x40.md)
+TRAFFIC_RATIO_PATCH_BATCH = (376.8448 + 43.41632) / 459.063756
+# nominal FP32 FMA rate: 148 SMs x 128 lanes x 2 flops x 1.965 GHz
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+BATCH_KERNELS = ["patch_apply1_batch", "spmv_batch_f32", "spmv_batch_f64op_f32vec", "spmv_batch_f64",
+                 "patch_apply2_batch"]
+FP64_KERNELS = ["spmv_c64", "patch_apply1", "multidot64", "cgs_update64"]
 
 
 def parse():
@@ -51,6 +58,8 @@ def parse():
                     help="hex grid nx,ny,nz of the same box/slab/ND2 problem (profiling runs use a smaller one)")
     ap.add_argument("--rtol", type=float, default=1e-10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernels", action="store_true",
+                    help="only time the hot kernels in isolation (--steps launches each) and print them")
     return ap.parse_args()
 
 
@@ -198,6 +207,24 @@ def config_dict(args):
             "l2": "operator arrays ~1 GB > 126 MB L2, no flush", "parallelism": f"replicas x{args.gpus}"}
 
 
+def kernel_profile(F, freq, nsys, reps, _lib):
+    """CUDA-event times of the hot kernels in isolation (library stream): the
+    batched path's kernels for nsys systems and the FP64 path's kernels."""
+    out = {}
+    b = np.zeros(15)
+    rc = _lib.lib().opem_profile_batch_kernels(F.h, freq, nsys, reps, b.ctypes.data_as(_lib.DP), 15)
+    f = np.zeros(12)
+    rc2 = _lib.lib().opem_profile_kernels(F.h, freq, reps, f.ctypes.data_as(_lib.DP), 12)
+    for names, arr, code in ((BATCH_KERNELS, b, rc), (FP64_KERNELS, f, rc2)):
+        for k, nm in enumerate(names):
+            if code != 0:
+                out[nm] = {"error": code}
+                continue
+            ms, by = float(arr[3 * k]), float(arr[3 * k + 1])
+            out[nm] = {"ms": ms, "bytes": by, "GBps": by / (ms * 1e-3) / 1e9 if ms > 0 else None}
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -217,6 +244,12 @@ def run_ours(args, rank, world, local_rank):
     F = Fem3D(prob, context=ctx).assemble()
     info = F.info()
     N = F.nports
+    if args.kernels:
+        if rank == 0:
+            kern = kernel_profile(F, float(freqs[len(freqs) // 2]), args.batch, max(1, args.steps), _lib)
+            print(json.dumps({"mesh": args.mesh, "ndofs": info["ndofs"], "nnz": info["nnz"],
+                              "systems": args.batch, "kernels": kern}), flush=True)
+        return
     plain_o = default_opts(rtol=args.rtol, restart=args.restart, deflate=args.deflate, maxits=5000)
     mixed_o = default_opts(rtol=args.rtol, restart=args.restart, deflate=args.deflate, maxits=3000,
                            precision=_lib.PREC_MIXED, poly_degree=args.poly)
@@ -305,17 +338,29 @@ def run_ours(args, rank, world, local_rank):
                      "S": Sd, "freqs": sorted(Sd.keys()), "clocks": clk.summary()}
         if mode == modes[0]:
             clk_summary = clk.summary()
-    prof = np.zeros(12)
-    rc = _lib.lib().opem_profile_kernels(F.h, float(freqs[len(freqs) // 2]), 20, prof.ctypes.data_as(_lib.DP), 12)
+    kern = kernel_profile(F, float(freqs[len(freqs) // 2]), args.batch, 20, _lib)
     if rank != 0:
         return
     peak, peak_kind = peaks()
-    names = ["spmv_c64", "patch_apply1", "multidot64", "cgs_update64"]
-    kern = {names[k]: {"ms": prof[3 * k], "bytes": prof[3 * k + 1],
-                       "GBps": prof[3 * k + 1] / (prof[3 * k] * 1e-3) / 1e9 if prof[3 * k] > 0 else None}
-            for k in range(4)} if rc == 0 else {"error": rc}
-    dom = "patch_apply1"
-    ach = kern[dom]["GBps"] if rc == 0 else None
+    if modes[0] == "mixed":
+        # the batched path's dominant kernel: FP32 block apply for one driving set of `batch` systems
+        dom, dom_label, ratio = ("patch_apply1_batch", f"patch_apply1_batch_kernel (FP32 blocks x {args.batch} systems)",
+                                 TRAFFIC_RATIO_PATCH_BATCH)
+        traffic_src = ("ncu dram__bytes of the same kernel on the 16x8x40 case "
+                       "(profiles/patch_apply1_batch_16x8x40.md), scaled by algorithmic bytes")
+    else:
+        dom, dom_label, ratio = "patch_apply1", "patch_apply1_kernel (FP64 path)", TRAFFIC_RATIO_PATCH
+        traffic_src = ("ncu dram__bytes of the same kernel on the 16x8x40 case "
+                       "(profiles/patch_apply1_16x8x40.md), scaled by algorithmic bytes")
+    ach = kern[dom].get("GBps")
+    fp32 = None
+    if dom == "patch_apply1_batch" and kern[dom].get("ms"):
+        sum_s2 = float(info["sum_patch_sq"]) if "sum_patch_sq" in info else None
+        if sum_s2:
+            fl = sum_s2 * args.batch * 8.0
+            tf = fl / (kern[dom]["ms"] * 1e-3) / 1e12
+            fp32 = {"flops_per_launch": fl, "tflops": tf, "peak_tflops_nominal": FP32_PEAK_TFLOPS,
+                    "frac": tf / FP32_PEAK_TFLOPS}
     head = res[modes[0]]
     value = head["units"] / head["t_dev"]
     e2e = head["units"] / head["t_wall"]
@@ -339,11 +384,10 @@ def run_ours(args, rank, world, local_rank):
             "gpu_launches": head["launches"],
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "what": "device time until a frequency point's S is available (its whole batch in mixed mode)"},
-            "roofline": {"bound": "hbm", "kernel": dom + " (FP64 path)", "achieved": ach, "peak": peak, "unit": "GB/s",
+            "roofline": {"bound": "hbm", "kernel": dom_label, "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": (ach / peak) if ach else None,
-                         "traffic": (kern[dom]["bytes"] * TRAFFIC_RATIO_PATCH) if rc == 0 else None,
-                         "traffic_source": "ncu dram__bytes of the same kernel on the 16x8x40 case (profiles/patch_apply1_16x8x40.md), scaled by algorithmic bytes",
-                         "peak_kind": peak_kind, "kernels": kern},
+                         "traffic": (kern[dom]["bytes"] * ratio) if kern[dom].get("bytes") else None,
+                         "traffic_source": traffic_src, "peak_kind": peak_kind, "fp32_fma": fp32, "kernels": kern},
             "solver": {"iterations_per_step": head["its"], "outer_steps": head["outer"],
                        "converged": head["conv"], "patches": info["npatches"], "max_patch": info["max_patch"]},
             "clocks": clk_summary}

@@ -102,7 +102,8 @@ int  opem_problem_set_port_te(opem_problem prob, int port, const double* desc);
  * independent operators on the device.                                         */
 int  opem_problem_assemble(opem_problem prob);
 /* info[0]=ndofs, [1]=nnz, [2]=nports, [3]=npatches, [4]=max patch size, [5]=local dofs,
- * [6]=device bytes held.                                                        */
+ * [6]=device bytes held, [7]=sum of patch sizes, [8]=sum of squared patch sizes
+ * (entries of the block-Jacobi blocks).                                         */
 int  opem_problem_info(opem_problem prob, int64_t* info, int ninfo);
 
 /* ---- the per-frequency solve (fem3D::solve + calculateSplits + calculateS) ----

@@ -725,8 +725,11 @@ int opem_problem_assemble(opem_problem prob) {
 int opem_problem_info(opem_problem prob, int64_t* info, int ninfo) {
     if (!prob || !info) return OPEM_ERR_ARG;
     const Problem& P = prob->p;
-    int64_t v[7] = {P.topo.n, (int64_t)P.topo.cols.size(), P.nports, P.npatch, P.topo.max_patch, P.topo.ld, P.device_bytes()};
-    for (int i = 0; i < ninfo && i < 7; ++i) info[i] = v[i];
+    const int64_t sum_s = (int64_t)P.topo.patch_dofs.size();
+    const int64_t sum_s2 = P.topo.patch_off.empty() ? 0 : P.topo.patch_off.back();
+    int64_t v[9] = {P.topo.n, (int64_t)P.topo.cols.size(), P.nports, P.npatch, P.topo.max_patch, P.topo.ld,
+                    P.device_bytes(), sum_s, sum_s2};
+    for (int i = 0; i < ninfo && i < 9; ++i) info[i] = v[i];
     return OPEM_OK;
 }
 

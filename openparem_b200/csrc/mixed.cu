@@ -637,6 +637,28 @@ __global__ void nrm2_finish_kernel(int nparts, const double* __restrict__ part, 
     if (threadIdx.x == 0) out[r] = sqrt(sh[0]);
 }
 
+// Second-pass test of classical Gram-Schmidt (Daniel, Gragg, Kaufman and
+// Stewart): after the first pass, |w'|^2 = |w|^2 - sum_i |h_i|^2; the pass is
+// repeated only if |w'|^2 < |w|^2 / 2, i.e. if the projection removed more than
+// a factor 1/sqrt(2) of the norm (the estimate is small, and the pass therefore
+// repeated, exactly when cancellation makes it inaccurate).
+__global__ void reorth_decide_kernel(int R, int nvec, const double2* __restrict__ h, const double* __restrict__ nrm0,
+                                     const uint8_t* __restrict__ act, uint8_t* __restrict__ act2) {
+    for (int r = threadIdx.x; r < R; r += blockDim.x) {
+        uint8_t need = 0;
+        if (act[r]) {
+            double s = 0;
+            for (int i = 0; i < nvec; ++i) {
+                const double2 v = h[(int64_t)r * nvec + i];
+                s += v.x * v.x + v.y * v.y;
+            }
+            const double w2 = nrm0[r] * nrm0[r];
+            need = (w2 - s < 0.5 * w2) ? 1 : 0;
+        }
+        act2[r] = need;
+    }
+}
+
 // dst[r] = src[r] / nrm[r]; also H[r][col+1] = nrm[r]
 __global__ void normalize_sys_kernel(int64_t n, const double2* __restrict__ src, int64_t lds, const double* __restrict__ nrm,
                                      const uint8_t* __restrict__ act, double2* __restrict__ dst, int64_t ldd,
@@ -1081,7 +1103,8 @@ struct InnerWork {
     DBuf<float2> x_il32, z_il32, t;
     DBuf<float2> pu, py, pt, pt2, pc;   // polynomial preconditioner work (interleaved FP32) and 1/theta table
     DBuf<double2> H;     // per system (m+1) x m FP64 Hessenberg
-    DBuf<double> nrm, npart;
+    DBuf<double> nrm, npart, nrm0;
+    DBuf<uint8_t> act2;   // systems whose second Gram-Schmidt pass is needed
     DBuf<int> ncols;
 };
 
@@ -1219,13 +1242,21 @@ static int inner_solve(Batch& B, InnerWork& W, const std::vector<PatchSet32>& se
             il_f2d_kernel<<<vgrid(P), 256, 0, B.s>>>(n * R, W.z_il32.p, W.z_il64.p);
             ++P.ctx->launches;
             apply_A(W.z_il64.p, W.w.p);
+            // classical Gram-Schmidt; the second pass only for the systems whose
+            // first pass removed more than half of |w|^2 (decided on the device)
+            nrm_sys_f64(B, W.w.p, n, W.npart, W.nrm0.p, B.act.p);
             for (int pass = 0; pass < 2; ++pass) {
-                multidot_sys_kernel<<<dim3(nb, R), 256, 0, B.s>>>(n, j + 1, W.V.p, ldV, W.w.p, B.act.p, W.part.p);
-                finish_sys_kernel<<<dim3(j + 1, R), 256, 0, B.s>>>(nb, j + 1, W.part.p, B.act.p, W.h.p,
+                const uint8_t* ap = pass == 0 ? B.act.p : W.act2.p;
+                multidot_sys_kernel<<<dim3(nb, R), 256, 0, B.s>>>(n, j + 1, W.V.p, ldV, W.w.p, ap, W.part.p);
+                finish_sys_kernel<<<dim3(j + 1, R), 256, 0, B.s>>>(nb, j + 1, W.part.p, ap, W.h.p,
                                                                    W.H.p + (int64_t)j * (m + 1), ldH, pass);
                 update_sys_kernel<<<dim3(gy, R), 256, (j + 1) * sizeof(double2), B.s>>>(n, j + 1, W.V.p, ldV, W.h.p,
-                                                                                       B.act.p, W.w.p);
+                                                                                       ap, W.w.p);
                 P.ctx->launches += 3;
+                if (pass == 0) {
+                    reorth_decide_kernel<<<1, 32, 0, B.s>>>(R, j + 1, W.h.p, W.nrm0.p, B.act.p, W.act2.p);
+                    ++P.ctx->launches;
+                }
             }
             nrm_sys_f64(B, W.w.p, n, W.npart, W.nrm.p, B.act.p);
             normalize_sys_kernel<<<dim3(gy, R), 256, 0, B.s>>>(n, W.w.p, n, W.nrm.p, B.act.p,
@@ -1576,6 +1607,8 @@ static void solve_batch(Problem& P, const std::vector<System>& systems, const op
     W.d.alloc(nR);
     W.H.alloc((size_t)R * (m + 1) * m);
     W.nrm.alloc(RMAX);
+    W.nrm0.alloc(RMAX);
+    W.act2.alloc(RMAX);
     W.npart.alloc((size_t)RMAX * 64);
     W.ncols.alloc(RMAX);
     if (o.poly_degree > 1) {

@@ -126,9 +126,10 @@ class Fem3D:
         return self
 
     def info(self):
-        a = np.zeros(7, dtype=np.int64)
-        _chk(self.ctx.h, _lib.lib().opem_problem_info(self.h, a.ctypes.data_as(_lib.I64P), 7), "info")
-        keys = ["ndofs", "nnz", "nports", "npatches", "max_patch", "local_dofs", "device_bytes"]
+        a = np.zeros(9, dtype=np.int64)
+        _chk(self.ctx.h, _lib.lib().opem_problem_info(self.h, a.ctypes.data_as(_lib.I64P), 9), "info")
+        keys = ["ndofs", "nnz", "nports", "npatches", "max_patch", "local_dofs", "device_bytes", "sum_patch",
+                "sum_patch_sq"]
         return dict(zip(keys, (int(v) for v in a)))
 
     def solve(self, freq, opts=None, allow_not_converged=False):
