@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="both", choices=["plain", "mixed", "both"])
     ap.add_argument("--batch", type=int, default=13, help="frequency points per mixed-precision batch")
-    ap.add_argument("--poly", type=int, default=8, help="GMRES-polynomial preconditioner degree of the batched path")
+    ap.add_argument("--poly", type=int, default=16, help="GMRES-polynomial preconditioner degree of the batched path")
     ap.add_argument("--restart", type=int, default=100)
     ap.add_argument("--deflate", type=int, default=30)
     ap.add_argument("--mesh", default="24,12,60",

@@ -275,44 +275,45 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 // (broadcast), 16 bytes at a time, each value feeding TR complex multiply-adds.
 // A stage that does not complete within the poll limit sets *err and the CTA
 // stops after waiting (again bounded) for its copies in flight.
-constexpr int PA_NS = 4;   // ring stages
-constexpr int PA_PW = 8;   // block columns per stage (even: keeps every panel 16-byte aligned)
+constexpr int PA_NS = 3;    // ring stages
+constexpr int PA_PW = 16;   // block columns per stage (even: keeps every panel 16-byte aligned)
 // bulk copy of block panel p (columns p*PA_PW ..) into ring stage p % PA_NS; the
 // size is rounded up to 16 bytes, so it may read 8 bytes past the block (the
 // FP32 block array ends with slack)
+template <int NS, int PW>
 __device__ __forceinline__ void pa_issue(int p, int s, int smax, const float2* Bv, float2* ring, uint64_t* bar) {
-    const int b0 = p * PA_PW, pw = min(PA_PW, s - b0);
+    const int b0 = p * PW, pw = min(PW, s - b0);
     const uint32_t bytes = (uint32_t)(((int64_t)pw * s * 8 + 15) & ~15ll);
-    uint64_t* bb = &bar[p % PA_NS];
+    uint64_t* bb = &bar[p % NS];
     mbar_expect_tx(bb, bytes);
-    bulk_g2s(ring + (size_t)(p % PA_NS) * PA_PW * smax, Bv + (int64_t)b0 * s, bytes, bb);
+    bulk_g2s(ring + (size_t)(p % NS) * PW * smax, Bv + (int64_t)b0 * s, bytes, bb);
 }
 
-template <int RC, int TR>
+template <int RC, int TR, int NS = PA_NS, int PW = PA_PW>
 __global__ void __launch_bounds__(512, 1) patch_apply1_batch_kernel(
     int npatch, int smax, const int32_t* __restrict__ pptr, const int32_t* __restrict__ pdofs,
     const int64_t* __restrict__ off32, const float2* __restrict__ B, const float2* __restrict__ x, int R, int r0, int Rd,
     float2* __restrict__ t, int* __restrict__ err) {
     constexpr int RCP = (RC + 1) & ~1;   // group stride in shared memory (16-byte aligned groups)
     constexpr int NV = RCP / 2;          // float4 loads per input row and group
-    __shared__ __align__(8) uint64_t bar[PA_NS];
+    __shared__ __align__(8) uint64_t bar[NS];
     extern __shared__ float4 smem4[];
     const int v = blockIdx.x;
     const int32_t p0 = pptr[v];
     const int s = pptr[v + 1] - p0;
     const int G = (Rd + RC - 1) / RC;
     const int RP = G * RCP;
-    float2* ring = reinterpret_cast<float2*>(smem4);          // PA_NS x (PA_PW * smax)
-    float2* xs = ring + (size_t)PA_NS * PA_PW * smax;           // s x RP
+    float2* ring = reinterpret_cast<float2*>(smem4);          // NS x (PW * smax)
+    float2* xs = ring + (size_t)NS * PW * smax;           // s x RP
     const float2* __restrict__ Bv = B + off32[v];
-    const int npanel = (s + PA_PW - 1) / PA_PW;
+    const int npanel = (s + PW - 1) / PW;
     if (threadIdx.x == 0) {
-        for (int k = 0; k < PA_NS; ++k) mbar_init(&bar[k], 1);
+        for (int k = 0; k < NS; ++k) mbar_init(&bar[k], 1);
         mbar_init_fence();
     }
     __syncthreads();
     if (threadIdx.x == 0)
-        for (int p = 0; p < min(PA_NS, npanel); ++p) pa_issue(p, s, smax, Bv, ring, bar);
+        for (int p = 0; p < min(NS, npanel); ++p) pa_issue<NS, PW>(p, s, smax, Bv, ring, bar);
     // stage X (s rows x G groups) while the first panels are in flight
     const int tot = s * RP;
     for (int e0 = threadIdx.x; e0 < tot; e0 += 4 * blockDim.x) {
@@ -351,12 +352,12 @@ __global__ void __launch_bounds__(512, 1) patch_apply1_batch_kernel(
     bool ok = true;
     int p = 0;
     for (; p < npanel; ++p) {
-        if (!mbar_wait(&bar[p % PA_NS], (uint32_t)((p / PA_NS) & 1))) { ok = false; break; }
-        const int b0 = p * PA_PW, pw = min(PA_PW, s - b0);
-        const float2* panel = ring + (size_t)(p % PA_NS) * PA_PW * smax;
+        if (!mbar_wait(&bar[p % NS], (uint32_t)((p / NS) & 1))) { ok = false; break; }
+        const int b0 = p * PW, pw = min(PW, s - b0);
+        const float2* panel = ring + (size_t)(p % NS) * PW * smax;
         if (work) {
 #pragma unroll
-            for (int bb = 0; bb < PA_PW; ++bb) {
+            for (int bb = 0; bb < PW; ++bb) {
                 if (bb < pw) {
                     float2 m[TR];
 #pragma unroll
@@ -379,13 +380,13 @@ __global__ void __launch_bounds__(512, 1) patch_apply1_batch_kernel(
             }
         }
         __syncthreads();   // every thread is done with this stage
-        if (threadIdx.x == 0 && p + PA_NS < npanel) pa_issue(p + PA_NS, s, smax, Bv, ring, bar);
+        if (threadIdx.x == 0 && p + NS < npanel) pa_issue<NS, PW>(p + NS, s, smax, Bv, ring, bar);
     }
     if (!ok) {
         // a stage never completed: flag it and drain the copies this CTA issued (bounded)
         if (threadIdx.x == 0) {
             atomicExch(err, 1);
-            for (int q = p; q < min(npanel, p + PA_NS); ++q) mbar_wait(&bar[q % PA_NS], (uint32_t)((q / PA_NS) & 1));
+            for (int q = p; q < min(npanel, p + NS); ++q) mbar_wait(&bar[q % NS], (uint32_t)((q / NS) & 1));
         }
         return;
     }
@@ -1018,25 +1019,23 @@ static void build_patchset(Batch& B, double f, int d, PatchSet32& ps) {
     OPEM_CUDA(cudaStreamSynchronize(B.s));
 }
 
-template <int RC, int TR>
+template <int RC, int TR, int NS = PA_NS, int PW = PA_PW>
 static void launch_patch_apply1(Problem& P, cudaStream_t s, const PatchSet32& ps, const float2* x_il, int R, int r0,
                                 int Rd, float2* t, int* err) {
     const int G = (Rd + RC - 1) / RC;
     const int RCP = (RC + 1) & ~1;
     const int smax = P.topo.max_patch;
-    const size_t smem = ((size_t)PA_NS * PA_PW * smax + (size_t)smax * G * RCP) * sizeof(float2);
+    const size_t smem = ((size_t)NS * PW * smax + (size_t)smax * G * RCP) * sizeof(float2);
     if (smem > 48 * 1024)
-        OPEM_CUDA(cudaFuncSetAttribute(patch_apply1_batch_kernel<RC, TR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem));
+        OPEM_CUDA(cudaFuncSetAttribute(patch_apply1_batch_kernel<RC, TR, NS, PW>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int items = (smax + TR - 1) / TR * G;
     const int threads = std::max(32, (items + 31) / 32 * 32);
     if (threads > 512) throw OpemError(OPEM_ERR_UNSUPPORTED, "vertex patch too large for the batched block apply");
-    patch_apply1_batch_kernel<RC, TR><<<P.npatch, threads, smem, s>>>(P.npatch, smax, P.d_patch_ptr.p,
-                                                                      P.d_patch_dofs.p, ps.off32.p, ps.B.p, x_il, R,
-                                                                      r0, Rd, t, err);
+    patch_apply1_batch_kernel<RC, TR, NS, PW><<<P.npatch, threads, smem, s>>>(
+        P.npatch, smax, P.d_patch_ptr.p, P.d_patch_dofs.p, ps.off32.p, ps.B.p, x_il, R, r0, Rd, t, err);
     ++P.ctx->launches;
 }
-
 
 template <int TR>
 static void patch_apply1_batch_tr(Problem& P, cudaStream_t s, const PatchSet32& ps, const float2* x_il, int R, int r0,
