@@ -153,6 +153,123 @@ __global__ void __launch_bounds__(256) spmv_batch_kernel(
     }
 }
 
+// ---------------------------------------------------------------------------
+// element-by-element batched product of the volume operators (ND2: LD = 20):
+//   y_r = sum_e P_e^T ( (1/mu_e) Khat_e + c_{e,r} Mhat_e ) P_e x_r,
+//   c_{e,r} = c_eps,r eps_e + c_tand,r eps_e tan_d_e + c_sig,r sigma_e,
+// with Khat_e = sum_s gK_s Kref_s and Mhat_e = sum_s gM_s Mref_s the element's
+// geometric curl-curl and mass matrices (the same sums the CSR assembly
+// forms).  The CSR product gathers R x-entries per nonzero (29M gathers of
+// R*8 bytes on the 681k-DOF case, served by L2); per element the 20 DOF
+// segments are gathered once and used 20 times.
+// Pass 1 (ebe_elem_kernel): a group of W lanes per element (lane = system)
+// builds Khat_e and Mhat_e in shared memory, gathers x_e into registers and
+// writes the element's 20 x R outputs to ye.  Pass 2 (ebe_sum_kernel): every
+// DOF sums its elements' entries in the fixed order of its element list (so
+// the result is deterministic) and zeroes the Dirichlet rows of each system.
+// ---------------------------------------------------------------------------
+template <class T, int LD>
+struct EbeMats {
+    T K[LD * LD];
+    T M[LD * LD];
+};
+
+template <class T2, class T, int LD, int W>
+__global__ void __launch_bounds__(256) ebe_elem_kernel(int64_t ne, int R, const int32_t* __restrict__ edofs,
+                                                       const ElemGeo* __restrict__ geo,
+                                                       const double* __restrict__ ecoef, const double* __restrict__ ref,
+                                                       const VC3<typename CplxOf<T>::type>* __restrict__ coef,
+                                                       const T2* __restrict__ x, T2* __restrict__ ye) {
+    using C2 = typename CplxOf<T>::type;
+    constexpr int SUB = 32 / W;
+    constexpr int LL = LD * LD;
+    extern __shared__ float4 ebe_smem[];
+    T* sref = reinterpret_cast<T*>(ebe_smem);                        // Kref (6 LL) | Mref (6 LL)
+    EbeMats<T, LD>* mats = reinterpret_cast<EbeMats<T, LD>*>(sref + 12 * LL);   // [8 warps][SUB]
+    for (int t = threadIdx.x; t < 12 * LL; t += blockDim.x) sref[t] = (T)ref[t];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, sub = lane / W, sl = lane - sub * W;
+    EbeMats<T, LD>& E = mats[wid * SUB + sub];
+    const bool act = sl < R;
+    VC3<C2> c{};
+    if (act) c = coef[sl];
+    const int64_t ngroups = (int64_t)gridDim.x * (blockDim.x >> 5) * SUB;
+    for (int64_t e = (blockIdx.x * (int64_t)(blockDim.x >> 5) + wid) * SUB + sub; e - sub < ne; e += ngroups) {
+        const bool ev = e < ne;
+        if (ev) {
+            const ElemGeo g = geo[e];
+            T gk[6], gm[6];
+#pragma unroll
+            for (int q = 0; q < 6; ++q) { gk[q] = (T)g.gK[q]; gm[q] = (T)g.gM[q]; }
+            for (int t = sl; t < LL; t += W) {
+                T kv = 0, mv = 0;
+#pragma unroll
+                for (int q = 0; q < 6; ++q) {
+                    kv = fma(gk[q], sref[q * LL + t], kv);
+                    mv = fma(gm[q], sref[(6 + q) * LL + t], mv);
+                }
+                E.K[t] = kv;
+                E.M[t] = mv;
+            }
+        }
+        __syncwarp();
+        if (ev && act) {
+            const T imu = (T)ecoef[4 * e + 0], eps = (T)ecoef[4 * e + 1], epst = (T)ecoef[4 * e + 2],
+                    sig = (T)ecoef[4 * e + 3];
+            const T cer = c.ce.x * eps + c.ct.x * epst + c.cs.x * sig;
+            const T cei = c.ce.y * eps + c.ct.y * epst + c.cs.y * sig;
+            T xr[LD], xi[LD];
+#pragma unroll
+            for (int j = 0; j < LD; ++j) {
+                const T2 v = x[(int64_t)__ldg(edofs + e * LD + j) * R + sl];
+                xr[j] = (T)v.x;
+                xi[j] = (T)v.y;
+            }
+            T2* out = ye + (e * LD) * (int64_t)R + sl;
+#pragma unroll 2
+            for (int i = 0; i < LD; ++i) {
+                T kr = 0, ki = 0, mr = 0, mi = 0;
+#pragma unroll
+                for (int j = 0; j < LD; ++j) {
+                    const T kv = E.K[i * LD + j], mv = E.M[i * LD + j];
+                    kr = fma(kv, xr[j], kr); ki = fma(kv, xi[j], ki);
+                    mr = fma(mv, xr[j], mr); mi = fma(mv, xi[j], mi);
+                }
+                const T yr = imu * kr + cer * mr - cei * mi;
+                const T yi = imu * ki + cer * mi + cei * mr;
+                out[(int64_t)i * R] = Cx<T2>::make((typename Cx<T2>::R)yr, (typename Cx<T2>::R)yi);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+template <class T2, int W>
+__global__ void __launch_bounds__(256) ebe_sum_kernel(int64_t n, int R, int LD, const int32_t* __restrict__ d2e_ptr,
+                                                      const int32_t* __restrict__ d2e_elem,
+                                                      const uint8_t* __restrict__ d2e_loc, const T2* __restrict__ ye,
+                                                      T2* __restrict__ y, const uint8_t* __restrict__ pec,
+                                                      const uint8_t* __restrict__ pm, const uint8_t* __restrict__ dsys) {
+    constexpr int SUB = 32 / W;
+    const int lane = threadIdx.x & 31, sub = lane / W, sl = lane - sub * W;
+    if (sl >= R) return;
+    const int d = dsys[sl];
+    const int64_t ngroups = (int64_t)gridDim.x * (blockDim.x >> 5) * SUB;
+    for (int64_t row = (blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5)) * SUB + sub; row < n;
+         row += ngroups) {
+        typename Cx<T2>::R re = 0, im = 0;
+        if (!(pec[row] || ((pm[row] >> d) & 1))) {
+            const int32_t t0 = d2e_ptr[row], t1 = d2e_ptr[row + 1];
+            for (int32_t t = t0; t < t1; ++t) {
+                const T2 v = ye[((int64_t)d2e_elem[t] * LD + d2e_loc[t]) * R + sl];
+                re += v.x;
+                im += v.y;
+            }
+        }
+        y[row * R + sl] = Cx<T2>::make(re, im);
+    }
+}
+
 // boundary groups: y_il[row] += sum_u (coef . R_u) x_il[col_u] on the group's rows
 template <class T2, class T>
 __global__ void bnd_batch_kernel(int nrows, int R, const int32_t* __restrict__ brow, const int32_t* __restrict__ bptr,
@@ -911,12 +1028,18 @@ struct Batch {
     std::vector<DBuf<BC5<double2>>> bc64;
     DBuf<uint8_t> dsys, act;
     DBuf<int> err;   // set by a kernel whose bounded wait ran out
+    DBuf<float2> ye32;    // element outputs of the element-by-element product (FP32 vectors)
+    DBuf<double2> ye64;   // the same for FP64 vectors
     std::vector<uint8_t> h_act;
     // systems per driving set occupy lanes [r0[d], r0[d]+Rd[d])
     std::vector<int> r0, Rd;
     explicit Batch(Problem& P_) : P(P_), s(P_.ctx->stream), n(P_.topo.n) {}
     unsigned grid1(int64_t work) const { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, 65535)); }
 };
+
+template <class T2> DBuf<T2>& ebe_buffer(Batch& B);
+template <> DBuf<float2>& ebe_buffer<float2>(Batch& B) { return B.ye32; }
+template <> DBuf<double2>& ebe_buffer<double2>(Batch& B) { return B.ye64; }
 
 static unsigned vgrid(const Problem& P) { return (unsigned)(P.ctx->sm_count * 4); }
 
@@ -929,11 +1052,50 @@ static int md_blocks_sys(int sms, int R, int64_t n) {
     return (int)std::max<int64_t>(1, std::min<int64_t>({by_sm, by_len, 512}));
 }
 
+// Element-by-element volume product y_il = (K + c Meps + ...) x_il for every
+// system (Dirichlet rows zeroed); returns false where it does not apply (it
+// is built for 20-DOF ND2 elements), leaving the CSR product to the caller.
+template <class T2, class T>
+static bool ebe_volume(Batch& B, const VC3<typename CplxOf<T>::type>* vc, const T2* x_il, T2* y_il) {
+    Problem& P = B.P;
+    constexpr int LD = 20;
+    if (P.topo.ld != LD) return false;
+    const int64_t ne = (int64_t)P.topo.ne;
+    DBuf<T2>& ye = ebe_buffer<T2>(B);
+    const size_t need = (size_t)ne * LD * B.R;
+    if (ye.n < need) ye.alloc(need);
+    const int W = B.R <= 16 ? 16 : 32;
+    const size_t smem = ((size_t)12 * LD * LD + (size_t)8 * (32 / W) * 2 * LD * LD) * sizeof(T);
+    const int grid = P.ctx->sm_count * 4;
+    if (W == 16) {
+        OPEM_CUDA(cudaFuncSetAttribute(ebe_elem_kernel<T2, T, LD, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+        ebe_elem_kernel<T2, T, LD, 16><<<grid, 256, smem, B.s>>>(ne, B.R, P.d_elem_dofs.p, P.d_geo.p,
+                                                                P.d_elemcoef.p, P.d_ref.p, vc, x_il, ye.p);
+        ebe_sum_kernel<T2, 16><<<P.ctx->sm_count * 8, 256, 0, B.s>>>(B.n, B.R, LD, P.d_d2e_ptr.p, P.d_d2e_elem.p,
+                                                                     P.d_d2e_loc.p, ye.p, y_il, P.d_pec.p,
+                                                                     P.d_portmask.p, B.dsys.p);
+    } else {
+        OPEM_CUDA(cudaFuncSetAttribute(ebe_elem_kernel<T2, T, LD, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+        ebe_elem_kernel<T2, T, LD, 32><<<grid, 256, smem, B.s>>>(ne, B.R, P.d_elem_dofs.p, P.d_geo.p,
+                                                                P.d_elemcoef.p, P.d_ref.p, vc, x_il, ye.p);
+        ebe_sum_kernel<T2, 32><<<P.ctx->sm_count * 8, 256, 0, B.s>>>(B.n, B.R, LD, P.d_d2e_ptr.p, P.d_d2e_elem.p,
+                                                                     P.d_d2e_loc.p, ye.p, y_il, P.d_pec.p,
+                                                                     P.d_portmask.p, B.dsys.p);
+    }
+    P.ctx->launches += 2;
+    return true;
+}
+
 template <class T2, class T>
 static void spmv_batch(Batch& B, const T* K, const T* Me, const T* Mt, const T* Ms,
                        const VC3<typename CplxOf<T>::type>* vc,
                        const std::vector<const BC5<typename CplxOf<T>::type>*>& bcs, const T2* x_il, T2* y_il) {
     Problem& P = B.P;
+    if (ebe_volume<T2, T>(B, vc, x_il, y_il)) {
+        // boundary groups below
+    } else {
     const int grid = P.ctx->sm_count * 16;
     const int32_t* rp = P.d_rowptr.p;
     const int32_t* cl = P.d_cols.p;
@@ -953,6 +1115,7 @@ static void spmv_batch(Batch& B, const T* K, const T* Me, const T* Mt, const T* 
     }
 #undef OPEM_SPMV_LAUNCH
     ++P.ctx->launches;
+    }
     for (size_t g = 0; g < P.groups.size(); ++g) {
         BGroup& G = P.groups[g];
         int nrows = (int)G.h_brow.size();
@@ -1719,7 +1882,8 @@ void solve_sweep_mixed(Problem& P, int nfreq, const double* freqs, const opem_so
         OPEM_CUDA(cudaMemGetInfo(&freeb, &totb));
         const int m = std::max(2, o.restart), kd = std::max(0, std::min(o.deflate, m - 2));
         const double per_sys = (double)P.topo.n * sizeof(double2) * (2.0 * (m + 1) + (kd + 1) + 16) +
-                               (double)P.topo.patch_dofs.size() * sizeof(float2);
+                               (double)P.topo.patch_dofs.size() * sizeof(float2) +
+                               (double)P.topo.ne * P.topo.ld * (sizeof(float2) + sizeof(double2));
         const double fixed = (double)P.topo.patch_off.back() * (sizeof(float2) * N + sizeof(double2));
         int Fm = (int)std::floor((0.5 * (double)freeb - fixed) / (per_sys * std::max(1, N)));
         if (Fm < 1) throw OpemError(OPEM_ERR_NOMEM, "not enough device memory for one batched frequency point");
@@ -1831,6 +1995,14 @@ void profile_batch(Problem& P, double f, int R, int reps, double* out) {
     };
     const double nops = 2.0 + (P.has_tand ? 1 : 0) + (P.has_sig ? 1 : 0);
     const double csr = (double)nnz * 4 + 4.0 * (n + 1) + 2.0 * n;   // cols, rowptr, masks
+    // element-by-element product (ND2): element data, x read once, element outputs
+    // written and read back, DOF -> element lists, y written
+    const bool ebe = P.topo.ld == 20;
+    const double ne_ld = (double)P.topo.ne * P.topo.ld;
+    auto ebe_bytes = [&](double vb) {
+        return (double)P.topo.ne * (sizeof(ElemGeo) + 32.0) + ne_ld * 4 + nR * vb + 2.0 * ne_ld * R * vb +
+               ne_ld * 5 + 4.0 * (n + 1) + 2.0 * n + nR * vb;
+    };
     out[0] = timeit([&] { patch_apply1_batch(P, B.s, set, x32.p, R, 0, R, t.p, B.err.p); });
     check_batch_err(B);
     out[1] = sum_s2 * 8 + (double)sum_s * (4 + 2.0 * R * 8) + P.npatch * 12.0;
@@ -1840,11 +2012,11 @@ void profile_batch(Problem& P, double f, int R, int reps, double* out) {
         spmv_batch<float2, float>(B, P.f_K.p, P.f_Meps.p, P.has_tand ? P.f_Mtand.p : nullptr,
                                   P.has_sig ? P.f_Msig.p : nullptr, B.vc32.p, bp32, x32.p, y32.p);
     });
-    out[4] = csr + nnz * 4.0 * nops + 2.0 * nR * 8;
+    out[4] = ebe ? ebe_bytes(8) : csr + nnz * 4.0 * nops + 2.0 * nR * 8;
     out[6] = timeit([&] { spmv_batch<float2, double>(B, P.d_K.p, P.d_Meps.p, Mt, Ms, B.vc64.p, bp64, x32.p, y32.p); });
-    out[7] = csr + nnz * 8.0 * nops + 2.0 * nR * 8;
+    out[7] = ebe ? ebe_bytes(8) : csr + nnz * 8.0 * nops + 2.0 * nR * 8;
     out[9] = timeit([&] { spmv_batch<double2, double>(B, P.d_K.p, P.d_Meps.p, Mt, Ms, B.vc64.p, bp64, x64.p, y64.p); });
-    out[10] = csr + nnz * 8.0 * nops + 2.0 * nR * 16;
+    out[10] = ebe ? ebe_bytes(16) : csr + nnz * 8.0 * nops + 2.0 * nR * 16;
     out[12] = timeit([&] {
         patch_apply2_batch_kernel<<<(unsigned)((nR + 255) / 256), 256, 0, B.s>>>(
             n, P.d_d2p_ptr.p, P.d_d2p_idx.p, t.p, R, 0, R, P.d_pec.p, P.d_portmask.p, 0, y32.p);

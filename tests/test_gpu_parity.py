@@ -163,7 +163,7 @@ def test_deflated_restart_cuts_iterations(ctx):
     assert st1["iterations"] < st0["iterations"]
 
 
-@pytest.mark.parametrize("case", ["c1_nd1", "slab_nd2", "copper_nd2", "radcap_nd1", "slab_nd3"])
+@pytest.mark.parametrize("case", ["c1_nd1", "slab_nd2", "copper_nd2", "radcap_nd1", "slab_nd3", "perelem_nd2"])
 def test_mixed_sweep_matches_fp64_and_oracle(ctx, case):
     """Batched FP32-inner / FP64-refinement sweep vs the FP64 solve and the oracle:
     |dS| <= 1e-6 with outer rtol 1e-10."""
