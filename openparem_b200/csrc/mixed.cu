@@ -407,7 +407,7 @@ __device__ __forceinline__ void pa_issue(int p, int s, int smax, const float2* B
 }
 
 template <int RC, int TR, int NS = PA_NS, int PW = PA_PW>
-__global__ void __launch_bounds__(512, 1) patch_apply1_batch_kernel(
+__global__ void __launch_bounds__(512, TR == 1 ? 2 : 1) patch_apply1_batch_kernel(
     int npatch, int smax, const int32_t* __restrict__ pptr, const int32_t* __restrict__ pdofs,
     const int64_t* __restrict__ off32, const float2* __restrict__ B, const float2* __restrict__ x, int R, int r0, int Rd,
     float2* __restrict__ t, int* __restrict__ err) {
@@ -473,27 +473,32 @@ __global__ void __launch_bounds__(512, 1) patch_apply1_batch_kernel(
         const int b0 = p * PW, pw = min(PW, s - b0);
         const float2* panel = ring + (size_t)(p % NS) * PW * smax;
         if (work) {
+            // one block column: TR row entries against the group's RC staged inputs
+            auto step = [&](const float2* __restrict__ col, const float4* __restrict__ xr) {
+                float2 m[TR];
 #pragma unroll
-            for (int bb = 0; bb < PW; ++bb) {
-                if (bb < pw) {
-                    float2 m[TR];
+                for (int r = 0; r < TR; ++r) m[r] = col[row[r]];
 #pragma unroll
-                    for (int r = 0; r < TR; ++r) m[r] = panel[bb * s + row[r]];
-                    const float4* xr = xg + (b0 + bb) * xstride;
+                for (int h = 0; h < NV; ++h) {
+                    const float4 xv = xr[h];
 #pragma unroll
-                    for (int h = 0; h < NV; ++h) {
-                        const float4 xv = xr[h];
-#pragma unroll
-                        for (int r = 0; r < TR; ++r) {
-                            re[r][2 * h] = fmaf(m[r].x, xv.x, fmaf(-m[r].y, xv.y, re[r][2 * h]));
-                            im[r][2 * h] = fmaf(m[r].x, xv.y, fmaf(m[r].y, xv.x, im[r][2 * h]));
-                            if (2 * h + 1 < RC) {
-                                re[r][2 * h + 1] = fmaf(m[r].x, xv.z, fmaf(-m[r].y, xv.w, re[r][2 * h + 1]));
-                                im[r][2 * h + 1] = fmaf(m[r].x, xv.w, fmaf(m[r].y, xv.z, im[r][2 * h + 1]));
-                            }
+                    for (int r = 0; r < TR; ++r) {
+                        re[r][2 * h] = fmaf(m[r].x, xv.x, fmaf(-m[r].y, xv.y, re[r][2 * h]));
+                        im[r][2 * h] = fmaf(m[r].x, xv.y, fmaf(m[r].y, xv.x, im[r][2 * h]));
+                        if (2 * h + 1 < RC) {
+                            re[r][2 * h + 1] = fmaf(m[r].x, xv.z, fmaf(-m[r].y, xv.w, re[r][2 * h + 1]));
+                            im[r][2 * h + 1] = fmaf(m[r].x, xv.w, fmaf(m[r].y, xv.z, im[r][2 * h + 1]));
                         }
                     }
                 }
+            };
+            const float2* col = panel;
+            const float4* xr = xg + b0 * xstride;
+            if (pw == PW) {   // full panel: no per-column test
+#pragma unroll
+                for (int bb = 0; bb < PW; ++bb, col += s, xr += xstride) step(col, xr);
+            } else {
+                for (int bb = 0; bb < pw; ++bb, col += s, xr += xstride) step(col, xr);
             }
         }
         __syncthreads();   // every thread is done with this stage
