@@ -141,6 +141,39 @@ int  opem_profile_kernels(opem_problem prob, double freq, int reps, double* out,
  * operators and FP32 vectors, 3 = FP64 operators and vectors, 4 = patch sum.     */
 int  opem_profile_batch_kernels(opem_problem prob, double freq, int nsys, int reps, double* out, int nout);
 
+/* ---- serving loop (no counterpart in the reference: it solves one project per
+ * process, OpenParEM3D.cpp:494-555) -------------------------------------------
+ * A server runs solve requests from any number of caller threads on one GPU.
+ * It has `slots` slot contexts (each with its own CUDA stream), so up to that
+ * many requests run at once and their kernels overlap on the device.  A queued
+ * request starts when a slot is free and its estimated device footprint fits
+ * in hbm_budget_bytes minus the footprints of the running requests (<= 0: 90 %
+ * of the free device memory at creation); it always starts when nothing runs.
+ * The queue is scanned in arrival order and the first request that fits starts;
+ * requests on the same problem run one after another.  Operators stay resident:
+ * a problem is assembled by its first request (if the caller has not) and kept.
+ * A submitted problem belongs to the server until opem_server_wait has returned
+ * its request: the caller must not use or destroy it meanwhile.  Each result is
+ * the same as the same request run alone (every kernel reads only its own
+ * request's data; reductions are deterministic).                               */
+typedef struct opem_server_s* opem_server;
+int  opem_server_create(int device, int slots, int64_t hbm_budget_bytes, opem_server* out);
+/* Waits for running requests; queued ones are dropped (their wait would fail).  */
+int  opem_server_destroy(opem_server srv);
+/* Queues nfreq frequency points of prob (the same result layout as
+ * opem_solve_sweep); returns at once with the request id.                      */
+int  opem_server_submit(opem_server srv, opem_problem prob, int nfreq, const double* freqs,
+                        const opem_solver_opts* opts, int64_t* request_id);
+/* Blocks until the request is done (timeout_s < 0: no limit; OPEM_ERR_TIMEOUT if
+ * it is still queued or running when timeout_s runs out, and it can be waited
+ * for again).  Then S_out (nfreq*nports*nports complex), stats (nfreq) and
+ * times_out[3] = {submitted, started, finished} in seconds since the server
+ * was created are filled (any may be NULL) and the request's status returned.  */
+int  opem_server_wait(opem_server srv, int64_t request_id, double timeout_s, double* S_out,
+                      opem_solve_stats* stats, double* times_out);
+/* info[0]=queued, [1]=running, [2]=completed, [3]=admitted bytes, [4]=budget, [5]=slots. */
+int  opem_server_info(opem_server srv, int64_t* info, int ninfo);
+
 /* ---- allocation-free assembly (no counterpart in the reference) -------------
  * For callers that cannot allocate device memory at the point of use: a
  * process whose HBM is already claimed by another allocator (a PETSc or Kokkos

@@ -571,8 +571,6 @@ static int coefficients_fixed(const Problem& P, double freq, int d, VolCoef& vc,
 // ===========================================================================
 using namespace opem;
 
-struct opem_context_s { Context c; };
-struct opem_problem_s { Problem p; };
 
 template <class F>
 static int guarded(Context* ctx, F&& f) {

@@ -89,6 +89,7 @@ struct Problem {
     int nports = 0;
     std::vector<PortMode> modes;
     bool assembled = false;
+    int64_t ws_cap = 0;         // device bytes a batched sweep may take for its workspace (0: half of free)
 
     // device mesh/operator data
     DBuf<double> d_verts;
@@ -151,5 +152,11 @@ std::vector<cd> s_matrix_solve(int N, const std::vector<cd>& Cp, const std::vect
 // ---- batched mixed-precision sweep (mixed.cu)
 void solve_sweep_mixed(Problem& P, int nfreq, const double* freqs, const opem_solver_opts& o,
                        std::vector<std::vector<cd>>& S, std::vector<opem_solve_stats>& st);
+// device bytes a request (nfreq points with options o) needs beyond what P already holds
+double request_bytes_estimate(const Problem& P, int nfreq, const opem_solver_opts& o);
 
 }  // namespace opem
+
+// opaque handles of the C ABI
+struct opem_context_s { opem::Context c; };
+struct opem_problem_s { opem::Problem p; };

@@ -1890,7 +1890,8 @@ void solve_sweep_mixed(Problem& P, int nfreq, const double* freqs, const opem_so
                                (double)P.topo.patch_dofs.size() * sizeof(float2) +
                                (double)P.topo.ne * P.topo.ld * (sizeof(float2) + sizeof(double2));
         const double fixed = (double)P.topo.patch_off.back() * (sizeof(float2) * N + sizeof(double2));
-        int Fm = (int)std::floor((0.5 * (double)freeb - fixed) / (per_sys * std::max(1, N)));
+        const double avail = P.ws_cap > 0 ? std::min(0.5 * (double)freeb, (double)P.ws_cap) : 0.5 * (double)freeb;
+        int Fm = (int)std::floor((avail - fixed) / (per_sys * std::max(1, N)));
         if (Fm < 1) throw OpemError(OPEM_ERR_NOMEM, "not enough device memory for one batched frequency point");
         F = std::min(F, Fm);
     }
@@ -2032,6 +2033,37 @@ void profile_batch(Problem& P, double f, int R, int reps, double* out) {
     OPEM_CUDA(cudaGetLastError());
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+}
+
+
+// Device bytes a request needs on top of what the problem holds: its operators
+// if it is not assembled yet (pattern and patch sizes estimated from the DOF
+// count and order), and the solve workspace (the FP64 path's system matrix,
+// blocks and Krylov basis, or the batched path's per-system bases, FP32
+// blocks and element buffers for one batch).
+double request_bytes_estimate(const Problem& P, int nfreq, const opem_solver_opts& o) {
+    const double n = (double)P.topo.n;
+    const int ld = P.topo.ld;
+    const double nnz = P.assembled ? (double)P.topo.cols.size() : n * (ld <= 6 ? 16 : ld <= 20 ? 43 : 85);
+    const double ss2 = (P.assembled && !P.topo.patch_off.empty()) ? (double)P.topo.patch_off.back()
+                                                                   : n * (ld <= 6 ? 32 : ld <= 20 ? 240 : 1100);
+    const double ss = P.assembled ? (double)P.topo.patch_dofs.size() : n * (ld <= 6 ? 5 : ld <= 20 ? 6 : 7);
+    const double ne = (double)P.topo.ne;
+    const int N = std::max(1, P.assembled ? P.nports : 2);
+    double b = 0;
+    if (!P.assembled) b += nnz * 60 + n * 64 + ne * (ld * 8.0 + 160) + ss * 12;
+    const int m = std::max(2, o.restart), kd = std::max(0, std::min(o.deflate, m - 2));
+    b += nnz * 16 + ss2 * 16;   // one system matrix and one FP64 block set (block inversion)
+    if (o.precision == OPEM_PREC_MIXED) {
+        const int F = std::max(1, std::min(nfreq, RMAX / N));
+        const double R = (double)F * N;
+        b += nnz * 16;   // FP32 operator copies
+        b += R * (n * 16.0 * (2.0 * (m + 1) + (kd + 1) + 16) + ss * 8 + ne * ld * 24.0);
+        b += ss2 * 8.0 * N;
+    } else {
+        b += n * 16.0 * (m + 1 + 24) + ss2 * 16;
+    }
+    return b;
 }
 
 }  // namespace opem

@@ -195,3 +195,63 @@ class Fem3D:
             self.close()
         except Exception:
             pass
+
+
+class Server:
+    """Serving loop on one GPU (opem_server_*): requests from any thread are
+    admitted into ``slots`` concurrent slots by device-memory footprint and
+    run overlapped on the device; problems keep their operators resident.
+
+    A submitted Fem3D belongs to the server until its request has been waited
+    for; use it (or close it) only afterwards."""
+
+    def __init__(self, device=0, slots=4, hbm_budget_bytes=0):
+        self.h = C.c_void_p()
+        rc = _lib.lib().opem_server_create(int(device), int(slots), int(hbm_budget_bytes), C.byref(self.h))
+        if rc != _lib.OK:
+            raise OpemError(rc, "opem_server_create")
+        self._pending = {}
+
+    def submit(self, fem, freqs, opts=None):
+        freqs = np.ascontiguousarray(np.atleast_1d(freqs), dtype=np.float64)
+        o = opts if opts is not None else default_opts()
+        rid = C.c_int64()
+        rc = _lib.lib().opem_server_submit(self.h, fem.h, len(freqs), _dp(freqs), C.byref(o), C.byref(rid))
+        if rc != _lib.OK:
+            raise OpemError(rc, "opem_server_submit")
+        self._pending[rid.value] = (fem, len(freqs), freqs)
+        return rid.value
+
+    def wait(self, rid, timeout=-1.0):
+        """-> (S (nfreq, N, N) complex, stats list, {"submitted", "started", "finished"} seconds)."""
+        fem, nf, _ = self._pending[rid]
+        N = fem.nports
+        S = np.zeros(2 * N * N * nf)
+        st = (SolveStats * nf)()
+        t = np.zeros(3)
+        rc = _lib.lib().opem_server_wait(self.h, int(rid), float(timeout), _dp(S), st, _dp(t))
+        if rc == _lib.ERR_TIMEOUT:
+            raise TimeoutError(f"request {rid} not finished")
+        del self._pending[rid]
+        if rc not in (_lib.OK, _lib.ERR_NOT_CONVERGED):
+            raise OpemError(rc, f"request {rid}")
+        times = {"submitted": t[0], "started": t[1], "finished": t[2]}
+        return (S[0::2] + 1j * S[1::2]).reshape(nf, N, N), [s.as_dict() for s in st], times
+
+    def info(self):
+        a = np.zeros(6, dtype=np.int64)
+        _lib.lib().opem_server_info(self.h, a.ctypes.data_as(_lib.I64P), 6)
+        return dict(zip(["queued", "running", "completed", "admitted_bytes", "budget_bytes", "slots"],
+                        (int(v) for v in a)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.lib().opem_server_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

@@ -70,3 +70,21 @@ def test_context_without_device_reports_error():
     rc = _lib.lib().opem_context_create(0, C.byref(h))
     assert rc in (_lib.ERR_CUDA, _lib.ERR_ARG)
     assert not h.value
+
+
+def test_server_without_gpu_reports_status(lib):
+    """Server creation on a machine without a usable device fails with a status
+    code (no crash), and null arguments are rejected."""
+    from openparem_b200 import _lib
+    L = _lib.lib()
+    h = C.c_void_p()
+    assert L.opem_server_create(0, 0, 0, C.byref(h)) == _lib.ERR_ARG
+    assert L.opem_server_create(0, 2, 0, None) == _lib.ERR_ARG
+    assert L.opem_server_destroy(None) == _lib.ERR_ARG
+    assert L.opem_server_wait(None, 1, 0.0, None, None, None) == _lib.ERR_ARG
+    rc = L.opem_server_create(0, 2, 0, C.byref(h))
+    if rc == _lib.OK:   # a GPU is present after all
+        assert L.opem_server_destroy(h) == _lib.OK
+    else:
+        assert rc in (_lib.ERR_CUDA, _lib.ERR_ARG) and not h
+
