@@ -58,6 +58,11 @@ def parse():
                     help="hex grid nx,ny,nz of the same box/slab/ND2 problem (profiling runs use a smaller one)")
     ap.add_argument("--rtol", type=float, default=1e-10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve", choices=["c4", "c5"], default=None,
+                    help="serving-loop workloads instead of the sweep: c4 = 64 uneven sections submitted at "
+                         "once, c5 = Poisson stream of 20k-2M DOF requests (one GPU, not the headline line)")
+    ap.add_argument("--serve-requests", type=int, default=24, help="requests of the c5 stream")
+    ap.add_argument("--slots", type=int, default=4, help="concurrent requests of the serving loop")
     ap.add_argument("--kernels", action="store_true",
                     help="only time the hot kernels in isolation (--steps launches each) and print them")
     return ap.parse_args()
@@ -409,6 +414,66 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_serve(args, local_rank):
+    """Serving-loop workloads through opem_server_* (the batched solver per request):
+    freq-points/s over the whole stream (first submission to last completion),
+    per-request latency p50/p99, and |dS| of a subset against FP64 solves of the
+    same requests."""
+    import torch
+    from openparem_b200 import meshgen, Fem3D, Server, default_opts, _lib
+    from openparem_b200.fem3d import Context
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    if args.serve == "c4":
+        reqs = [(0.0, p, f) for p, f in meshgen.config4()]
+        workload = "64 uneven WR90 sections, L ~ U(10,60) mm, 3 hex/cm, ND1/ND2, 5 mm radiation cap, 1 freq each"
+    else:
+        reqs = meshgen.config5(count=args.serve_requests)
+        workload = (f"{len(reqs)} requests, Poisson 200 req/s, guides a ~ U(20,24) mm, L ~ U(10,60) mm, ND1-3, "
+                    "eps_r block U(1,10) tan_d 0.01, 1-4 freqs, 20k-2M DOF log-uniform")
+    ctx = Context(dev)
+    fems = [Fem3D(p, context=ctx) for _, p, _ in reqs]   # assembled by their first request
+    opts = default_opts(rtol=args.rtol, restart=args.restart, deflate=args.deflate, maxits=3000,
+                        precision=_lib.PREC_MIXED, poly_degree=args.poly)
+    srv = Server(dev, slots=args.slots)
+    t0 = time.perf_counter()
+    ids = []
+    for (ta, _, f), F in zip(reqs, fems):
+        dt = t0 + ta - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        ids.append(srv.submit(F, f, opts))
+    res = [srv.wait(i) for i in ids]
+    t_first = min(r[2]["submitted"] for r in res)
+    t_last = max(r[2]["finished"] for r in res)
+    points = sum(len(f) for _, _, f in reqs)
+    lat = np.array([r[2]["finished"] - r[2]["submitted"] for r in res]) * 1e3
+    conv = all(s["converged"] == 1 for r in res for s in r[1])
+    # |dS| against FP64 solves of the smallest requests (after the timed stream)
+    order = np.argsort([F.info()["ndofs"] for F in fems])[:6]
+    plain = default_opts(rtol=1e-12, restart=200, maxits=6000)
+    ids2 = [srv.submit(fems[k], reqs[k][2], plain) for k in order]
+    dS = max(float(np.abs(srv.wait(i)[0] - res[k][0]).max()) for i, k in zip(ids2, order))
+    info = srv.info()
+    srv.close()
+    dofs = [F.info()["ndofs"] for F in fems]
+    line = {"mode": "serve", "workload": args.serve, "metric": METRIC, "value": points / (t_last - t_first),
+            "unit": UNIT, "n_gpus": 1, "requests": len(reqs), "points": points, "slots": args.slots,
+            "seconds": t_last - t_first, "latency_ms": {"p50": float(np.percentile(lat, 50)),
+                                                         "p99": float(np.percentile(lat, 99)),
+                                                         "what": "request submitted -> S available"},
+            "converged": conv, "dS_vs_fp64": {"max": dS, "requests": len(order), "tolerance": 1e-6},
+            "dofs": {"min": int(min(dofs)), "max": int(max(dofs)), "total": int(sum(dofs))},
+            "config": {"workload": workload, "poly_degree": args.poly, "rtol": args.rtol,
+                       "budget_bytes": info["budget_bytes"]},
+            "data": "synthetic", "dtype": "c128 Krylov, c64 block-Jacobi+polynomial",
+            "per_request": [{"ndofs": int(d), "order": int(p["order"]), "freqs": len(f),
+                             "its": int(r[1][0]["iterations"]), "converged": all(x["converged"] == 1 for x in r[1]),
+                             "latency_ms": float(l)}
+                            for d, (_, p, f), r, l in zip(dofs, reqs, res, lat)]}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -416,6 +481,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.serve:
+        if rank == 0:
+            run_serve(args, local_rank)
         return
     if world > 1:
         import torch.distributed as dist

@@ -1892,6 +1892,8 @@ void solve_sweep_mixed(Problem& P, int nfreq, const double* freqs, const opem_so
         const double fixed = (double)P.topo.patch_off.back() * (sizeof(float2) * N + sizeof(double2));
         const double avail = P.ws_cap > 0 ? std::min(0.5 * (double)freeb, (double)P.ws_cap) : 0.5 * (double)freeb;
         int Fm = (int)std::floor((avail - fixed) / (per_sys * std::max(1, N)));
+        if (Fm < 1 && P.ws_cap > 0)   // the cap is advisory: fall back to the free memory for one point
+            Fm = (int)std::floor((0.5 * (double)freeb - fixed) / (per_sys * std::max(1, N)));
         if (Fm < 1) throw OpemError(OPEM_ERR_NOMEM, "not enough device memory for one batched frequency point");
         F = std::min(F, Fm);
     }

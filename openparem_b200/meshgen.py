@@ -156,5 +156,56 @@ def config3(nfreq=101, seed=0):
     return prob, np.linspace(8e9, 12e9, nfreq)
 
 
+def config4(seed=0, count=64):
+    """64 uneven waveguide sections: length U(10, 60) mm, 3 hex per cm in z over a
+    6x3 WR90 cross-section, ND1 or ND2 (coin flip), one frequency U(8, 12) GHz
+    each, a 5 mm air cap at z_max closed by a first-order radiation boundary
+    (the section's only port is at z = 0).  -> list of (problem, freqs)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        L = rng.uniform(10e-3, 60e-3)
+        nz = max(1, int(round(3 * L * 100)))
+        order = int(rng.integers(1, 3))
+        f = rng.uniform(8e9, 12e9)
+        prob = waveguide_problem(WR_A, WR_B, L, 6, 3, nz, order, ports=("zmin",), radiation_cap=5e-3, cap_nz=2)
+        out.append((prob, np.array([f])))
+    return out
+
+
+# DOF per hexahedron (Kuhn split) for ND1 / ND2 / ND3 on large structured grids
+DOF_PER_HEX = {1: 7.43, 2: 39.4, 3: 114.0}
+
+
+def config5(seed=0, count=24, rate=200.0, max_dofs=2_000_000):
+    """Serving stream: Poisson arrivals at `rate` req/s; each request is a guide of
+    width a ~ U(20, 24) mm (TE10 the only mode above cutoff in the air sections over
+    8-12 GHz), height a/2, length U(10, 60) mm, ND order 1-3, a dielectric block
+    eps_r ~ U(1, 10) with tan_d = 0.01 over the middle half of its length, 1-4
+    frequencies in 8-12 GHz, meshed for a DOF count drawn log-uniformly from 20k to
+    max_dofs.  The block's small loss damps the higher modes trapped in it (they do
+    not couple to the TE10 ports, so without loss their resonances make the system
+    singular).  -> list of (arrival time s, problem, freqs)."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for _ in range(count):
+        t += rng.exponential(1.0 / rate)
+        a = rng.uniform(20e-3, 24e-3)
+        b = a / 2
+        L = rng.uniform(10e-3, 60e-3)
+        order = int(rng.integers(1, 4))
+        er = rng.uniform(1.0, 10.0)
+        nf = int(rng.integers(1, 5))
+        freqs = np.sort(rng.uniform(8e9, 12e9, nf))
+        target = np.exp(rng.uniform(np.log(2e4), np.log(max_dofs)))
+        nhex = target / DOF_PER_HEX[order]
+        h = (a * b * L / nhex) ** (1.0 / 3.0)
+        nx, ny, nz = (max(2, int(round(d / h))) for d in (a, b, L))
+        prob = waveguide_problem(a, b, L, nx, ny, nz, order, slab=(0.25 * L, 0.75 * L, er, 0.01))
+        out.append((t, prob, freqs))
+    return out
+
+
 def small_case(order=1, nx=3, ny=2, nz=4, L=20e-3, **kw):
     return waveguide_problem(WR_A, WR_B, L, nx, ny, nz, order, **kw)
