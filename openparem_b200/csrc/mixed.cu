@@ -760,11 +760,17 @@ __global__ void nrm2_finish_kernel(int nparts, const double* __restrict__ part, 
     if (threadIdx.x == 0) out[r] = sqrt(sh[0]);
 }
 
-// Second-pass test of classical Gram-Schmidt (Daniel, Gragg, Kaufman and
-// Stewart): after the first pass, |w'|^2 = |w|^2 - sum_i |h_i|^2; the pass is
-// repeated only if |w'|^2 < |w|^2 / 2, i.e. if the projection removed more than
-// a factor 1/sqrt(2) of the norm (the estimate is small, and the pass therefore
-// repeated, exactly when cancellation makes it inaccurate).
+// Second-pass test of classical Gram-Schmidt: after the first pass,
+// |w'|^2 = |w|^2 - sum_i |h_i|^2 (Pythagoras, no extra read), and the pass is
+// repeated only if |w'| < eta |w| with eta = 0.01, i.e. only when the
+// projection cancelled all but 1 % of w and the first pass's result is
+// dominated by rounding (the estimate is small, and the pass therefore
+// repeated, exactly when cancellation makes it inaccurate).  The classical
+// Daniel-Gragg-Kaufman-Stewart threshold eta = 1/sqrt(2) asked for the second
+// pass at every step of the benchmark; with eta = 0.01 the Krylov step counts
+// are unchanged there, and each step loses at most ~u/eta of orthogonality.
+// Accuracy does not rest on it: the batched solver's FP64 outer refinement
+// checks the true residual.
 __global__ void reorth_decide_kernel(int R, int nvec, const double2* __restrict__ h, const double* __restrict__ nrm0,
                                      const uint8_t* __restrict__ act, uint8_t* __restrict__ act2) {
     for (int r = threadIdx.x; r < R; r += blockDim.x) {
@@ -776,7 +782,7 @@ __global__ void reorth_decide_kernel(int R, int nvec, const double2* __restrict_
                 s += v.x * v.x + v.y * v.y;
             }
             const double w2 = nrm0[r] * nrm0[r];
-            need = (w2 - s < 0.5 * w2) ? 1 : 0;
+            need = (w2 - s < 1e-4 * w2) ? 1 : 0;
         }
         act2[r] = need;
     }
@@ -1410,7 +1416,7 @@ static int inner_solve(Batch& B, InnerWork& W, const std::vector<PatchSet32>& se
             ++P.ctx->launches;
             apply_A(W.z_il64.p, W.w.p);
             // classical Gram-Schmidt; the second pass only for the systems whose
-            // first pass removed more than half of |w|^2 (decided on the device)
+            // first pass cancelled all but 1 % of |w| (decided on the device)
             nrm_sys_f64(B, W.w.p, n, W.npart, W.nrm0.p, B.act.p);
             for (int pass = 0; pass < 2; ++pass) {
                 const uint8_t* ap = pass == 0 ? B.act.p : W.act2.p;
