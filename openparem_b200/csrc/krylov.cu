@@ -611,7 +611,9 @@ static void patch_setup(Problem& P, PatchPrec& pc, const double2* A, const uint8
     while ((size_t)(smax + 1) * (smax + 1) * sizeof(double2) <= budget) ++smax;
     smax = std::min(smax, T.max_patch);
     smem = (size_t)smax * smax * sizeof(double2);
-    OPEM_CUDA(cudaFuncSetAttribute(patch_invert_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // the attribute is per function and process-wide: set the same device-wide value on
+    // every call (concurrent problems with other patch sizes must not lower it)
+    OPEM_CUDA(cudaFuncSetAttribute(patch_invert_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)budget));
     if (T.max_patch > 512) throw OpemError(OPEM_ERR_UNSUPPORTED, "vertex patch larger than 512 dofs");
     patch_invert_kernel<<<P.npatch, 256, smem, s>>>(P.npatch, P.d_patch_ptr.p, P.d_patch_off.p, pc.B.p, smax, pc.status.p); ++P.ctx->launches;
     OPEM_CUDA(cudaGetLastError());

@@ -19,6 +19,9 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "dense.h"
 #include "engine.h"
@@ -379,8 +382,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 
 // The FP32 blocks are stored column-major per patch (element (a, b) at
 // off32[v] + b*s + a; off32[v] a multiple of 16 elements).  One CTA per patch.
-// The block streams through shared memory in panels of PA_PW columns (each
-// panel is contiguous in HBM) with bulk copies (TMA) into a PA_NS-stage ring
+// The block streams through shared memory in panels of PW columns (each
+// panel is contiguous in HBM) with bulk copies (TMA) into an NS-stage ring
 // whose stages complete on mbarriers; thread 0 refills a stage as soon as the
 // CTA has consumed it.  The driving set's systems are split into G =
 // ceil(Rd / RC) groups of at most RC systems, the block rows into SA =
@@ -392,13 +395,15 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 // (broadcast), 16 bytes at a time, each value feeding TR complex multiply-adds.
 // A stage that does not complete within the poll limit sets *err and the CTA
 // stops after waiting (again bounded) for its copies in flight.
-constexpr int PA_NS = 3;    // ring stages
-constexpr int PA_PW = 16;   // block columns per stage (even: keeps every panel 16-byte aligned)
-// bulk copy of block panel p (columns p*PA_PW ..) into ring stage p % PA_NS; the
-// size is rounded up to 16 bytes, so it may read 8 bytes past the block (the
-// FP32 block array ends with slack)
-template <int NS, int PW>
-__device__ __forceinline__ void pa_issue(int p, int s, int smax, const float2* Bv, float2* ring, uint64_t* bar) {
+// The ring shape (NS stages of PW columns, NS <= PA_NS_MAX, PW a multiple of 4)
+// is a launch parameter picked per (patch size, systems) by a short timing run
+// on first use (tune_ring below).
+constexpr int PA_NS_MAX = 4;
+// bulk copy of block panel p (columns p*PW ..) into ring stage p % NS; the size is
+// rounded up to 16 bytes, so it may read 8 bytes past the block (the FP32 block
+// array ends with slack)
+__device__ __forceinline__ void pa_issue(int p, int NS, int PW, int s, int smax, const float2* Bv, float2* ring,
+                                         uint64_t* bar) {
     const int b0 = p * PW, pw = min(PW, s - b0);
     const uint32_t bytes = (uint32_t)(((int64_t)pw * s * 8 + 15) & ~15ll);
     uint64_t* bb = &bar[p % NS];
@@ -406,14 +411,14 @@ __device__ __forceinline__ void pa_issue(int p, int s, int smax, const float2* B
     bulk_g2s(ring + (size_t)(p % NS) * PW * smax, Bv + (int64_t)b0 * s, bytes, bb);
 }
 
-template <int RC, int TR, int NS = PA_NS, int PW = PA_PW>
+template <int RC, int TR>
 __global__ void __launch_bounds__(512, TR == 1 ? 2 : 1) patch_apply1_batch_kernel(
-    int npatch, int smax, const int32_t* __restrict__ pptr, const int32_t* __restrict__ pdofs,
+    int npatch, int smax, int NS, int PW, const int32_t* __restrict__ pptr, const int32_t* __restrict__ pdofs,
     const int64_t* __restrict__ off32, const float2* __restrict__ B, const float2* __restrict__ x, int R, int r0, int Rd,
     float2* __restrict__ t, int* __restrict__ err) {
     constexpr int RCP = (RC + 1) & ~1;   // group stride in shared memory (16-byte aligned groups)
     constexpr int NV = RCP / 2;          // float4 loads per input row and group
-    __shared__ __align__(8) uint64_t bar[NS];
+    __shared__ __align__(8) uint64_t bar[PA_NS_MAX];
     extern __shared__ float4 smem4[];
     const int v = blockIdx.x;
     const int32_t p0 = pptr[v];
@@ -430,7 +435,7 @@ __global__ void __launch_bounds__(512, TR == 1 ? 2 : 1) patch_apply1_batch_kerne
     }
     __syncthreads();
     if (threadIdx.x == 0)
-        for (int p = 0; p < min(NS, npanel); ++p) pa_issue<NS, PW>(p, s, smax, Bv, ring, bar);
+        for (int p = 0; p < min(NS, npanel); ++p) pa_issue(p, NS, PW, s, smax, Bv, ring, bar);
     // stage X (s rows x G groups) while the first panels are in flight
     const int tot = s * RP;
     for (int e0 = threadIdx.x; e0 < tot; e0 += 4 * blockDim.x) {
@@ -494,15 +499,17 @@ __global__ void __launch_bounds__(512, TR == 1 ? 2 : 1) patch_apply1_batch_kerne
             };
             const float2* col = panel;
             const float4* xr = xg + b0 * xstride;
-            if (pw == PW) {   // full panel: no per-column test
+            if (pw == PW) {   // full panel: no per-column test (PW is a multiple of 4)
+                for (int bb = 0; bb < PW; bb += 4) {
 #pragma unroll
-                for (int bb = 0; bb < PW; ++bb, col += s, xr += xstride) step(col, xr);
+                    for (int u = 0; u < 4; ++u, col += s, xr += xstride) step(col, xr);
+                }
             } else {
                 for (int bb = 0; bb < pw; ++bb, col += s, xr += xstride) step(col, xr);
             }
         }
         __syncthreads();   // every thread is done with this stage
-        if (threadIdx.x == 0 && p + NS < npanel) pa_issue<NS, PW>(p + NS, s, smax, Bv, ring, bar);
+        if (threadIdx.x == 0 && p + NS < npanel) pa_issue(p + NS, NS, PW, s, smax, Bv, ring, bar);
     }
     if (!ok) {
         // a stage never completed: flag it and drain the copies this CTA issued (bounded)
@@ -1193,36 +1200,100 @@ static void build_patchset(Batch& B, double f, int d, PatchSet32& ps) {
     OPEM_CUDA(cudaStreamSynchronize(B.s));
 }
 
-template <int RC, int TR, int NS = PA_NS, int PW = PA_PW>
+struct Ring { int ns, pw; };
+
+template <int RC, int TR>
 static void launch_patch_apply1(Problem& P, cudaStream_t s, const PatchSet32& ps, const float2* x_il, int R, int r0,
-                                int Rd, float2* t, int* err) {
+                                int Rd, float2* t, int* err, Ring ring) {
     const int G = (Rd + RC - 1) / RC;
     const int RCP = (RC + 1) & ~1;
     const int smax = P.topo.max_patch;
-    const size_t smem = ((size_t)NS * PW * smax + (size_t)smax * G * RCP) * sizeof(float2);
-    if (smem > 48 * 1024)
-        OPEM_CUDA(cudaFuncSetAttribute(patch_apply1_batch_kernel<RC, TR, NS, PW>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const size_t smem = ((size_t)ring.ns * ring.pw * smax + (size_t)smax * G * RCP) * sizeof(float2);
+    if (smem > 48 * 1024) {
+        // per function and process-wide: always the same device-wide value, so that
+        // concurrent launches with other ring shapes or patch sizes cannot lower it
+        int optin = 0;
+        OPEM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, P.ctx->device));
+        OPEM_CUDA(cudaFuncSetAttribute(patch_apply1_batch_kernel<RC, TR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       optin - 1024));
+    }
     const int items = (smax + TR - 1) / TR * G;
     const int threads = std::max(32, (items + 31) / 32 * 32);
     if (threads > 512) throw OpemError(OPEM_ERR_UNSUPPORTED, "vertex patch too large for the batched block apply");
-    patch_apply1_batch_kernel<RC, TR, NS, PW><<<P.npatch, threads, smem, s>>>(
-        P.npatch, smax, P.d_patch_ptr.p, P.d_patch_dofs.p, ps.off32.p, ps.B.p, x_il, R, r0, Rd, t, err);
+    patch_apply1_batch_kernel<RC, TR><<<P.npatch, threads, smem, s>>>(P.npatch, smax, ring.ns, ring.pw,
+                                                                      P.d_patch_ptr.p, P.d_patch_dofs.p, ps.off32.p,
+                                                                      ps.B.p, x_il, R, r0, Rd, t, err);
     ++P.ctx->launches;
+}
+
+// Ring shape autotuner: on the first call for a (device, largest patch, systems)
+// combination, every candidate shape that fits in shared memory is run once to
+// warm up and twice timed (CUDA events on the caller's stream, the call's own
+// inputs; the apply overwrites its output, and every shape gives bitwise the
+// same result), and the fastest is kept for the life of the process.
+static std::mutex g_ring_mu;
+static std::map<std::tuple<int, int, int>, Ring> g_ring_choice;
+
+template <class Launch>
+static Ring tune_ring(Problem& P, cudaStream_t s, int Rd, int RC, int G, Launch&& launch) {
+    const auto key = std::make_tuple(P.ctx->device, P.topo.max_patch, Rd);
+    {
+        std::lock_guard<std::mutex> lk(g_ring_mu);
+        auto it = g_ring_choice.find(key);
+        if (it != g_ring_choice.end()) return it->second;
+    }
+    static const Ring cands[] = {{3, 16}, {4, 8}, {2, 32}, {3, 8}, {2, 8}, {4, 4}};
+    int optin = 0;
+    OPEM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, P.ctx->device));
+    const int RCP = (RC + 1) & ~1;
+    cudaEvent_t e0, e1;
+    OPEM_CUDA(cudaEventCreate(&e0));
+    OPEM_CUDA(cudaEventCreate(&e1));
+    Ring best{0, 0};
+    float best_ms = 1e30f;
+    for (const Ring& c : cands) {
+        const size_t smem = ((size_t)c.ns * c.pw * P.topo.max_patch + (size_t)P.topo.max_patch * G * RCP) * 8;
+        if (smem > (size_t)optin - 1024) continue;
+        launch(c);
+        OPEM_CUDA(cudaEventRecord(e0, s));
+        launch(c);
+        launch(c);
+        OPEM_CUDA(cudaEventRecord(e1, s));
+        OPEM_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        OPEM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best_ms) { best_ms = ms; best = c; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (best.ns == 0) throw OpemError(OPEM_ERR_UNSUPPORTED, "vertex patch too large for the batched block apply");
+    std::lock_guard<std::mutex> lk(g_ring_mu);
+    g_ring_choice[key] = best;
+    return best;
+}
+
+template <int RC, int TR>
+static void launch_patch_apply1_tuned(Problem& P, cudaStream_t s, const PatchSet32& ps, const float2* x_il, int R,
+                                      int r0, int Rd, float2* t, int* err) {
+    const int G = (Rd + RC - 1) / RC;
+    const Ring ring = tune_ring(P, s, Rd, RC, G, [&](Ring c) {
+        launch_patch_apply1<RC, TR>(P, s, ps, x_il, R, r0, Rd, t, err, c);
+    });
+    launch_patch_apply1<RC, TR>(P, s, ps, x_il, R, r0, Rd, t, err, ring);
 }
 
 template <int TR>
 static void patch_apply1_batch_tr(Problem& P, cudaStream_t s, const PatchSet32& ps, const float2* x_il, int R, int r0,
                                   int Rd, float2* t, int* err) {
     switch (patch_rc(Rd)) {
-        case 1: launch_patch_apply1<1, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
-        case 2: launch_patch_apply1<2, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
-        case 3: launch_patch_apply1<3, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
-        case 4: launch_patch_apply1<4, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
-        case 5: launch_patch_apply1<5, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
-        case 6: launch_patch_apply1<6, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
-        case 7: launch_patch_apply1<7, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
-        default: launch_patch_apply1<8, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
+        case 1: launch_patch_apply1_tuned<1, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
+        case 2: launch_patch_apply1_tuned<2, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
+        case 3: launch_patch_apply1_tuned<3, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
+        case 4: launch_patch_apply1_tuned<4, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
+        case 5: launch_patch_apply1_tuned<5, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
+        case 6: launch_patch_apply1_tuned<6, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
+        case 7: launch_patch_apply1_tuned<7, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
+        default: launch_patch_apply1_tuned<8, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
     }
 }
 
