@@ -1995,6 +1995,25 @@ void solve_sweep_mixed(Problem& P, int nfreq, const double* freqs, const opem_so
             for (int f = f0; f < f1; ++f) sys.push_back({fs[f], d});
         BatchOut bo;
         solve_batch(P, sys, o, bo);
+        if (!bo.converged && o.restart < 1024) {
+            // Restart escalation: vertex-patch block Jacobi is weak on under-resolved,
+            // strongly indefinite meshes, where a short restart cycle stagnates (a 26k-DOF
+            // ND3 guide with an eps_r 7.6 block: GMRES-DR(100, 30) stalls for 3000 steps,
+            // (300, 60) converges in 222).  Retry the batch once with a 3x longer cycle
+            // and twice the deflation space if its Krylov bases fit in half of the free memory.
+            opem_solver_opts o2 = o;
+            o2.restart = std::min(1024, 3 * o.restart);
+            o2.deflate = std::min(2 * std::max(o.deflate, 1), o2.restart - 2);
+            size_t freeb = 0, totb = 0;
+            OPEM_CUDA(cudaMemGetInfo(&freeb, &totb));
+            const double need = (double)sys.size() * P.topo.n * sizeof(double2) *
+                                (2.0 * (o2.restart + 1) + (o2.deflate + 1) + 16);
+            if (need < 0.5 * (double)freeb) {
+                BatchOut bo2;
+                solve_batch(P, sys, o2, bo2);
+                if (bo2.converged || bo2.worst < bo.worst) bo = std::move(bo2);
+            }
+        }
         OPEM_CUDA(cudaEventRecord(e1, P.ctx->stream));
         OPEM_CUDA(cudaEventSynchronize(e1));
         float ms = 0;
