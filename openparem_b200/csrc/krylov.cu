@@ -29,11 +29,24 @@ __global__ void spmv_c64_kernel(int64_t n, const int32_t* __restrict__ rowptr, c
     int lane = (int)(t % TPR);
     double re = 0, im = 0;
     if (r < n) {
-        for (int32_t k = rowptr[r] + lane; k < rowptr[r + 1]; k += TPR) {
-            double2 a = A[k];
-            double2 v = x[cols[k]];
-            re += a.x * v.x - a.y * v.y;
-            im += a.x * v.y + a.y * v.x;
+        const int32_t k1 = __ldg(rowptr + r + 1);
+        int32_t k = __ldg(rowptr + r) + lane;
+        // three slots of the row per lane in flight: column indices, then values and
+        // gathers, then the products (rows of up to 3*TPR nonzeros take one round)
+        for (; k < k1; k += 3 * TPR) {
+            int32_t c[3];
+            double2 a[3], v[3];
+#pragma unroll
+            for (int u = 0; u < 3; ++u) c[u] = (k + u * TPR < k1) ? __ldg(cols + k + u * TPR) : -1;
+#pragma unroll
+            for (int u = 0; u < 3; ++u)
+                if (c[u] >= 0) { a[u] = __ldg(A + k + u * TPR); v[u] = __ldg(x + c[u]); }
+#pragma unroll
+            for (int u = 0; u < 3; ++u)
+                if (c[u] >= 0) {
+                    re += a[u].x * v[u].x - a[u].y * v[u].y;
+                    im += a[u].x * v[u].y + a[u].y * v[u].x;
+                }
         }
     }
 #pragma unroll
@@ -56,11 +69,20 @@ __global__ void spmv_rc64_kernel(int64_t n, const int32_t* __restrict__ rowptr, 
     int lane = (int)(t % TPR);
     double re = 0, im = 0;
     if (r < n) {
-        for (int32_t k = rowptr[r] + lane; k < rowptr[r + 1]; k += TPR) {
-            double a = A[k];
-            double2 v = x[cols[k]];
-            re += a * v.x;
-            im += a * v.y;
+        const int32_t k1 = __ldg(rowptr + r + 1);
+        int32_t k = __ldg(rowptr + r) + lane;
+        for (; k < k1; k += 3 * TPR) {   // three slots per lane in flight, as in spmv_c64_kernel
+            int32_t c[3];
+            double a[3];
+            double2 v[3];
+#pragma unroll
+            for (int u = 0; u < 3; ++u) c[u] = (k + u * TPR < k1) ? __ldg(cols + k + u * TPR) : -1;
+#pragma unroll
+            for (int u = 0; u < 3; ++u)
+                if (c[u] >= 0) { a[u] = __ldg(A + k + u * TPR); v[u] = __ldg(x + c[u]); }
+#pragma unroll
+            for (int u = 0; u < 3; ++u)
+                if (c[u] >= 0) { re += a[u] * v[u].x; im += a[u] * v[u].y; }
         }
     }
 #pragma unroll
