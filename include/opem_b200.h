@@ -36,6 +36,7 @@ extern "C" {
 #define OPEM_ERR_BREAKDOWN    (-7)   /* NaN/Inf or Krylov breakdown                    */
 #define OPEM_ERR_TIMEOUT      (-8)   /* device-side iteration/time budget exhausted    */
 #define OPEM_ERR_UNSUPPORTED  (-9)   /* order or feature not built                     */
+#define OPEM_ERR_CANCELLED    (-10)  /* request cancelled (serving loop)                */
 
 /* ---- boundary types (BoundaryDatabase attributes, src/OpenParEM3D/port.cpp:6885-7026) */
 #define OPEM_BDR_PEC        1   /* essential, E_t = 0 (fem3D.cpp:80-99)                      */
@@ -171,8 +172,22 @@ int  opem_server_submit(opem_server srv, opem_problem prob, int nfreq, const dou
  * was created are filled (any may be NULL) and the request's status returned.  */
 int  opem_server_wait(opem_server srv, int64_t request_id, double timeout_s, double* S_out,
                       opem_solve_stats* stats, double* times_out);
+/* Cancels a request: a queued one is dropped at once, a running one stops at its
+ * next Krylov step (the solvers poll a per-problem flag between steps); either way
+ * its wait returns OPEM_ERR_CANCELLED.  OPEM_ERR_ARG for an unknown id, OPEM_OK
+ * if the request had already finished (its result stands).                     */
+int  opem_server_cancel(opem_server srv, int64_t request_id);
 /* info[0]=queued, [1]=running, [2]=completed, [3]=admitted bytes, [4]=budget, [5]=slots. */
 int  opem_server_info(opem_server srv, int64_t* info, int ninfo);
+
+/* ---- failure-detection self-test (no reference counterpart) -----------------
+ * Launches one kernel whose bounded mbarrier wait (the wait the batched block
+ * apply uses for its bulk copies) is made to run out: it waits for a barrier
+ * phase that nothing completes, gives up after `polls` polls (1..2^24), records
+ * the timeout in a device status word and returns.  Returns OPEM_ERR_TIMEOUT
+ * when the status word reported the timeout and the context still runs a
+ * kernel afterwards, another status otherwise.                                   */
+int  opem_selftest_wait_timeout(opem_context ctx, int polls);
 
 /* ---- allocation-free assembly (no counterpart in the reference) -------------
  * For callers that cannot allocate device memory at the point of use: a

@@ -12,6 +12,7 @@ LIB_PATH = os.path.join(HERE, "libopem_b200.so")
 OK = 0
 ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_STATE, ERR_MESH = -1, -2, -3, -4, -5
 ERR_NOT_CONVERGED, ERR_BREAKDOWN, ERR_TIMEOUT, ERR_UNSUPPORTED = -6, -7, -8, -9
+ERR_CANCELLED = -10
 BDR_PEC, BDR_PMC, BDR_PORT, BDR_IMPEDANCE, BDR_RADIATION = 1, 2, 3, 4, 5
 PREC_FP64, PREC_MIXED = 0, 1
 NOALLOC_MAX_NNZ = 1 << 20
@@ -19,7 +20,7 @@ NOALLOC_MAX_NNZ = 1 << 20
 ERROR_NAMES = {ERR_ARG: "OPEM_ERR_ARG", ERR_CUDA: "OPEM_ERR_CUDA", ERR_NOMEM: "OPEM_ERR_NOMEM",
                ERR_STATE: "OPEM_ERR_STATE", ERR_MESH: "OPEM_ERR_MESH", ERR_NOT_CONVERGED: "OPEM_ERR_NOT_CONVERGED",
                ERR_BREAKDOWN: "OPEM_ERR_BREAKDOWN", ERR_TIMEOUT: "OPEM_ERR_TIMEOUT",
-               ERR_UNSUPPORTED: "OPEM_ERR_UNSUPPORTED"}
+               ERR_UNSUPPORTED: "OPEM_ERR_UNSUPPORTED", ERR_CANCELLED: "OPEM_ERR_CANCELLED"}
 
 
 class SolverOpts(C.Structure):
@@ -68,6 +69,8 @@ SIGNATURES = [
     ("opem_server_submit", C.c_int, [P, P, C.c_int, DP, P, C.POINTER(C.c_int64)]),
     ("opem_server_wait", C.c_int, [P, C.c_int64, C.c_double, DP, P, DP]),
     ("opem_server_info", C.c_int, [P, I64P, C.c_int]),
+    ("opem_server_cancel", C.c_int, [P, C.c_int64]),
+    ("opem_selftest_wait_timeout", C.c_int, [P, C.c_int]),
     ("opem_system_matrix_noalloc", C.c_int, [P, C.c_double, C.c_int, DP]),
 ]
 

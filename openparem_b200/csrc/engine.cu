@@ -886,6 +886,16 @@ int opem_profile_batch_kernels(opem_problem prob, double freq, int nsys, int rep
     });
 }
 
+int opem_selftest_wait_timeout(opem_context ctx, int polls) {
+    if (!ctx || polls < 1 || polls > (1 << 24)) return OPEM_ERR_ARG;
+    int code = OPEM_OK;
+    int rc = guarded(&ctx->c, [&] {
+        OPEM_CUDA(cudaSetDevice(ctx->c.device));
+        code = selftest_wait_timeout(ctx->c, polls);
+    });
+    return rc != OPEM_OK ? rc : code;
+}
+
 // No counterpart in the reference.  See include/opem_b200.h for the contract.
 int opem_system_matrix_noalloc(opem_problem prob, double freq, int d, double* vals) {
     if (!prob || !vals || !(freq > 0)) return OPEM_ERR_ARG;

@@ -1,5 +1,6 @@
 // Host-side engine state shared by the .cu files (internal).
 #pragma once
+#include <atomic>
 #include <memory>
 #include <string>
 #include <vector>
@@ -90,6 +91,7 @@ struct Problem {
     std::vector<PortMode> modes;
     bool assembled = false;
     int64_t ws_cap = 0;         // device bytes a batched sweep may take for its workspace (0: half of free)
+    std::atomic<int> cancel{0}; // set from another thread: the solvers stop at their next Krylov step
 
     // device mesh/operator data
     DBuf<double> d_verts;
@@ -154,6 +156,8 @@ void solve_sweep_mixed(Problem& P, int nfreq, const double* freqs, const opem_so
                        std::vector<std::vector<cd>>& S, std::vector<opem_solve_stats>& st);
 // device bytes a request (nfreq points with options o) needs beyond what P already holds
 double request_bytes_estimate(const Problem& P, int nfreq, const opem_solver_opts& o);
+// failure-detection self-test (mixed.cu): OPEM_ERR_TIMEOUT when the bounded wait ran out
+int selftest_wait_timeout(Context& C, int polls);
 
 }  // namespace opem
 

@@ -753,6 +753,7 @@ SolveResult solve_plain_fp64(Problem& P, const double2* A, const uint8_t* dmask,
             OPEM_CUDA(cudaGetLastError());
             OPEM_CUDA(cudaMemcpyAsync(colbuf.data(), Hcol, (j + 2) * sizeof(double2), cudaMemcpyDeviceToHost, s));
             OPEM_CUDA(cudaStreamSynchronize(s));
+            if (P.cancel.load(std::memory_order_relaxed)) throw OpemError(OPEM_ERR_CANCELLED, "request cancelled");
             for (int i = 0; i <= j + 1; ++i) Hh[i + (size_t)j * (m + 1)] = cd(colbuf[i].x, colbuf[i].y);
             est = L.add_column(j, &Hh[(size_t)j * (m + 1)], j + 1);
             ++its;

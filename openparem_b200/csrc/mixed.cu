@@ -1509,6 +1509,7 @@ static int inner_solve(Batch& B, InnerWork& W, const std::vector<PatchSet32>& se
             OPEM_CUDA(cudaMemcpy2DAsync(hcol.data(), (m + 2) * sizeof(double2), W.H.p + (int64_t)j * (m + 1),
                                         ldH * sizeof(double2), (j + 2) * sizeof(double2), R, cudaMemcpyDeviceToHost, B.s));
             OPEM_CUDA(cudaStreamSynchronize(B.s));
+            if (P.cancel.load(std::memory_order_relaxed)) throw OpemError(OPEM_ERR_CANCELLED, "request cancelled");
             ++its;
             for (int r = 0; r < R; ++r) {
                 if (!iact[r]) continue;
@@ -2160,6 +2161,42 @@ double request_bytes_estimate(const Problem& P, int nfreq, const opem_solver_opt
         b += n * 16.0 * (m + 1 + 24) + ss2 * 16;
     }
     return b;
+}
+
+
+// Failure-detection self-test: a bounded wait on an mbarrier phase that nothing
+// completes (the barrier expects one arrival and gets none) gives up after
+// `polls` polls and records the timeout in *status, as the batched block apply
+// does when a bulk copy never lands.
+__global__ void selftest_wait_kernel(int polls, int* __restrict__ status) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    bool done = false;
+    for (int it = 0; it < polls && !done; ++it) done = mbar_try_wait(&bar, 0);
+    __syncthreads();
+    if (!done && threadIdx.x == 0) atomicExch(status, 1);
+}
+
+__global__ void selftest_touch_kernel(int* __restrict__ v) { if (threadIdx.x == 0) v[1] = 7; }
+
+int selftest_wait_timeout(Context& C, int polls) {
+    DBuf<int> st(2);
+    OPEM_CUDA(cudaMemsetAsync(st.p, 0, 2 * sizeof(int), C.stream));
+    selftest_wait_kernel<<<1, 32, 0, C.stream>>>(polls, st.p);
+    ++C.launches;
+    OPEM_CUDA(cudaGetLastError());
+    selftest_touch_kernel<<<1, 32, 0, C.stream>>>(st.p);   // the context still runs kernels
+    ++C.launches;
+    OPEM_CUDA(cudaGetLastError());
+    int h[2] = {0, 0};
+    OPEM_CUDA(cudaMemcpyAsync(h, st.p, sizeof(h), cudaMemcpyDeviceToHost, C.stream));
+    OPEM_CUDA(cudaStreamSynchronize(C.stream));
+    if (h[1] != 7) return OPEM_ERR_CUDA;
+    return h[0] == 1 ? OPEM_ERR_TIMEOUT : OPEM_ERR_STATE;
 }
 
 }  // namespace opem

@@ -14,7 +14,9 @@
 // may overtake a waiting large one); requests on the same problem never run
 // at the same time.  Results do not depend on what else runs: every kernel of
 // a request reads only that request's data, and all reductions are
-// deterministic.
+// deterministic.  A request can be cancelled: dropped if still queued, or
+// stopped at its next Krylov step through the problem's cancel flag, which
+// the FP64 and batched solvers poll between steps.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -120,6 +122,7 @@ void worker(opem_server_s* S, int slot) {
             rq = *it;
             S->queue.erase(it);
             S->busy.insert(rq->prob);
+            rq->prob->p.cancel.store(0);   // under the lock: a cancel from now on is seen
             S->in_use += rq->bytes;
             ++S->running;
             rq->t_start = now_s();
@@ -247,6 +250,29 @@ int opem_server_wait(opem_server srv, int64_t request_id, double timeout_s, doub
         times_out[2] = rq->t_end - srv->epoch;
     }
     return rq->status;
+}
+
+int opem_server_cancel(opem_server srv, int64_t request_id) {
+    if (!srv) return OPEM_ERR_ARG;
+    {
+        std::lock_guard<std::mutex> lk(srv->mu);
+        auto it = srv->table.find(request_id);
+        if (it == srv->table.end()) return OPEM_ERR_ARG;
+        std::shared_ptr<Request> rq = it->second;
+        if (rq->done) return OPEM_OK;
+        auto q = std::find(srv->queue.begin(), srv->queue.end(), rq);
+        if (q == srv->queue.end()) {   // running: the solver stops at its next Krylov step
+            rq->prob->p.cancel.store(1);
+            return OPEM_OK;
+        }
+        srv->queue.erase(q);
+        rq->done = true;
+        rq->status = OPEM_ERR_CANCELLED;
+        rq->error = "cancelled before it started";
+        rq->t_start = rq->t_end = now_s();
+    }
+    srv->cv_done.notify_all();
+    return OPEM_OK;
 }
 
 int opem_server_info(opem_server srv, int64_t* info, int ninfo) {

@@ -238,6 +238,13 @@ class Server:
         times = {"submitted": t[0], "started": t[1], "finished": t[2]}
         return (S[0::2] + 1j * S[1::2]).reshape(nf, N, N), [s.as_dict() for s in st], times
 
+    def cancel(self, rid):
+        """Queued: dropped at once; running: stops at its next Krylov step.  Its wait
+        then raises OpemError with code ERR_CANCELLED (unless it had finished)."""
+        rc = _lib.lib().opem_server_cancel(self.h, int(rid))
+        if rc != _lib.OK:
+            raise OpemError(rc, f"cancel {rid}")
+
     def info(self):
         a = np.zeros(6, dtype=np.int64)
         _lib.lib().opem_server_info(self.h, a.ctypes.data_as(_lib.I64P), 6)

@@ -107,3 +107,43 @@ def test_wait_timeout_and_bad_requests(ctx):
             srv.wait(12345)
     finally:
         srv.close()
+
+
+def test_cancel_queued_and_running(ctx):
+    """Cancelled requests: a queued one is dropped, a running one stops at its next
+    Krylov step; both waits report ERR_CANCELLED and the problems stay usable."""
+    from openparem_b200.fem3d import OpemError
+    big = Fem3D(meshgen.waveguide_problem(meshgen.WR_A, meshgen.WR_B, 50e-3, 12, 6, 30, 2,
+                                          slab=(20e-3, 30e-3, 4.4, 0.02)), context=ctx).assemble()
+    small = Fem3D(_problems()[0][1], context=ctx).assemble()
+    srv = Server(0, slots=1)
+    try:
+        opts = default_opts(rtol=1e-12, restart=100)
+        r_big = srv.submit(big, np.linspace(8e9, 12e9, 6), opts)    # FP64 path, several seconds
+        r_small = srv.submit(small, [10e9], opts)                   # queued behind it (one slot)
+        srv.cancel(r_small)
+        with pytest.raises(OpemError) as e1:
+            srv.wait(r_small, timeout=60.0)
+        assert e1.value.code == _lib.ERR_CANCELLED
+        import time
+        t0 = time.time()
+        while srv.info()["running"] == 0 and time.time() - t0 < 60:
+            time.sleep(0.01)
+        srv.cancel(r_big)
+        with pytest.raises(OpemError) as e2:
+            srv.wait(r_big, timeout=300.0)
+        assert e2.value.code == _lib.ERR_CANCELLED
+        S, st, _ = srv.wait(srv.submit(small, [10e9], opts))   # the flag is cleared for the next request
+        assert st[0]["converged"] == 1
+    finally:
+        srv.close()
+
+
+def test_bounded_wait_timeout_selftest(ctx):
+    """The device-side bounded wait gives up, reports OPEM_ERR_TIMEOUT through its
+    status word, and the context keeps working."""
+    L = _lib.lib()
+    assert L.opem_selftest_wait_timeout(ctx.h, 1 << 14) == _lib.ERR_TIMEOUT
+    F = Fem3D(_problems()[0][1], context=ctx).assemble()
+    S, _, st = F.solve(10e9)
+    assert st["converged"] == 1
