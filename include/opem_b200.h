@@ -142,6 +142,20 @@ int  opem_profile_kernels(opem_problem prob, double freq, int reps, double* out,
  * operators and FP32 vectors, 3 = FP64 operators and vectors, 4 = patch sum.     */
 int  opem_profile_batch_kernels(opem_problem prob, double freq, int nsys, int reps, double* out, int nout);
 
+/* ---- S-parameter post-processing (host only, no GPU needed) -----------------
+ * Renormalises S (nports x nports complex, interleaved, row = portOut) from the
+ * port impedances Zo (nports complex, as opem_solve_frequency returns them) to
+ * one reference impedance zref: Z = k (I+S)(I-S)^-1 k with k = diag(sqrt(Zo)),
+ * S' = (Z/zref + I)^-1 (Z/zref - I)  (Result::renormalize, results.cpp:567-580).
+ * OPEM_ERR_BREAKDOWN if I-S or Z/zref+I is singular.                            */
+int  opem_s_renormalize(int nports, const double* S, const double* Zo, double zref_re, double zref_im,
+                        double* S_out);
+/* Writes a Touchstone 1.1 file (ResultDatabase::saveTouchstone, results.cpp:1055-1208):
+ * nfreq points of renormalised S (layout as opem_solve_sweep returns), reference
+ * impedance zref (ohm, > 0), format "RI" | "MA" | "DB", unit "Hz" | "kHz" | "MHz" | "GHz". */
+int  opem_write_touchstone(const char* path, int nfreq, const double* freqs, int nports, const double* S,
+                           double zref, const char* format, const char* unit);
+
 /* ---- serving loop (no counterpart in the reference: it solves one project per
  * process, OpenParEM3D.cpp:494-555) -------------------------------------------
  * A server runs solve requests from any number of caller threads on one GPU.

@@ -262,3 +262,36 @@ class Server:
         except Exception:
             pass
 
+
+def renormalize(S, Zo, zref=50.0):
+    """S (nfreq, N, N) or (N, N) with port impedances Zo ((nfreq,) N) -> S referred to
+    zref on every port (opem_s_renormalize)."""
+    S = np.asarray(S, dtype=np.complex128)
+    Zo = np.asarray(Zo, dtype=np.complex128)
+    one = S.ndim == 2
+    S3 = S[None] if one else S
+    Z2 = np.broadcast_to(Zo, (S3.shape[0], S3.shape[1]))
+    out = np.empty_like(S3)
+    N = S3.shape[1]
+    for q in range(S3.shape[0]):
+        si = np.ascontiguousarray(S3[q]).view(np.float64).ravel()
+        zi = np.ascontiguousarray(Z2[q]).view(np.float64).ravel()
+        so = np.zeros(2 * N * N)
+        rc = _lib.lib().opem_s_renormalize(N, _dp(si), _dp(zi), float(np.real(zref)), float(np.imag(zref)), _dp(so))
+        if rc != _lib.OK:
+            raise OpemError(rc, "opem_s_renormalize")
+        out[q] = (so[0::2] + 1j * so[1::2]).reshape(N, N)
+    return out[0] if one else out
+
+
+def write_touchstone(path, freqs, S, zref=50.0, fmt="RI", unit="GHz"):
+    """Touchstone 1.1 file of renormalised S (nfreq, N, N) (opem_write_touchstone)."""
+    freqs = np.ascontiguousarray(freqs, dtype=np.float64)
+    S = np.ascontiguousarray(S, dtype=np.complex128)
+    N = S.shape[1]
+    flat = S.view(np.float64).ravel()
+    rc = _lib.lib().opem_write_touchstone(str(path).encode(), len(freqs), _dp(freqs), N, _dp(flat), float(zref),
+                                          fmt.encode(), unit.encode())
+    if rc != _lib.OK:
+        raise OpemError(rc, "opem_write_touchstone")
+
