@@ -142,6 +142,28 @@ int  opem_profile_kernels(opem_problem prob, double freq, int reps, double* out,
  * operators and FP32 vectors, 3 = FP64 operators and vectors, 4 = patch sum.     */
 int  opem_profile_batch_kernels(opem_problem prob, double freq, int nsys, int reps, double* out, int nout);
 
+/* ---- OpenParEM3D project input (project.c, mesh.cpp:449-588, port.cpp:6369-7078,
+ * OpenParEMmaterials.cpp) --------------------------------------------------------
+ * Reads a .proj file with its gmsh 2.2 mesh (physical volumes named after
+ * materials), ports file and materials databases, and creates the problem:
+ * regions and materials, exterior faces classified into ports (closed
+ * rectangular Path of each Port, ordered by Sport), Boundary blocks
+ * (surface_impedance with the material's conductivity and Rz,
+ * perfect_electric_conductor, perfect_magnetic_conductor, radiation) and PEC for
+ * every other exterior face; each port is driven by the TE10 mode of its
+ * rectangle (a = the wide side) with the voltage path of its Line block.  order
+ * > 0 replaces mesh.order (orders 1-3 are built).  The frequency plan
+ * (point, point.refine and linear entries, sorted, duplicates removed) goes to
+ * freqs (up to max_freqs) and its length to *nfreq.                            */
+int  opem_project_load(opem_context ctx, const char* proj_path, int order, opem_problem* out, int* nfreq,
+                       double* freqs, int max_freqs);
+/* The same reading without a device (host only): info[0]=vertices, [1]=tets,
+ * [2]=regions, [3]=exterior faces, [4]=port faces, [5]=Boundary-block faces,
+ * [6]=PEC faces, [7]=ports, [8]=frequency points, [9]=order; msg receives the
+ * reason when the project cannot be read (OPEM_ERR_ARG).                       */
+int  opem_project_info(const char* proj_path, int order, int64_t* info, int ninfo, double* freqs, int max_freqs,
+                       char* msg, int msg_len);
+
 /* ---- S-parameter post-processing (host only, no GPU needed) -----------------
  * Renormalises S (nports x nports complex, interleaved, row = portOut) from the
  * port impedances Zo (nports complex, as opem_solve_frequency returns them) to

@@ -78,6 +78,21 @@ _BTYPES = {"pec": _lib.BDR_PEC, "pmc": _lib.BDR_PMC, "port": _lib.BDR_PORT, "imp
            "radiation": _lib.BDR_RADIATION}
 
 
+def project_info(proj_path, order=0):
+    """Host-only reading of an OpenParEM3D project (opem_project_info) -> (counts, freqs)."""
+    a = np.zeros(10, dtype=np.int64)
+    fr = np.zeros(4096)
+    msg = C.create_string_buffer(512)
+    rc = _lib.lib().opem_project_info(str(proj_path).encode(), int(order), a.ctypes.data_as(_lib.I64P), 10, _dp(fr),
+                                      len(fr), msg, 512)
+    if rc != _lib.OK:
+        raise OpemError(rc, f"opem_project_info: {msg.value.decode()}")
+    keys = ["vertices", "tets", "regions", "exterior_faces", "port_faces", "boundary_faces", "pec_faces", "ports",
+            "frequencies", "order"]
+    info = dict(zip(keys, (int(v) for v in a)))
+    return info, fr[:min(info["frequencies"], len(fr))]
+
+
 class Fem3D:
     """One mesh + materials + boundaries resident on the device."""
 
@@ -118,6 +133,25 @@ class Fem3D:
             _chk(self.ctx.h, L.opem_problem_set_port_te(self.h, k, _dp(d)), "set_port_te")
         self.nports = len(prob["ports"])
         self._assembled = False
+
+    @classmethod
+    def from_project(cls, proj_path, order=0, context=None, device=0):
+        """An OpenParEM3D project (.proj with its gmsh 2.2 mesh, ports file and
+        materials databases) -> (Fem3D, frequency plan).  order > 0 replaces
+        mesh.order (orders 1-3 are built)."""
+        info, freqs = project_info(proj_path, order)
+        self = cls.__new__(cls)
+        self.ctx = context if context is not None else Context(device)
+        self.prob = None
+        self.h = C.c_void_p()
+        nf = C.c_int()
+        fr = np.zeros(max(1, info["frequencies"]))
+        rc = _lib.lib().opem_project_load(self.ctx.h, str(proj_path).encode(), int(order), C.byref(self.h),
+                                          C.byref(nf), _dp(fr), len(fr))
+        _chk(self.ctx.h, rc, "opem_project_load")
+        self.nports = info["ports"]
+        self._assembled = False
+        return self, fr[:nf.value]
 
     # fem3D::build_fe_spaces + build_A's frequency-independent part
     def assemble(self):

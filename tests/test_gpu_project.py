@@ -1,0 +1,30 @@
+"""GPU: a problem read from OpenParEM3D project files (gmsh 2.2 mesh, ports file,
+materials database, .proj) solves to the same S as the same guide built in
+memory (|dS| <= 1e-10, solver rtol 1e-12)."""
+import numpy as np
+import pytest
+
+from openparem_b200 import meshgen, Fem3D, default_opts
+from openparem_b200.fem3d import Context
+from project_files import write_guide_project
+
+pytestmark = pytest.mark.gpu
+
+
+def test_project_matches_in_memory_problem(tmp_path):
+    ctx = Context(0)
+    proj = write_guide_project(str(tmp_path), order=1)
+    F, freqs = Fem3D.from_project(proj, context=ctx)
+    assert np.allclose(freqs, [9e9, 10e9, 10.5e9, 11e9])
+    F.assemble()
+    G = Fem3D(meshgen.waveguide_problem(meshgen.WR_A, meshgen.WR_B, 50e-3, 6, 3, 15, 1), context=ctx).assemble()
+    o = default_opts(rtol=1e-12, restart=200)
+    for f in (9e9, 10.5e9):
+        S1, _, st1 = F.solve(f, o)
+        S2, _, _ = G.solve(f, o)
+        assert st1["converged"] == 1
+        assert np.abs(S1 - S2).max() <= 1e-10, f
+    # an order override reads the same files at ND2
+    F2, _ = Fem3D.from_project(proj, order=2, context=ctx)
+    S3, _, st3 = F2.assemble().solve(10e9, o)
+    assert st3["converged"] == 1 and np.abs(S3).max() <= 1 + 1e-9

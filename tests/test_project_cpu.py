@@ -1,0 +1,43 @@
+"""CPU tests of the OpenParEM3D project reader (opem_project_info: host only)."""
+import os
+
+import numpy as np
+import pytest
+
+from openparem_b200.fem3d import project_info, OpemError
+from project_files import write_guide_project
+
+
+def test_synthetic_guide_project(tmp_path):
+    proj = write_guide_project(str(tmp_path), copper_wall=True)
+    info, fr = project_info(proj)
+    assert info["tets"] == 1620 and info["regions"] == 1 and info["ports"] == 2 and info["order"] == 1
+    assert info["port_faces"] == 2 * 6 * 3 * 2
+    assert info["boundary_faces"] == 3 * 15 * 2               # the x = a/2 wall, copper
+    assert info["pec_faces"] == info["exterior_faces"] - info["port_faces"] - info["boundary_faces"]
+    assert np.allclose(fr, [9e9, 10e9, 10.5e9, 11e9])
+    info3, _ = project_info(proj, order=3)
+    assert info3["order"] == 3
+
+
+def test_project_errors(tmp_path):
+    proj = write_guide_project(str(tmp_path))
+    os.remove(os.path.join(str(tmp_path), "materials.txt"))
+    with pytest.raises(OpemError) as e:
+        project_info(proj)
+    assert "material" in str(e.value)
+    with pytest.raises(OpemError):
+        project_info(os.path.join(str(tmp_path), "missing.proj"))
+
+
+REF = "/root/reference/regression/OpenParEM3D/WR90/straight/straight.proj"
+
+
+@pytest.mark.skipif(not os.path.exists(REF), reason="the reference tree is not mounted here")
+def test_reference_wr90_straight_project():
+    """The reference's own regression project reads: 282 tets, two TE10 ports,
+    its three frequency points, mesh order 6."""
+    info, fr = project_info(REF)
+    assert info["tets"] == 282 and info["ports"] == 2 and info["order"] == 6
+    assert info["port_faces"] > 0 and info["pec_faces"] > 0
+    assert np.allclose(fr, [9e9, 9.999999999e9, 11e9])
