@@ -7,7 +7,8 @@ Reads, from the reference tree given on the command line (default
                                                           recorded found values)
 and writes
   tests/golden/wr90_straight_mesh.npz   vertex coordinates (m) and tetrahedra
-  tests/golden/wr90_expected.json       found S-parameter values per case
+  tests/golden/wr90_expected.json       found S-parameter values per case (straight,
+                                        straight-lossy, straight-loaded)
 
 Run once in a container that has the reference tree; the outputs are
 committed so the tests never need the reference at run time.
@@ -73,7 +74,8 @@ def main(ref):
     np.savez_compressed(os.path.join(HERE, "wr90_straight_mesh.npz"), verts=xyz, tets=tets, phys=phys)
     res = read_results(os.path.join(ref, "regression", "OpenParEM3D", "regression_results.csv.current"))
     keep = {}
-    for proj in ("./WR90/straight/straight.proj", "./WR90/straight-lossy/straight.proj"):
+    for proj in ("./WR90/straight/straight.proj", "./WR90/straight-lossy/straight.proj",
+                 "./WR90/straight-loaded/straight-loaded.proj"):
         keep[proj] = res[proj]
     meta = {
         "source": "regression/OpenParEM3D/regression_results.csv.current",
