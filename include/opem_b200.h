@@ -164,6 +164,21 @@ int  opem_project_load(opem_context ctx, const char* proj_path, int order, opem_
 int  opem_project_info(const char* proj_path, int order, int64_t* info, int ninfo, double* freqs, int max_freqs,
                        char* msg, int msg_len);
 
+/* ---- port eigenmode of a cross-section (host only; the modal problem the
+ * reference hands to OpenParEM2D, port.cpp:5081-5176) ----------------------------
+ * Fundamental mode of a guide with PEC walls on a triangle mesh: nodes xy
+ * (2 doubles each), triangles (3 node indices each), per-triangle complex eps_r
+ * and mu_r (interleaved re, im; mu_r may be NULL for 1).  Lowest-order edge
+ * elements for e_t, linear nodal elements for e_z.  beta_out = beta (complex,
+ * exp(-j beta z)).  Edges are the sorted vertex pairs in lexicographic order,
+ * oriented from the lower to the higher node index; *nedges is their count
+ * (call with edges_out, et_out and ez_out all NULL to query it).  et_out: edge
+ * coefficients (2 doubles each), scaled so the largest is 1; ez_out: nodal e_z
+ * (2 doubles each).  OPEM_ERR_NOT_CONVERGED if inverse iteration stalls.       */
+int  opem_port_mode_2d(int64_t nnodes, const double* xy, int64_t ntri, const int64_t* tris, const double* eps_r,
+                       const double* mu_r, double freq, double* beta_out, int64_t* nedges, int64_t* edges_out,
+                       double* et_out, double* ez_out);
+
 /* ---- S-parameter post-processing (host only, no GPU needed) -----------------
  * Renormalises S (nports x nports complex, interleaved, row = portOut) from the
  * port impedances Zo (nports complex, as opem_solve_frequency returns them) to

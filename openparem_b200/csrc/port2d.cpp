@@ -1,0 +1,298 @@
+// Port eigenmode of a waveguide cross-section on the host (the modal problem
+// OpenParEM3D hands to its 2D solver, src/OpenParEM3D/port.cpp:5081-5176, solved
+// there by OpenParEM2D with SLEPc).  Lowest-order edge elements for the
+// transverse field e_t, linear nodal elements for e_z, PEC on the outer
+// boundary, per-triangle complex eps_r and mu_r.  With psi = j e_z / beta the
+// problem is the symmetric pencil (Lee, Sun and Cendes, IEEE MTT 1991)
+//
+//     [S - k0^2 T_eps  0] x = -beta^2 [T_mu  -G; -G^T  Kz] x,
+//
+// and the fundamental mode (largest beta^2) is found by inverse iteration with
+// the shift -k0^2 max Re(eps_r mu_r).  The shifted matrix is factorised once by
+// banded LU with partial pivoting after a reverse Cuthill-McKee ordering (2D
+// meshes keep the band near sqrt(n)).
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <queue>
+#include <vector>
+
+#include "../../include/opem_b200.h"
+
+namespace {
+
+using cd = std::complex<double>;
+constexpr double MU0 = 4e-7 * M_PI, EPS0 = 8.8541878176e-12;
+
+struct Triplet { int r, c; cd v; };
+
+// banded LU with partial pivoting (kl sub-, ku super-diagonals; ku grows by kl)
+struct Banded {
+    int n = 0, kl = 0, ku0 = 0, ku = 0, ld = 0;   // ku = ku0 + kl: upper band after pivoting
+    std::vector<cd> a;   // column-major band storage: a[(kl + ku0 + i - j) + j * ld] (LAPACK's layout)
+    std::vector<int> piv;
+    cd& at(int i, int j) { return a[(size_t)(kl + ku0 + i - j) + (size_t)j * ld]; }
+    void init(int n_, int kl_, int ku_) {
+        n = n_; kl = kl_; ku0 = ku_; ku = ku_ + kl_; ld = 2 * kl + ku0 + 1;
+        a.assign((size_t)ld * n, 0.0);
+        piv.assign(n, 0);
+    }
+    bool factor() {
+        for (int j = 0; j < n; ++j) {
+            const int imax = std::min(n - 1, j + kl);
+            int p = j;
+            double best = std::abs(at(j, j));
+            for (int i = j + 1; i <= imax; ++i)
+                if (std::abs(at(i, j)) > best) { best = std::abs(at(i, j)); p = i; }
+            if (!(best > 0)) return false;
+            piv[j] = p;
+            const int jmax = std::min(n - 1, j + ku);
+            if (p != j)
+                for (int k = j; k <= jmax; ++k) std::swap(at(j, k), at(p, k));
+            const cd d = 1.0 / at(j, j);
+            for (int i = j + 1; i <= imax; ++i) {
+                cd& l = at(i, j);
+                l *= d;
+                if (l == 0.0) continue;
+                for (int k = j + 1; k <= jmax; ++k) at(i, k) -= l * at(j, k);
+            }
+        }
+        return true;
+    }
+    void solve(std::vector<cd>& b) {
+        for (int j = 0; j < n; ++j) {
+            if (piv[j] != j) std::swap(b[j], b[piv[j]]);
+            const int imax = std::min(n - 1, j + kl);
+            for (int i = j + 1; i <= imax; ++i) b[i] -= at(i, j) * b[j];
+        }
+        for (int j = n - 1; j >= 0; --j) {
+            b[j] /= at(j, j);
+            const int imin = std::max(0, j - ku);
+            for (int i = imin; i < j; ++i) b[i] -= at(i, j) * b[j];
+        }
+    }
+};
+
+// reverse Cuthill-McKee order of a symmetric sparsity pattern
+std::vector<int> rcm(int n, const std::vector<std::vector<int>>& adj) {
+    std::vector<int> order, deg(n);
+    for (int i = 0; i < n; ++i) deg[i] = (int)adj[i].size();
+    std::vector<char> seen(n, 0);
+    for (int root0 = 0; root0 < n; ++root0) {
+        if (seen[root0]) continue;
+        int root = root0;   // a pseudo-peripheral start: lowest degree in the component's first BFS level set
+        for (int pass = 0; pass < 2; ++pass) {
+            std::vector<int> lvl(n, -1);
+            std::queue<int> q;
+            q.push(root);
+            lvl[root] = 0;
+            int last = root;
+            while (!q.empty()) {
+                int u = q.front();
+                q.pop();
+                last = u;
+                for (int w : adj[u])
+                    if (lvl[w] < 0) { lvl[w] = lvl[u] + 1; q.push(w); }
+            }
+            int best = last;
+            for (int i = 0; i < n; ++i)
+                if (lvl[i] == lvl[last] && deg[i] < deg[best]) best = i;
+            root = best;
+        }
+        std::queue<int> q;
+        q.push(root);
+        seen[root] = 1;
+        while (!q.empty()) {
+            int u = q.front();
+            q.pop();
+            order.push_back(u);
+            std::vector<int> nb;
+            for (int w : adj[u])
+                if (!seen[w]) { seen[w] = 1; nb.push_back(w); }
+            std::sort(nb.begin(), nb.end(), [&](int x, int y) { return deg[x] < deg[y]; });
+            for (int w : nb) q.push(w);
+        }
+    }
+    std::reverse(order.begin(), order.end());
+    return order;
+}
+
+}  // namespace
+
+extern "C" {
+
+int opem_port_mode_2d(int64_t nnodes, const double* xy, int64_t ntri, const int64_t* tris, const double* eps_r,
+                      const double* mu_r, double freq, double* beta_out, int64_t* nedges, int64_t* edges_out,
+                      double* et_out, double* ez_out) {
+    if (nnodes < 3 || !xy || ntri < 1 || !tris || !eps_r || !(freq > 0) || !beta_out || !nedges) return OPEM_ERR_ARG;
+    for (int64_t t = 0; t < 3 * ntri; ++t)
+        if (tris[t] < 0 || tris[t] >= nnodes) return OPEM_ERR_ARG;
+    const double k0 = 2 * M_PI * freq * std::sqrt(MU0 * EPS0);
+    // edges: sorted vertex pairs, numbered in lexicographic order; orientation low -> high vertex
+    std::map<std::pair<int64_t, int64_t>, int> eid;
+    std::vector<std::array<int64_t, 3>> st(ntri);
+    for (int64_t t = 0; t < ntri; ++t) {
+        std::array<int64_t, 3> v = {tris[3 * t], tris[3 * t + 1], tris[3 * t + 2]};
+        std::sort(v.begin(), v.end());
+        st[t] = v;
+        static const int LP[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+        for (auto& lp : LP) eid[{v[lp[0]], v[lp[1]]}] = 0;
+    }
+    int ne = 0;
+    std::vector<std::pair<int64_t, int64_t>> edges;
+    for (auto& kv : eid) { kv.second = ne++; edges.push_back(kv.first); }
+    *nedges = ne;
+    if (!et_out && !ez_out && !edges_out) return OPEM_OK;   // size query
+    if (edges_out)
+        for (int e = 0; e < ne; ++e) { edges_out[2 * e] = edges[e].first; edges_out[2 * e + 1] = edges[e].second; }
+    // element matrices
+    std::vector<Triplet> Aee, Bee, Ben, Bnn;   // A = S - k0^2 T_eps; B blocks T_mu, -G, Kz
+    std::vector<int> ecount(ne, 0);
+    double emax = 0;
+    static const int LP[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+    for (int64_t t = 0; t < ntri; ++t) {
+        const auto& v = st[t];
+        double P[3][2];
+        for (int k = 0; k < 3; ++k) { P[k][0] = xy[2 * v[k]]; P[k][1] = xy[2 * v[k] + 1]; }
+        const double J00 = P[1][0] - P[0][0], J01 = P[2][0] - P[0][0], J10 = P[1][1] - P[0][1], J11 = P[2][1] - P[0][1];
+        const double det = J00 * J11 - J01 * J10;
+        if (!(std::fabs(det) > 0)) return OPEM_ERR_ARG;
+        const double area = 0.5 * std::fabs(det);
+        // grad lambda: rows of J^-T applied to (-1,-1), (1,0), (0,1)
+        const double i00 = J11 / det, i01 = -J01 / det, i10 = -J10 / det, i11 = J00 / det;   // J^-1
+        double g[3][2];
+        const double r[3][2] = {{-1, -1}, {1, 0}, {0, 1}};
+        for (int k = 0; k < 3; ++k) {   // grad = J^-T r
+            g[k][0] = i00 * r[k][0] + i10 * r[k][1];
+            g[k][1] = i01 * r[k][0] + i11 * r[k][1];
+        }
+        auto dotg = [&](int p, int q) { return g[p][0] * g[q][0] + g[p][1] * g[q][1]; };
+        auto Mll = [&](int p, int q) { return area / 12.0 * (p == q ? 2.0 : 1.0); };
+        double curl[3];
+        for (int i = 0; i < 3; ++i) {
+            const int a = LP[i][0], b = LP[i][1];
+            curl[i] = 2.0 * (g[a][0] * g[b][1] - g[a][1] * g[b][0]);
+        }
+        const cd er(eps_r[2 * t], eps_r[2 * t + 1]);
+        const cd mr = mu_r ? cd(mu_r[2 * t], mu_r[2 * t + 1]) : cd(1.0, 0.0);
+        const cd im = 1.0 / mr;
+        emax = std::max(emax, std::real(er * mr));
+        int ge[3];
+        for (int i = 0; i < 3; ++i) { ge[i] = eid[{v[LP[i][0]], v[LP[i][1]]}]; ++ecount[ge[i]]; }
+        for (int i = 0; i < 3; ++i) {
+            const int a = LP[i][0], b = LP[i][1];
+            for (int j = 0; j < 3; ++j) {
+                const int c = LP[j][0], d = LP[j][1];
+                const double m = Mll(a, c) * dotg(b, d) - Mll(a, d) * dotg(b, c) - Mll(b, c) * dotg(a, d) + Mll(b, d) * dotg(a, c);
+                Aee.push_back({ge[i], ge[j], im * curl[i] * curl[j] * area - k0 * k0 * er * m});
+                Bee.push_back({ge[i], ge[j], im * m});
+            }
+            for (int k = 0; k < 3; ++k) {
+                const double ng = area / 3.0 * ((g[b][0] - g[a][0]) * g[k][0] + (g[b][1] - g[a][1]) * g[k][1]);
+                Ben.push_back({ge[i], (int)v[k], -im * ng});
+            }
+        }
+        for (int k = 0; k < 3; ++k)
+            for (int l = 0; l < 3; ++l)
+                Bnn.push_back({(int)v[k], (int)v[l], im * area * dotg(k, l) - k0 * k0 * er * Mll(k, l)});
+    }
+    // PEC: boundary edges (in one triangle) and their nodes are removed
+    std::vector<int> emap(ne, -1), nmap(nnodes, -1);
+    std::vector<char> bnode(nnodes, 0);
+    for (int e = 0; e < ne; ++e)
+        if (ecount[e] == 1) { bnode[edges[e].first] = 1; bnode[edges[e].second] = 1; }
+    int nu = 0;
+    for (int e = 0; e < ne; ++e)
+        if (ecount[e] != 1) emap[e] = nu++;
+    const int nue = nu;
+    std::vector<char> used(nnodes, 0);
+    for (int64_t t = 0; t < 3 * ntri; ++t) used[tris[t]] = 1;
+    for (int64_t i = 0; i < nnodes; ++i)
+        if (used[i] && !bnode[i]) nmap[i] = nu++;
+    const int n = nu;
+    if (n == 0) return OPEM_ERR_ARG;
+    // global sparse A and B in the unknown numbering
+    std::vector<Triplet> A, Bm;
+    for (auto& x : Aee) if (emap[x.r] >= 0 && emap[x.c] >= 0) A.push_back({emap[x.r], emap[x.c], x.v});
+    for (auto& x : Bee) if (emap[x.r] >= 0 && emap[x.c] >= 0) Bm.push_back({emap[x.r], emap[x.c], x.v});
+    for (auto& x : Ben)
+        if (emap[x.r] >= 0 && nmap[x.c] >= 0) {
+            Bm.push_back({emap[x.r], nmap[x.c], x.v});
+            Bm.push_back({nmap[x.c], emap[x.r], x.v});
+        }
+    for (auto& x : Bnn) if (nmap[x.r] >= 0 && nmap[x.c] >= 0) Bm.push_back({nmap[x.r], nmap[x.c], x.v});
+    // ordering and band
+    std::vector<std::vector<int>> adj(n);
+    for (auto* T : {&A, &Bm})
+        for (auto& x : *T)
+            if (x.r != x.c) adj[x.r].push_back(x.c);
+    for (auto& a : adj) { std::sort(a.begin(), a.end()); a.erase(std::unique(a.begin(), a.end()), a.end()); }
+    std::vector<int> ord = rcm(n, adj), pos(n);
+    for (int i = 0; i < n; ++i) pos[ord[i]] = i;
+    int bw = 0;
+    for (int i = 0; i < n; ++i)
+        for (int j : adj[i]) bw = std::max(bw, std::abs(pos[i] - pos[j]));
+    const double sigma = -k0 * k0 * emax;
+    Banded M;
+    M.init(n, bw, bw);
+    for (auto& x : A) M.at(pos[x.r], pos[x.c]) += x.v;
+    for (auto& x : Bm) M.at(pos[x.r], pos[x.c]) -= sigma * x.v;
+    if (!M.factor()) return OPEM_ERR_BREAKDOWN;
+    // inverse iteration: y = (A - sigma B)^-1 B x; its dominant eigenvalue mu gives lambda = sigma + 1/mu
+    auto Bmul = [&](const std::vector<cd>& x, std::vector<cd>& y) {
+        std::fill(y.begin(), y.end(), 0.0);
+        for (auto& t : Bm) y[pos[t.r]] += t.v * x[pos[t.c]];
+    };
+    std::vector<cd> x(n), y(n), bx(n);
+    for (int i = 0; i < n; ++i) x[i] = cd(1.0 + 0.001 * (i % 7), 0.0005 * (i % 5));
+    cd lam = 0, lam_prev = 0;
+    bool ok = false;
+    for (int it = 0; it < 2000; ++it) {
+        Bmul(x, bx);
+        y = bx;
+        M.solve(y);
+        // Rayleigh-type estimate mu = (x^H B y) / (x^H B x), B symmetric
+        std::vector<cd> by(n);
+        Bmul(y, by);
+        cd num = 0, den = 0;
+        for (int i = 0; i < n; ++i) { num += std::conj(x[i]) * by[i]; den += std::conj(x[i]) * bx[i]; }
+        double nrm = 0;
+        for (auto& v : y) nrm += std::norm(v);
+        nrm = std::sqrt(nrm);
+        if (!(nrm > 0) || den == 0.0) return OPEM_ERR_BREAKDOWN;
+        for (int i = 0; i < n; ++i) x[i] = y[i] / nrm;
+        const cd mu = num / den;
+        lam = sigma + 1.0 / mu;
+        if (it > 3 && std::abs(lam - lam_prev) <= 1e-14 * std::abs(lam)) { ok = true; break; }
+        lam_prev = lam;
+    }
+    if (!ok) return OPEM_ERR_NOT_CONVERGED;
+    cd beta = std::sqrt(-lam);
+    if (beta.real() < 0) beta = -beta;
+    beta_out[0] = beta.real();
+    beta_out[1] = beta.imag();
+    // scale: the largest e_t coefficient becomes 1
+    cd big = 0.0;
+    for (int e = 0; e < ne; ++e)
+        if (emap[e] >= 0 && std::abs(x[pos[emap[e]]]) > std::abs(big)) big = x[pos[emap[e]]];
+    const cd s = std::abs(big) > 0 ? 1.0 / big : cd(1.0);
+    if (et_out)
+        for (int e = 0; e < ne; ++e) {
+            const cd v = emap[e] >= 0 ? x[pos[emap[e]]] * s : cd(0.0);
+            et_out[2 * e] = v.real();
+            et_out[2 * e + 1] = v.imag();
+        }
+    if (ez_out)
+        for (int64_t i = 0; i < nnodes; ++i) {
+            const cd v = nmap[i] >= 0 ? -cd(0, 1) * beta * x[pos[nmap[i]]] * s : cd(0.0);   // e_z = -j beta psi
+            ez_out[2 * i] = v.real();
+            ez_out[2 * i + 1] = v.imag();
+        }
+    return OPEM_OK;
+}
+
+}  // extern "C"
