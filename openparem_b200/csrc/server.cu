@@ -45,7 +45,7 @@ struct Request {
     opem_problem prob = nullptr;
     std::vector<double> freqs;
     opem_solver_opts opts{};
-    double bytes = 0;   // admitted footprint
+    double bytes = -1;  // admitted footprint (estimated when the request is first considered)
     bool done = false;
     int status = OPEM_OK;
     std::string error;
@@ -76,11 +76,14 @@ struct opem_server_s {
 
 namespace {
 
-// first queued request that may start now (caller holds the lock)
+// first queued request that may start now (caller holds the lock).  The
+// footprint is estimated here, while no request runs on the problem, so the
+// estimate never reads a problem that a worker is assembling.
 std::deque<std::shared_ptr<Request>>::iterator pick(opem_server_s* S) {
     for (auto it = S->queue.begin(); it != S->queue.end(); ++it) {
-        const Request& r = **it;
+        Request& r = **it;
         if (S->busy.count(r.prob)) continue;
+        if (r.bytes < 0) r.bytes = request_bytes_estimate(r.prob->p, (int)r.freqs.size(), r.opts);
         if (S->running == 0 || S->in_use + r.bytes <= S->budget) return it;
     }
     return S->queue.end();
@@ -210,7 +213,6 @@ int opem_server_submit(opem_server srv, opem_problem prob, int nfreq, const doub
     rq->prob = prob;
     rq->freqs.assign(freqs, freqs + nfreq);
     rq->opts = *opts;
-    rq->bytes = request_bytes_estimate(prob->p, nfreq, *opts);
     rq->t_submit = now_s();
     {
         std::lock_guard<std::mutex> lk(srv->mu);
