@@ -38,8 +38,39 @@ def te_field(mode):
     return Et, nh
 
 
+def slab_te10_field(mode, freq):
+    """TE10-like mode of a guide loaded by a centred full-height slab (width w along
+    the wide side u, permittivity eps_slab; eps_air outside): E = v Ev(x),
+    Ev = cos(kd x) for |x| < w/2 and cos(kd w/2) sin(ka (a/2 - |x|)) / sin(ka (a - w)/2)
+    outside (x measured from the centre of the wide side), beta from the dispersion
+    relation (port2d.slab_beta).  Peak |Ev| = 1."""
+    from .port2d import slab_beta
+    o, uh, vh, nh = _frame(mode)
+    a, w = mode["a"], mode["w"]
+    k0 = 2 * np.pi * freq * np.sqrt(MU0 * EPS0)
+    beta = slab_beta(a, w, mode["eps_slab"], freq, eps_air=mode["eps_air"])
+    kd = np.sqrt(mode["eps_slab"] * k0 ** 2 - beta ** 2 + 0j)
+    ka = np.sqrt(mode["eps_air"] * k0 ** 2 - beta ** 2 + 0j)
+    outer = np.cos(kd * w / 2) / np.sin(ka * (a - w) / 2)
+
+    def prof(x):
+        ax = np.abs(x)
+        return np.where(ax < w / 2, np.cos(kd * x), outer * np.sin(ka * (a / 2 - ax)))
+
+    xs = np.linspace(-a / 2, a / 2, 4001)
+    peak = np.abs(prof(xs)).max()
+
+    def Et(X):
+        X = np.atleast_2d(X)
+        x = (X - o) @ uh - a / 2
+        return (prof(x) / peak)[:, None] * vh[None, :].astype(np.complex128)
+    return Et, nh, beta
+
+
 def mode_metrics(mode, freq, eps_c, mu_r):
     """gamma, Z, V, Pz and the field callables at one frequency."""
+    if mode.get("kind") == "SLAB_TE10":
+        return _slab_metrics(mode, freq, mu_r)
     assert mode.get("kind", "TE") == "TE"
     w = 2 * np.pi * freq
     k0 = w * np.sqrt(MU0 * EPS0)
@@ -72,3 +103,34 @@ def mode_metrics(mode, freq, eps_c, mu_r):
     Pz = 0.5 * np.sum(W * (np.cross(E, np.conj(H)) @ nh))
     Z = 0.5 * V * np.conj(V) / np.conj(Pz)
     return {"gamma": gamma, "Z": Z, "V": V, "Pz": Pz, "Et": Et, "Ht": Ht}
+
+
+def _slab_metrics(mode, freq, mu_r):
+    w_ = 2 * np.pi * freq
+    Et, nh, beta = slab_te10_field(mode, freq)
+    gamma = 1j * beta
+    fac = gamma / (1j * w_ * mu_r * MU0)
+
+    def Ht(X):
+        return fac * np.cross(nh[None, :], Et(X))
+
+    p0 = np.asarray(mode["vpath"][0], dtype=np.float64)
+    p1 = np.asarray(mode["vpath"][1], dtype=np.float64)
+    x, wq = roots_legendre(24)
+    s = 0.5 * (x + 1)
+    X = p0[None, :] + s[:, None] * (p1 - p0)[None, :]
+    V = -np.sum(0.5 * wq * (Et(X) @ (p1 - p0)))
+    # Pz over the rectangle, split at the slab faces so every piece is smooth
+    o, uh, vh, _ = _frame(mode)
+    a, b, w = mode["a"], mode["b"], mode["w"]
+    xq, wx = roots_legendre(32)
+    cuts = [0.0, (a - w) / 2, (a + w) / 2, a]
+    Pz = 0.0
+    for u0, u1 in zip(cuts[:-1], cuts[1:]):
+        U, Vv = np.meshgrid(u0 + 0.5 * (u1 - u0) * (xq + 1), 0.5 * b * (xq + 1), indexing="ij")
+        W = np.outer(0.5 * (u1 - u0) * wx, 0.5 * b * wx).ravel()
+        Xr = o[None, :] + U.ravel()[:, None] * uh[None, :] + Vv.ravel()[:, None] * vh[None, :]
+        Pz = Pz + 0.5 * np.sum(W * (np.cross(Et(Xr), np.conj(Ht(Xr))) @ nh))
+    Z = 0.5 * V * np.conj(V) / np.conj(Pz)
+    return {"gamma": gamma, "Z": Z, "V": V, "Pz": Pz, "Et": Et, "Ht": Ht}
+

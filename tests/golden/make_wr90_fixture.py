@@ -3,10 +3,13 @@
 Reads, from the reference tree given on the command line (default
 /root/reference):
   regression/OpenParEM3D/WR90/straight/straight.msh      (gmsh 2.2 mesh, 282 tets)
+  regression/OpenParEM3D/WR90/straight-loaded/straight-loaded.msh
   regression/OpenParEM3D/regression_results.csv.current  (the reference's own
                                                           recorded found values)
 and writes
   tests/golden/wr90_straight_mesh.npz   vertex coordinates (m) and tetrahedra
+  tests/golden/wr90_loaded_mesh.npz     the same for straight-loaded.msh (physical
+                                        volume 1 = air, 2 = teflon)
   tests/golden/wr90_expected.json       found S-parameter values per case (straight,
                                         straight-lossy, straight-loaded)
 
@@ -72,6 +75,8 @@ def main(ref):
     wr = os.path.join(ref, "regression", "OpenParEM3D", "WR90")
     xyz, tets, phys = read_gmsh22(os.path.join(wr, "straight", "straight.msh"))
     np.savez_compressed(os.path.join(HERE, "wr90_straight_mesh.npz"), verts=xyz, tets=tets, phys=phys)
+    xyz, tets, phys = read_gmsh22(os.path.join(wr, "straight-loaded", "straight-loaded.msh"))
+    np.savez_compressed(os.path.join(HERE, "wr90_loaded_mesh.npz"), verts=xyz, tets=tets, phys=phys)
     res = read_results(os.path.join(ref, "regression", "OpenParEM3D", "regression_results.csv.current"))
     keep = {}
     for proj in ("./WR90/straight/straight.proj", "./WR90/straight-lossy/straight.proj",

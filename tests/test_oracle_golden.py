@@ -10,6 +10,12 @@ port 2 the z=0 plane; both are driven by the analytic TE10 mode.
 Tolerances: the reference prints 15 digits and used 2D FEM port modes; with
 analytic TE10 modes the oracle agrees to ~1e-8 deg in arg(S21) (lossless)
 and ~3e-6 deg (lossy); |S21| in dB to 1e-7 dB.
+
+The slab-loaded guide (WR90/straight-loaded, 252-tet mesh
+tests/golden/wr90_loaded_mesh.npz: teflon eps_r 2.2 for |x| < 1 mm, air
+elsewhere, 8.3 GHz) is driven by the exact TE10-like slab mode
+(oracle.modes SLAB_TE10); at ND order 6 the oracle reproduces the reference's
+found arg(S21) to ~1e-7 deg.
 """
 import json
 import os
@@ -95,3 +101,37 @@ def test_analytic_phase_convergence():
         errs.append(abs(np.angle(S[1, 0], deg=True) - exact))
         assert abs(abs(S[1, 0]) - 1) < 1e-3
     assert errs[1] < errs[0] / 10
+
+
+def loaded_problem(order):
+    d = np.load(os.path.join(HERE, "golden", "wr90_loaded_mesh.npz"))
+    verts, tets, phys = d["verts"], d["tets"], d["phys"]
+    tris = meshgen.boundary_faces(tets)
+    tz = verts[tris][:, :, 2]
+    attr = np.ones(len(tris), dtype=np.int64)
+    attr[np.all(np.abs(tz - 0.1) < 1e-9, axis=1)] = 2
+    attr[np.all(np.abs(tz - 0.0) < 1e-9, axis=1)] = 3
+    a, b = 22.86e-3, 10.16e-3
+
+    def mode(z, outward):
+        m = meshgen.te10_mode(a, b, z, outward)
+        m.update(kind="SLAB_TE10", w=2e-3, eps_slab=2.2, eps_air=1.0006)
+        return m
+    return {"verts": verts, "tets": tets, "tet_region": (phys - 1).astype(np.int64),
+            "bdr_tris": tris, "bdr_attr": attr, "order": order,
+            "eps_r": np.array([1.0006, 2.2]), "tand": np.zeros(2), "sigma": np.zeros(2), "mu_r": np.ones(2),
+            "boundaries": {1: {"type": "pec"}, 2: {"type": "port", "port": 0}, 3: {"type": "port", "port": 1}},
+            "ports": [{"mode": mode(0.1, +1)}, {"mode": mode(0.0, -1)}]}
+
+
+def test_wr90_loaded_nd6_pin():
+    d = np.load(os.path.join(HERE, "golden", "wr90_loaded_mesh.npz"))
+    assert d["tets"].shape == (252, 4) and set(np.unique(d["phys"])) == {1, 2}
+    c = expected("./WR90/straight-loaded/straight-loaded.proj")
+    f = 8.3e9
+    S = fem.solve_frequency(fem.Operators(loaded_problem(6)), f)["S"]
+    assert abs(np.angle(S[1, 0], deg=True) - found(c, f, "argS(deg)", 2, 1)) < 1e-6
+    assert abs(np.angle(S[0, 1], deg=True) - found(c, f, "argS(deg)", 1, 2)) < 1e-6
+    assert abs(20 * np.log10(abs(S[1, 0])) - found(c, f, "magS(dB)", 2, 1)) < 1e-9
+    assert abs(20 * np.log10(abs(S[0, 0])) - found(c, f, "magS(dB)", 1, 1)) < 0.05
+
