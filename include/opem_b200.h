@@ -163,6 +163,17 @@ int  opem_project_load(opem_context ctx, const char* proj_path, int order, opem_
  * reason when the project cannot be read (OPEM_ERR_ARG).                       */
 int  opem_project_info(const char* proj_path, int order, int64_t* info, int ninfo, double* freqs, int max_freqs,
                        char* msg, int msg_len);
+/* The problem arrays opem_project_load would pass to opem_problem_create and the
+ * set_* calls, on the host: counts[8] = {vertices, tets, regions, exterior faces,
+ * boundary attributes, ports, frequency points, order}; then (any may be NULL)
+ * verts (3 per vertex), tets (4 per tet), region (per tet), region_mat
+ * (eps_r, tan_d, sigma, mu_r per region), tris (3 per face), attr (per face,
+ * 1-based), bdr_type and bdr_params (3 per attribute: port index | sigma, Rz,
+ * mu_r | eta), port_desc (22 per port, as opem_problem_set_port_te), freqs.
+ * Call once with only counts to size the buffers.                              */
+int  opem_project_read(const char* proj_path, int order, int64_t* counts, double* verts, int64_t* tets,
+                       int32_t* region, double* region_mat, int64_t* tris, int32_t* attr, int32_t* bdr_type,
+                       double* bdr_params, double* port_desc, double* freqs, char* msg, int msg_len);
 
 /* ---- port eigenmode of a cross-section (host only; the modal problem the
  * reference hands to OpenParEM2D, port.cpp:5081-5176) ----------------------------

@@ -451,6 +451,48 @@ int opem_project_info(const char* proj_path, int order, int64_t* info, int ninfo
     return OPEM_OK;
 }
 
+int opem_project_read(const char* proj_path, int order, int64_t* counts, double* verts, int64_t* tets,
+                      int32_t* region, double* region_mat, int64_t* tris, int32_t* attr, int32_t* bdr_type,
+                      double* bdr_params, double* port_desc, double* freqs, char* msg, int msg_len) {
+    if (!proj_path || !counts) return OPEM_ERR_ARG;
+    Project P;
+    try {
+        build(proj_path, order, P);
+    } catch (const std::exception& e) {
+        if (msg && msg_len > 0) { std::strncpy(msg, e.what(), msg_len - 1); msg[msg_len - 1] = 0; }
+        return OPEM_ERR_ARG;
+    }
+    const int64_t nv = (int64_t)P.verts.size() / 3, ne = (int64_t)P.tets.size() / 4, nr = (int64_t)P.region_mat.size();
+    const int64_t nf = (int64_t)P.attr.size(), na = (int64_t)P.bdr.size(), np = (int64_t)P.port_desc.size();
+    const int64_t nq = (int64_t)P.freqs.size();
+    counts[0] = nv; counts[1] = ne; counts[2] = nr; counts[3] = nf; counts[4] = na; counts[5] = np; counts[6] = nq;
+    counts[7] = P.order;
+    if (verts) std::memcpy(verts, P.verts.data(), P.verts.size() * sizeof(double));
+    if (tets) std::memcpy(tets, P.tets.data(), P.tets.size() * sizeof(int64_t));
+    if (region) std::memcpy(region, P.region.data(), P.region.size() * sizeof(int32_t));
+    if (region_mat)
+        for (int64_t r = 0; r < nr; ++r) {
+            region_mat[4 * r + 0] = P.region_mat[r].er;
+            region_mat[4 * r + 1] = P.region_mat[r].tand;
+            region_mat[4 * r + 2] = P.region_mat[r].sigma;
+            region_mat[4 * r + 3] = P.region_mat[r].mur;
+        }
+    if (tris) std::memcpy(tris, P.tris.data(), P.tris.size() * sizeof(int64_t));
+    if (attr) std::memcpy(attr, P.attr.data(), P.attr.size() * sizeof(int32_t));
+    for (int64_t a = 0; a < na; ++a) {
+        if (bdr_type) bdr_type[a] = P.bdr[a].first;
+        if (bdr_params)
+            for (int i = 0; i < 3; ++i) bdr_params[3 * a + i] = P.bdr[a].second[i];
+    }
+    if (port_desc)
+        for (int64_t p = 0; p < np; ++p)
+            for (int i = 0; i < 22; ++i) port_desc[22 * p + i] = P.port_desc[p][i];
+    if (freqs)
+        for (int64_t q = 0; q < nq; ++q) freqs[q] = P.freqs[q];
+    if (msg && msg_len > 0) msg[0] = 0;
+    return OPEM_OK;
+}
+
 int opem_project_load(opem_context ctx, const char* proj_path, int order, opem_problem* out, int* nfreq,
                       double* freqs, int max_freqs) {
     if (!ctx || !proj_path || !out) return OPEM_ERR_ARG;

@@ -93,6 +93,53 @@ def project_info(proj_path, order=0):
     return info, fr[:min(info["frequencies"], len(fr))]
 
 
+def project_problem(proj_path, order=0):
+    """An OpenParEM3D project read on the host (opem_project_read) as a problem
+    dict (the format of meshgen's problems, accepted by Fem3D and by the oracle)
+    plus its frequency plan."""
+    L = _lib.lib()
+    cnt = np.zeros(8, dtype=np.int64)
+    msg = C.create_string_buffer(512)
+    path = str(proj_path).encode()
+    nul = None
+    rc = L.opem_project_read(path, int(order), cnt.ctypes.data_as(_lib.I64P), nul, nul, nul, nul, nul, nul, nul, nul,
+                             nul, nul, msg, 512)
+    if rc != _lib.OK:
+        raise OpemError(rc, f"opem_project_read: {msg.value.decode()}")
+    nv, ne, nr, nf, na, npt, nq, p = (int(v) for v in cnt)
+    verts = np.zeros((nv, 3)); tets = np.zeros((ne, 4), dtype=np.int64); reg = np.zeros(ne, dtype=np.int32)
+    mat = np.zeros((nr, 4)); tris = np.zeros((nf, 3), dtype=np.int64); attr = np.zeros(nf, dtype=np.int32)
+    bt = np.zeros(na, dtype=np.int32); bp = np.zeros((na, 3)); pd = np.zeros((max(npt, 1), 22)); fr = np.zeros(max(nq, 1))
+    rc = L.opem_project_read(path, int(order), cnt.ctypes.data_as(_lib.I64P), _dp(verts), tets.ctypes.data_as(_lib.I64P),
+                             reg.ctypes.data_as(_lib.I32P), _dp(mat), tris.ctypes.data_as(_lib.I64P),
+                             attr.ctypes.data_as(_lib.I32P), bt.ctypes.data_as(_lib.I32P), _dp(bp), _dp(pd), _dp(fr),
+                             msg, 512)
+    if rc != _lib.OK:
+        raise OpemError(rc, f"opem_project_read: {msg.value.decode()}")
+    names = {v: k for k, v in _BTYPES.items()}
+    bnd = {}
+    for a in range(na):
+        t = names[int(bt[a])]
+        if t == "port":
+            bnd[a + 1] = {"type": "port", "port": int(bp[a, 0])}
+        elif t == "impedance":
+            bnd[a + 1] = {"type": "impedance", "sigma": bp[a, 0], "Rz": bp[a, 1], "mu_r": bp[a, 2]}
+        elif t == "radiation":
+            bnd[a + 1] = {"type": "radiation", "wave_impedance": bp[a, 0]}
+        else:
+            bnd[a + 1] = {"type": t}
+    ports = []
+    for k in range(npt):
+        d = pd[k]
+        ports.append({"mode": {"kind": "TE", "m": int(d[14]), "n": int(d[15]), "a": d[12], "b": d[13],
+                               "origin": d[0:3].tolist(), "u": d[3:6].tolist(), "v": d[6:9].tolist(),
+                               "normal": d[9:12].tolist(), "vpath": (d[16:19].tolist(), d[19:22].tolist())}})
+    prob = {"verts": verts, "tets": tets, "tet_region": reg.astype(np.int64), "bdr_tris": tris,
+            "bdr_attr": attr.astype(np.int64), "order": p, "eps_r": mat[:, 0], "tand": mat[:, 1],
+            "sigma": mat[:, 2], "mu_r": mat[:, 3], "boundaries": bnd, "ports": ports}
+    return prob, fr[:nq]
+
+
 class Fem3D:
     """One mesh + materials + boundaries resident on the device."""
 

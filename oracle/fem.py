@@ -308,7 +308,9 @@ def solve_frequency(ops, freq, return_fields=False, reciprocal=True):
     Cm = np.zeros((N, N), dtype=np.complex128)
     fields = []
     P = ops.M1.tocsc()
-    Plu = spla.splu(P)
+    # minimum degree on A+A^T (FEM matrices are structurally symmetric); the
+    # mass matrix is symmetric positive definite, so no pivoting is needed
+    Plu = spla.splu(P, permc_spec="MMD_AT_PLUS_A", options=dict(SymmetricMode=True, DiagPivotThresh=0.0))
     for d in range(N):
         A = assemble_A(ops, freq, d)
         A = eliminate(A, ops.pec_dofs)
@@ -318,7 +320,7 @@ def solve_frequency(ops, freq, return_fields=False, reciprocal=True):
         b = -(A @ x0)
         b[pd] = x0[pd]
         A = eliminate(A, pd)
-        e = spla.splu(A.tocsc()).solve(b)
+        e = spla.splu(A.tocsc(), permc_spec="MMD_AT_PLUS_A").solve(b)
         qe = (ops.Q_mu @ e) / (w * MU0)
         h = 1j * (Plu.solve(qe.real) + 1j * Plu.solve(qe.imag))
         for k in range(N):

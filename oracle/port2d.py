@@ -117,7 +117,7 @@ def solve_mode(pts, tris, freq, eps_r, mu_r=None):
     A = A[keep][:, keep].tocsc()
     B = B[keep][:, keep].tocsc()
     sigma = -k0 ** 2 * np.max(np.real(eps_r * mu_r))
-    lu = spla.splu((A - sigma * B).tocsc())
+    lu = spla.splu((A - sigma * B).tocsc(), permc_spec="MMD_AT_PLUS_A")
     op = spla.LinearOperator(A.shape, matvec=lambda x: lu.solve(B @ x), dtype=complex)
     mu, vec = spla.eigs(op, k=1, which="LM")
     lam = sigma + 1.0 / mu[0]

@@ -11,7 +11,14 @@ and writes
   tests/golden/wr90_loaded_mesh.npz     the same for straight-loaded.msh (physical
                                         volume 1 = air, 2 = teflon)
   tests/golden/wr90_expected.json       found S-parameter values per case (straight,
-                                        straight-lossy, straight-loaded)
+                                        straight-lossy, straight-loaded, and the
+                                        projects below)
+and, for the project-reader pins, from
+  regression/OpenParEM3D/WR90/{straight-flipped,straight-rotated-xyz,shorted,opened}
+  tests/golden/wr90_projects.npz        their meshes (vertices, tetrahedra, physical tags)
+  tests/golden/wr90_projects.json       their ports files (paths, boundaries, ports)
+                                        as data, mesh order, frequency points and
+                                        the database entries of their materials
 
 Run once in a container that has the reference tree; the outputs are
 committed so the tests never need the reference at run time.
@@ -71,6 +78,122 @@ def read_results(path):
     return out
 
 
+def read_physical_names(path):
+    with open(path) as f:
+        lines = [ln.strip() for ln in f]
+    if "$PhysicalNames" not in lines:
+        return {}
+    i = lines.index("$PhysicalNames")
+    out = {}
+    for ln in lines[i + 2:i + 2 + int(lines[i + 1])]:
+        dim, tag, name = ln.split(maxsplit=2)
+        if dim == "3":
+            out[int(tag)] = name.strip('"')
+    return out
+
+
+def _point(v):
+    return [float(t) for t in v.strip().strip("()").split(",")]
+
+
+def read_ports_file(path):
+    """The Path, Boundary and Port blocks of an OpenParEM ports file as plain data
+    (File blocks and comments dropped)."""
+    spec = {"paths": [], "boundaries": [], "ports": []}
+    block, port_line, ipath = None, None, None
+    with open(path) as f:
+        for raw in f:
+            ln = raw.split("//")[0].strip()
+            if not ln or ln.startswith("#"):
+                continue
+            if ln in ("Path", "Boundary", "Port", "File"):
+                block = {"kind": ln, "paths": [], "points": [], "lines": []}
+                continue
+            if ln in ("EndPath", "EndBoundary", "EndPort", "EndFile"):
+                k = block["kind"]
+                if k == "Path":
+                    spec["paths"].append({"name": block["name"], "points": block["points"],
+                                          "closed": block.get("closed", "false") == "true"})
+                elif k == "Boundary":
+                    spec["boundaries"].append({"name": block["name"], "type": block["type"],
+                                               "material": block.get("material"), "paths": block["paths"]})
+                elif k == "Port":
+                    spec["ports"].append({"name": block["name"], "paths": block["paths"],
+                                          "impedance_definition": block.get("impedance_definition"),
+                                          "impedance_calculation": block.get("impedance_calculation"),
+                                          "lines": block["lines"]})
+                block = None
+                continue
+            if block is None or block["kind"] == "File":
+                continue
+            if ln == "Line":
+                port_line = {"Sport": None, "integration": []}
+                continue
+            if ln == "EndLine":
+                block["lines"].append(port_line)
+                port_line = None
+                continue
+            if ln == "IntegrationPath":
+                ipath = {"type": None, "paths": []}
+                continue
+            if ln == "EndIntegrationPath":
+                port_line["integration"].append(ipath)
+                ipath = None
+                continue
+            key, val = (t.strip() for t in ln.split("=", 1))
+            if ipath is not None:
+                if key == "path":
+                    ipath["paths"].append(val)
+                else:
+                    ipath[key] = val
+            elif port_line is not None:
+                port_line[key] = int(val) if key == "Sport" else val
+            elif key == "point":
+                block["points"].append(_point(val))
+            elif key == "path":
+                block["paths"].append(val)
+            else:
+                block[key] = val
+    return spec
+
+
+def read_proj(path):
+    out = {"freqs": []}
+    with open(path) as f:
+        for ln in f:
+            t = ln.split("//")[0].split()
+            if len(t) < 2:
+                continue
+            if t[0] == "mesh.order":
+                out["order"] = int(t[1])
+            elif t[0] == "frequency.plan.point":
+                out["freqs"].append(float(t[1]))
+            elif t[0] in ("mesh.file", "port.definition.file", "materials.global.path", "materials.global.name"):
+                out[t[0]] = t[1]
+    return out
+
+
+def read_material(path, name):
+    """er, mur, tand, conductivity, Rz of one material of a materials database
+    (the temperature=any / frequency=any entry)."""
+    with open(path) as f:
+        lines = [ln.strip() for ln in f]
+    i = lines.index(f"name={name}")
+    out = {}
+    for ln in lines[i + 1:]:
+        if ln == "EndMaterial":
+            break
+        if "=" in ln:
+            k, v = ln.split("=", 1)
+            if k in ("er", "mur", "tand", "conductivity", "Rz"):
+                out[k] = float(v)
+    return out
+
+
+PROJECTS = {"straight-flipped": "straight-flipped", "straight-rotated-xyz": "straight-rotated",
+            "shorted": "shorted", "opened": "opened"}
+
+
 def main(ref):
     wr = os.path.join(ref, "regression", "OpenParEM3D", "WR90")
     xyz, tets, phys = read_gmsh22(os.path.join(wr, "straight", "straight.msh"))
@@ -82,6 +205,23 @@ def main(ref):
     for proj in ("./WR90/straight/straight.proj", "./WR90/straight-lossy/straight.proj",
                  "./WR90/straight-loaded/straight-loaded.proj"):
         keep[proj] = res[proj]
+    arrays, projects = {}, {}
+    for d, stem in PROJECTS.items():
+        pd = os.path.join(wr, d)
+        pj = read_proj(os.path.join(pd, stem + ".proj"))
+        xyz, tets, phys = read_gmsh22(os.path.join(pd, pj["mesh.file"]))
+        key = d.replace("-", "_")
+        arrays[key + "_verts"], arrays[key + "_tets"], arrays[key + "_phys"] = xyz, tets, phys
+        names = read_physical_names(os.path.join(pd, pj["mesh.file"]))
+        mdb = os.path.join(pd, pj["materials.global.path"], pj["materials.global.name"])
+        projects[d] = {"stem": stem, "npz_key": key, "order": pj["order"], "freqs": pj["freqs"],
+                       "physical_names": {str(k): v for k, v in names.items()},
+                       "materials": {v: read_material(mdb, v) for v in sorted(set(names.values()))},
+                       "ports_file": read_ports_file(os.path.join(pd, pj["port.definition.file"]))}
+        keep[f"./WR90/{d}/{stem}.proj"] = res[f"./WR90/{d}/{stem}.proj"]
+    np.savez_compressed(os.path.join(HERE, "wr90_projects.npz"), **arrays)
+    with open(os.path.join(HERE, "wr90_projects.json"), "w") as f:
+        json.dump({"source": "regression/OpenParEM3D/WR90", "projects": projects}, f, indent=1, sort_keys=True)
     meta = {
         "source": "regression/OpenParEM3D/regression_results.csv.current",
         "mesh": "regression/OpenParEM3D/WR90/straight/straight.msh",

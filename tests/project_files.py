@@ -7,18 +7,107 @@ import numpy as np
 from openparem_b200 import meshgen
 
 
-def write_gmsh22(path, verts, tets, tag=1, name="air"):
+def write_gmsh22(path, verts, tets, tag=1, name="air", names=None):
+    """tag: one physical volume tag, or one per tetrahedron (then names maps
+    tag -> physical name)."""
+    tags = np.broadcast_to(np.asarray(tag, dtype=np.int64), (len(tets),))
+    names = names if names is not None else {int(tag): name}
     with open(path, "w") as f:
         f.write("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n")
-        f.write(f'$PhysicalNames\n1\n3 {tag} "{name}"\n$EndPhysicalNames\n')
+        f.write(f"$PhysicalNames\n{len(names)}\n")
+        for t, nm in sorted(names.items()):
+            f.write(f'3 {int(t)} "{nm}"\n')
+        f.write("$EndPhysicalNames\n")
         f.write(f"$Nodes\n{len(verts)}\n")
         for i, v in enumerate(verts):
             f.write(f"{i + 1} {float(v[0]):.17g} {float(v[1]):.17g} {float(v[2]):.17g}\n")
         f.write("$EndNodes\n")
         f.write(f"$Elements\n{len(tets)}\n")
         for e, t in enumerate(tets):
-            f.write(f"{e + 1} 4 2 {tag} 1 {t[0] + 1} {t[1] + 1} {t[2] + 1} {t[3] + 1}\n")
+            f.write(f"{e + 1} 4 2 {tags[e]} 1 {t[0] + 1} {t[1] + 1} {t[2] + 1} {t[3] + 1}\n")
         f.write("$EndElements\n")
+
+
+def write_ports_file(path, spec):
+    """A ports file from plain data: spec = {"paths": [{name, points, closed}],
+    "boundaries": [{name, type, material, paths}], "ports": [{name, paths,
+    impedance_definition, impedance_calculation, lines: [{Sport, integration:
+    [{type, paths}]}]}]}."""
+    out = ["#OpenParEMports 1.0", ""]
+    for pth in spec["paths"]:
+        out.append("Path")
+        out.append(f"   name={pth['name']}")
+        for x in pth["points"]:
+            out.append(f"   point=({x[0]!r},{x[1]!r},{x[2]!r})")
+        out.append(f"   closed={'true' if pth['closed'] else 'false'}")
+        out += ["EndPath", ""]
+    for b in spec["boundaries"]:
+        out += ["Boundary", f"   name={b['name']}", f"   type={b['type']}"]
+        if b.get("material"):
+            out.append(f"   material={b['material']}")
+        out += [f"   path={q}" for q in b["paths"]]
+        out += ["EndBoundary", ""]
+    for p in spec["ports"]:
+        out += ["Port", f"   name={p['name']}"]
+        out += [f"   path={q}" for q in p["paths"]]
+        for k in ("impedance_definition", "impedance_calculation"):
+            if p.get(k):
+                out.append(f"   {k}={p[k]}")
+        for ln in p["lines"]:
+            out += ["   Line", f"      Sport={ln['Sport']}"]
+            for ip in ln["integration"]:
+                out += ["      IntegrationPath", f"         type={ip['type']}"]
+                out += [f"         path={q}" for q in ip["paths"]]
+                out.append("      EndIntegrationPath")
+            out.append("   EndLine")
+        out += ["EndPort", ""]
+    with open(path, "w") as f:
+        f.write("\n".join(out) + "\n")
+
+
+def write_materials(path, mats):
+    """A materials database with one temperature=any / frequency=any entry per material."""
+    with open(path, "w") as f:
+        f.write("#OpenParEMmaterials 1.0\n\n")
+        for name, m in mats.items():
+            body = "\n".join(f"         {k}={v!r}" for k, v in m.items())
+            f.write(f"Material\n   name={name}\n   Temperature\n      temperature=any\n      Frequency\n"
+                    f"         frequency=any\n{body}\n      EndFrequency\n   EndTemperature\n"
+                    f"   Source\n   EndSource\nEndMaterial\n\n")
+
+
+def write_project(d, stem, verts, tets, phys, names, ports_spec, materials, order, freqs):
+    """A complete project in directory d (stem.proj, stem.msh, stem_ports.txt,
+    materials.txt); returns the .proj path."""
+    write_gmsh22(os.path.join(d, stem + ".msh"), verts, tets, tag=phys, names=names)
+    write_ports_file(os.path.join(d, stem + "_ports.txt"), ports_spec)
+    write_materials(os.path.join(d, "materials.txt"), materials)
+    proj = os.path.join(d, stem + ".proj")
+    with open(proj, "w") as f:
+        f.write("#OpenParEM3Dproject 1.0\n\n")
+        f.write(f"mesh.file                      {stem}.msh\nmesh.order                     {order}\n")
+        f.write(f"port.definition.file           {stem}_ports.txt\n")
+        f.write("materials.global.path          ./\nmaterials.global.name          materials.txt\n")
+        f.write("materials.local.path           ./\nmaterials.local.name           //local_materials.txt\n")
+        for fr in freqs:
+            f.write(f"frequency.plan.point           {fr!r}\n")
+        f.write("solution.3D.tolerance          1e-14\n")
+    return proj
+
+
+def reference_project(d, name):
+    """One of the reference's WR90 regression projects (tests/golden/wr90_projects.*)
+    written out in directory d; returns (.proj path, its fixture record)."""
+    import json
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    with open(os.path.join(here, "wr90_projects.json")) as f:
+        rec = json.load(f)["projects"][name]
+    z = np.load(os.path.join(here, "wr90_projects.npz"))
+    k = rec["npz_key"]
+    names = {int(t): v for t, v in rec["physical_names"].items()}
+    proj = write_project(d, rec["stem"], z[k + "_verts"], z[k + "_tets"], z[k + "_phys"], names,
+                         rec["ports_file"], rec["materials"], rec["order"], rec["freqs"])
+    return proj, rec
 
 
 def _rect(name, a, b, z):

@@ -28,3 +28,24 @@ def test_project_matches_in_memory_problem(tmp_path):
     F2, _ = Fem3D.from_project(proj, order=2, context=ctx)
     S3, _, st3 = F2.assemble().solve(10e9, o)
     assert st3["converged"] == 1 and np.abs(S3).max() <= 1 + 1e-9
+
+
+@pytest.mark.parametrize("name", ["straight-rotated-xyz", "shorted", "opened"])
+def test_reference_projects_match_oracle(tmp_path, name):
+    """The reference's rotated, shorted and opened WR90 projects, read by the
+    C++ reader, solve on the device (ND2) to the oracle's S on the problem the
+    same reader produced (|dS| <= 1e-8, solver rtol 1e-12)."""
+    from oracle import fem
+    from openparem_b200.fem3d import project_problem
+    from project_files import reference_project
+    proj, _ = reference_project(str(tmp_path), name)
+    F, _ = Fem3D.from_project(proj, order=2, context=Context(0))
+    F.assemble()
+    prob, _ = project_problem(proj, order=2)
+    ops = fem.Operators(prob)
+    o = default_opts(rtol=1e-12, restart=200, maxits=6000, h_rtol=1e-13)
+    for f in (9e9, 11e9):
+        S, _, st = F.solve(f, o)
+        assert st["converged"] == 1
+        ref = fem.solve_frequency(ops, f)["S"]
+        assert np.abs(S - ref).max() <= 1e-8, (name, f, S, ref)

@@ -1,0 +1,86 @@
+"""The project reader (opem_project_read) pinned to the reference's own results.
+
+Four of the reference's WR90 regression projects (tests/golden/wr90_projects.*,
+made by tests/golden/make_wr90_fixture.py) are written out as project files,
+read by the C++ reader, and solved by the oracle at their own mesh order (6):
+  straight-flipped       the guide with its ports swapped in the ports file
+  straight-rotated-xyz   the guide rotated about x, y and z: port planes, mode
+                         frames and voltage paths off every axis
+  shorted                one port, the far end PEC
+  opened                 one port, the far end a perfect_magnetic_conductor
+                         boundary
+The oracle, fed what the reader produced, reproduces the reference's recorded
+found values to ~1e-8 deg in arg S; the test allows 1e-6 deg.  This checks the
+reader's face classification (port polygons, named boundaries, the PEC rest),
+its TE10 frames (origin, wide side, outward normal) and its voltage paths
+against the reference's own answers.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import fem
+from openparem_b200.fem3d import project_problem, project_info
+from project_files import reference_project
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+F = 9e9
+
+
+def found(name, stem, var, pout, pin, freq=F):
+    with open(os.path.join(HERE, "golden", "wr90_expected.json")) as f:
+        cases = json.load(f)["cases"][f"./WR90/{name}/{stem}.proj"]
+    for v in cases.values():
+        if v["frequency"] == freq and v["variable"] == var and v["portOut"] == pout and v["portIn"] == pin:
+            return v["found"]
+    raise KeyError((name, freq, var, pout, pin))
+
+
+def test_reference_projects_read(tmp_path):
+    expect = {"straight-flipped": (289, 2, []), "straight-rotated-xyz": (288, 2, []),
+              "shorted": (165, 1, []), "opened": (165, 1, ["pmc"])}
+    for name, (ntet, nport, extra) in expect.items():
+        d = tmp_path / name
+        d.mkdir()
+        proj, rec = reference_project(str(d), name)
+        info, fr = project_info(proj)
+        assert info["tets"] == ntet and info["ports"] == nport and info["order"] == 6, name
+        assert np.allclose(fr, rec["freqs"])
+        prob, fr2 = project_problem(proj)
+        assert np.array_equal(fr, fr2)
+        types = sorted(v["type"] for v in prob["boundaries"].values())
+        assert types == sorted(["pec"] + ["port"] * nport + extra), name
+        assert np.allclose(prob["eps_r"], [1.0006])
+        for p in prob["ports"]:
+            m = p["mode"]
+            assert abs(m["a"] - 22.86e-3) < 1e-9 and abs(m["b"] - 10.16e-3) < 1e-9
+            assert abs(np.linalg.norm(m["normal"]) - 1) < 1e-12
+            # the outward normal points away from the mesh
+            c = prob["verts"].mean(axis=0)
+            centre = np.asarray(m["origin"]) + 0.5 * m["a"] * np.asarray(m["u"]) + 0.5 * m["b"] * np.asarray(m["v"])
+            assert np.dot(centre - c, m["normal"]) > 0
+
+
+@pytest.mark.parametrize("name,stem", [("straight-flipped", "straight-flipped"),
+                                       ("straight-rotated-xyz", "straight-rotated")])
+def test_two_port_nd6_pin(tmp_path, name, stem):
+    proj, _ = reference_project(str(tmp_path), name)
+    prob, _ = project_problem(proj)
+    S = fem.solve_frequency(fem.Operators(prob), F)["S"]
+    assert abs(np.angle(S[1, 0], deg=True) - found(name, stem, "argS(deg)", 2, 1)) < 1e-6
+    assert abs(np.angle(S[0, 1], deg=True) - found(name, stem, "argS(deg)", 1, 2)) < 1e-6
+    # recorded |S11|, |S22| (about -131 dB: discretisation reflection)
+    assert abs(20 * np.log10(abs(S[0, 0])) - found(name, stem, "magS(dB)", 1, 1)) < 0.05
+    assert abs(20 * np.log10(abs(S[1, 1])) - found(name, stem, "magS(dB)", 2, 2)) < 0.05
+
+
+@pytest.mark.parametrize("name", ["shorted", "opened"])
+def test_one_port_nd6_pin(tmp_path, name):
+    proj, _ = reference_project(str(tmp_path), name)
+    prob, _ = project_problem(proj)
+    S = fem.solve_frequency(fem.Operators(prob), F)["S"]
+    assert S.shape == (1, 1)
+    assert abs(np.angle(S[0, 0], deg=True) - found(name, name, "argS(deg)", 1, 1)) < 1e-6
+    assert abs(20 * np.log10(abs(S[0, 0]))) < 1e-9          # total reflection
