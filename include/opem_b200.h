@@ -99,6 +99,12 @@ int  opem_problem_set_boundary(opem_problem prob, int attr, int type, const doub
  * desc = {origin xyz, u-axis xyz, v-axis xyz, outward normal xyz, a, b, m, n,
  *         voltage path start xyz, voltage path end xyz}  (22 doubles).          */
 int  opem_problem_set_port_te(opem_problem prob, int port, const double* desc);
+/* Port driven by the fundamental mode of its own cross-section, solved at every
+ * frequency on the port faces split nsub x nsub (1..64) with the materials of
+ * the tetrahedra behind them (the 2D solve the reference spawns per frequency,
+ * port.cpp:5081-5176; opem_port_mode_2d does the eigensolve).  desc as for
+ * opem_problem_set_port_te; its a, b, m, n are not used.                       */
+int  opem_problem_set_port_fem2d(opem_problem prob, int port, const double* desc, int nsub);
 /* Builds DOF numbering, CSR pattern, vertex patches, and assembles the frequency-
  * independent operators on the device.                                         */
 int  opem_problem_assemble(opem_problem prob);
@@ -169,11 +175,14 @@ int  opem_project_info(const char* proj_path, int order, int64_t* info, int ninf
  * verts (3 per vertex), tets (4 per tet), region (per tet), region_mat
  * (eps_r, tan_d, sigma, mu_r per region), tris (3 per face), attr (per face,
  * 1-based), bdr_type and bdr_params (3 per attribute: port index | sigma, Rz,
- * mu_r | eta), port_desc (22 per port, as opem_problem_set_port_te), freqs.
+ * mu_r | eta), port_desc (22 per port, as opem_problem_set_port_te), port_nsub
+ * (per port: 0 = analytic TE10, n > 0 = its own 2D mode with faces split n x n,
+ * chosen for ports whose faces see more than one material), freqs.
  * Call once with only counts to size the buffers.                              */
 int  opem_project_read(const char* proj_path, int order, int64_t* counts, double* verts, int64_t* tets,
                        int32_t* region, double* region_mat, int64_t* tris, int32_t* attr, int32_t* bdr_type,
-                       double* bdr_params, double* port_desc, double* freqs, char* msg, int msg_len);
+                       double* bdr_params, double* port_desc, int32_t* port_nsub, double* freqs, char* msg,
+                       int msg_len);
 
 /* ---- port eigenmode of a cross-section (host only; the modal problem the
  * reference hands to OpenParEM2D, port.cpp:5081-5176) ----------------------------
@@ -189,6 +198,18 @@ int  opem_project_read(const char* proj_path, int order, int64_t* counts, double
 int  opem_port_mode_2d(int64_t nnodes, const double* xy, int64_t ntri, const int64_t* tris, const double* eps_r,
                        const double* mu_r, double freq, double* beta_out, int64_t* nedges, int64_t* edges_out,
                        double* et_out, double* ez_out);
+/* The mode opem_problem_set_port_fem2d uses, on the host: port faces given as
+ * vertex triples (face_verts, 3 per face, in the face's local vertex order) of
+ * verts (3 doubles each), eps_face / mu_face complex per face (interleaved;
+ * mu_face may be NULL), desc and nsub as for opem_problem_set_port_fem2d.
+ * metrics = {gamma, Z, V, Pz} (4 complex, interleaved).  For npts points, each
+ * given as a face (pt_face) and its parameters (pt_s: s1, s2 with
+ * X = P0 + s1 (P1 - P0) + s2 (P2 - P0)), E_out and Hy_out (3 complex each, may
+ * be NULL) receive E_t and H_t / y, y = gamma / (j w mu0 mu_r(face 0)).        */
+int  opem_port_mode_faces(int64_t nverts, const double* verts, int64_t nface, const int64_t* face_verts,
+                          const double* eps_face, const double* mu_face, const double* desc, int nsub, double freq,
+                          double* metrics, int64_t npts, const int64_t* pt_face, const double* pt_s, double* E_out,
+                          double* Hy_out);
 
 /* ---- S-parameter post-processing (host only, no GPU needed) -----------------
  * Renormalises S (nports x nports complex, interleaved, row = portOut) from the

@@ -71,7 +71,54 @@ static void te_eval(const double* d, const double* X, double* E) {
     for (int i = 0; i < 3; ++i) E[i] = Eu * u[i] / nu + Ev * v[i] / nv;
 }
 
+static const int FV[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
+
+bool has_fem2d_ports(const Problem& P) {
+    for (int k = 0; k < P.nports && k < (int)P.modes.size(); ++k)
+        if (P.modes[k].kind == 1) return true;
+    return false;
+}
+
+// The 2D mode of port k at freq, from the cache or solved now.  The port faces
+// are taken in the order port_traces visits them.
+static std::shared_ptr<const PortFem2D> port_fem2d(const Problem& P, int k, double freq) {
+    const PortMode& pm = P.modes[k];
+    std::lock_guard<std::mutex> lk(pm.fem->mu);
+    for (auto& e : pm.fem->sols)
+        if (e.first == freq) return e.second;
+    const Topology& T = P.topo;
+    std::vector<int64_t> fv;
+    std::vector<cd> eps, mu;
+    const double w = 2 * M_PI * freq;
+    for (const BGroup& G : P.groups) {
+        if (G.type != OPEM_BDR_PORT || G.port != k) continue;
+        for (int32_t f : G.faces) {
+            const int t = T.face_owner[f], lf = T.face_lface[f];
+            for (int c = 0; c < 3; ++c) fv.push_back(T.tets[4 * (size_t)t + FV[lf][c]]);
+            const int r = T.region[t];
+            eps.push_back(P.eps_r[r] * cd(1.0, -P.tand[r]) - cd(0.0, P.sigma[r] / (w * EPS0)));
+            mu.push_back(cd(P.mu_r[r], 0.0));
+        }
+    }
+    if (fv.empty()) throw OpemError(OPEM_ERR_ARG, "port without faces");
+    auto sol = std::make_shared<PortFem2D>();
+    std::string err;
+    int rc = port_fem2d_solve(T.verts.data(), (int64_t)fv.size() / 3, fv.data(), eps.data(), mu.data(), pm.desc,
+                              pm.nsub, freq, mu[0].real(), *sol, err);
+    if (rc != OPEM_OK) throw OpemError(rc, err);
+    pm.fem->sols.emplace_back(freq, sol);
+    if (pm.fem->sols.size() > 8) pm.fem->sols.erase(pm.fem->sols.begin());
+    return sol;
+}
+
 void port_gamma_Z_V(const Problem& P, int k, double freq, cd& gamma, cd& Z, cd& V) {
+    if (P.modes[k].kind == 1) {
+        auto sol = port_fem2d(P, k, freq);
+        gamma = sol->gamma;
+        Z = sol->Z;
+        V = sol->V;
+        return;
+    }
     const double* d = P.modes[k].desc;
     int r = port_region(P, k);
     double w = 2 * M_PI * freq, k0 = w * std::sqrt(MU0 * EPS0);
@@ -105,12 +152,19 @@ void port_gamma_Z_V(const Problem& P, int k, double freq, cd& gamma, cd& Z, cd& 
 
 // Trace DOFs of a tangential field on one port (Mode::fillX's data, port.cpp:3234-3341):
 // the edge and face moment functionals applied to E_t and n x E_t.
-static void port_traces(Problem& P, int k, std::vector<double>& et, std::vector<double>& nxe) {
+static void port_traces_fem2d(Problem& P, int k, std::vector<double>& et, std::vector<double>& nxe, double freq);
+
+static void port_traces(Problem& P, int k, std::vector<double>& et, std::vector<double>& nxe, double freq) {
+    if (P.modes[k].kind == 1) {
+        port_traces_fem2d(P, k, et, nxe, freq);
+        return;
+    }
     const Topology& T = P.topo;
     const NDRef& R = nd_reference(T.p);
     const int p = T.p;
     et.assign(2 * T.n, 0.0);
     nxe.assign(2 * T.n, 0.0);
+    std::vector<uint8_t> cnt(T.n, 0);
     const double* d = P.modes[k].desc;
     double nrm[3] = {d[9], d[10], d[11]};
     double nn = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
@@ -123,12 +177,14 @@ static void port_traces(Problem& P, int k, std::vector<double>& et, std::vector<
     std::vector<double> T2;
     if (p >= 2) T2 = tri_test_polys(p - 2, mon2);
     int nq2 = (int)mon2.size() / 2;
-    static const int FV[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
-    auto fields = [&](const double* X, double* E, double* NE) {
-        te_eval(d, X, E);
-        NE[0] = nrm[1] * E[2] - nrm[2] * E[1];
-        NE[1] = nrm[2] * E[0] - nrm[0] * E[2];
-        NE[2] = nrm[0] * E[1] - nrm[1] * E[0];
+    // E_t and n x E_t of the analytic mode at X
+    auto fields = [&](const double* X, cd* E, cd* NE) {
+        double Er[3];
+        te_eval(d, X, Er);
+        for (int i = 0; i < 3; ++i) E[i] = Er[i];
+        NE[0] = nrm[1] * Er[2] - nrm[2] * Er[1];
+        NE[1] = nrm[2] * Er[0] - nrm[0] * Er[2];
+        NE[2] = nrm[0] * Er[1] - nrm[1] * Er[0];
     };
     for (const BGroup& G : P.groups) {
         if (G.type != OPEM_BDR_PORT || G.port != k) continue;
@@ -139,15 +195,17 @@ static void port_traces(Problem& P, int k, std::vector<double>& et, std::vector<
             double Pv[3][3];
             for (int c = 0; c < 3; ++c)
                 for (int i = 0; i < 3; ++i) Pv[c][i] = T.verts[3 * (size_t)tv[FV[lf][c]] + i];
-            std::vector<double> ve, vn;
+            std::vector<cd> ve, vn;
             const int pairs[3][2] = {{0, 1}, {0, 2}, {1, 2}};
-            for (auto& pr : pairs) {
+            for (int e = 0; e < 3; ++e) {
+                const int* pr = pairs[e];
                 double tv3[3];
                 for (int i = 0; i < 3; ++i) tv3[i] = Pv[pr[1]][i] - Pv[pr[0]][i];
                 for (int kk = 0; kk < p; ++kk) {
-                    double ae = 0, an = 0;
+                    cd ae = 0, an = 0;
                     for (size_t q = 0; q < s.size(); ++q) {
-                        double X[3], E[3], NE[3];
+                        double X[3];
+                        cd E[3], NE[3];
                         for (int i = 0; i < 3; ++i) X[i] = Pv[pr[0]][i] + s[q] * tv3[i];
                         fields(X, E, NE);
                         double L = shifted_legendre(kk, s[q]);
@@ -164,9 +222,10 @@ static void port_traces(Problem& P, int k, std::vector<double>& et, std::vector<
                 for (int r = 0; r < nq2; ++r)
                     for (int tm = 0; tm < 2; ++tm) {
                         const double* tt = tm ? t2 : t1;
-                        double ae = 0, an = 0;
+                        cd ae = 0, an = 0;
                         for (size_t q = 0; q < wt.size(); ++q) {
-                            double X[3], E[3], NE[3];
+                            double X[3];
+                            cd E[3], NE[3];
                             for (int i = 0; i < 3; ++i) X[i] = Pv[0][i] + s1[q] * t1[i] + s2[q] * t2[i];
                             fields(X, E, NE);
                             double qv = 0;
@@ -181,11 +240,148 @@ static void port_traces(Problem& P, int k, std::vector<double>& et, std::vector<
             }
             for (int a2 = 0; a2 < T.ldf; ++a2) {
                 int32_t g = ed[R.face_dofs[lf][a2]];
-                et[2 * (size_t)g] = ve[a2];
-                nxe[2 * (size_t)g] = vn[a2];
+                et[2 * (size_t)g] += ve[a2].real();
+                et[2 * (size_t)g + 1] += ve[a2].imag();
+                nxe[2 * (size_t)g] += vn[a2].real();
+                nxe[2 * (size_t)g + 1] += vn[a2].imag();
+                cnt[g] += 1;
             }
         }
     }
+    // an edge inside the port gets the mean of its two faces' moments (equal:
+    // both faces evaluate the same points of a continuous field)
+    for (size_t g = 0; g < cnt.size(); ++g)
+        if (cnt[g] > 1)
+            for (int c = 0; c < 2; ++c) {
+                et[2 * g + c] /= cnt[g];
+                nxe[2 * g + c] /= cnt[g];
+            }
+}
+
+// Trace DOFs of a port's 2D mode: the same moment functionals as port_traces,
+// integrated cell by cell over the face's split (composite rules: the mode is
+// piecewise linear on the sub-triangles), E_t and H_t / y evaluated on the face
+// being traced.  An edge inside the port gets the mean of its two faces'
+// moments: E_t's tangential trace is the same from both sides, H_t's (a normal
+// component of the edge-element field) jumps between cells.
+static void port_traces_fem2d(Problem& P, int k, std::vector<double>& et, std::vector<double>& nxe, double freq) {
+    const Topology& T = P.topo;
+    std::shared_ptr<const PortFem2D> fem = port_fem2d(P, k, freq);
+    const NDRef& R = nd_reference(T.p);
+    const int p = T.p, N = fem->nsub;
+    et.assign(2 * T.n, 0.0);
+    nxe.assign(2 * T.n, 0.0);
+    std::vector<uint8_t> cnt(T.n, 0);
+    std::vector<double> s, ws;
+    gauss_legendre01(p + 4, s, ws);
+    std::vector<double> s1, s2, wt;
+    tri_rule(2 * p + 4, s1, s2, wt);
+    std::vector<int> mon2;
+    std::vector<double> T2;
+    if (p >= 2) T2 = tri_test_polys(p - 2, mon2);
+    const int nq2 = (int)mon2.size() / 2;
+    auto dot3 = [](const cd* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+    int64_t fidx = 0;   // port-face index, in the order port_fem2d lists the faces
+    for (const BGroup& G : P.groups) {
+        if (G.type != OPEM_BDR_PORT || G.port != k) continue;
+        for (int32_t f : G.faces) {
+            const int t = T.face_owner[f], lf = T.face_lface[f];
+            const int32_t* tv = &T.tets[4 * (size_t)t];
+            const int32_t* ed = &T.elem_dofs[(size_t)t * T.ld];
+            double Pv[3][3];
+            for (int c = 0; c < 3; ++c)
+                for (int i = 0; i < 3; ++i) Pv[c][i] = T.verts[3 * (size_t)tv[FV[lf][c]] + i];
+            std::vector<cd> ve, vn;
+            const int pairs[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+            for (int e = 0; e < 3; ++e) {
+                const int* pr = pairs[e];
+                double tv3[3];
+                for (int i = 0; i < 3; ++i) tv3[i] = Pv[pr[1]][i] - Pv[pr[0]][i];
+                std::vector<cd> ae(p, 0.0), an(p, 0.0);
+                for (int m = 0; m < N; ++m)
+                    for (size_t q = 0; q < s.size(); ++q) {
+                        const double sp = (m + s[q]) / N, wq = ws[q] / N;
+                        double X[3];
+                        for (int i = 0; i < 3; ++i) X[i] = Pv[pr[0]][i] + sp * tv3[i];
+                        // face parameters of the edge point: (s,0), (0,s), (1-s,s)
+                        const double a1 = e == 0 ? sp : (e == 1 ? 0.0 : 1.0 - sp);
+                        const double a2 = e == 0 ? 0.0 : sp;
+                        cd E[3], H[3];
+                        fem->eval_face(fidx, a1, a2, X, E, H);
+                        const cd et_ = dot3(E, tv3), hn_ = dot3(H, tv3);
+                        for (int kk = 0; kk < p; ++kk) {
+                            const double L = shifted_legendre(kk, sp);
+                            ae[kk] += wq * L * et_;
+                            an[kk] += wq * L * hn_;
+                        }
+                    }
+                for (int kk = 0; kk < p; ++kk) { ve.push_back(ae[kk]); vn.push_back(an[kk]); }
+            }
+            if (p >= 2) {
+                double t1[3], t2[3];
+                for (int i = 0; i < 3; ++i) { t1[i] = Pv[1][i] - Pv[0][i]; t2[i] = Pv[2][i] - Pv[0][i]; }
+                std::vector<cd> ae(2 * nq2, 0.0), an(2 * nq2, 0.0);
+                for (int i = 0; i < N; ++i)
+                    for (int j = 0; j < N - i; ++j)
+                        for (int up = 0; up < 2; ++up) {
+                            if (up && i + j > N - 2) continue;
+                            const int64_t tri = fem->sub[(((size_t)fidx * (N + 1) + i) * (N + 1) + j) * 2 + up];
+                            for (size_t q = 0; q < wt.size(); ++q) {
+                                const double a1 = up ? (i + 1 - s1[q]) / N : (i + s1[q]) / N;
+                                const double a2 = up ? (j + 1 - s2[q]) / N : (j + s2[q]) / N;
+                                const double w = wt[q] / ((double)N * N);
+                                double X[3];
+                                for (int c = 0; c < 3; ++c) X[c] = Pv[0][c] + a1 * t1[c] + a2 * t2[c];
+                                cd E[3], H[3];
+                                fem->eval_tri(tri, X, E, H);
+                                const cd e1 = dot3(E, t1), e2 = dot3(E, t2), h1 = dot3(H, t1), h2 = dot3(H, t2);
+                                for (int r = 0; r < nq2; ++r) {
+                                    double qv = 0;
+                                    for (int c = 0; c < nq2; ++c)
+                                        qv += T2[r * nq2 + c] * std::pow(a1, mon2[2 * c]) * std::pow(a2, mon2[2 * c + 1]);
+                                    ae[2 * r] += w * qv * e1;
+                                    ae[2 * r + 1] += w * qv * e2;
+                                    an[2 * r] += w * qv * h1;
+                                    an[2 * r + 1] += w * qv * h2;
+                                }
+                            }
+                        }
+                for (int r = 0; r < 2 * nq2; ++r) { ve.push_back(ae[r]); vn.push_back(an[r]); }
+            }
+            for (int a2 = 0; a2 < T.ldf; ++a2) {
+                int32_t g = ed[R.face_dofs[lf][a2]];
+                et[2 * (size_t)g] += ve[a2].real();
+                et[2 * (size_t)g + 1] += ve[a2].imag();
+                nxe[2 * (size_t)g] += vn[a2].real();
+                nxe[2 * (size_t)g + 1] += vn[a2].imag();
+                cnt[g] += 1;
+            }
+            ++fidx;
+        }
+    }
+    for (size_t g = 0; g < cnt.size(); ++g)
+        if (cnt[g] > 1)
+            for (int c = 0; c < 2; ++c) {
+                et[2 * g + c] /= cnt[g];
+                nxe[2 * g + c] /= cnt[g];
+            }
+}
+
+void refresh_port_traces(Problem& P, double freq) {
+    if (!has_fem2d_ports(P) || P.trace_freq == freq) return;
+    const int64_t n = P.topo.n;
+    cudaStream_t s = P.ctx->stream;
+    for (int k = 0; k < P.nports; ++k) {
+        if (P.modes[k].kind != 1) continue;
+        std::vector<double> et, nx;
+        port_traces(P, k, et, nx, freq);
+        OPEM_CUDA(cudaMemcpyAsync(P.d_et.p + (size_t)2 * n * k, et.data(), et.size() * sizeof(double),
+                                  cudaMemcpyHostToDevice, s));
+        OPEM_CUDA(cudaMemcpyAsync(P.d_nxe.p + (size_t)2 * n * k, nx.data(), nx.size() * sizeof(double),
+                                  cudaMemcpyHostToDevice, s));
+    }
+    OPEM_CUDA(cudaStreamSynchronize(s));
+    P.trace_freq = freq;
 }
 
 void system_coefficients(const Problem& P, double freq, int d, VolCoef& vc, std::vector<BCoef>& bc) {
@@ -318,6 +514,7 @@ static void solve_frequency_plain(Problem& P, double freq, const opem_solver_opt
     DBuf<uint8_t> dm(n);
     std::vector<cd> Cp(N * N), Cm(N * N), gam(N), Z(N), V(N);
     double w = 2 * M_PI * freq;
+    refresh_port_traces(P, freq);
     for (int k = 0; k < N; ++k) port_gamma_Z_V(P, k, freq, gam[k], Z[k], V[k]);
     out.st = opem_solve_stats{};
     out.st.converged = 1;
@@ -488,13 +685,17 @@ static void assemble_problem(Problem& P) {
     // port traces
     std::vector<double> et_all((size_t)2 * T.n * std::max(1, P.nports), 0.0), nx_all(et_all.size(), 0.0);
     for (int k = 0; k < P.nports; ++k) {
+        if (P.modes[k].kind == 1) continue;   // 2D modes: traced per frequency (refresh_port_traces)
         std::vector<double> et, nx;
-        port_traces(P, k, et, nx);
+        port_traces(P, k, et, nx, 0.0);
         std::copy(et.begin(), et.end(), et_all.begin() + (size_t)2 * T.n * k);
         std::copy(nx.begin(), nx.end(), nx_all.begin() + (size_t)2 * T.n * k);
     }
     P.d_et.upload(et_all, s);
     P.d_nxe.upload(nx_all, s);
+    P.trace_freq = -1;
+    for (int k = 0; k < P.nports; ++k)
+        if (P.modes[k].kind == 1) P.modes[k].fem = std::make_shared<PortFemCache>();   // geometry may have changed
     OPEM_CUDA(cudaStreamSynchronize(s));
     P.assembled = true;
 }
@@ -706,7 +907,25 @@ int opem_problem_set_port_te(opem_problem prob, int port, const double* desc) {
     Problem& P = prob->p;
     if ((int)P.modes.size() <= port) P.modes.resize(port + 1);
     P.modes[port].set = true;
+    P.modes[port].kind = 0;
+    P.modes[port].fem.reset();
     std::memcpy(P.modes[port].desc, desc, 22 * sizeof(double));
+    P.assembled = false;
+    return OPEM_OK;
+}
+
+int opem_problem_set_port_fem2d(opem_problem prob, int port, const double* desc, int nsub) {
+    if (!prob || !desc || port < 0 || port > 7 || nsub < 1 || nsub > 64) return OPEM_ERR_ARG;
+    for (int i = 0; i < 22; ++i)
+        if (!std::isfinite(desc[i])) return OPEM_ERR_ARG;
+    Problem& P = prob->p;
+    if ((int)P.modes.size() <= port) P.modes.resize(port + 1);
+    PortMode& m = P.modes[port];
+    m.set = true;
+    m.kind = 1;
+    m.nsub = nsub;
+    m.fem = std::make_shared<PortFemCache>();
+    std::memcpy(m.desc, desc, 22 * sizeof(double));
     P.assembled = false;
     return OPEM_OK;
 }

@@ -2,11 +2,13 @@
 #pragma once
 #include <atomic>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
 #include "opem_device.h"
 #include "opem_internal.h"
+#include "portfem.h"
 
 namespace opem {
 
@@ -75,9 +77,18 @@ struct BGroup {
     DBuf<int32_t> brow, bptr;
 };
 
+// Modes a port was solved with, per frequency (ports driven by their own 2D mode)
+struct PortFemCache {
+    std::mutex mu;
+    std::vector<std::pair<double, std::shared_ptr<const PortFem2D>>> sols;   // most recent last
+};
+
 struct PortMode {
     bool set = false;
     double desc[26];
+    int kind = 0;    // 0: analytic TE_mn (desc), 1: 2D mode of the port faces
+    int nsub = 0;    // kind 1: split of each port face
+    std::shared_ptr<PortFemCache> fem;
 };
 
 struct Problem {
@@ -89,6 +100,7 @@ struct Problem {
     std::vector<std::pair<int, Bdr>> bdr;           // attr -> type
     int nports = 0;
     std::vector<PortMode> modes;
+    double trace_freq = -1;     // frequency of the device traces of ports driven by their 2D mode
     bool assembled = false;
     int64_t ws_cap = 0;         // device bytes a batched sweep may take for its workspace (0: half of free)
     std::atomic<int> cancel{0}; // set from another thread: the solvers stop at their next Krylov step
@@ -131,6 +143,10 @@ void form_system_matrix_n(Problem& P, const VolCoef& vc, const BCoef* bc, size_t
 // host: coefficients of A(freq) for driving set d
 void system_coefficients(const Problem& P, double freq, int d, VolCoef& vc, std::vector<BCoef>& bc);
 void port_gamma_Z_V(const Problem& P, int port, double freq, cd& gamma, cd& Z, cd& V);
+// Re-computes the device traces of the ports driven by their own 2D mode for
+// freq (no-op when there are none or they are current); synchronises the stream.
+void refresh_port_traces(Problem& P, double freq);
+bool has_fem2d_ports(const Problem& P);
 // overlaps <a, B_port b> for port k: out = conj(a)^T R_one b over the port's slots
 void port_overlap(Problem& P, int k, const double2* a, const double2* b, double2* out_dev);
 

@@ -1973,6 +1973,9 @@ void solve_sweep_mixed(Problem& P, int nfreq, const double* freqs, const opem_so
         if (Fm < 1) throw OpemError(OPEM_ERR_NOMEM, "not enough device memory for one batched frequency point");
         F = std::min(F, Fm);
     }
+    // ports driven by their own 2D mode have traces that change with frequency:
+    // one frequency point per batch, traces refreshed before it
+    if (has_fem2d_ports(P)) F = 1;
     int nb = (nfreq + F - 1) / F;
     F = (nfreq + nb - 1) / nb;   // balance the batches
     S.assign(nfreq, {});
@@ -1994,6 +1997,7 @@ void solve_sweep_mixed(Problem& P, int nfreq, const double* freqs, const opem_so
         std::vector<System> sys;
         for (int d = 0; d < N; ++d)
             for (int f = f0; f < f1; ++f) sys.push_back({fs[f], d});
+        refresh_port_traces(P, fs[f0]);
         BatchOut bo;
         solve_batch(P, sys, o, bo);
         if (!bo.converged && o.restart < 1024) {

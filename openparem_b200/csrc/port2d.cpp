@@ -247,11 +247,13 @@ int opem_port_mode_2d(int64_t nnodes, const double* xy, int64_t ntri, const int6
         std::fill(y.begin(), y.end(), 0.0);
         for (auto& t : Bm) y[pos[t.r]] += t.v * x[pos[t.c]];
     };
-    std::vector<cd> x(n), y(n), bx(n);
+    std::vector<cd> x(n), y(n), bx(n), xold(n);
     for (int i = 0; i < n; ++i) x[i] = cd(1.0 + 0.001 * (i % 7), 0.0005 * (i % 5));
     cd lam = 0, lam_prev = 0;
     bool ok = false;
-    for (int it = 0; it < 2000; ++it) {
+    int lam_done = 0;
+    for (int it = 0; it < 4000; ++it) {
+        xold = x;
         Bmul(x, bx);
         y = bx;
         M.solve(y);
@@ -267,7 +269,18 @@ int opem_port_mode_2d(int64_t nnodes, const double* xy, int64_t ntri, const int6
         for (int i = 0; i < n; ++i) x[i] = y[i] / nrm;
         const cd mu = num / den;
         lam = sigma + 1.0 / mu;
-        if (it > 3 && std::abs(lam - lam_prev) <= 1e-14 * std::abs(lam)) { ok = true; break; }
+        // converged when the eigenvalue has settled and the unit eigenvector stops
+        // moving (up to phase): the eigenvalue settles about twice as fast, and
+        // small components such as e_z of a TE-like mode need the vector itself
+        if (it > 3 && std::abs(lam - lam_prev) <= 1e-14 * std::abs(lam)) ++lam_done;
+        if (lam_done) {
+            cd c = 0;
+            for (int i = 0; i < n; ++i) c += std::conj(xold[i]) * x[i];
+            const cd ph = std::abs(c) > 0 ? c / std::abs(c) : cd(1.0);
+            double dx = 0;
+            for (int i = 0; i < n; ++i) dx += std::norm(x[i] - ph * xold[i]);
+            if (std::sqrt(dx) <= 1e-13 || lam_done > 200) { ok = true; break; }
+        }
         lam_prev = lam;
     }
     if (!ok) return OPEM_ERR_NOT_CONVERGED;

@@ -1,0 +1,330 @@
+// Port modes solved on the port's own faces (host).
+//
+// The reference drives every port with the mode its 2D solver finds on the
+// port's cross-section: OpenParEM3D writes the port faces out as a 2D mesh,
+// spawns OpenParEM2D (src/OpenParEM3D/port.cpp:5081-5176), reads back the modal
+// fields and metrics (load_modeMetrics, port.cpp:5302-5453) and interpolates the
+// fields onto the 3D port trace (Mode::fillX, port.cpp:3234-3341).  Here the
+// chain runs in-process:
+//   * the 2D mesh is a conforming split of the port faces, each into nsub x nsub
+//     similar triangles, with each sub-triangle's material taken from the
+//     tetrahedron that owns its face;
+//   * the fundamental mode comes from opem_port_mode_2d (lowest-order edge
+//     elements for e_t, linear nodal e_z, PEC on the outer boundary),
+//     gamma = j beta;
+//   * for propagation along the outward normal n (the convention of the
+//     analytic TE modes) H_t = n x (gamma e_t + grad_t e_z) / (j w mu);
+//   * V = -int E . dl along the voltage path (composite 4-point Gauss on
+//     16 nsub pieces), Pz = 1/2 int (E x H*) . n (edge-midpoint rule, exact for
+//     the piecewise-quadratic integrand), Z = V V* / (2 Pz*) (the PV definition).
+// The 3D port trace is then the moment interpolation of this field on each
+// port face (engine.cu port_traces), as for the analytic modes.
+#include "portfem.h"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <map>
+
+#include "../../include/opem_b200.h"
+#include "opem_internal.h"
+
+namespace opem {
+
+namespace {
+using cd = std::complex<double>;
+constexpr double MU0 = 4e-7 * M_PI;
+const int LP[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+
+void unit(const double* a, double* out) {
+    const double s = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+    for (int i = 0; i < 3; ++i) out[i] = a[i] / s;
+}
+
+// n x (gx u + gy v) for complex plane components
+void n_cross_plane(const double n[3], const double u[3], const double v[3], cd gx, cd gy, cd out[3]) {
+    cd w[3];
+    for (int i = 0; i < 3; ++i) w[i] = gx * u[i] + gy * v[i];
+    out[0] = n[1] * w[2] - n[2] * w[1];
+    out[1] = n[2] * w[0] - n[0] * w[2];
+    out[2] = n[0] * w[1] - n[1] * w[0];
+}
+}  // namespace
+
+void PortFem2D::eval_tri(int64_t t, const double X[3], cd E[3], cd Hy[3]) const {
+    const double d0 = (X[0] - o[0]) * u[0] + (X[1] - o[1]) * u[1] + (X[2] - o[2]) * u[2] - P0[2 * t];
+    const double d1 = (X[0] - o[0]) * v[0] + (X[1] - o[1]) * v[1] + (X[2] - o[2]) * v[2] - P0[2 * t + 1];
+    const double* Ji = &Jinv[4 * t];
+    const double l1 = Ji[0] * d0 + Ji[1] * d1, l2 = Ji[2] * d0 + Ji[3] * d1;
+    const double lam[3] = {1 - l1 - l2, l1, l2};
+    const double* gg = &g[6 * t];
+    cd ex = 0.0, ey = 0.0;
+    for (int i = 0; i < 3; ++i) {
+        const int a = LP[i][0], b = LP[i][1];
+        const double nx = lam[a] * gg[2 * b] - lam[b] * gg[2 * a];
+        const double ny = lam[a] * gg[2 * b + 1] - lam[b] * gg[2 * a + 1];
+        ex += ce[3 * t + i] * nx;
+        ey += ce[3 * t + i] * ny;
+    }
+    for (int i = 0; i < 3; ++i) E[i] = ex * u[i] + ey * v[i];
+    // H_t / y = (mu_port / mu) n x (e_t + grad e_z / gamma)
+    const cd s = mu_port / mu[t];
+    n_cross_plane(n, u, v, s * (ex + gz[2 * t] / gamma), s * (ey + gz[2 * t + 1] / gamma), Hy);
+}
+
+void PortFem2D::eval_face(int64_t f, double s1, double s2, const double X[3], cd E[3], cd Hy[3]) const {
+    const int N = nsub;
+    int i = (int)std::floor(N * std::max(0.0, s1));
+    i = std::min(i, N - 1);
+    int j = (int)std::floor(N * std::max(0.0, s2));
+    j = std::min(j, N - 1 - i);
+    const double fi = N * s1 - i, fj = N * s2 - j;
+    const int up = (fi + fj > 1.0 && i + j <= N - 2) ? 1 : 0;
+    const int64_t t = sub[(((size_t)f * (N + 1) + i) * (N + 1) + j) * 2 + up];
+    eval_tri(t, X, E, Hy);
+}
+
+int64_t PortFem2D::locate(const double X[3]) const {
+    const double x0 = (X[0] - o[0]) * u[0] + (X[1] - o[1]) * u[1] + (X[2] - o[2]) * u[2];
+    const double x1 = (X[0] - o[0]) * v[0] + (X[1] - o[1]) * v[1] + (X[2] - o[2]) * v[2];
+    int64_t best = 0;
+    double bv = -1e300;
+    const int64_t T = (int64_t)st.size() / 3;
+    for (int64_t t = 0; t < T; ++t) {
+        const double d0 = x0 - P0[2 * t], d1 = x1 - P0[2 * t + 1];
+        const double* Ji = &Jinv[4 * t];
+        const double l1 = Ji[0] * d0 + Ji[1] * d1, l2 = Ji[2] * d0 + Ji[3] * d1;
+        const double m = std::min(1 - l1 - l2, std::min(l1, l2));
+        if (m > bv) { bv = m; best = t; }
+    }
+    return best;
+}
+
+int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* fv, const cd* eps_face, const cd* mu_face,
+                     const double* desc, int nsub, double freq, double mu_port, PortFem2D& M, std::string& err) {
+    if (nface < 1 || nsub < 1 || nsub > 64 || !(freq > 0)) { err = "port mode: bad arguments"; return OPEM_ERR_ARG; }
+    M = PortFem2D{};
+    M.nsub = nsub;
+    M.nface = nface;
+    M.freq = freq;
+    M.mu_port = mu_port;
+    for (int i = 0; i < 3; ++i) M.o[i] = desc[i];
+    unit(desc + 3, M.u);
+    unit(desc + 6, M.v);
+    unit(desc + 9, M.n);
+    const int N = nsub;
+    // conforming split: corner nodes by vertex, edge nodes by (low vertex, high
+    // vertex, step from the low one), interior nodes by (face, i, j)
+    std::map<std::array<int64_t, 4>, int64_t> key;
+    std::vector<double> X3;
+    auto node = [&](const std::array<int64_t, 4>& k, const double* X) {
+        auto it = key.find(k);
+        if (it != key.end()) return it->second;
+        const int64_t id = (int64_t)X3.size() / 3;
+        key.emplace(k, id);
+        X3.insert(X3.end(), X, X + 3);
+        return id;
+    };
+    auto edge_node = [&](int64_t ga, int64_t gb, int m) {
+        if (m == 0) return node({0, ga, 0, 0}, verts + 3 * ga);
+        if (m == N) return node({0, gb, 0, 0}, verts + 3 * gb);
+        const int64_t lo = std::min(ga, gb), hi = std::max(ga, gb);
+        const int mm = ga < gb ? m : N - m;
+        const double t = (double)mm / N;
+        double X[3];
+        for (int c = 0; c < 3; ++c) X[c] = verts[3 * lo + c] + t * (verts[3 * hi + c] - verts[3 * lo + c]);
+        return node({1, lo, hi, mm}, X);
+    };
+    std::vector<int64_t> tris, tri_face;
+    M.sub.assign((size_t)nface * (N + 1) * (N + 1) * 2, -1);
+    std::vector<int64_t> ids((size_t)(N + 1) * (N + 1));
+    for (int64_t f = 0; f < nface; ++f) {
+        const int64_t g0 = fv[3 * f], g1 = fv[3 * f + 1], g2 = fv[3 * f + 2];
+        const double *A = verts + 3 * g0, *B = verts + 3 * g1, *C = verts + 3 * g2;
+        for (int i = 0; i <= N; ++i)
+            for (int j = 0; j <= N - i; ++j) {
+                int64_t id;
+                if (j == 0) id = edge_node(g0, g1, i);
+                else if (i == 0) id = edge_node(g0, g2, j);
+                else if (i + j == N) id = edge_node(g1, g2, j);
+                else {
+                    const double ti = (double)i / N, tj = (double)j / N;
+                    double X[3];
+                    for (int c = 0; c < 3; ++c) X[c] = A[c] + ti * (B[c] - A[c]) + tj * (C[c] - A[c]);
+                    id = node({2, f, i, j}, X);
+                }
+                ids[(size_t)i * (N + 1) + j] = id;
+            }
+        auto at = [&](int i, int j) { return ids[(size_t)i * (N + 1) + j]; };
+        for (int i = 0; i < N; ++i)
+            for (int j = 0; j < N - i; ++j) {
+                M.sub[(((size_t)f * (N + 1) + i) * (N + 1) + j) * 2] = (int64_t)tri_face.size();
+                tris.insert(tris.end(), {at(i, j), at(i + 1, j), at(i, j + 1)});
+                tri_face.push_back(f);
+                if (i + j <= N - 2) {
+                    M.sub[(((size_t)f * (N + 1) + i) * (N + 1) + j) * 2 + 1] = (int64_t)tri_face.size();
+                    tris.insert(tris.end(), {at(i + 1, j), at(i + 1, j + 1), at(i, j + 1)});
+                    tri_face.push_back(f);
+                }
+            }
+    }
+    const int64_t nn = (int64_t)X3.size() / 3, T = (int64_t)tri_face.size();
+    M.xy.resize(2 * nn);
+    for (int64_t p = 0; p < nn; ++p) {
+        const double* X = &X3[3 * p];
+        const double d[3] = {X[0] - M.o[0], X[1] - M.o[1], X[2] - M.o[2]};
+        M.xy[2 * p] = d[0] * M.u[0] + d[1] * M.u[1] + d[2] * M.u[2];
+        M.xy[2 * p + 1] = d[0] * M.v[0] + d[1] * M.v[1] + d[2] * M.v[2];
+    }
+    std::vector<double> eps2(2 * T), mu2(2 * T);
+    M.mu.resize(T);
+    for (int64_t t = 0; t < T; ++t) {
+        const cd e = eps_face[tri_face[t]], m = mu_face ? mu_face[tri_face[t]] : cd(1.0);
+        eps2[2 * t] = e.real(); eps2[2 * t + 1] = e.imag();
+        mu2[2 * t] = m.real(); mu2[2 * t + 1] = m.imag();
+        M.mu[t] = m;
+    }
+    double beta[2];
+    int64_t ne = 0;
+    int rc = opem_port_mode_2d(nn, M.xy.data(), T, tris.data(), eps2.data(), mu2.data(), freq, beta, &ne, nullptr,
+                               nullptr, nullptr);
+    if (rc != OPEM_OK) { err = "port mode: 2D mesh rejected"; return rc; }
+    std::vector<int64_t> edges(2 * ne);
+    std::vector<double> et(2 * ne), ez(2 * nn);
+    rc = opem_port_mode_2d(nn, M.xy.data(), T, tris.data(), eps2.data(), mu2.data(), freq, beta, &ne, edges.data(),
+                           et.data(), ez.data());
+    if (rc != OPEM_OK) { err = "port mode: 2D eigensolve failed"; return rc; }
+    M.gamma = cd(-beta[1], beta[0]);   // j beta
+    std::map<std::pair<int64_t, int64_t>, int64_t> eid;
+    for (int64_t e = 0; e < ne; ++e) eid[{edges[2 * e], edges[2 * e + 1]}] = e;
+    M.st.resize(3 * T);
+    M.P0.resize(2 * T);
+    M.Jinv.resize(4 * T);
+    M.g.resize(6 * T);
+    M.ce.resize(3 * T);
+    M.gz.resize(2 * T);
+    std::vector<double> area(T);
+    for (int64_t t = 0; t < T; ++t) {
+        int64_t s[3] = {tris[3 * t], tris[3 * t + 1], tris[3 * t + 2]};
+        std::sort(s, s + 3);
+        for (int k = 0; k < 3; ++k) M.st[3 * t + k] = s[k];
+        const double* p0 = &M.xy[2 * s[0]];
+        const double* p1 = &M.xy[2 * s[1]];
+        const double* p2 = &M.xy[2 * s[2]];
+        const double J00 = p1[0] - p0[0], J01 = p2[0] - p0[0], J10 = p1[1] - p0[1], J11 = p2[1] - p0[1];
+        const double det = J00 * J11 - J01 * J10;
+        area[t] = 0.5 * std::fabs(det);
+        double* Ji = &M.Jinv[4 * t];
+        Ji[0] = J11 / det; Ji[1] = -J01 / det; Ji[2] = -J10 / det; Ji[3] = J00 / det;
+        M.P0[2 * t] = p0[0];
+        M.P0[2 * t + 1] = p0[1];
+        const double r[3][2] = {{-1, -1}, {1, 0}, {0, 1}};
+        for (int k = 0; k < 3; ++k) {   // grad lambda_k = J^-T r_k
+            M.g[6 * t + 2 * k] = Ji[0] * r[k][0] + Ji[2] * r[k][1];
+            M.g[6 * t + 2 * k + 1] = Ji[1] * r[k][0] + Ji[3] * r[k][1];
+        }
+        for (int i = 0; i < 3; ++i) {
+            const int64_t e = eid.at({s[LP[i][0]], s[LP[i][1]]});
+            M.ce[3 * t + i] = cd(et[2 * e], et[2 * e + 1]);
+        }
+        cd gx = 0.0, gy = 0.0;
+        for (int k = 0; k < 3; ++k) {
+            const cd z(ez[2 * s[k]], ez[2 * s[k] + 1]);
+            gx += z * M.g[6 * t + 2 * k];
+            gy += z * M.g[6 * t + 2 * k + 1];
+        }
+        M.gz[2 * t] = gx;
+        M.gz[2 * t + 1] = gy;
+    }
+    // V = -int E . dl along the voltage path
+    {
+        const double* p0 = desc + 16;
+        const double* p1 = desc + 19;
+        const double dl[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+        std::vector<double> x, w;
+        gauss_legendre01(4, x, w);
+        const int K = 16 * N;
+        cd vint = 0.0;
+        for (int k = 0; k < K; ++k)
+            for (int q = 0; q < 4; ++q) {
+                const double s = (k + x[q]) / K;
+                const double X[3] = {p0[0] + s * dl[0], p0[1] + s * dl[1], p0[2] + s * dl[2]};
+                cd E[3], Hy[3];
+                M.eval_tri(M.locate(X), X, E, Hy);
+                vint += (w[q] / K) * (E[0] * dl[0] + E[1] * dl[1] + E[2] * dl[2]);
+            }
+        M.V = -vint;
+    }
+    // Pz = 1/2 int (E x H*) . n, H = y Hy
+    {
+        const double w = 2 * M_PI * freq;
+        const cd y = M.gamma / cd(0.0, w * MU0 * mu_port);
+        cd pz = 0.0;
+        for (int64_t t = 0; t < T; ++t) {
+            cd acc = 0.0;
+            for (int m = 0; m < 3; ++m) {
+                const int a = LP[m][0], b = LP[m][1];
+                const double x2[2] = {0.5 * (M.xy[2 * M.st[3 * t + a]] + M.xy[2 * M.st[3 * t + b]]),
+                                      0.5 * (M.xy[2 * M.st[3 * t + a] + 1] + M.xy[2 * M.st[3 * t + b] + 1])};
+                double X[3];
+                for (int c = 0; c < 3; ++c) X[c] = M.o[c] + x2[0] * M.u[c] + x2[1] * M.v[c];
+                cd E[3], Hy[3];
+                M.eval_tri(t, X, E, Hy);
+                cd H[3];
+                for (int c = 0; c < 3; ++c) H[c] = y * Hy[c];
+                const cd cx = E[1] * std::conj(H[2]) - E[2] * std::conj(H[1]);
+                const cd cy = E[2] * std::conj(H[0]) - E[0] * std::conj(H[2]);
+                const cd cz = E[0] * std::conj(H[1]) - E[1] * std::conj(H[0]);
+                acc += cx * M.n[0] + cy * M.n[1] + cz * M.n[2];
+            }
+            pz += area[t] / 3.0 * acc;
+        }
+        M.Pz = 0.5 * pz;
+    }
+    M.Z = 0.5 * M.V * std::conj(M.V) / std::conj(M.Pz);
+    return OPEM_OK;
+}
+
+}  // namespace opem
+
+extern "C" int opem_port_mode_faces(int64_t nverts, const double* verts, int64_t nface, const int64_t* face_verts,
+                                    const double* eps_face, const double* mu_face, const double* desc, int nsub,
+                                    double freq, double* metrics, int64_t npts, const int64_t* pt_face,
+                                    const double* pt_s, double* E_out, double* Hy_out) {
+    using cd = std::complex<double>;
+    if (nverts < 3 || !verts || nface < 1 || !face_verts || !eps_face || !desc || !metrics) return OPEM_ERR_ARG;
+    if (npts > 0 && (!pt_face || !pt_s)) return OPEM_ERR_ARG;
+    for (int64_t i = 0; i < 3 * nface; ++i)
+        if (face_verts[i] < 0 || face_verts[i] >= nverts) return OPEM_ERR_ARG;
+    for (int64_t p = 0; p < npts; ++p)
+        if (pt_face[p] < 0 || pt_face[p] >= nface) return OPEM_ERR_ARG;
+    std::vector<cd> eps(nface), mu(nface, cd(1.0));
+    for (int64_t f = 0; f < nface; ++f) {
+        eps[f] = cd(eps_face[2 * f], eps_face[2 * f + 1]);
+        if (mu_face) mu[f] = cd(mu_face[2 * f], mu_face[2 * f + 1]);
+    }
+    opem::PortFem2D M;
+    std::string err;
+    int rc = opem::port_fem2d_solve(verts, nface, face_verts, eps.data(), mu.data(), desc, nsub, freq, mu[0].real(), M,
+                                    err);
+    if (rc != OPEM_OK) return rc;
+    const cd m4[4] = {M.gamma, M.Z, M.V, M.Pz};
+    for (int i = 0; i < 4; ++i) { metrics[2 * i] = m4[i].real(); metrics[2 * i + 1] = m4[i].imag(); }
+    for (int64_t p = 0; p < npts; ++p) {
+        const int64_t f = pt_face[p];
+        const double s1 = pt_s[2 * p], s2 = pt_s[2 * p + 1];
+        const double* A = verts + 3 * face_verts[3 * f];
+        const double* B = verts + 3 * face_verts[3 * f + 1];
+        const double* C = verts + 3 * face_verts[3 * f + 2];
+        double X[3];
+        for (int c = 0; c < 3; ++c) X[c] = A[c] + s1 * (B[c] - A[c]) + s2 * (C[c] - A[c]);
+        cd E[3], Hy[3];
+        M.eval_face(f, s1, s2, X, E, Hy);
+        for (int c = 0; c < 3; ++c) {
+            if (E_out) { E_out[6 * p + 2 * c] = E[c].real(); E_out[6 * p + 2 * c + 1] = E[c].imag(); }
+            if (Hy_out) { Hy_out[6 * p + 2 * c] = Hy[c].real(); Hy_out[6 * p + 2 * c + 1] = Hy[c].imag(); }
+        }
+    }
+    return OPEM_OK;
+}

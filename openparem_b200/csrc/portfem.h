@@ -1,0 +1,43 @@
+// Port modes solved on the port's own faces (host only, internal).
+#pragma once
+#include <complex>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace opem {
+
+// The fundamental mode of one port at one frequency, found on a conforming
+// split of the port's faces (each face into nsub x nsub similar triangles).
+struct PortFem2D {
+    using cd = std::complex<double>;
+    int nsub = 0;
+    int64_t nface = 0;
+    double o[3], u[3], v[3], n[3];    // unit frame of the port plane; n = outward normal
+    double freq = 0, mu_port = 1;
+    cd gamma, V, Z, Pz;
+    std::vector<double> xy;           // 2D nodes
+    std::vector<int64_t> st;          // 3 sorted node ids per sub-triangle
+    std::vector<double> P0, Jinv, g;  // per sub-triangle: first node (2), J^-1 (4), grad lambda (3x2)
+    std::vector<cd> ce, gz, mu;       // edge coefficients (3), grad e_z (2), mu_r (1)
+    std::vector<int64_t> sub;         // per face: (i, j, upper) -> sub-triangle
+
+    // E_t and H_t / y (y = gamma / (j w mu0 mu_port)) at the 3D point X of
+    // sub-triangle t
+    void eval_tri(int64_t t, const double X[3], cd E[3], cd Hy[3]) const;
+    // the same at X = P0 + s1 (P1 - P0) + s2 (P2 - P0) of port face f
+    void eval_face(int64_t f, double s1, double s2, const double X[3], cd E[3], cd Hy[3]) const;
+    // the sub-triangle a point of the port plane is deepest inside
+    int64_t locate(const double X[3]) const;
+};
+
+// Builds and solves the mode.  verts: 3D vertices; face_verts: 3 vertex ids per
+// port face in the face's local order; eps_face / mu_face: complex relative
+// permittivity / permeability per face (from the owning tetrahedron);
+// desc: the 22-double port descriptor (origin, u, v, outward normal, a, b, m, n,
+// voltage path); mu_port: mu_r used to scale H_t / y.  Returns an OPEM_* code.
+int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* face_verts,
+                     const std::complex<double>* eps_face, const std::complex<double>* mu_face, const double* desc,
+                     int nsub, double freq, double mu_port, PortFem2D& out, std::string& err);
+
+}  // namespace opem

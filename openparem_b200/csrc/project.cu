@@ -41,6 +41,7 @@ struct Project {
     std::vector<int32_t> attr;        // per face
     std::vector<int64_t> tri_opp;     // vertex of the owning tet opposite the face
     std::vector<std::array<double, 22>> port_desc;
+    std::vector<int> port_nsub;       // 0: analytic TE10; > 0: the port's own 2D mode on faces split nsub x nsub
     std::vector<std::pair<int, std::array<double, 3>>> bdr;   // attr -> (type, params)
     std::vector<double> freqs;
     int order = 1;
@@ -331,15 +332,17 @@ void build(const std::string& proj_path, int order_override, Project& P) {
     P.freqs.erase(std::unique(P.freqs.begin(), P.freqs.end()), P.freqs.end());
     // exterior faces with the opposite vertex of their tet
     const int64_t ne = (int64_t)P.tets.size() / 4;
-    std::map<std::array<int64_t, 3>, std::pair<int, int64_t>> faces;
+    struct FaceUse { int count = 0; int64_t second = -1, tet = -1; };   // uses, opposite vertex, owning tet
+    std::map<std::array<int64_t, 3>, FaceUse> faces;
     static const int F[4][4] = {{1, 2, 3, 0}, {0, 2, 3, 1}, {0, 1, 3, 2}, {0, 1, 2, 3}};
     for (int64_t e = 0; e < ne; ++e)
         for (auto& f : F) {
             std::array<int64_t, 3> k = {P.tets[4 * e + f[0]], P.tets[4 * e + f[1]], P.tets[4 * e + f[2]]};
             std::sort(k.begin(), k.end());
             auto& c = faces[k];
-            c.first += 1;
+            c.count += 1;
             c.second = P.tets[4 * e + f[3]];
+            c.tet = e;
         }
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
     for (size_t i = 0; i < P.verts.size(); ++i) {
@@ -364,15 +367,24 @@ void build(const std::string& proj_path, int order_override, Project& P) {
         for (auto& r : bdrs[j].paths) bdr_poly[j].emplace_back(path_points(paths, r), tol);
     auto vtx = [&](int64_t i) { return V3{P.verts[3 * i], P.verts[3 * i + 1], P.verts[3 * i + 2]}; };
     const int np = (int)ports.size(), nb = (int)bdrs.size();
-    std::vector<int64_t> port_opp(np, -1), port_face0(np, -1);
+    std::vector<int64_t> port_opp(np, -1), port_face0(np, -1), port_nface(np, 0);
+    std::vector<int> port_mixed(np, 0), port_reg0(np, -1);   // faces of more than one material behind the port
+    auto same_mat = [&](int r0, int r1) {
+        const Mat &A = P.region_mat[r0], &B = P.region_mat[r1];
+        return A.er == B.er && A.tand == B.tand && A.sigma == B.sigma && A.mur == B.mur;
+    };
     for (auto& kvf : faces) {
-        if (kvf.second.first != 1) continue;
+        if (kvf.second.count != 1) continue;
         const auto& k = kvf.first;
         int a = 1;   // PEC
         for (int p = 0; p < np && a == 1; ++p)
             if (port_poly[p].contains(vtx(k[0])) && port_poly[p].contains(vtx(k[1])) && port_poly[p].contains(vtx(k[2]))) {
                 a = 2 + p;
                 if (port_opp[p] < 0) { port_opp[p] = kvf.second.second; port_face0[p] = k[0]; }
+                const int r = P.region[kvf.second.tet];
+                if (port_reg0[p] < 0) port_reg0[p] = r;
+                else if (!same_mat(port_reg0[p], r)) port_mixed[p] = 1;
+                ++port_nface[p];
             }
         for (int j = 0; j < nb && a == 1; ++j)
             for (auto& poly : bdr_poly[j])
@@ -406,6 +418,11 @@ void build(const std::string& proj_path, int order_override, Project& P) {
         }
         for (int i = 0; i < 3; ++i) { d[16 + i] = vs[i]; d[19 + i] = ve[i]; }
         P.port_desc.push_back(d);
+        // a port whose faces see more than one material is driven by its own 2D
+        // mode (as the reference drives every port); the split keeps the 2D mesh
+        // near 4096 triangles
+        const int nsub = (int)std::lround(std::sqrt(4096.0 / (double)std::max<int64_t>(1, port_nface[p])));
+        P.port_nsub.push_back(port_mixed[p] ? std::min(16, std::max(1, nsub)) : 0);
     }
     // boundary conditions: attribute 1 PEC, ports 2.., the Boundary blocks after them
     P.bdr.push_back({OPEM_BDR_PEC, {0, 0, 0}});
@@ -453,7 +470,8 @@ int opem_project_info(const char* proj_path, int order, int64_t* info, int ninfo
 
 int opem_project_read(const char* proj_path, int order, int64_t* counts, double* verts, int64_t* tets,
                       int32_t* region, double* region_mat, int64_t* tris, int32_t* attr, int32_t* bdr_type,
-                      double* bdr_params, double* port_desc, double* freqs, char* msg, int msg_len) {
+                      double* bdr_params, double* port_desc, int32_t* port_nsub, double* freqs, char* msg,
+                      int msg_len) {
     if (!proj_path || !counts) return OPEM_ERR_ARG;
     Project P;
     try {
@@ -487,6 +505,8 @@ int opem_project_read(const char* proj_path, int order, int64_t* counts, double*
     if (port_desc)
         for (int64_t p = 0; p < np; ++p)
             for (int i = 0; i < 22; ++i) port_desc[22 * p + i] = P.port_desc[p][i];
+    if (port_nsub)
+        for (int64_t p = 0; p < np; ++p) port_nsub[p] = P.port_nsub[p];
     if (freqs)
         for (int64_t q = 0; q < nq; ++q) freqs[q] = P.freqs[q];
     if (msg && msg_len > 0) msg[0] = 0;
@@ -525,7 +545,8 @@ int opem_project_load(opem_context ctx, const char* proj_path, int order, opem_p
         rc = opem_problem_set_boundary(prob, (int)a + 1, type, np ? P.bdr[a].second.data() : nullptr, np);
     }
     for (size_t p = 0; rc == OPEM_OK && p < P.port_desc.size(); ++p)
-        rc = opem_problem_set_port_te(prob, (int)p, P.port_desc[p].data());
+        rc = P.port_nsub[p] > 0 ? opem_problem_set_port_fem2d(prob, (int)p, P.port_desc[p].data(), P.port_nsub[p])
+                                : opem_problem_set_port_te(prob, (int)p, P.port_desc[p].data());
     if (rc != OPEM_OK) {
         opem_problem_destroy(prob);
         return rc;

@@ -69,7 +69,7 @@ def te_descriptor(mode):
     """Pack a rectangular TE_mn mode dict into the ABI's 22 doubles."""
     d = np.zeros(22)
     d[0:3] = mode["origin"]; d[3:6] = mode["u"]; d[6:9] = mode["v"]; d[9:12] = mode["normal"]
-    d[12] = mode["a"]; d[13] = mode["b"]; d[14] = mode["m"]; d[15] = mode["n"]
+    d[12] = mode.get("a", 0.0); d[13] = mode.get("b", 0.0); d[14] = mode.get("m", 0); d[15] = mode.get("n", 0)
     d[16:19] = mode["vpath"][0]; d[19:22] = mode["vpath"][1]
     return d
 
@@ -93,6 +93,32 @@ def project_info(proj_path, order=0):
     return info, fr[:min(info["frequencies"], len(fr))]
 
 
+def port_mode_faces(verts, face_verts, eps_face, mode, nsub, freq, pt_face=None, pt_s=None, mu_face=None):
+    """The 2D mode of a port given by its faces (opem_port_mode_faces, host only):
+    -> (metrics {gamma, Z, V, Pz}, E_t (npts,3), H_t / y (npts,3)) at the points
+    (pt_face, pt_s = (s1, s2) face parameters)."""
+    verts = np.ascontiguousarray(verts, dtype=np.float64)
+    fv = np.ascontiguousarray(face_verts, dtype=np.int64)
+    eps = np.ascontiguousarray(np.stack([np.real(eps_face), np.imag(eps_face)], axis=1), dtype=np.float64)
+    mu = None if mu_face is None else np.ascontiguousarray(np.stack([np.real(mu_face), np.imag(mu_face)], axis=1))
+    d = te_descriptor(mode)
+    npts = 0 if pt_face is None else len(pt_face)
+    pf = np.ascontiguousarray(pt_face if npts else np.zeros(1), dtype=np.int64)
+    ps = np.ascontiguousarray(pt_s if npts else np.zeros((1, 2)), dtype=np.float64)
+    m = np.zeros(8)
+    E = np.zeros((max(npts, 1), 6))
+    Hy = np.zeros((max(npts, 1), 6))
+    rc = _lib.lib().opem_port_mode_faces(len(verts), _dp(verts), len(fv), fv.ctypes.data_as(_lib.I64P), _dp(eps),
+                                         None if mu is None else _dp(mu), _dp(d), int(nsub), float(freq), _dp(m),
+                                         npts, pf.ctypes.data_as(_lib.I64P), _dp(ps), _dp(E), _dp(Hy))
+    if rc != _lib.OK:
+        raise OpemError(rc, "opem_port_mode_faces")
+    c = m[0::2] + 1j * m[1::2]
+    E = (E[:, 0::2] + 1j * E[:, 1::2])[:npts]
+    Hy = (Hy[:, 0::2] + 1j * Hy[:, 1::2])[:npts]
+    return {"gamma": c[0], "Z": c[1], "V": c[2], "Pz": c[3]}, E, Hy
+
+
 def project_problem(proj_path, order=0):
     """An OpenParEM3D project read on the host (opem_project_read) as a problem
     dict (the format of meshgen's problems, accepted by Fem3D and by the oracle)
@@ -103,17 +129,18 @@ def project_problem(proj_path, order=0):
     path = str(proj_path).encode()
     nul = None
     rc = L.opem_project_read(path, int(order), cnt.ctypes.data_as(_lib.I64P), nul, nul, nul, nul, nul, nul, nul, nul,
-                             nul, nul, msg, 512)
+                             nul, nul, nul, msg, 512)
     if rc != _lib.OK:
         raise OpemError(rc, f"opem_project_read: {msg.value.decode()}")
     nv, ne, nr, nf, na, npt, nq, p = (int(v) for v in cnt)
     verts = np.zeros((nv, 3)); tets = np.zeros((ne, 4), dtype=np.int64); reg = np.zeros(ne, dtype=np.int32)
     mat = np.zeros((nr, 4)); tris = np.zeros((nf, 3), dtype=np.int64); attr = np.zeros(nf, dtype=np.int32)
     bt = np.zeros(na, dtype=np.int32); bp = np.zeros((na, 3)); pd = np.zeros((max(npt, 1), 22)); fr = np.zeros(max(nq, 1))
+    ns = np.zeros(max(npt, 1), dtype=np.int32)
     rc = L.opem_project_read(path, int(order), cnt.ctypes.data_as(_lib.I64P), _dp(verts), tets.ctypes.data_as(_lib.I64P),
                              reg.ctypes.data_as(_lib.I32P), _dp(mat), tris.ctypes.data_as(_lib.I64P),
-                             attr.ctypes.data_as(_lib.I32P), bt.ctypes.data_as(_lib.I32P), _dp(bp), _dp(pd), _dp(fr),
-                             msg, 512)
+                             attr.ctypes.data_as(_lib.I32P), bt.ctypes.data_as(_lib.I32P), _dp(bp), _dp(pd),
+                             ns.ctypes.data_as(_lib.I32P), _dp(fr), msg, 512)
     if rc != _lib.OK:
         raise OpemError(rc, f"opem_project_read: {msg.value.decode()}")
     names = {v: k for k, v in _BTYPES.items()}
@@ -131,9 +158,12 @@ def project_problem(proj_path, order=0):
     ports = []
     for k in range(npt):
         d = pd[k]
-        ports.append({"mode": {"kind": "TE", "m": int(d[14]), "n": int(d[15]), "a": d[12], "b": d[13],
-                               "origin": d[0:3].tolist(), "u": d[3:6].tolist(), "v": d[6:9].tolist(),
-                               "normal": d[9:12].tolist(), "vpath": (d[16:19].tolist(), d[19:22].tolist())}})
+        mode = {"kind": "TE", "m": int(d[14]), "n": int(d[15]), "a": d[12], "b": d[13],
+                "origin": d[0:3].tolist(), "u": d[3:6].tolist(), "v": d[6:9].tolist(),
+                "normal": d[9:12].tolist(), "vpath": (d[16:19].tolist(), d[19:22].tolist())}
+        if ns[k] > 0:   # the port's own 2D mode
+            mode.update(kind="FEM2D", nsub=int(ns[k]))
+        ports.append({"mode": mode})
     prob = {"verts": verts, "tets": tets, "tet_region": reg.astype(np.int64), "bdr_tris": tris,
             "bdr_attr": attr.astype(np.int64), "order": p, "eps_r": mat[:, 0], "tand": mat[:, 1],
             "sigma": mat[:, 2], "mu_r": mat[:, 3], "boundaries": bnd, "ports": ports}
@@ -177,7 +207,11 @@ class Fem3D:
                  "set_boundary")
         for k, port in enumerate(prob["ports"]):
             d = te_descriptor(port["mode"])
-            _chk(self.ctx.h, L.opem_problem_set_port_te(self.h, k, _dp(d)), "set_port_te")
+            if port["mode"].get("kind", "TE") == "FEM2D":
+                _chk(self.ctx.h, L.opem_problem_set_port_fem2d(self.h, k, _dp(d), int(port["mode"]["nsub"])),
+                     "set_port_fem2d")
+            else:
+                _chk(self.ctx.h, L.opem_problem_set_port_te(self.h, k, _dp(d)), "set_port_te")
         self.nports = len(prob["ports"])
         self._assembled = False
 

@@ -231,25 +231,61 @@ class Operators:
             st, wt = tri_rule(2 * p + 4)
             M2 = monomials2(p - 2)
             Q2 = ((st[:, 0:1] ** M2[None, :, 0]) * (st[:, 1:2] ** M2[None, :, 1])) @ tri_test_polys(p - 2).T
-        for f in self.ports[k]["faces"]:
+        # A field known per port face (a 2D mode, linear on each sub-triangle of
+        # the face's nsub x nsub split) is evaluated on the face being traced,
+        # with the rules applied cell by cell.  The two faces of an edge inside
+        # the port give its edge moments as their mean (equal for a continuous
+        # field; a 2D mode's H_t, a normal component of an edge-element field,
+        # jumps between cells).
+        at_face = getattr(field, "at_face", None)
+        if at_face is not None:
+            N = field.nsub
+            sp = ((np.arange(N)[:, None] + s[None, :]) / N).ravel()
+            wsp = np.tile(ws / N, N)
+            Lc = np.array([shifted_legendre(k_, sp) for k_ in range(p)])
+            zero = np.zeros_like(sp)
+            edge_par = (np.stack([sp, zero], 1), np.stack([zero, sp], 1), np.stack([1 - sp, sp], 1))
+            if p >= 2:
+                cells = [(i, j, up) for i in range(N) for j in range(N - i) for up in (0, 1)
+                         if not (up and i + j > N - 2)]
+                A1 = np.concatenate([((i + 1 - st[:, 0]) if up else (i + st[:, 0])) / N for i, j, up in cells])
+                A2 = np.concatenate([((j + 1 - st[:, 1]) if up else (j + st[:, 1])) / N for i, j, up in cells])
+                wc = np.tile(wt / N ** 2, len(cells))
+                Qc = ((A1[:, None] ** M2[None, :, 0]) * (A2[:, None] ** M2[None, :, 1])) @ tri_test_polys(p - 2).T
+        cnt = np.zeros(topo.n)
+        for fi, f in enumerate(self.ports[k]["faces"]):
             t, lf = topo.face_owner[f], topo.face_lface[f]
             a, b, c = FACES[lf]
             Pv = verts[topo.tets[t]]
             gd = topo.dof[t, B.face_dofs(lf)]
             vals = []
-            for (i, j) in ((a, b), (a, c), (b, c)):
+            for e, (i, j) in enumerate(((a, b), (a, c), (b, c))):
                 tv = Pv[j] - Pv[i]
-                X = Pv[i][None, :] + s[:, None] * tv[None, :]
-                Et = field(X) @ tv
-                vals.extend((L * (ws * Et)[None, :]).sum(axis=1))
+                if at_face is not None:
+                    X = Pv[i][None, :] + sp[:, None] * tv[None, :]
+                    Et = at_face(fi, edge_par[e], X) @ tv
+                    vals.extend((Lc * (wsp * Et)[None, :]).sum(axis=1))
+                else:
+                    X = Pv[i][None, :] + s[:, None] * tv[None, :]
+                    Et = field(X) @ tv
+                    vals.extend((L * (ws * Et)[None, :]).sum(axis=1))
             if p >= 2:
                 t1 = Pv[b] - Pv[a]; t2 = Pv[c] - Pv[a]
-                X = Pv[a][None, :] + st[:, 0:1] * t1[None, :] + st[:, 1:2] * t2[None, :]
-                F = field(X)
-                for r in range(Q2.shape[1]):
-                    for tv in (t1, t2):
-                        vals.append(np.sum(wt * Q2[:, r] * (F @ tv)))
-            x[gd] = np.array(vals)
+                if at_face is not None:
+                    X = Pv[a][None, :] + A1[:, None] * t1[None, :] + A2[:, None] * t2[None, :]
+                    F = at_face(fi, np.stack([A1, A2], 1), X)
+                    for r in range(Qc.shape[1]):
+                        for tv in (t1, t2):
+                            vals.append(np.sum(wc * Qc[:, r] * (F @ tv)))
+                else:
+                    X = Pv[a][None, :] + st[:, 0:1] * t1[None, :] + st[:, 1:2] * t2[None, :]
+                    F = field(X)
+                    for r in range(Q2.shape[1]):
+                        for tv in (t1, t2):
+                            vals.append(np.sum(wt * Q2[:, r] * (F @ tv)))
+            x[gd] += np.array(vals)
+            cnt[gd] += 1
+        x[cnt > 1] /= cnt[cnt > 1]
         return x
 
 
@@ -289,6 +325,14 @@ def assemble_A(ops, freq, driven):
 def port_mode(ops, k, freq):
     prob = ops.prob
     port = ops.ports[k]
+    mode = prob["ports"][k]["mode"]
+    if mode.get("kind") == "FEM2D":
+        # the port's own 2D eigenmode (oracle.portmode), cached per frequency
+        cache = ops.__dict__.setdefault("_fem2d", {})
+        if (k, freq) not in cache:
+            from .portmode import Fem2DMode
+            cache[(k, freq)] = Fem2DMode(prob, ops.topo, port["faces"], mode, freq).metrics()
+        return cache[(k, freq)]
     r = port["region"]
     eps_c = materials.relative_eps(freq, prob["eps_r"][r], prob["tand"][r], prob["sigma"][r])
     return modes.mode_metrics(prob["ports"][k]["mode"], freq, eps_c, prob["mu_r"][r])

@@ -1,0 +1,201 @@
+"""Port modes computed on the port's own faces (oracle; test infrastructure only).
+
+The reference drives every port with the mode its 2D solver finds on the port's
+cross-section: OpenParEM3D writes the port faces out as a 2D mesh, spawns
+OpenParEM2D (src/OpenParEM3D/port.cpp:5081-5176), reads back the modal fields
+and metrics (load_modeMetrics, port.cpp:5302-5453) and interpolates the fields
+onto the 3D port trace (Mode::fillX, port.cpp:3234-3341).  This module restates
+that chain for one mode per port:
+
+* the 2D mesh is the port's faces, each split into nsub x nsub similar triangles
+  (nodes on shared edges are shared, so the mesh is conforming), with each
+  sub-triangle's material taken from the tetrahedron that owns its face;
+* the fundamental mode is the Lee-Sun-Cendes eigenpair of oracle.port2d
+  (lowest-order edge elements for e_t, linear nodal e_z, PEC on the outer
+  boundary), gamma = j beta;
+* for propagation along the port's outward normal n (the convention of the
+  analytic modes), H_t = n x (gamma e_t + grad_t e_z) / (j w mu);
+* V = -int E . dl along the voltage path (composite 4-point Gauss on 16 nsub
+  pieces), Pz = 1/2 int (E x H*) . n over the sub-triangles (exact rule for the
+  piecewise-quadratic integrand), Z = V V* / (2 Pz*) (the PV definition).
+"""
+import numpy as np
+
+from .materials import MU0, EPS0, relative_eps
+from .modes import _frame
+from .nd_basis import FACES
+from .port2d import solve_mode
+from .quadrature import tri_rule
+
+
+def port_submesh(verts, face_verts, nsub, origin, uh, vh):
+    """Conforming split of the port faces.  face_verts: (F,3) global vertex ids in
+    each face's local order (P0, P1, P2).  Returns nodes (N,3), xy (N,2),
+    tris (T,3), tri_face (T,)."""
+    n = int(nsub)
+    key_id = {}
+    nodes = []
+
+    def node(key, X):
+        if key not in key_id:
+            key_id[key] = len(nodes)
+            nodes.append(X)
+        return key_id[key]
+
+    def edge_node(ga, gb, m):   # m/n of the way from ga to gb
+        if m == 0:
+            return node(("v", ga), verts[ga])
+        if m == n:
+            return node(("v", gb), verts[gb])
+        lo, hi, mm = (ga, gb, m) if ga < gb else (gb, ga, n - m)
+        return node(("e", lo, hi, mm), verts[lo] + (mm / n) * (verts[hi] - verts[lo]))
+
+    tris, tri_face = [], []
+    sub = np.full((len(face_verts), n + 1, n + 1, 2), -1, dtype=np.int64)   # (face, i, j, upper) -> sub-triangle
+    for f, (g0, g1, g2) in enumerate(face_verts):
+        P0, P1, P2 = verts[g0], verts[g1], verts[g2]
+        ids = {}
+        for i in range(n + 1):
+            for j in range(n + 1 - i):
+                if j == 0:
+                    ids[i, j] = edge_node(g0, g1, i)
+                elif i == 0:
+                    ids[i, j] = edge_node(g0, g2, j)
+                elif i + j == n:
+                    ids[i, j] = edge_node(g1, g2, j)
+                else:
+                    ids[i, j] = node(("f", f, i, j), P0 + (i / n) * (P1 - P0) + (j / n) * (P2 - P0))
+        for i in range(n):
+            for j in range(n - i):
+                sub[f, i, j, 0] = len(tris)
+                tris.append([ids[i, j], ids[i + 1, j], ids[i, j + 1]])
+                tri_face.append(f)
+                if i + j <= n - 2:
+                    sub[f, i, j, 1] = len(tris)
+                    tris.append([ids[i + 1, j], ids[i + 1, j + 1], ids[i, j + 1]])
+                    tri_face.append(f)
+    X = np.array(nodes, dtype=np.float64)
+    xy = np.stack([(X - origin) @ uh, (X - origin) @ vh], axis=1)
+    return X, xy, np.array(tris, dtype=np.int64), np.array(tri_face, dtype=np.int64), sub
+
+
+class Fem2DMode:
+    """The fundamental mode of one port on its split faces at one frequency."""
+
+    def __init__(self, prob, topo, faces, mode, freq):
+        verts = np.asarray(prob["verts"], dtype=np.float64)
+        o, uh, vh, nh = _frame(mode)
+        self.o, self.uh, self.vh, self.nh = o, uh, vh, nh
+        fv = np.array([topo.tets[topo.face_owner[f]][list(FACES[topo.face_lface[f]])] for f in faces], dtype=np.int64)
+        X, xy, tris, tri_face, self.sub = port_submesh(verts, fv, mode["nsub"], o, uh, vh)
+        self.nsub = int(mode["nsub"])
+        reg = np.asarray(prob["tet_region"], dtype=np.int64)[topo.face_owner[np.asarray(faces)]][tri_face]
+        eps = relative_eps(freq, np.asarray(prob["eps_r"], dtype=np.float64)[reg],
+                           np.asarray(prob["tand"], dtype=np.float64)[reg],
+                           np.asarray(prob["sigma"], dtype=np.float64)[reg])
+        mu = np.asarray(prob["mu_r"], dtype=np.float64)[reg].astype(np.complex128)
+        beta, et, ez, edges = solve_mode(xy, tris, freq, eps, mu)
+        big = et[np.argmax(np.abs(et))]
+        et, ez = et / big, ez / big
+        self.freq, self.beta, self.gamma = freq, beta, 1j * beta
+        self.xy, self.tris, self.mu = xy, tris, mu
+        self.mu_port = float(np.real(mu[0]))
+        # per sub-triangle: vertex order sorted by node id, gradients, edge coefficients
+        st = np.sort(tris, axis=1)
+        P = xy[st]                                           # (T,3,2)
+        J = np.stack([P[:, 1] - P[:, 0], P[:, 2] - P[:, 0]], axis=2)   # columns
+        det = J[:, 0, 0] * J[:, 1, 1] - J[:, 0, 1] * J[:, 1, 0]
+        Jinv = np.stack([np.stack([J[:, 1, 1], -J[:, 0, 1]], 1), np.stack([-J[:, 1, 0], J[:, 0, 0]], 1)], 1) / det[:, None, None]
+        r = np.array([[-1.0, -1.0], [1.0, 0.0], [0.0, 1.0]])
+        self.g = np.einsum("tji,kj->tki", Jinv, r)          # grad lambda_k = J^-T r_k : (T,3,2)
+        self.area = 0.5 * np.abs(det)
+        self.st, self.P0, self.Jinv = st, P[:, 0], Jinv
+        eid = {(int(a), int(b)): e for e, (a, b) in enumerate(edges)}
+        lp = [(0, 1), (0, 2), (1, 2)]
+        self.ce = np.array([[et[eid[(int(t[a]), int(t[b]))]] for a, b in lp] for t in st])   # (T,3)
+        self.cz = ez[st]                                     # (T,3)
+        self.gz = np.einsum("tk,tki->ti", self.cz, self.g)   # grad e_z (T,2)
+        self.w = 2 * np.pi * freq
+        # metrics
+        p0 = np.asarray(mode["vpath"][0], dtype=np.float64)
+        p1 = np.asarray(mode["vpath"][1], dtype=np.float64)
+        K = 16 * int(mode["nsub"])
+        xg, wg = np.polynomial.legendre.leggauss(4)
+        s = ((np.arange(K)[:, None] + 0.5 * (xg[None, :] + 1)) / K).ravel()
+        ws = np.tile(0.5 * wg / K, K)
+        Xp = p0[None, :] + s[:, None] * (p1 - p0)[None, :]
+        self.V = -np.sum(ws * (self.Et(Xp) @ (p1 - p0)))
+        q, wq = tri_rule(4)
+        T, nq = len(st), len(wq)
+        tt = np.repeat(np.arange(T), nq)
+        X2 = (self.P0[tt] + np.tile(q[:, 0], T)[:, None] * (P[tt, 1] - P[tt, 0])
+              + np.tile(q[:, 1], T)[:, None] * (P[tt, 2] - P[tt, 0]))
+        E, H = self._eval(tt, X2)
+        # weights sum to 1/2 on the unit triangle: int = 2 area sum(w f)
+        self.Pz = 0.5 * np.sum(2 * self.area[tt] * np.tile(wq, T) * (np.cross(E, np.conj(H)) @ nh))
+        self.Z = 0.5 * self.V * np.conj(self.V) / np.conj(self.Pz)
+
+    def _locate(self, X2):
+        """Sub-triangle of each 2D point: the one it is deepest inside."""
+        out = np.empty(len(X2), dtype=np.int64)
+        for c in range(0, len(X2), 256):
+            d = X2[c:c + 256, None, :] - self.P0[None, :, :]            # (p,T,2)
+            lam = np.einsum("tij,ptj->pti", self.Jinv, d)              # (p,T,2): lambda_1, lambda_2
+            l0 = 1 - lam[..., 0] - lam[..., 1]
+            out[c:c + 256] = np.argmax(np.minimum(l0, np.minimum(lam[..., 0], lam[..., 1])), axis=1)
+        return out
+
+    def _eval(self, t, X2):
+        d = X2 - self.P0[t]
+        lam12 = np.einsum("pij,pj->pi", self.Jinv[t], d)
+        lam = np.stack([1 - lam12[:, 0] - lam12[:, 1], lam12[:, 0], lam12[:, 1]], axis=1)   # (p,3)
+        g = self.g[t]                                               # (p,3,2)
+        e2 = np.zeros((len(t), 2), dtype=np.complex128)
+        for i, (a, b) in enumerate([(0, 1), (0, 2), (1, 2)]):
+            Ni = lam[:, a:a + 1] * g[:, b] - lam[:, b:b + 1] * g[:, a]
+            e2 += self.ce[t, i][:, None] * Ni
+        E = e2[:, 0:1] * self.uh[None, :] + e2[:, 1:2] * self.vh[None, :]
+        G = self.gamma * e2 + self.gz[t]
+        G3 = G[:, 0:1] * self.uh[None, :] + G[:, 1:2] * self.vh[None, :]
+        H = np.cross(self.nh[None, :], G3) / (1j * self.w * MU0 * self.mu[t][:, None])
+        return E, H
+
+    def _xy(self, X):
+        X = np.atleast_2d(np.asarray(X, dtype=np.float64))
+        return np.stack([(X - self.o) @ self.uh, (X - self.o) @ self.vh], axis=1)
+
+    def Et(self, X):
+        X2 = self._xy(X)
+        return self._eval(self._locate(X2), X2)[0]
+
+    def Ht(self, X):
+        X2 = self._xy(X)
+        return self._eval(self._locate(X2), X2)[1]
+
+    def face_tri(self, f, S12):
+        """Sub-triangle of port face f holding the points of face parameters
+        S12 = (s1, s2): cell (i, j) of the split, its upper half when the
+        fractional parts add up to more than one."""
+        n = self.nsub
+        s1, s2 = S12[:, 0], S12[:, 1]
+        i = np.minimum(np.floor(n * np.maximum(0.0, s1)).astype(np.int64), n - 1)
+        j = np.minimum(np.floor(n * np.maximum(0.0, s2)).astype(np.int64), n - 1 - i)
+        up = ((n * s1 - i) + (n * s2 - j) > 1.0) & (i + j <= n - 2)
+        return self.sub[f, i, j, up.astype(np.int64)]
+
+    def metrics(self):
+        mode = self
+
+        class _Field:
+            def __init__(self, which):
+                self.which = which
+                self.nsub = mode.nsub
+
+            def __call__(self, X):
+                X2 = mode._xy(X)
+                return mode._eval(mode._locate(X2), X2)[self.which]
+
+            def at_face(self, f, S12, X):
+                return mode._eval(mode.face_tri(f, S12), mode._xy(X))[self.which]
+
+        return {"gamma": self.gamma, "Z": self.Z, "V": self.V, "Pz": self.Pz, "Et": _Field(0), "Ht": _Field(1)}

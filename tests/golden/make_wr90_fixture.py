@@ -14,7 +14,8 @@ and writes
                                         straight-lossy, straight-loaded, and the
                                         projects below)
 and, for the project-reader pins, from
-  regression/OpenParEM3D/WR90/{straight-flipped,straight-rotated-xyz,shorted,opened}
+  regression/OpenParEM3D/WR90/{straight-flipped,straight-rotated-xyz,shorted,opened,
+                              straight-loaded}
   tests/golden/wr90_projects.npz        their meshes (vertices, tetrahedra, physical tags)
   tests/golden/wr90_projects.json       their ports files (paths, boundaries, ports)
                                         as data, mesh order, frequency points and
@@ -168,16 +169,23 @@ def read_proj(path):
                 out["order"] = int(t[1])
             elif t[0] == "frequency.plan.point":
                 out["freqs"].append(float(t[1]))
-            elif t[0] in ("mesh.file", "port.definition.file", "materials.global.path", "materials.global.name"):
+            elif t[0] in ("mesh.file", "port.definition.file", "materials.global.path", "materials.global.name",
+                          "materials.local.path", "materials.local.name"):
                 out[t[0]] = t[1]
     return out
 
 
-def read_material(path, name):
-    """er, mur, tand, conductivity, Rz of one material of a materials database
-    (the temperature=any / frequency=any entry)."""
-    with open(path) as f:
-        lines = [ln.strip() for ln in f]
+def read_material(paths, name):
+    """er, mur, tand, conductivity, Rz of one material of the first materials
+    database (of paths: the local one, then the global one) that has it (the
+    temperature=any / frequency=any entry)."""
+    for path in paths:
+        if not os.path.exists(path):
+            continue
+        with open(path) as f:
+            lines = [ln.strip() for ln in f]
+        if f"name={name}" in lines:
+            break
     i = lines.index(f"name={name}")
     out = {}
     for ln in lines[i + 1:]:
@@ -191,7 +199,7 @@ def read_material(path, name):
 
 
 PROJECTS = {"straight-flipped": "straight-flipped", "straight-rotated-xyz": "straight-rotated",
-            "shorted": "shorted", "opened": "opened"}
+            "shorted": "shorted", "opened": "opened", "straight-loaded": "straight-loaded"}
 
 
 def main(ref):
@@ -213,7 +221,8 @@ def main(ref):
         key = d.replace("-", "_")
         arrays[key + "_verts"], arrays[key + "_tets"], arrays[key + "_phys"] = xyz, tets, phys
         names = read_physical_names(os.path.join(pd, pj["mesh.file"]))
-        mdb = os.path.join(pd, pj["materials.global.path"], pj["materials.global.name"])
+        mdb = [os.path.join(pd, pj.get("materials.local.path", "./"), pj.get("materials.local.name", "-")),
+               os.path.join(pd, pj["materials.global.path"], pj["materials.global.name"])]
         projects[d] = {"stem": stem, "npz_key": key, "order": pj["order"], "freqs": pj["freqs"],
                        "physical_names": {str(k): v for k, v in names.items()},
                        "materials": {v: read_material(mdb, v) for v in sorted(set(names.values()))},

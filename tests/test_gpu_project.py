@@ -49,3 +49,31 @@ def test_reference_projects_match_oracle(tmp_path, name):
         assert st["converged"] == 1
         ref = fem.solve_frequency(ops, f)["S"]
         assert np.abs(S - ref).max() <= 1e-8, (name, f, S, ref)
+
+
+def test_loaded_project_2d_mode_ports_match_oracle(tmp_path):
+    """The reference's slab-loaded WR90 project: its ports see air and teflon, so
+    the reader drives them by their own 2D modes (solved per frequency on the
+    port faces split 16 x 16).  ND2 on the device, plain FP64 and the batched
+    mixed sweep, against the oracle on the problem the same reader produced
+    (|dS| <= 1e-8 plain with solver rtol 1e-12; <= 1e-6 mixed)."""
+    from oracle import fem
+    from openparem_b200 import _lib
+    from openparem_b200.fem3d import project_problem
+    from project_files import reference_project
+    proj, _ = reference_project(str(tmp_path), "straight-loaded")
+    F, _ = Fem3D.from_project(proj, order=2, context=Context(0))
+    F.assemble()
+    prob, _ = project_problem(proj, order=2)
+    assert [p["mode"]["kind"] for p in prob["ports"]] == ["FEM2D", "FEM2D"]
+    ops = fem.Operators(prob)
+    o = default_opts(rtol=1e-12, restart=200, maxits=6000, h_rtol=1e-13)
+    fr = [8.3e9, 9.5e9]
+    refs = [fem.solve_frequency(ops, f)["S"] for f in fr]
+    for f, ref in zip(fr, refs):
+        S, _, st = F.solve(f, o)
+        assert st["converged"] == 1
+        assert np.abs(S - ref).max() <= 1e-8, (f, S, ref)
+    Sm, stm = F.sweep(fr, default_opts(precision=_lib.PREC_MIXED, rtol=1e-10))
+    for i in range(len(fr)):
+        assert np.abs(Sm[i] - refs[i]).max() <= 1e-6

@@ -1,0 +1,98 @@
+"""Ports driven by their own 2D mode (CPU: oracle and the library's host side).
+
+The reference drives every port with the mode its 2D solver finds on the port
+faces (port.cpp:5081-5176, :5302-5453, :3234-3341).  opem_problem_set_port_fem2d
+does the same in-process: the port faces split nsub x nsub, the fundamental
+Lee-Sun-Cendes mode (opem_port_mode_2d), H_t = n x (gamma e_t + grad e_z)/(j w mu),
+V along the voltage path and Z = V V*/(2 Pz*).  Here:
+  * the library's mode (opem_port_mode_faces) equals the oracle's
+    (oracle/portmode.py) on the slab-loaded WR90 ports: gamma and Z to 1e-10,
+    E_t and H_t at points of the port faces to 1e-10 (up to the mode's
+    arbitrary complex scale, which S does not depend on);
+  * on the empty guide the oracle's S with 2D-mode ports converges to the S
+    with the analytic TE10 at second order in the split;
+  * through the project reader (which picks 2D modes for ports whose faces see
+    more than one material) the oracle at the reference's ND6 on its
+    slab-loaded WR90 project comes within 3e-3 deg of the reference's found
+    arg S21 (1.3e-3 deg at the reader's split of 16: the lowest-order 2D
+    elements limit the mode's accuracy).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import fem
+from oracle.materials import relative_eps
+from oracle.nd_basis import FACES
+from oracle.portmode import Fem2DMode
+from openparem_b200.fem3d import port_mode_faces, project_problem
+from project_files import reference_project
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def loaded(order):
+    from test_oracle_golden import loaded_problem
+    return loaded_problem(order)
+
+
+def test_library_mode_equals_oracle():
+    prob = loaded(1)
+    ops = fem.Operators(prob)
+    topo = ops.topo
+    f = 8.3e9
+    rng = np.random.default_rng(3)
+    for k in range(2):
+        mode = dict(prob["ports"][k]["mode"], kind="FEM2D", nsub=6)
+        faces = ops.ports[k]["faces"]
+        om = Fem2DMode(prob, topo, faces, mode, f)
+        fv = np.array([topo.tets[topo.face_owner[x]][list(FACES[topo.face_lface[x]])] for x in faces])
+        reg = np.asarray(prob["tet_region"])[topo.face_owner[faces]]
+        eps = relative_eps(f, prob["eps_r"][reg], prob["tand"][reg], prob["sigma"][reg])
+        pf = rng.integers(0, len(faces), 300)
+        a = rng.random((300, 2))
+        a = np.where(a.sum(1, keepdims=True) > 1, 1 - a[:, ::-1], a)
+        met, E, Hy = port_mode_faces(prob["verts"], fv, eps, mode, 6, f, pf, a)
+        V = np.asarray(prob["verts"])
+        X = V[fv[pf, 0]] + a[:, 0:1] * (V[fv[pf, 1]] - V[fv[pf, 0]]) + a[:, 1:2] * (V[fv[pf, 2]] - V[fv[pf, 0]])
+        Eo = np.concatenate([om.metrics()["Et"].at_face(pf[i], a[i:i + 1], X[i:i + 1]) for i in range(len(pf))])
+        Ho = np.concatenate([om.metrics()["Ht"].at_face(pf[i], a[i:i + 1], X[i:i + 1]) for i in range(len(pf))])
+        y = om.gamma / (1j * 2 * np.pi * f * 4e-7 * np.pi * om.mu_port)
+        c = np.vdot(E.ravel(), Eo.ravel()) / np.vdot(E.ravel(), E.ravel())   # the modes' relative scale
+        assert abs(met["gamma"] - om.gamma) <= 1e-10 * abs(om.gamma)
+        assert abs(met["Z"] - om.Z) <= 1e-10 * abs(om.Z)
+        assert abs(c * met["V"] - om.V) <= 1e-10 * abs(om.V)
+        assert np.abs(Eo - c * E).max() <= 1e-10 * np.abs(Eo).max()
+        assert np.abs(Ho - c * y * Hy).max() <= 1e-10 * np.abs(Ho).max()
+        # the loaded guide's mode is slower than the empty guide's TE10
+        assert om.gamma.imag > np.sqrt((2 * np.pi * f / 299792458.0) ** 2 * 1.0006 - (np.pi / 22.86e-3) ** 2)
+
+
+def test_empty_guide_converges_to_analytic_te10():
+    from test_oracle_golden import wr90_problem
+    prob = wr90_problem(2)
+    ref = fem.solve_frequency(fem.Operators(prob), 9e9)["S"]
+    errs = []
+    for nsub in (2, 4, 8):
+        p2 = dict(prob)
+        p2["ports"] = [{"mode": dict(p["mode"], kind="FEM2D", nsub=nsub)} for p in prob["ports"]]
+        S = fem.solve_frequency(fem.Operators(p2), 9e9)["S"]
+        errs.append(np.abs(S - ref).max())
+    assert errs[2] < 1e-3
+    assert errs[1] / errs[2] > 3.0      # second order in the split
+
+
+def test_reader_loaded_project_nd6_near_reference(tmp_path):
+    proj, rec = reference_project(str(tmp_path), "straight-loaded")
+    prob, fr = project_problem(proj)
+    assert [p["mode"]["kind"] for p in prob["ports"]] == ["FEM2D", "FEM2D"]
+    assert all(p["mode"]["nsub"] == 16 for p in prob["ports"]) and np.allclose(fr, [8.3e9])
+    S = fem.solve_frequency(fem.Operators(prob), 8.3e9)["S"]
+    import json
+    with open(os.path.join(HERE, "golden", "wr90_expected.json")) as f:
+        cases = json.load(f)["cases"]["./WR90/straight-loaded/straight-loaded.proj"]
+    found = [v["found"] for v in cases.values() if v["variable"] == "argS(deg)" and v["portOut"] == 2
+             and v["portIn"] == 1][0]
+    assert abs(np.angle(S[1, 0], deg=True) - found) < 3e-3
+    assert 20 * np.log10(abs(S[0, 0])) < -60
