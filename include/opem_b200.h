@@ -122,6 +122,16 @@ int  opem_solve_frequency(opem_problem prob, double freq, const opem_solver_opts
  * S_out: nfreq*nports*nports complex.  stats: nfreq entries (may be NULL).      */
 int  opem_solve_sweep(opem_problem prob, int nfreq, const double* freqs, const opem_solver_opts* opts,
                       double* S_out, opem_solve_stats* stats);
+/* Zienkiewicz-Zhu error indicator on the H fields of the last
+ * opem_solve_frequency (fem3D::calculateMeshErrors, fem3D.cpp:1162-1420):
+ * per element sqrt((int |Re(s - F)|)^2 + (int |Im(s - F)|)^2) with F = curl H / mu_r
+ * and s its L2 projection onto the edge elements, the larger over the driving
+ * sets (errors_out, ne doubles, may be NULL); marked_out receives up to
+ * max_marked element indices of the floor(ne * fraction) (at least 1) largest
+ * errors, largest first; *nmarked that count; *max_error the largest error.
+ * OPEM_ERR_STATE before a solve.                                                 */
+int  opem_mesh_errors(opem_problem prob, double fraction, double* errors_out, int64_t* marked_out,
+                      int64_t max_marked, int64_t* nmarked, double* max_error);
 /* E and H DOF vectors (ndofs complex each, interleaved) of the last single-frequency
  * solve for driving set d (0-based).  Either pointer may be NULL.               */
 int  opem_get_fields(opem_problem prob, int d, double* e_out, double* h_out);

@@ -55,6 +55,7 @@ SIGNATURES = [
     ("opem_problem_set_boundary", C.c_int, [P, C.c_int, C.c_int, DP, C.c_int]),
     ("opem_problem_set_port_te", C.c_int, [P, C.c_int, DP]),
     ("opem_problem_set_port_fem2d", C.c_int, [P, C.c_int, DP, C.c_int]),
+    ("opem_mesh_errors", C.c_int, [P, C.c_double, DP, I64P, C.c_int64, I64P, DP]),
     ("opem_problem_assemble", C.c_int, [P]),
     ("opem_problem_info", C.c_int, [P, I64P, C.c_int]),
     ("opem_solve_frequency", C.c_int, [P, C.c_double, C.POINTER(SolverOpts), DP, DP, C.POINTER(SolveStats)]),

@@ -412,6 +412,22 @@ static std::unique_ptr<NDRef> build_ref(int p) {
             evalv(&curl[(size_t)k * dim], V.data(), nm, &CV[((size_t)k * nq + q) * 3]);
         }
     }
+    {   // tables for the error indicator (degree 2p+2 rule)
+        std::vector<double> Xe, we;
+        tet_rule(2 * p + 2, Xe, we);
+        const int nqe = (int)we.size();
+        R->nq_err = nqe;
+        R->w_err = we;
+        R->phi_err.assign((size_t)nqe * ld * 3, 0.0);
+        R->curl_err.assign((size_t)nqe * ld * 3, 0.0);
+        for (int q = 0; q < nqe; ++q) {
+            C.vander(&Xe[3 * q], V.data());
+            for (int k = 0; k < ld; ++k) {
+                evalv(&R->coef[(size_t)k * dim], V.data(), nm, &R->phi_err[((size_t)q * ld + k) * 3]);
+                evalv(&curl[(size_t)k * dim], V.data(), nm, &R->curl_err[((size_t)q * ld + k) * 3]);
+            }
+        }
+    }
     static const int SA[6] = {0, 1, 2, 0, 0, 1}, SB[6] = {0, 1, 2, 1, 2, 2};
     R->Mh.assign((size_t)6 * ld * ld, 0.0);
     R->Kh.assign((size_t)6 * ld * ld, 0.0);

@@ -1026,6 +1026,36 @@ int opem_solve_sweep(opem_problem prob, int nfreq, const double* freqs, const op
     return worst;
 }
 
+// fem3D::calculateMeshErrors marking (src/OpenParEM3D/fem3D.cpp:1321-1350): the
+// floor(NE * fraction) (at least one) largest errors, largest first (ties by
+// element index), and the largest error.
+int opem_mesh_errors(opem_problem prob, double fraction, double* errors_out, int64_t* marked_out, int64_t max_marked,
+                     int64_t* nmarked, double* max_error) {
+    if (!prob || !(fraction >= 0) || !(fraction <= 1) || max_marked < 0 || (max_marked > 0 && !marked_out))
+        return OPEM_ERR_ARG;
+    Problem& P = prob->p;
+    if (!P.assembled) return OPEM_ERR_STATE;
+    bool have = false;
+    for (auto& v : P.last_h) have |= !v.empty();
+    if (!have) return OPEM_ERR_STATE;
+    return guarded(P.ctx, [&] {
+        OPEM_CUDA(cudaSetDevice(P.ctx->device));
+        const int64_t ne = P.topo.ne;
+        std::vector<double> e;
+        mesh_error_indicator(P, e);
+        if (errors_out) std::memcpy(errors_out, e.data(), ne * sizeof(double));
+        int64_t count = std::max<int64_t>(1, (int64_t)((double)ne * fraction));
+        count = std::min(count, ne);
+        std::vector<int64_t> idx(ne);
+        for (int64_t i = 0; i < ne; ++i) idx[i] = i;
+        std::partial_sort(idx.begin(), idx.begin() + count, idx.end(),
+                          [&](int64_t a, int64_t b) { return e[a] > e[b] || (e[a] == e[b] && a < b); });
+        for (int64_t i = 0; i < std::min(count, max_marked); ++i) marked_out[i] = idx[i];
+        if (nmarked) *nmarked = count;
+        if (max_error) *max_error = e[idx[0]];
+    });
+}
+
 int opem_get_fields(opem_problem prob, int d, double* e_out, double* h_out) {
     if (!prob) return OPEM_ERR_ARG;
     Problem& P = prob->p;

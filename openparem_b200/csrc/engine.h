@@ -147,6 +147,9 @@ void port_gamma_Z_V(const Problem& P, int port, double freq, cd& gamma, cd& Z, c
 // freq (no-op when there are none or they are current); synchronises the stream.
 void refresh_port_traces(Problem& P, double freq);
 bool has_fem2d_ports(const Problem& P);
+// ZZ error indicator of the H fields kept by the last opem_solve_frequency
+// (estimate.cu): per element, the larger over the driving sets.
+void mesh_error_indicator(Problem& P, std::vector<double>& err);
 // overlaps <a, B_port b> for port k: out = conj(a)^T R_one b over the port's slots
 void port_overlap(Problem& P, int k, const double2* a, const double2* b, double2* out_dev);
 

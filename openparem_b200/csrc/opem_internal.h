@@ -33,6 +33,10 @@ struct NDRef {
     std::vector<int> face_dofs[4];   // ldf local dof ids per face
     std::vector<double> coef;        // ld*3*nmon basis coefficients
     std::vector<int> mon;            // nmon*3 exponents
+    // values and curls of the basis at the collapsed Gauss-Legendre tet rule of
+    // degree 2p+2 (the error indicator's rule): w_err[q], phi_err / curl_err [q][i][3]
+    int nq_err = 0;
+    std::vector<double> w_err, phi_err, curl_err;
 };
 
 // Builds (and caches) the tables for order p; throws std::runtime_error.

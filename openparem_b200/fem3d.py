@@ -176,6 +176,7 @@ class Fem3D:
     def __init__(self, prob, context=None, device=0):
         self.ctx = context if context is not None else Context(device)
         self.prob = prob
+        self._ne = len(prob["tets"])
         L = _lib.lib()
         verts = np.ascontiguousarray(prob["verts"], dtype=np.float64)
         tets = np.ascontiguousarray(prob["tets"], dtype=np.int64)
@@ -231,6 +232,7 @@ class Fem3D:
                                           C.byref(nf), _dp(fr), len(fr))
         _chk(self.ctx.h, rc, "opem_project_load")
         self.nports = info["ports"]
+        self._ne = info["tets"]
         self._assembled = False
         return self, fr[:nf.value]
 
@@ -269,6 +271,19 @@ class Fem3D:
         rc = _lib.lib().opem_solve_sweep(self.h, len(freqs), _dp(freqs), C.byref(o), _dp(S), st)
         _chk(self.ctx.h, rc, "opem_solve_sweep")
         return (S[0::2] + 1j * S[1::2]).reshape(len(freqs), N, N), [s.as_dict() for s in st]
+
+    def mesh_errors(self, fraction):
+        """ZZ error indicator of the last solve() (opem_mesh_errors) ->
+        (errors per element, marked elements largest first, max error)."""
+        ne = self._ne
+        err = np.zeros(ne)
+        cap = max(1, int(ne * fraction))
+        marked = np.zeros(cap, dtype=np.int64)
+        nm = C.c_int64()
+        mx = C.c_double()
+        _chk(self.ctx.h, _lib.lib().opem_mesh_errors(self.h, float(fraction), _dp(err), marked.ctypes.data_as(_lib.I64P),
+                                                     cap, C.byref(nm), C.byref(mx)), "opem_mesh_errors")
+        return err, marked[:nm.value], mx.value
 
     def fields(self, d):
         n = self.info()["ndofs"]

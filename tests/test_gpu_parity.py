@@ -187,3 +187,21 @@ def test_mixed_single_frequency_entry(ctx):
     S0, Z0, _ = F.solve(9.9e9)
     assert np.abs(S1 - S0).max() <= 1e-6 and np.allclose(Z1, Z0)
     assert st1["outer"] >= 1
+
+
+def test_mesh_error_indicator_matches_oracle(ctx):
+    """ZZ error indicator and marking (opem_mesh_errors) on the device against
+    oracle/estimate.py applied to the device's own H fields (ND2, lossy slab):
+    errors to 1e-7 of the largest, the same marked set."""
+    from oracle import fem
+    from oracle.estimate import mesh_errors
+    prob = meshgen.waveguide_problem(meshgen.WR_A, meshgen.WR_B, 50e-3, 6, 3, 15, 2, slab=(20e-3, 30e-3, 4.4, 0.02))
+    F = Fem3D(prob, context=ctx).assemble()
+    S, _, st = F.solve(10e9, default_opts(**TIGHT))
+    assert st["converged"] == 1
+    err, marked, mx = F.mesh_errors(0.05)
+    hs = [F.fields(d)[1] for d in range(2)]
+    ref, mref, mxref = mesh_errors(fem.Operators(prob), hs, 0.05)
+    assert np.abs(err - ref).max() <= 1e-7 * ref.max()
+    assert len(marked) == len(mref) == 81 and abs(mx - mxref) <= 1e-7 * mxref
+    assert np.allclose(np.sort(ref[marked]), np.sort(ref[mref]), rtol=1e-6, atol=0)
