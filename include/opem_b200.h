@@ -234,6 +234,17 @@ int  opem_s_renormalize(int nports, const double* S, const double* Zo, double zr
  * impedance zref (ohm, > 0), format "RI" | "MA" | "DB", unit "Hz" | "kHz" | "MHz" | "GHz". */
 int  opem_write_touchstone(const char* path, int nfreq, const double* freqs, int nports, const double* S,
                            double zref, const char* format, const char* unit);
+/* Mixed-mode conversion of S already renormalised to zref (fem3D::build_Mc_Ms with
+ * conversion 1, fem3D.cpp:1586-1900; Result::SparameterConversion, results.cpp:587-630):
+ * npairs differential pairs, pairs = {P1, N1, P2, N2, ...} (1-based S-ports); S-port
+ * P becomes the pair's common mode (Zo = zref/2), N its differential mode
+ * (Zo = 2 zref).  Zo_out (nports complex, may be NULL) receives the new impedances.  */
+int  opem_s_mixed_mode(int nports, const double* S, int npairs, const int* pairs, double zref, double* S_out,
+                       double* Zo_out);
+/* Touchstone 2.0 (the reference's mixed-mode writer, results.cpp:1210-1372): as
+ * opem_write_touchstone plus the 2.0 keywords and, with pairs, [Mixed-Mode Order]. */
+int  opem_write_touchstone2(const char* path, int nfreq, const double* freqs, int nports, const double* S,
+                            double zref, const char* format, const char* unit, int npairs, const int* pairs);
 
 /* ---- serving loop (no counterpart in the reference: it solves one project per
  * process, OpenParEM3D.cpp:494-555) -------------------------------------------

@@ -425,3 +425,32 @@ def write_touchstone(path, freqs, S, zref=50.0, fmt="RI", unit="GHz"):
     if rc != _lib.OK:
         raise OpemError(rc, "opem_write_touchstone")
 
+
+
+def mixed_mode(S, pairs, zref=50.0):
+    """Mixed-mode S of single-ended S (N, N) renormalised to zref (opem_s_mixed_mode):
+    pairs = [(P, N), ...] 1-based S-ports -> (S_mm, Zo)."""
+    S = np.ascontiguousarray(S, dtype=np.complex128)
+    n = S.shape[0]
+    pr = np.ascontiguousarray(np.asarray(pairs, dtype=np.int32).reshape(-1, 2))
+    out = np.zeros((n, n), dtype=np.complex128)
+    zo = np.zeros(n, dtype=np.complex128)
+    rc = _lib.lib().opem_s_mixed_mode(n, _dp(S.view(np.float64).ravel()), len(pr),
+                                      pr.ctypes.data_as(C.POINTER(C.c_int)), float(zref),
+                                      _dp(out.view(np.float64).ravel()), _dp(zo.view(np.float64).ravel()))
+    if rc != _lib.OK:
+        raise OpemError(rc, "opem_s_mixed_mode")
+    return out, zo
+
+
+def write_touchstone2(path, freqs, S, zref=50.0, fmt="RI", unit="GHz", pairs=()):
+    """Touchstone 2.0 file (opem_write_touchstone2); pairs mark mixed-mode S-ports."""
+    freqs = np.ascontiguousarray(freqs, dtype=np.float64)
+    S = np.ascontiguousarray(S, dtype=np.complex128)
+    N = S.shape[1]
+    pr = np.ascontiguousarray(np.asarray(pairs, dtype=np.int32).reshape(-1, 2))
+    rc = _lib.lib().opem_write_touchstone2(str(path).encode(), len(freqs), _dp(freqs), N,
+                                           _dp(S.view(np.float64).ravel()), float(zref), fmt.encode(), unit.encode(),
+                                           len(pr), pr.ctypes.data_as(C.POINTER(C.c_int)))
+    if rc != _lib.OK:
+        raise OpemError(rc, "opem_write_touchstone2")

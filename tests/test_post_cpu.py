@@ -100,3 +100,70 @@ def test_touchstone_many_ports_and_formats(tmp_path):
     assert np.abs(pairs2[:, 0] - np.abs(want)).max() < 1e-13
     with pytest.raises(OpemError):
         write_touchstone(tmp_path / "x.s5p", f, S, 75.0, "XY", "GHz")
+
+
+def _ref_mixed(S, pairs, zref):
+    """fem3D::build_Mc_Ms (conversion 1) + Result::SparameterConversion restated in numpy."""
+    n = S.shape[0]
+    za = np.full(n, zref, dtype=complex)
+    zb = za.copy()
+    Kv = np.eye(n, dtype=complex)
+    Ki = np.eye(n, dtype=complex)
+    for p, q in pairs:
+        p -= 1; q -= 1
+        zb[p], zb[q] = zref / 2, 2 * zref
+        Kv[p, p], Kv[p, q], Kv[q, p], Kv[q, q] = 0.5, 0.5, 1, -1
+        Ki[p, p], Ki[p, q], Ki[q, p], Ki[q, q] = 1, 1, 0.5, -0.5
+    t1 = np.diag(1 / np.sqrt(zb)) @ Kv @ np.diag(np.sqrt(za))
+    t2 = np.diag(np.sqrt(zb)) @ Ki @ np.diag(1 / np.sqrt(za))
+    Ms, Mc = 0.5 * (t1 + t2), 0.5 * (t1 - t2)
+    return (Mc + Ms @ S) @ np.linalg.inv(Ms + Mc @ S), zb
+
+
+def test_mixed_mode_matches_reference_formula():
+    from openparem_b200.fem3d import mixed_mode
+    rng = np.random.default_rng(11)
+    for n, pairs in ((2, [(1, 2)]), (4, [(1, 2), (3, 4)]), (4, [(2, 4)]), (5, [(1, 3), (4, 5)])):
+        S = _random_s(n, rng)
+        S = 0.5 * (S + S.T)
+        out, zo = mixed_mode(S, pairs, 50.0)
+        ref, zb = _ref_mixed(S, pairs, 50.0)
+        assert np.abs(out - ref).max() < 1e-12 and np.allclose(zo, zb)
+
+
+def test_mixed_mode_of_two_uncoupled_lines():
+    """Two identical matched 50-ohm thru lines (1->3, 2->4): the common (25 ohm) and
+    differential (100 ohm) modes are matched, both carry the thru, no mode conversion."""
+    from openparem_b200.fem3d import mixed_mode
+    t = 0.8 * np.exp(-0.7j)
+    S = np.zeros((4, 4), dtype=complex)
+    S[0, 2] = S[2, 0] = S[1, 3] = S[3, 1] = t
+    out, zo = mixed_mode(S, [(1, 2), (3, 4)], 50.0)
+    assert np.allclose(zo, [25, 100, 25, 100])
+    assert abs(out[2, 0] - t) < 1e-14 and abs(out[3, 1] - t) < 1e-14      # Scc21, Sdd21
+    assert abs(out[0, 0]) < 1e-14 and abs(out[1, 1]) < 1e-14              # matched modes
+    assert abs(out[3, 0]) < 1e-14 and abs(out[2, 1]) < 1e-14              # no conversion
+    with pytest.raises(OpemError):
+        mixed_mode(S, [(1, 1)], 50.0)
+
+
+def test_touchstone2_layout(tmp_path):
+    from openparem_b200.fem3d import write_touchstone2
+    rng = np.random.default_rng(5)
+    fr = np.array([9e9, 10e9])
+    S = np.stack([_random_s(4, rng) for _ in fr])
+    path = tmp_path / "mm.s4p"
+    write_touchstone2(path, fr, S, 50.0, "RI", "GHz", pairs=[(1, 2), (3, 4)])
+    lines = open(path).read().splitlines()
+    assert "[Version] 2.0" in lines and "[Number of Ports] 4" in lines and "[Number of Frequencies] 2" in lines
+    assert "[Matrix Format] Full" in lines and lines[-1] == "[End]"
+    assert "[Mixed-Mode Order] C1,2 D1,2 C3,4 D3,4" in lines
+    assert "! S-port comm_net1_net2" in lines and "! S-port diff_net3_net4" in lines
+    data = lines[lines.index("[Network Data]") + 1:-1]
+    vals = np.array([float(x) for ln in data for x in ln.split("!")[0].split()])
+    assert len(vals) == 2 * (1 + 2 * 16)
+    assert abs(vals[0] - 9.0) < 1e-12 and abs(vals[1] - S[0, 0, 0].real) < 1e-14
+    # two ports: 21_12 order keyword, data column by column as in version 1.1
+    write_touchstone2(tmp_path / "a.s2p", fr, S[:, :2, :2], 50.0, "MA", "GHz")
+    l2 = open(tmp_path / "a.s2p").read().splitlines()
+    assert "[Two-Port Data Order] 21_12" in l2 and not any(x.startswith("[Mixed-Mode") for x in l2)
