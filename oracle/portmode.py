@@ -24,7 +24,7 @@ import numpy as np
 from .materials import MU0, EPS0, relative_eps
 from .modes import _frame
 from .nd_basis import FACES
-from .port2d import solve_mode
+from .port2d import solve_mode, solve_mode_p2, LP2
 from .quadrature import tri_rule
 
 
@@ -94,9 +94,15 @@ class Fem2DMode:
                            np.asarray(prob["tand"], dtype=np.float64)[reg],
                            np.asarray(prob["sigma"], dtype=np.float64)[reg])
         mu = np.asarray(prob["mu_r"], dtype=np.float64)[reg].astype(np.complex128)
-        beta, et, ez, edges = solve_mode(xy, tris, freq, eps, mu)
-        big = et[np.argmax(np.abs(et))]
-        et, ez = et / big, ez / big
+        self.order = int(mode.get("order2d", 1))
+        if self.order == 2:
+            beta, ct, cz, _ = solve_mode_p2(xy, tris, freq, eps, mu)
+            big = ct[:, :3].ravel()[np.argmax(np.abs(ct[:, :3]).ravel())]   # largest Whitney coefficient
+            self.ct, self.cz2 = ct / big, cz / big
+        else:
+            beta, et, ez, edges = solve_mode(xy, tris, freq, eps, mu)
+            big = et[np.argmax(np.abs(et))]
+            et, ez = et / big, ez / big
         self.freq, self.beta, self.gamma = freq, beta, 1j * beta
         self.xy, self.tris, self.mu = xy, tris, mu
         self.mu_port = float(np.real(mu[0]))
@@ -110,11 +116,12 @@ class Fem2DMode:
         self.g = np.einsum("tji,kj->tki", Jinv, r)          # grad lambda_k = J^-T r_k : (T,3,2)
         self.area = 0.5 * np.abs(det)
         self.st, self.P0, self.Jinv = st, P[:, 0], Jinv
-        eid = {(int(a), int(b)): e for e, (a, b) in enumerate(edges)}
-        lp = [(0, 1), (0, 2), (1, 2)]
-        self.ce = np.array([[et[eid[(int(t[a]), int(t[b]))]] for a, b in lp] for t in st])   # (T,3)
-        self.cz = ez[st]                                     # (T,3)
-        self.gz = np.einsum("tk,tki->ti", self.cz, self.g)   # grad e_z (T,2)
+        if self.order == 1:
+            eid = {(int(a), int(b)): e for e, (a, b) in enumerate(edges)}
+            lp = [(0, 1), (0, 2), (1, 2)]
+            self.ce = np.array([[et[eid[(int(t[a]), int(t[b]))]] for a, b in lp] for t in st])   # (T,3)
+            self.cz = ez[st]                                     # (T,3)
+            self.gz = np.einsum("tk,tki->ti", self.cz, self.g)   # grad e_z (T,2)
         self.w = 2 * np.pi * freq
         # metrics
         p0 = np.asarray(mode["vpath"][0], dtype=np.float64)
@@ -151,11 +158,25 @@ class Fem2DMode:
         lam = np.stack([1 - lam12[:, 0] - lam12[:, 1], lam12[:, 0], lam12[:, 1]], axis=1)   # (p,3)
         g = self.g[t]                                               # (p,3,2)
         e2 = np.zeros((len(t), 2), dtype=np.complex128)
-        for i, (a, b) in enumerate([(0, 1), (0, 2), (1, 2)]):
-            Ni = lam[:, a:a + 1] * g[:, b] - lam[:, b:b + 1] * g[:, a]
-            e2 += self.ce[t, i][:, None] * Ni
+        if self.order == 2:
+            gz = np.zeros((len(t), 2), dtype=np.complex128)
+            for i, (a, b) in enumerate(LP2):
+                W = lam[:, a:a + 1] * g[:, b] - lam[:, b:b + 1] * g[:, a]
+                Gr = lam[:, a:a + 1] * g[:, b] + lam[:, b:b + 1] * g[:, a]
+                e2 += self.ct[t, i][:, None] * W + self.ct[t, 3 + i][:, None] * Gr
+                gz += self.cz2[t, 3 + i][:, None] * Gr
+            for k, (c, (a, b)) in enumerate(((2, (0, 1)), (0, (1, 2)))):
+                W = lam[:, a:a + 1] * g[:, b] - lam[:, b:b + 1] * g[:, a]
+                e2 += self.ct[t, 6 + k][:, None] * lam[:, c:c + 1] * W
+            for k in range(3):
+                gz += self.cz2[t, k][:, None] * g[:, k]
+        else:
+            for i, (a, b) in enumerate([(0, 1), (0, 2), (1, 2)]):
+                Ni = lam[:, a:a + 1] * g[:, b] - lam[:, b:b + 1] * g[:, a]
+                e2 += self.ce[t, i][:, None] * Ni
+            gz = self.gz[t]
         E = e2[:, 0:1] * self.uh[None, :] + e2[:, 1:2] * self.vh[None, :]
-        G = self.gamma * e2 + self.gz[t]
+        G = self.gamma * e2 + gz
         G3 = G[:, 0:1] * self.uh[None, :] + G[:, 1:2] * self.vh[None, :]
         H = np.cross(self.nh[None, :], G3) / (1j * self.w * MU0 * self.mu[t][:, None])
         return E, H
