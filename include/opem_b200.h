@@ -102,9 +102,11 @@ int  opem_problem_set_port_te(opem_problem prob, int port, const double* desc);
 /* Port driven by the fundamental mode of its own cross-section, solved at every
  * frequency on the port faces split nsub x nsub (1..64) with the materials of
  * the tetrahedra behind them (the 2D solve the reference spawns per frequency,
- * port.cpp:5081-5176; opem_port_mode_2d does the eigensolve).  desc as for
+ * port.cpp:5081-5176).  order 1: lowest-order edge elements for e_t and linear
+ * nodal e_z (opem_port_mode_2d's solve); order 2: degree-2 edge elements and
+ * quadratic nodal e_z (beta converges at fourth order in the split).  desc as for
  * opem_problem_set_port_te; its a, b, m, n are not used.                       */
-int  opem_problem_set_port_fem2d(opem_problem prob, int port, const double* desc, int nsub);
+int  opem_problem_set_port_fem2d(opem_problem prob, int port, const double* desc, int nsub, int order);
 /* Builds DOF numbering, CSR pattern, vertex patches, and assembles the frequency-
  * independent operators on the device.                                         */
 int  opem_problem_assemble(opem_problem prob);
@@ -211,15 +213,15 @@ int  opem_port_mode_2d(int64_t nnodes, const double* xy, int64_t ntri, const int
 /* The mode opem_problem_set_port_fem2d uses, on the host: port faces given as
  * vertex triples (face_verts, 3 per face, in the face's local vertex order) of
  * verts (3 doubles each), eps_face / mu_face complex per face (interleaved;
- * mu_face may be NULL), desc and nsub as for opem_problem_set_port_fem2d.
+ * mu_face may be NULL), desc, nsub and order as for opem_problem_set_port_fem2d.
  * metrics = {gamma, Z, V, Pz} (4 complex, interleaved).  For npts points, each
  * given as a face (pt_face) and its parameters (pt_s: s1, s2 with
  * X = P0 + s1 (P1 - P0) + s2 (P2 - P0)), E_out and Hy_out (3 complex each, may
  * be NULL) receive E_t and H_t / y, y = gamma / (j w mu0 mu_r(face 0)).        */
 int  opem_port_mode_faces(int64_t nverts, const double* verts, int64_t nface, const int64_t* face_verts,
-                          const double* eps_face, const double* mu_face, const double* desc, int nsub, double freq,
-                          double* metrics, int64_t npts, const int64_t* pt_face, const double* pt_s, double* E_out,
-                          double* Hy_out);
+                          const double* eps_face, const double* mu_face, const double* desc, int nsub, int order,
+                          double freq, double* metrics, int64_t npts, const int64_t* pt_face, const double* pt_s,
+                          double* E_out, double* Hy_out);
 
 /* ---- S-parameter post-processing (host only, no GPU needed) -----------------
  * Renormalises S (nports x nports complex, interleaved, row = portOut) from the

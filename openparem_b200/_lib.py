@@ -54,7 +54,7 @@ SIGNATURES = [
     ("opem_problem_set_regions", C.c_int, [P, C.c_int, DP, DP, DP, DP]),
     ("opem_problem_set_boundary", C.c_int, [P, C.c_int, C.c_int, DP, C.c_int]),
     ("opem_problem_set_port_te", C.c_int, [P, C.c_int, DP]),
-    ("opem_problem_set_port_fem2d", C.c_int, [P, C.c_int, DP, C.c_int]),
+    ("opem_problem_set_port_fem2d", C.c_int, [P, C.c_int, DP, C.c_int, C.c_int]),
     ("opem_mesh_errors", C.c_int, [P, C.c_double, DP, I64P, C.c_int64, I64P, DP]),
     ("opem_problem_assemble", C.c_int, [P]),
     ("opem_problem_info", C.c_int, [P, I64P, C.c_int]),
@@ -78,7 +78,7 @@ SIGNATURES = [
     ("opem_project_read", C.c_int, [C.c_char_p, C.c_int, I64P, DP, I64P, I32P, DP, I64P, I32P, I32P, DP, DP, I32P,
                                      DP, C.c_char_p, C.c_int]),
     ("opem_port_mode_2d", C.c_int, [C.c_int64, DP, C.c_int64, I64P, DP, DP, C.c_double, DP, I64P, I64P, DP, DP]),
-    ("opem_port_mode_faces", C.c_int, [C.c_int64, DP, C.c_int64, I64P, DP, DP, DP, C.c_int, C.c_double, DP,
+    ("opem_port_mode_faces", C.c_int, [C.c_int64, DP, C.c_int64, I64P, DP, DP, DP, C.c_int, C.c_int, C.c_double, DP,
                                         C.c_int64, I64P, DP, DP, DP]),
     ("opem_s_renormalize", C.c_int, [C.c_int, DP, DP, C.c_double, C.c_double, DP]),
     ("opem_write_touchstone", C.c_int, [C.c_char_p, C.c_int, DP, C.c_int, DP, C.c_double, C.c_char_p, C.c_char_p]),

@@ -104,7 +104,7 @@ static std::shared_ptr<const PortFem2D> port_fem2d(const Problem& P, int k, doub
     auto sol = std::make_shared<PortFem2D>();
     std::string err;
     int rc = port_fem2d_solve(T.verts.data(), (int64_t)fv.size() / 3, fv.data(), eps.data(), mu.data(), pm.desc,
-                              pm.nsub, freq, mu[0].real(), *sol, err);
+                              pm.nsub, pm.order2d, freq, mu[0].real(), *sol, err);
     if (rc != OPEM_OK) throw OpemError(rc, err);
     pm.fem->sols.emplace_back(freq, sol);
     if (pm.fem->sols.size() > 8) pm.fem->sols.erase(pm.fem->sols.begin());
@@ -914,8 +914,8 @@ int opem_problem_set_port_te(opem_problem prob, int port, const double* desc) {
     return OPEM_OK;
 }
 
-int opem_problem_set_port_fem2d(opem_problem prob, int port, const double* desc, int nsub) {
-    if (!prob || !desc || port < 0 || port > 7 || nsub < 1 || nsub > 64) return OPEM_ERR_ARG;
+int opem_problem_set_port_fem2d(opem_problem prob, int port, const double* desc, int nsub, int order) {
+    if (!prob || !desc || port < 0 || port > 7 || nsub < 1 || nsub > 64 || order < 1 || order > 2) return OPEM_ERR_ARG;
     for (int i = 0; i < 22; ++i)
         if (!std::isfinite(desc[i])) return OPEM_ERR_ARG;
     Problem& P = prob->p;
@@ -924,6 +924,7 @@ int opem_problem_set_port_fem2d(opem_problem prob, int port, const double* desc,
     m.set = true;
     m.kind = 1;
     m.nsub = nsub;
+    m.order2d = order;
     m.fem = std::make_shared<PortFemCache>();
     std::memcpy(m.desc, desc, 22 * sizeof(double));
     P.assembled = false;

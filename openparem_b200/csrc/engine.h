@@ -88,6 +88,7 @@ struct PortMode {
     double desc[26];
     int kind = 0;    // 0: analytic TE_mn (desc), 1: 2D mode of the port faces
     int nsub = 0;    // kind 1: split of each port face
+    int order2d = 1; // kind 1: 2D element order
     std::shared_ptr<PortFemCache> fem;
 };
 

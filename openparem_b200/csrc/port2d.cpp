@@ -22,6 +22,8 @@
 #include <vector>
 
 #include "../../include/opem_b200.h"
+#include "opem_internal.h"
+#include "portfem.h"
 
 namespace {
 
@@ -119,6 +121,77 @@ std::vector<int> rcm(int n, const std::vector<std::vector<int>>& adj) {
     }
     std::reverse(order.begin(), order.end());
     return order;
+}
+
+// Fundamental eigenpair of the pencil A x = -beta^2 B x (largest beta^2) by
+// inverse iteration with the shift sigma: RCM ordering, banded LU of A - sigma B,
+// converged when the eigenvalue has settled and the unit eigenvector stops
+// moving (up to phase).  Returns an OPEM_* code; lam = -beta^2, xout unit norm
+// in the caller's numbering.
+int solve_pencil(int n, const std::vector<Triplet>& A, const std::vector<Triplet>& Bm, double sigma, cd& lam,
+                 std::vector<cd>& xout) {
+    // ordering and band
+    std::vector<std::vector<int>> adj(n);
+    for (auto* T : {&A, &Bm})
+        for (auto& x : *T)
+            if (x.r != x.c) adj[x.r].push_back(x.c);
+    for (auto& a : adj) { std::sort(a.begin(), a.end()); a.erase(std::unique(a.begin(), a.end()), a.end()); }
+    std::vector<int> ord = rcm(n, adj), pos(n);
+    for (int i = 0; i < n; ++i) pos[ord[i]] = i;
+    int bw = 0;
+    for (int i = 0; i < n; ++i)
+        for (int j : adj[i]) bw = std::max(bw, std::abs(pos[i] - pos[j]));
+    Banded M;
+    M.init(n, bw, bw);
+    for (auto& x : A) M.at(pos[x.r], pos[x.c]) += x.v;
+    for (auto& x : Bm) M.at(pos[x.r], pos[x.c]) -= sigma * x.v;
+    if (!M.factor()) return OPEM_ERR_BREAKDOWN;
+    // inverse iteration: y = (A - sigma B)^-1 B x; its dominant eigenvalue mu gives lambda = sigma + 1/mu
+    auto Bmul = [&](const std::vector<cd>& x, std::vector<cd>& y) {
+        std::fill(y.begin(), y.end(), 0.0);
+        for (auto& t : Bm) y[pos[t.r]] += t.v * x[pos[t.c]];
+    };
+    std::vector<cd> x(n), y(n), bx(n), xold(n);
+    for (int i = 0; i < n; ++i) x[i] = cd(1.0 + 0.001 * (i % 7), 0.0005 * (i % 5));
+    cd lam_prev = 0;
+    lam = 0;
+    bool ok = false;
+    int lam_done = 0;
+    for (int it = 0; it < 4000; ++it) {
+        xold = x;
+        Bmul(x, bx);
+        y = bx;
+        M.solve(y);
+        // Rayleigh-type estimate mu = (x^H B y) / (x^H B x), B symmetric
+        std::vector<cd> by(n);
+        Bmul(y, by);
+        cd num = 0, den = 0;
+        for (int i = 0; i < n; ++i) { num += std::conj(x[i]) * by[i]; den += std::conj(x[i]) * bx[i]; }
+        double nrm = 0;
+        for (auto& v : y) nrm += std::norm(v);
+        nrm = std::sqrt(nrm);
+        if (!(nrm > 0) || den == 0.0) return OPEM_ERR_BREAKDOWN;
+        for (int i = 0; i < n; ++i) x[i] = y[i] / nrm;
+        const cd mu = num / den;
+        lam = sigma + 1.0 / mu;
+        // converged when the eigenvalue has settled and the unit eigenvector stops
+        // moving (up to phase): the eigenvalue settles about twice as fast, and
+        // small components such as e_z of a TE-like mode need the vector itself
+        if (it > 3 && std::abs(lam - lam_prev) <= 1e-14 * std::abs(lam)) ++lam_done;
+        if (lam_done) {
+            cd c = 0;
+            for (int i = 0; i < n; ++i) c += std::conj(xold[i]) * x[i];
+            const cd ph = std::abs(c) > 0 ? c / std::abs(c) : cd(1.0);
+            double dx = 0;
+            for (int i = 0; i < n; ++i) dx += std::norm(x[i] - ph * xold[i]);
+            if (std::sqrt(dx) <= 1e-13 || lam_done > 200) { ok = true; break; }
+        }
+        lam_prev = lam;
+    }
+    if (!ok) return OPEM_ERR_NOT_CONVERGED;
+    xout.assign(n, 0.0);
+    for (int i = 0; i < n; ++i) xout[i] = x[pos[i]];
+    return OPEM_OK;
 }
 
 }  // namespace
@@ -225,65 +298,13 @@ int opem_port_mode_2d(int64_t nnodes, const double* xy, int64_t ntri, const int6
             Bm.push_back({nmap[x.c], emap[x.r], x.v});
         }
     for (auto& x : Bnn) if (nmap[x.r] >= 0 && nmap[x.c] >= 0) Bm.push_back({nmap[x.r], nmap[x.c], x.v});
-    // ordering and band
-    std::vector<std::vector<int>> adj(n);
-    for (auto* T : {&A, &Bm})
-        for (auto& x : *T)
-            if (x.r != x.c) adj[x.r].push_back(x.c);
-    for (auto& a : adj) { std::sort(a.begin(), a.end()); a.erase(std::unique(a.begin(), a.end()), a.end()); }
-    std::vector<int> ord = rcm(n, adj), pos(n);
-    for (int i = 0; i < n; ++i) pos[ord[i]] = i;
-    int bw = 0;
-    for (int i = 0; i < n; ++i)
-        for (int j : adj[i]) bw = std::max(bw, std::abs(pos[i] - pos[j]));
     const double sigma = -k0 * k0 * emax;
-    Banded M;
-    M.init(n, bw, bw);
-    for (auto& x : A) M.at(pos[x.r], pos[x.c]) += x.v;
-    for (auto& x : Bm) M.at(pos[x.r], pos[x.c]) -= sigma * x.v;
-    if (!M.factor()) return OPEM_ERR_BREAKDOWN;
-    // inverse iteration: y = (A - sigma B)^-1 B x; its dominant eigenvalue mu gives lambda = sigma + 1/mu
-    auto Bmul = [&](const std::vector<cd>& x, std::vector<cd>& y) {
-        std::fill(y.begin(), y.end(), 0.0);
-        for (auto& t : Bm) y[pos[t.r]] += t.v * x[pos[t.c]];
-    };
-    std::vector<cd> x(n), y(n), bx(n), xold(n);
-    for (int i = 0; i < n; ++i) x[i] = cd(1.0 + 0.001 * (i % 7), 0.0005 * (i % 5));
-    cd lam = 0, lam_prev = 0;
-    bool ok = false;
-    int lam_done = 0;
-    for (int it = 0; it < 4000; ++it) {
-        xold = x;
-        Bmul(x, bx);
-        y = bx;
-        M.solve(y);
-        // Rayleigh-type estimate mu = (x^H B y) / (x^H B x), B symmetric
-        std::vector<cd> by(n);
-        Bmul(y, by);
-        cd num = 0, den = 0;
-        for (int i = 0; i < n; ++i) { num += std::conj(x[i]) * by[i]; den += std::conj(x[i]) * bx[i]; }
-        double nrm = 0;
-        for (auto& v : y) nrm += std::norm(v);
-        nrm = std::sqrt(nrm);
-        if (!(nrm > 0) || den == 0.0) return OPEM_ERR_BREAKDOWN;
-        for (int i = 0; i < n; ++i) x[i] = y[i] / nrm;
-        const cd mu = num / den;
-        lam = sigma + 1.0 / mu;
-        // converged when the eigenvalue has settled and the unit eigenvector stops
-        // moving (up to phase): the eigenvalue settles about twice as fast, and
-        // small components such as e_z of a TE-like mode need the vector itself
-        if (it > 3 && std::abs(lam - lam_prev) <= 1e-14 * std::abs(lam)) ++lam_done;
-        if (lam_done) {
-            cd c = 0;
-            for (int i = 0; i < n; ++i) c += std::conj(xold[i]) * x[i];
-            const cd ph = std::abs(c) > 0 ? c / std::abs(c) : cd(1.0);
-            double dx = 0;
-            for (int i = 0; i < n; ++i) dx += std::norm(x[i] - ph * xold[i]);
-            if (std::sqrt(dx) <= 1e-13 || lam_done > 200) { ok = true; break; }
-        }
-        lam_prev = lam;
+    cd lam = 0;
+    std::vector<cd> xs;
+    {
+        int rc = solve_pencil(n, A, Bm, sigma, lam, xs);
+        if (rc != OPEM_OK) return rc;
     }
-    if (!ok) return OPEM_ERR_NOT_CONVERGED;
     cd beta = std::sqrt(-lam);
     if (beta.real() < 0) beta = -beta;
     beta_out[0] = beta.real();
@@ -291,17 +312,17 @@ int opem_port_mode_2d(int64_t nnodes, const double* xy, int64_t ntri, const int6
     // scale: the largest e_t coefficient becomes 1
     cd big = 0.0;
     for (int e = 0; e < ne; ++e)
-        if (emap[e] >= 0 && std::abs(x[pos[emap[e]]]) > std::abs(big)) big = x[pos[emap[e]]];
+        if (emap[e] >= 0 && std::abs(xs[emap[e]]) > std::abs(big)) big = xs[emap[e]];
     const cd s = std::abs(big) > 0 ? 1.0 / big : cd(1.0);
     if (et_out)
         for (int e = 0; e < ne; ++e) {
-            const cd v = emap[e] >= 0 ? x[pos[emap[e]]] * s : cd(0.0);
+            const cd v = emap[e] >= 0 ? xs[emap[e]] * s : cd(0.0);
             et_out[2 * e] = v.real();
             et_out[2 * e + 1] = v.imag();
         }
     if (ez_out)
         for (int64_t i = 0; i < nnodes; ++i) {
-            const cd v = nmap[i] >= 0 ? -cd(0, 1) * beta * x[pos[nmap[i]]] * s : cd(0.0);   // e_z = -j beta psi
+            const cd v = nmap[i] >= 0 ? -cd(0, 1) * beta * xs[nmap[i]] * s : cd(0.0);   // e_z = -j beta psi
             ez_out[2 * i] = v.real();
             ez_out[2 * i + 1] = v.imag();
         }
@@ -309,3 +330,180 @@ int opem_port_mode_2d(int64_t nnodes, const double* xy, int64_t ntri, const int6
 }
 
 }  // extern "C"
+
+namespace opem {
+
+// Second-order elements for the same pencil (the oracle's port2d.solve_mode_p2):
+// with the triangle's vertices sorted by node id and l_0..2 their barycentrics,
+//   e_t: W_ab = l_a grad l_b - l_b grad l_a and G_ab = grad(l_a l_b) for the edges
+//        (a,b) = (0,1), (0,2), (1,2) (shared by the edge's triangles), then the
+//        face functions l_2 W_01 and l_0 W_12 (no tangential trace);
+//   e_z: l_0, l_1, l_2 and the edge bubbles l_a l_b.
+// Whitney functions plus edge gradients span the complete linear fields and the
+// face functions complete the degree-2 first-kind space (Webb, IEEE TAP 47(8)
+// 1999); grad of the quadratic nodal space lies in it, as the pencil needs.
+// Element integrals by the degree-4 triangle rule (exact for these products).
+// Outputs per triangle: ct (8 e_t coefficients), cz (6 e_z coefficients), st
+// (the sorted vertex ids), scaled so the largest Whitney coefficient is 1.
+int port_mode_2d_p2(int64_t nnodes, const double* xy, int64_t ntri, const int64_t* tris, const cd* eps_r,
+                    const cd* mu_r, double freq, cd& beta, std::vector<cd>& ct, std::vector<cd>& cz,
+                    std::vector<int64_t>& st) {
+    if (nnodes < 3 || !xy || ntri < 1 || !tris || !eps_r || !(freq > 0)) return OPEM_ERR_ARG;
+    for (int64_t t = 0; t < 3 * ntri; ++t)
+        if (tris[t] < 0 || tris[t] >= nnodes) return OPEM_ERR_ARG;
+    static const int LP[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+    const double k0 = 2 * M_PI * freq * std::sqrt(MU0 * EPS0);
+    st.resize(3 * ntri);
+    std::map<std::pair<int64_t, int64_t>, int> eid;
+    for (int64_t t = 0; t < ntri; ++t) {
+        int64_t v[3] = {tris[3 * t], tris[3 * t + 1], tris[3 * t + 2]};
+        std::sort(v, v + 3);
+        for (int k = 0; k < 3; ++k) st[3 * t + k] = v[k];
+        for (auto& lp : LP) eid[{v[lp[0]], v[lp[1]]}] = 0;
+    }
+    int ne = 0;
+    std::vector<std::pair<int64_t, int64_t>> edges;
+    for (auto& kv : eid) { kv.second = ne++; edges.push_back(kv.first); }
+    // global numbering: e_t = [W (ne), G (ne), face (2 ntri)], e_z = [vertex (nnodes), bubble (ne)]
+    const int64_t net = 2 * (int64_t)ne + 2 * ntri, nz = nnodes + ne;
+    std::vector<int64_t> tdof(8 * ntri), zdof(6 * ntri);
+    std::vector<int> ecount(ne, 0);
+    for (int64_t t = 0; t < ntri; ++t) {
+        for (int i = 0; i < 3; ++i) {
+            const int e = eid[{st[3 * t + LP[i][0]], st[3 * t + LP[i][1]]}];
+            ++ecount[e];
+            tdof[8 * t + i] = e;
+            tdof[8 * t + 3 + i] = ne + e;
+            zdof[6 * t + i] = st[3 * t + i];
+            zdof[6 * t + 3 + i] = nnodes + e;
+        }
+        tdof[8 * t + 6] = 2 * (int64_t)ne + 2 * t;
+        tdof[8 * t + 7] = 2 * (int64_t)ne + 2 * t + 1;
+    }
+    std::vector<double> q1, q2, qw;
+    tri_rule(4, q1, q2, qw);
+    const int nq = (int)qw.size();
+    std::vector<Triplet> Aee, Bee, Ben, Bnn;
+    double emax = 0;
+    auto cross = [](const double* a, const double* b) { return a[0] * b[1] - a[1] * b[0]; };
+    for (int64_t t = 0; t < ntri; ++t) {
+        const double* p0 = xy + 2 * st[3 * t];
+        const double* p1 = xy + 2 * st[3 * t + 1];
+        const double* p2 = xy + 2 * st[3 * t + 2];
+        const double J00 = p1[0] - p0[0], J01 = p2[0] - p0[0], J10 = p1[1] - p0[1], J11 = p2[1] - p0[1];
+        const double det = J00 * J11 - J01 * J10;
+        if (!(std::fabs(det) > 0)) return OPEM_ERR_ARG;
+        const double area = 0.5 * std::fabs(det);
+        const double i00 = J11 / det, i01 = -J01 / det, i10 = -J10 / det, i11 = J00 / det;
+        double g[3][2];
+        const double r[3][2] = {{-1, -1}, {1, 0}, {0, 1}};
+        for (int k = 0; k < 3; ++k) {
+            g[k][0] = i00 * r[k][0] + i10 * r[k][1];
+            g[k][1] = i01 * r[k][0] + i11 * r[k][1];
+        }
+        const cd er = eps_r[t], mr = mu_r ? mu_r[t] : cd(1.0), im = 1.0 / mr;
+        emax = std::max(emax, std::real(er * mr));
+        double M[8][8] = {}, C[8][8] = {}, Gm[8][6] = {}, Kg[6][6] = {}, Ml[6][6] = {};
+        for (int q = 0; q < nq; ++q) {
+            const double lam[3] = {1 - q1[q] - q2[q], q1[q], q2[q]};
+            const double w = 2 * area * qw[q];
+            double N[8][2], cN[8], L[6], dL[6][2];
+            for (int i = 0; i < 3; ++i) {
+                const int a = LP[i][0], b = LP[i][1];
+                for (int c = 0; c < 2; ++c) {
+                    N[i][c] = lam[a] * g[b][c] - lam[b] * g[a][c];
+                    N[3 + i][c] = lam[a] * g[b][c] + lam[b] * g[a][c];
+                    dL[3 + i][c] = N[3 + i][c];
+                    dL[i][c] = g[i][c];
+                }
+                cN[i] = 2.0 * cross(g[a], g[b]);
+                cN[3 + i] = 0.0;
+                L[i] = lam[i];
+                L[3 + i] = lam[a] * lam[b];
+            }
+            const int FC[2][3] = {{2, 0, 1}, {0, 1, 2}};   // (c, a, b): l_c W_ab
+            for (int k = 0; k < 2; ++k) {
+                const int c = FC[k][0], a = FC[k][1], b = FC[k][2];
+                double W[2];
+                for (int d = 0; d < 2; ++d) W[d] = lam[a] * g[b][d] - lam[b] * g[a][d];
+                for (int d = 0; d < 2; ++d) N[6 + k][d] = lam[c] * W[d];
+                cN[6 + k] = cross(g[c], W) + lam[c] * 2.0 * cross(g[a], g[b]);
+            }
+            for (int i = 0; i < 8; ++i) {
+                for (int j = 0; j < 8; ++j) {
+                    M[i][j] += w * (N[i][0] * N[j][0] + N[i][1] * N[j][1]);
+                    C[i][j] += w * cN[i] * cN[j];
+                }
+                for (int j = 0; j < 6; ++j) Gm[i][j] += w * (N[i][0] * dL[j][0] + N[i][1] * dL[j][1]);
+            }
+            for (int i = 0; i < 6; ++i)
+                for (int j = 0; j < 6; ++j) {
+                    Kg[i][j] += w * (dL[i][0] * dL[j][0] + dL[i][1] * dL[j][1]);
+                    Ml[i][j] += w * L[i] * L[j];
+                }
+        }
+        for (int i = 0; i < 8; ++i) {
+            for (int j = 0; j < 8; ++j) {
+                Aee.push_back({(int)tdof[8 * t + i], (int)tdof[8 * t + j], im * C[i][j] - k0 * k0 * er * M[i][j]});
+                Bee.push_back({(int)tdof[8 * t + i], (int)tdof[8 * t + j], im * M[i][j]});
+            }
+            for (int j = 0; j < 6; ++j) Ben.push_back({(int)tdof[8 * t + i], (int)zdof[6 * t + j], -im * Gm[i][j]});
+        }
+        for (int i = 0; i < 6; ++i)
+            for (int j = 0; j < 6; ++j)
+                Bnn.push_back({(int)zdof[6 * t + i], (int)zdof[6 * t + j], im * Kg[i][j] - k0 * k0 * er * Ml[i][j]});
+    }
+    // PEC: both edge functions of boundary edges, boundary vertices and bubbles
+    std::vector<int> tmap(net, -1), zmap(nz, -1);
+    std::vector<char> bnode(nnodes, 0), bedge(ne, 0);
+    for (int e = 0; e < ne; ++e)
+        if (ecount[e] == 1) { bedge[e] = 1; bnode[edges[e].first] = 1; bnode[edges[e].second] = 1; }
+    int nu = 0;
+    for (int64_t i = 0; i < net; ++i) {
+        const bool drop = (i < ne && bedge[i]) || (i >= ne && i < 2 * ne && bedge[i - ne]);
+        if (!drop) tmap[i] = nu++;
+    }
+    const int nut = nu;
+    std::vector<char> used(nnodes, 0);
+    for (int64_t t = 0; t < 3 * ntri; ++t) used[tris[t]] = 1;
+    for (int64_t i = 0; i < nz; ++i) {
+        const bool drop = i < nnodes ? (!used[i] || bnode[i]) : (bool)bedge[i - nnodes];
+        if (!drop) zmap[i] = nu++;
+    }
+    const int n = nu;
+    if (nut == 0) return OPEM_ERR_ARG;
+    std::vector<Triplet> A, Bm;
+    for (auto& x : Aee) if (tmap[x.r] >= 0 && tmap[x.c] >= 0) A.push_back({tmap[x.r], tmap[x.c], x.v});
+    for (auto& x : Bee) if (tmap[x.r] >= 0 && tmap[x.c] >= 0) Bm.push_back({tmap[x.r], tmap[x.c], x.v});
+    for (auto& x : Ben)
+        if (tmap[x.r] >= 0 && zmap[x.c] >= 0) {
+            Bm.push_back({tmap[x.r], zmap[x.c], x.v});
+            Bm.push_back({zmap[x.c], tmap[x.r], x.v});
+        }
+    for (auto& x : Bnn) if (zmap[x.r] >= 0 && zmap[x.c] >= 0) Bm.push_back({zmap[x.r], zmap[x.c], x.v});
+    cd lam = 0;
+    std::vector<cd> xs;
+    int rc = solve_pencil(n, A, Bm, -k0 * k0 * emax, lam, xs);
+    if (rc != OPEM_OK) return rc;
+    beta = std::sqrt(-lam);
+    if (beta.real() < 0) beta = -beta;
+    cd big = 0.0;
+    for (int e = 0; e < ne; ++e)
+        if (tmap[e] >= 0 && std::abs(xs[tmap[e]]) > std::abs(big)) big = xs[tmap[e]];
+    const cd sc = std::abs(big) > 0 ? 1.0 / big : cd(1.0);
+    ct.assign(8 * ntri, 0.0);
+    cz.assign(6 * ntri, 0.0);
+    for (int64_t t = 0; t < ntri; ++t) {
+        for (int i = 0; i < 8; ++i) {
+            const int m = tmap[tdof[8 * t + i]];
+            ct[8 * t + i] = m >= 0 ? xs[m] * sc : cd(0.0);
+        }
+        for (int i = 0; i < 6; ++i) {
+            const int m = zmap[zdof[6 * t + i]];
+            cz[6 * t + i] = m >= 0 ? -cd(0, 1) * beta * xs[m] * sc : cd(0.0);   // e_z = -j beta psi
+        }
+    }
+    return OPEM_OK;
+}
+
+}  // namespace opem

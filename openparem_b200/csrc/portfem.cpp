@@ -59,18 +59,45 @@ void PortFem2D::eval_tri(int64_t t, const double X[3], cd E[3], cd Hy[3]) const 
     const double l1 = Ji[0] * d0 + Ji[1] * d1, l2 = Ji[2] * d0 + Ji[3] * d1;
     const double lam[3] = {1 - l1 - l2, l1, l2};
     const double* gg = &g[6 * t];
-    cd ex = 0.0, ey = 0.0;
-    for (int i = 0; i < 3; ++i) {
-        const int a = LP[i][0], b = LP[i][1];
-        const double nx = lam[a] * gg[2 * b] - lam[b] * gg[2 * a];
-        const double ny = lam[a] * gg[2 * b + 1] - lam[b] * gg[2 * a + 1];
-        ex += ce[3 * t + i] * nx;
-        ey += ce[3 * t + i] * ny;
+    cd ex = 0.0, ey = 0.0, zx, zy;
+    if (order == 2) {
+        // W_ab, G_ab = grad(l_a l_b) per edge, then l_2 W_01 and l_0 W_12; e_z quadratic
+        zx = 0.0;
+        zy = 0.0;
+        for (int i = 0; i < 3; ++i) {
+            const int a = LP[i][0], b = LP[i][1];
+            const double wx = lam[a] * gg[2 * b] - lam[b] * gg[2 * a];
+            const double wy = lam[a] * gg[2 * b + 1] - lam[b] * gg[2 * a + 1];
+            const double gx = lam[a] * gg[2 * b] + lam[b] * gg[2 * a];
+            const double gy = lam[a] * gg[2 * b + 1] + lam[b] * gg[2 * a + 1];
+            ex += ct[8 * t + i] * wx + ct[8 * t + 3 + i] * gx;
+            ey += ct[8 * t + i] * wy + ct[8 * t + 3 + i] * gy;
+            zx += cz[6 * t + 3 + i] * gx + cz[6 * t + i] * gg[2 * i];
+            zy += cz[6 * t + 3 + i] * gy + cz[6 * t + i] * gg[2 * i + 1];
+        }
+        const int FC[2][3] = {{2, 0, 1}, {0, 1, 2}};
+        for (int k = 0; k < 2; ++k) {
+            const int c = FC[k][0], a = FC[k][1], b = FC[k][2];
+            const double wx = lam[a] * gg[2 * b] - lam[b] * gg[2 * a];
+            const double wy = lam[a] * gg[2 * b + 1] - lam[b] * gg[2 * a + 1];
+            ex += ct[8 * t + 6 + k] * (lam[c] * wx);
+            ey += ct[8 * t + 6 + k] * (lam[c] * wy);
+        }
+    } else {
+        for (int i = 0; i < 3; ++i) {
+            const int a = LP[i][0], b = LP[i][1];
+            const double nx = lam[a] * gg[2 * b] - lam[b] * gg[2 * a];
+            const double ny = lam[a] * gg[2 * b + 1] - lam[b] * gg[2 * a + 1];
+            ex += ce[3 * t + i] * nx;
+            ey += ce[3 * t + i] * ny;
+        }
+        zx = gz[2 * t];
+        zy = gz[2 * t + 1];
     }
     for (int i = 0; i < 3; ++i) E[i] = ex * u[i] + ey * v[i];
     // H_t / y = (mu_port / mu) n x (e_t + grad e_z / gamma)
     const cd s = mu_port / mu[t];
-    n_cross_plane(n, u, v, s * (ex + gz[2 * t] / gamma), s * (ey + gz[2 * t + 1] / gamma), Hy);
+    n_cross_plane(n, u, v, s * (ex + zx / gamma), s * (ey + zy / gamma), Hy);
 }
 
 void PortFem2D::eval_face(int64_t f, double s1, double s2, const double X[3], cd E[3], cd Hy[3]) const {
@@ -102,10 +129,15 @@ int64_t PortFem2D::locate(const double X[3]) const {
 }
 
 int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* fv, const cd* eps_face, const cd* mu_face,
-                     const double* desc, int nsub, double freq, double mu_port, PortFem2D& M, std::string& err) {
-    if (nface < 1 || nsub < 1 || nsub > 64 || !(freq > 0)) { err = "port mode: bad arguments"; return OPEM_ERR_ARG; }
+                     const double* desc, int nsub, int order, double freq, double mu_port, PortFem2D& M,
+                     std::string& err) {
+    if (nface < 1 || nsub < 1 || nsub > 64 || order < 1 || order > 2 || !(freq > 0)) {
+        err = "port mode: bad arguments";
+        return OPEM_ERR_ARG;
+    }
     M = PortFem2D{};
     M.nsub = nsub;
+    M.order = order;
     M.nface = nface;
     M.freq = freq;
     M.mu_port = mu_port;
@@ -187,14 +219,28 @@ int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* fv, cons
     }
     double beta[2];
     int64_t ne = 0;
-    int rc = opem_port_mode_2d(nn, M.xy.data(), T, tris.data(), eps2.data(), mu2.data(), freq, beta, &ne, nullptr,
-                               nullptr, nullptr);
-    if (rc != OPEM_OK) { err = "port mode: 2D mesh rejected"; return rc; }
-    std::vector<int64_t> edges(2 * ne);
-    std::vector<double> et(2 * ne), ez(2 * nn);
-    rc = opem_port_mode_2d(nn, M.xy.data(), T, tris.data(), eps2.data(), mu2.data(), freq, beta, &ne, edges.data(),
-                           et.data(), ez.data());
-    if (rc != OPEM_OK) { err = "port mode: 2D eigensolve failed"; return rc; }
+    std::vector<int64_t> edges;
+    std::vector<double> et, ez;
+    if (order == 2) {
+        std::vector<cd> epsc(T), muc(T);
+        for (int64_t t = 0; t < T; ++t) { epsc[t] = cd(eps2[2 * t], eps2[2 * t + 1]); muc[t] = M.mu[t]; }
+        cd b2;
+        std::vector<int64_t> st2;
+        int rc = port_mode_2d_p2(nn, M.xy.data(), T, tris.data(), epsc.data(), muc.data(), freq, b2, M.ct, M.cz, st2);
+        if (rc != OPEM_OK) { err = "port mode: 2D eigensolve failed"; return rc; }
+        beta[0] = b2.real();
+        beta[1] = b2.imag();
+    } else {
+        int rc = opem_port_mode_2d(nn, M.xy.data(), T, tris.data(), eps2.data(), mu2.data(), freq, beta, &ne, nullptr,
+                                   nullptr, nullptr);
+        if (rc != OPEM_OK) { err = "port mode: 2D mesh rejected"; return rc; }
+        edges.resize(2 * ne);
+        et.resize(2 * ne);
+        ez.resize(2 * nn);
+        rc = opem_port_mode_2d(nn, M.xy.data(), T, tris.data(), eps2.data(), mu2.data(), freq, beta, &ne, edges.data(),
+                               et.data(), ez.data());
+        if (rc != OPEM_OK) { err = "port mode: 2D eigensolve failed"; return rc; }
+    }
     M.gamma = cd(-beta[1], beta[0]);   // j beta
     std::map<std::pair<int64_t, int64_t>, int64_t> eid;
     for (int64_t e = 0; e < ne; ++e) eid[{edges[2 * e], edges[2 * e + 1]}] = e;
@@ -224,6 +270,7 @@ int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* fv, cons
             M.g[6 * t + 2 * k] = Ji[0] * r[k][0] + Ji[2] * r[k][1];
             M.g[6 * t + 2 * k + 1] = Ji[1] * r[k][0] + Ji[3] * r[k][1];
         }
+        if (order == 2) continue;   // coefficients per triangle already (ct, cz)
         for (int i = 0; i < 3; ++i) {
             const int64_t e = eid.at({s[LP[i][0]], s[LP[i][1]]});
             M.ce[3 * t + i] = cd(et[2 * e], et[2 * e + 1]);
@@ -260,13 +307,26 @@ int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* fv, cons
     {
         const double w = 2 * M_PI * freq;
         const cd y = M.gamma / cd(0.0, w * MU0 * mu_port);
+        // edge-midpoint rule (exact for the quadratic integrand of order 1), or
+        // the degree-4 triangle rule (order 2: quartic integrand)
+        std::vector<double> r1, r2, rw;
+        if (order == 2) {
+            tri_rule(4, r1, r2, rw);
+            for (double& x : rw) x *= 6.0;   // weights of the midpoint form: area/3 * sum -> sum_q 2 w_q area
+        } else {
+            r1 = {0.5, 0.0, 0.5};
+            r2 = {0.0, 0.5, 0.5};
+            rw = {1.0, 1.0, 1.0};
+        }
         cd pz = 0.0;
         for (int64_t t = 0; t < T; ++t) {
             cd acc = 0.0;
-            for (int m = 0; m < 3; ++m) {
-                const int a = LP[m][0], b = LP[m][1];
-                const double x2[2] = {0.5 * (M.xy[2 * M.st[3 * t + a]] + M.xy[2 * M.st[3 * t + b]]),
-                                      0.5 * (M.xy[2 * M.st[3 * t + a] + 1] + M.xy[2 * M.st[3 * t + b] + 1])};
+            const double* q0 = &M.xy[2 * M.st[3 * t]];
+            const double* q1 = &M.xy[2 * M.st[3 * t + 1]];
+            const double* q2 = &M.xy[2 * M.st[3 * t + 2]];
+            for (size_t m = 0; m < rw.size(); ++m) {
+                const double x2[2] = {q0[0] + r1[m] * (q1[0] - q0[0]) + r2[m] * (q2[0] - q0[0]),
+                                      q0[1] + r1[m] * (q1[1] - q0[1]) + r2[m] * (q2[1] - q0[1])};
                 double X[3];
                 for (int c = 0; c < 3; ++c) X[c] = M.o[c] + x2[0] * M.u[c] + x2[1] * M.v[c];
                 cd E[3], Hy[3];
@@ -276,7 +336,7 @@ int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* fv, cons
                 const cd cx = E[1] * std::conj(H[2]) - E[2] * std::conj(H[1]);
                 const cd cy = E[2] * std::conj(H[0]) - E[0] * std::conj(H[2]);
                 const cd cz = E[0] * std::conj(H[1]) - E[1] * std::conj(H[0]);
-                acc += cx * M.n[0] + cy * M.n[1] + cz * M.n[2];
+                acc += rw[m] * (cx * M.n[0] + cy * M.n[1] + cz * M.n[2]);
             }
             pz += area[t] / 3.0 * acc;
         }
@@ -290,7 +350,7 @@ int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* fv, cons
 
 extern "C" int opem_port_mode_faces(int64_t nverts, const double* verts, int64_t nface, const int64_t* face_verts,
                                     const double* eps_face, const double* mu_face, const double* desc, int nsub,
-                                    double freq, double* metrics, int64_t npts, const int64_t* pt_face,
+                                    int order, double freq, double* metrics, int64_t npts, const int64_t* pt_face,
                                     const double* pt_s, double* E_out, double* Hy_out) {
     using cd = std::complex<double>;
     if (nverts < 3 || !verts || nface < 1 || !face_verts || !eps_face || !desc || !metrics) return OPEM_ERR_ARG;
@@ -306,7 +366,7 @@ extern "C" int opem_port_mode_faces(int64_t nverts, const double* verts, int64_t
     }
     opem::PortFem2D M;
     std::string err;
-    int rc = opem::port_fem2d_solve(verts, nface, face_verts, eps.data(), mu.data(), desc, nsub, freq, mu[0].real(), M,
+    int rc = opem::port_fem2d_solve(verts, nface, face_verts, eps.data(), mu.data(), desc, nsub, order, freq, mu[0].real(), M,
                                     err);
     if (rc != OPEM_OK) return rc;
     const cd m4[4] = {M.gamma, M.Z, M.V, M.Pz};

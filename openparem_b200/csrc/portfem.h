@@ -9,9 +9,18 @@ namespace opem {
 
 // The fundamental mode of one port at one frequency, found on a conforming
 // split of the port's faces (each face into nsub x nsub similar triangles).
+// Second-order edge / quadratic nodal solve of the port pencil (port2d.cpp):
+// per triangle 8 e_t and 6 e_z coefficients of the hierarchical basis and the
+// sorted vertex ids.
+int port_mode_2d_p2(int64_t nnodes, const double* xy, int64_t ntri, const int64_t* tris,
+                    const std::complex<double>* eps_r, const std::complex<double>* mu_r, double freq,
+                    std::complex<double>& beta, std::vector<std::complex<double>>& ct,
+                    std::vector<std::complex<double>>& cz, std::vector<int64_t>& st);
+
 struct PortFem2D {
     using cd = std::complex<double>;
     int nsub = 0;
+    int order = 1;                    // 2D element order (1 or 2)
     int64_t nface = 0;
     double o[3], u[3], v[3], n[3];    // unit frame of the port plane; n = outward normal
     double freq = 0, mu_port = 1;
@@ -19,7 +28,8 @@ struct PortFem2D {
     std::vector<double> xy;           // 2D nodes
     std::vector<int64_t> st;          // 3 sorted node ids per sub-triangle
     std::vector<double> P0, Jinv, g;  // per sub-triangle: first node (2), J^-1 (4), grad lambda (3x2)
-    std::vector<cd> ce, gz, mu;       // edge coefficients (3), grad e_z (2), mu_r (1)
+    std::vector<cd> ce, gz, mu;       // order 1: edge coefficients (3), grad e_z (2); mu_r (1)
+    std::vector<cd> ct, cz;           // order 2: e_t (8) and e_z (6) coefficients
     std::vector<int64_t> sub;         // per face: (i, j, upper) -> sub-triangle
 
     // E_t and H_t / y (y = gamma / (j w mu0 mu_port)) at the 3D point X of
@@ -35,9 +45,10 @@ struct PortFem2D {
 // port face in the face's local order; eps_face / mu_face: complex relative
 // permittivity / permeability per face (from the owning tetrahedron);
 // desc: the 22-double port descriptor (origin, u, v, outward normal, a, b, m, n,
-// voltage path); mu_port: mu_r used to scale H_t / y.  Returns an OPEM_* code.
+// voltage path); order: 2D element order (1 or 2); mu_port: mu_r used to scale
+// H_t / y.  Returns an OPEM_* code.
 int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* face_verts,
                      const std::complex<double>* eps_face, const std::complex<double>* mu_face, const double* desc,
-                     int nsub, double freq, double mu_port, PortFem2D& out, std::string& err);
+                     int nsub, int order, double freq, double mu_port, PortFem2D& out, std::string& err);
 
 }  // namespace opem

@@ -419,9 +419,9 @@ void build(const std::string& proj_path, int order_override, Project& P) {
         for (int i = 0; i < 3; ++i) { d[16 + i] = vs[i]; d[19 + i] = ve[i]; }
         P.port_desc.push_back(d);
         // a port whose faces see more than one material is driven by its own 2D
-        // mode (as the reference drives every port); the split keeps the 2D mesh
-        // near 4096 triangles
-        const int nsub = (int)std::lround(std::sqrt(4096.0 / (double)std::max<int64_t>(1, port_nface[p])));
+        // mode (as the reference drives every port), with second-order 2D elements
+        // on a split that keeps the 2D mesh near 1024 triangles
+        const int nsub = (int)std::lround(std::sqrt(1024.0 / (double)std::max<int64_t>(1, port_nface[p])));
         P.port_nsub.push_back(port_mixed[p] ? std::min(16, std::max(1, nsub)) : 0);
     }
     // boundary conditions: attribute 1 PEC, ports 2.., the Boundary blocks after them
@@ -545,7 +545,7 @@ int opem_project_load(opem_context ctx, const char* proj_path, int order, opem_p
         rc = opem_problem_set_boundary(prob, (int)a + 1, type, np ? P.bdr[a].second.data() : nullptr, np);
     }
     for (size_t p = 0; rc == OPEM_OK && p < P.port_desc.size(); ++p)
-        rc = P.port_nsub[p] > 0 ? opem_problem_set_port_fem2d(prob, (int)p, P.port_desc[p].data(), P.port_nsub[p])
+        rc = P.port_nsub[p] > 0 ? opem_problem_set_port_fem2d(prob, (int)p, P.port_desc[p].data(), P.port_nsub[p], 2)
                                 : opem_problem_set_port_te(prob, (int)p, P.port_desc[p].data());
     if (rc != OPEM_OK) {
         opem_problem_destroy(prob);

@@ -93,7 +93,7 @@ def project_info(proj_path, order=0):
     return info, fr[:min(info["frequencies"], len(fr))]
 
 
-def port_mode_faces(verts, face_verts, eps_face, mode, nsub, freq, pt_face=None, pt_s=None, mu_face=None):
+def port_mode_faces(verts, face_verts, eps_face, mode, nsub, freq, pt_face=None, pt_s=None, mu_face=None, order=1):
     """The 2D mode of a port given by its faces (opem_port_mode_faces, host only):
     -> (metrics {gamma, Z, V, Pz}, E_t (npts,3), H_t / y (npts,3)) at the points
     (pt_face, pt_s = (s1, s2) face parameters)."""
@@ -109,7 +109,8 @@ def port_mode_faces(verts, face_verts, eps_face, mode, nsub, freq, pt_face=None,
     E = np.zeros((max(npts, 1), 6))
     Hy = np.zeros((max(npts, 1), 6))
     rc = _lib.lib().opem_port_mode_faces(len(verts), _dp(verts), len(fv), fv.ctypes.data_as(_lib.I64P), _dp(eps),
-                                         None if mu is None else _dp(mu), _dp(d), int(nsub), float(freq), _dp(m),
+                                         None if mu is None else _dp(mu), _dp(d), int(nsub), int(order), float(freq),
+                                         _dp(m),
                                          npts, pf.ctypes.data_as(_lib.I64P), _dp(ps), _dp(E), _dp(Hy))
     if rc != _lib.OK:
         raise OpemError(rc, "opem_port_mode_faces")
@@ -161,8 +162,8 @@ def project_problem(proj_path, order=0):
         mode = {"kind": "TE", "m": int(d[14]), "n": int(d[15]), "a": d[12], "b": d[13],
                 "origin": d[0:3].tolist(), "u": d[3:6].tolist(), "v": d[6:9].tolist(),
                 "normal": d[9:12].tolist(), "vpath": (d[16:19].tolist(), d[19:22].tolist())}
-        if ns[k] > 0:   # the port's own 2D mode
-            mode.update(kind="FEM2D", nsub=int(ns[k]))
+        if ns[k] > 0:   # the port's own 2D mode (the reader uses second-order 2D elements)
+            mode.update(kind="FEM2D", nsub=int(ns[k]), order2d=2)
         ports.append({"mode": mode})
     prob = {"verts": verts, "tets": tets, "tet_region": reg.astype(np.int64), "bdr_tris": tris,
             "bdr_attr": attr.astype(np.int64), "order": p, "eps_r": mat[:, 0], "tand": mat[:, 1],
@@ -209,7 +210,8 @@ class Fem3D:
         for k, port in enumerate(prob["ports"]):
             d = te_descriptor(port["mode"])
             if port["mode"].get("kind", "TE") == "FEM2D":
-                _chk(self.ctx.h, L.opem_problem_set_port_fem2d(self.h, k, _dp(d), int(port["mode"]["nsub"])),
+                _chk(self.ctx.h, L.opem_problem_set_port_fem2d(self.h, k, _dp(d), int(port["mode"]["nsub"]),
+                                                               int(port["mode"].get("order2d", 1))),
                      "set_port_fem2d")
             else:
                 _chk(self.ctx.h, L.opem_problem_set_port_te(self.h, k, _dp(d)), "set_port_te")
