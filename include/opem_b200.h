@@ -247,6 +247,19 @@ int  opem_s_mixed_mode(int nports, const double* S, int npairs, const int* pairs
  * opem_write_touchstone plus the 2.0 keywords and, with pairs, [Mixed-Mode Order]. */
 int  opem_write_touchstone2(const char* path, int nfreq, const double* freqs, int nports, const double* S,
                             double zref, const char* format, const char* unit, int npairs, const int* pairs);
+/* Results CSV in the reference's _results.csv layout (ResultDatabase::saveCSV,
+ * results.cpp:940-1052): header keys, one "#S-port" line per port (zref <= 0:
+ * "not renormalized"), S(row;col) values with the driven port (column) outer.  */
+int  opem_write_results_csv(const char* path, int nfreq, const double* freqs, int nports, const double* S,
+                            double zref, const char* format, const char* unit);
+/* The reference's regression comparator (process3D, process3D.cpp:105-560): the
+ * S-parameter test cases of test_cases_path (magS(dB) / argS(deg) with equal,
+ * lessthan, greaterthan) evaluated against a results CSV, written to out_path in
+ * the _test_results.csv layout and order; *ncases and *npassed (may be NULL).
+ * OPEM_ERR_ARG for unreadable or malformed files, OPEM_ERR_UNSUPPORTED for
+ * antenna-metric cases.                                                          */
+int  opem_evaluate_test_cases(const char* test_cases_path, const char* results_csv_path, const char* out_path,
+                              int* ncases, int* npassed);
 
 /* ---- serving loop (no counterpart in the reference: it solves one project per
  * process, OpenParEM3D.cpp:494-555) -------------------------------------------

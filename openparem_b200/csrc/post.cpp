@@ -1,5 +1,6 @@
 // S-parameter post-processing on the host: renormalisation to a reference
-// impedance, mixed-mode conversion, and Touchstone 1.1 / 2.0 output (the reference's Result::S2Z / Z2S /
+// impedance, mixed-mode conversion, Touchstone 1.1 / 2.0 and results-CSV output,
+// and the regression comparator (test cases against a results CSV) (the reference's Result::S2Z / Z2S /
 // renormalize, src/OpenParEM3D/results.cpp:455-580, and
 // ResultDatabase::saveTouchstone, results.cpp:1055-1208).  The file layout
 // follows the Touchstone 1.1 conventions the reference writes: "# <unit> S
@@ -10,6 +11,8 @@
 #include <complex>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -266,6 +269,248 @@ int opem_write_touchstone(const char* path, int nfreq, const double* freqs, int 
     for (int q = 0; q < nfreq; ++q) write_point(f, n, S + (size_t)2 * n * n * q, freqs[q] * scale, fmt);
     const bool ok = std::ferror(f) == 0;
     std::fclose(f);
+    return ok ? OPEM_OK : OPEM_ERR_ARG;
+}
+
+// Results CSV (ResultDatabase::saveCSV, results.cpp:940-1052, and
+// Result::saveCSV, :205-230): "#Touchstone format,F", "#frequency unit,U",
+// "#number of frequencies,n", "#number of ports,N", one "#S-port i,neti,zref"
+// line per port ("not renormalized" for zref <= 0), the column header, then one
+// line per frequency.  Values are written in the header's order, S(row;col)
+// with the column (driven port) outer and the row (receiving port) inner, which
+// is the order the reference's reader and comparator take them in.
+int opem_write_results_csv(const char* path, int nfreq, const double* freqs, int nports, const double* S, double zref,
+                           const char* format, const char* unit) {
+    if (!path || nfreq < 1 || !freqs || nports < 1 || !S || !format || !unit) return OPEM_ERR_ARG;
+    const std::string fmt(format), un(unit);
+    if (fmt != "RI" && fmt != "MA" && fmt != "DB") return OPEM_ERR_ARG;
+    const double scale = unit_scale(un);
+    if (scale == 0) return OPEM_ERR_ARG;
+    FILE* f = std::fopen(path, "w");
+    if (!f) return OPEM_ERR_ARG;
+    const int n = nports;
+    std::fprintf(f, "#opem-b200\n#Touchstone format,%s\n#frequency unit,%s\n#number of frequencies,%d\n"
+                    "#number of ports,%d\n", fmt.c_str(), un.c_str(), nfreq, n);
+    for (int i = 0; i < n; ++i) {
+        if (zref > 0) std::fprintf(f, "#S-port %d,net%d,%.15g\n", i + 1, i + 1, zref);
+        else std::fprintf(f, "#S-port %d,net%d,not renormalized\n", i + 1, i + 1);
+    }
+    std::fprintf(f, "#Frequency(%s)", un.c_str());
+    const char* h1 = fmt == "RI" ? "Re" : (fmt == "MA" ? "mag" : "dB");
+    const char* h2 = fmt == "RI" ? "Im" : "deg";
+    for (int col = 0; col < n; ++col)
+        for (int row = 0; row < n; ++row)
+            std::fprintf(f, ",%s(S(%d;%d)),%s(S(%d;%d))", h1, row + 1, col + 1, h2, row + 1, col + 1);
+    std::fprintf(f, "\n");
+    for (int q = 0; q < nfreq; ++q) {
+        const double* Sq = S + (size_t)2 * n * n * q;
+        std::fprintf(f, "%.15g", freqs[q] * scale);
+        for (int col = 0; col < n; ++col)
+            for (int row = 0; row < n; ++row) {
+                const cd v(Sq[2 * (row * n + col)], Sq[2 * (row * n + col) + 1]);
+                double a, b;
+                if (fmt == "RI") { a = v.real(); b = v.imag(); }
+                else if (fmt == "MA") { a = std::abs(v); b = std::arg(v) * 180.0 / M_PI; }
+                else { a = 20.0 * std::log10(std::abs(v)); b = std::arg(v) * 180.0 / M_PI; }
+                std::fprintf(f, ",%.15g,%.15g", a, b);
+            }
+        std::fprintf(f, "\n");
+    }
+    const bool ok = std::ferror(f) == 0;
+    std::fclose(f);
+    return ok ? OPEM_OK : OPEM_ERR_ARG;
+}
+
+}  // extern "C"
+
+namespace {
+
+// the reference's frequency match (double_compare, OpenParEMCommon/misc.cpp:76-84)
+bool same_value(double a, double b, double tol) {
+    if (a == b) return true;
+    if (a == 0 && std::fabs(b) < tol) return true;
+    if (b == 0 && std::fabs(a) < tol) return true;
+    if (std::fabs(a) < tol && std::fabs(b) < tol) return true;
+    return std::fabs((a - b) / a) < tol;
+}
+
+bool parse_double(const std::string& t, double& v) {
+    try {
+        size_t k = 0;
+        v = std::stod(t, &k);
+        return k == t.size() || t.find_first_not_of(" \t\r", k) == std::string::npos;
+    } catch (...) {
+        return false;
+    }
+}
+
+bool parse_int(const std::string& t, int& v) {
+    double d;
+    if (!parse_double(t, d) || d != std::floor(d)) return false;
+    v = (int)d;
+    return true;
+}
+
+struct TestCase {
+    std::string name, var, fn;
+    double freq = 0, value = 0, tol = 0, found = 0, error = 0;
+    int out = 0, in = 0;
+    bool passed = false;
+};
+
+}  // namespace
+
+extern "C" {
+
+// Regression comparator (process3D, src/OpenParEM3D/process3D.cpp:105-462,
+// 481-560): test cases "name,frequency,magS(dB)|argS(deg),portOut,portIn,
+// equal|lessthan|greaterthan,expected|threshold[,tolerance]" (after a
+// "# ResultDatabase::save_as_test" line; '#' lines and "//" tails are comments)
+// evaluated against a results CSV: the first result whose frequency matches to
+// 1e-12 relative, magS(dB) / argS(deg) of S(portOut;portIn) (values in the
+// CSV's format, converted to dB and degrees; the reference's files are written
+// in DB), "equal" as relative error against the tolerance (argS over +-360
+// deg), "lessthan" / "greaterthan" against the threshold (argS wrapped into
+// (-180, 180)).  The cases are ordered by |error| (equal) or |found value|
+// (the others), largest first, by the reference's own exchange procedure, and
+// written to out_path in its _test_results.csv layout.  Antenna-metric cases
+// (PatternDatabase) are not supported (OPEM_ERR_UNSUPPORTED).
+int opem_evaluate_test_cases(const char* test_cases_path, const char* results_csv_path, const char* out_path,
+                             int* ncases, int* npassed) {
+    if (!test_cases_path || !results_csv_path || !out_path) return OPEM_ERR_ARG;
+    std::ifstream tc(test_cases_path);
+    if (!tc) return OPEM_ERR_ARG;
+    std::vector<TestCase> cases;
+    std::string line;
+    while (std::getline(tc, line)) {
+        if (!line.empty() && line.back() == '\r') line.pop_back();
+        if (line.empty()) continue;
+        if (line == "# PatternDatabase::save_as_test") return OPEM_ERR_UNSUPPORTED;
+        const size_t first = line.find_first_not_of(" \t");
+        if (first == std::string::npos || line[first] == '#') continue;
+        line = line.substr(0, line.find("//"));
+        std::vector<std::string> v;
+        std::stringstream ss(line);
+        std::string e;
+        while (std::getline(ss, e, ',')) v.push_back(e);
+        TestCase c;
+        if (v.size() < 7) return OPEM_ERR_ARG;
+        c.name = v[0];
+        c.var = v[2];
+        c.fn = v[5];
+        if (!parse_double(v[1], c.freq) || !parse_int(v[3], c.out) || !parse_int(v[4], c.in)) return OPEM_ERR_ARG;
+        if (c.var != "magS(dB)" && c.var != "argS(deg)") return OPEM_ERR_ARG;
+        if (c.fn != "equal" && c.fn != "lessthan" && c.fn != "greaterthan") return OPEM_ERR_ARG;
+        if (v.size() != (c.fn == "equal" ? 8u : 7u)) return OPEM_ERR_ARG;
+        if (!parse_double(v[6], c.value)) return OPEM_ERR_ARG;
+        if (c.fn == "equal" && !parse_double(v[7], c.tol)) return OPEM_ERR_ARG;
+        cases.push_back(c);
+    }
+    // results CSV
+    std::ifstream rc(results_csv_path);
+    if (!rc) return OPEM_ERR_ARG;
+    std::string fmt = "DB", unit = "Hz";
+    int N = 0;
+    std::vector<std::pair<double, std::vector<cd>>> results;   // frequency, (value pairs in file order)
+    while (std::getline(rc, line)) {
+        if (!line.empty() && line.back() == '\r') line.pop_back();
+        if (line.empty()) continue;
+        std::vector<std::string> v;
+        std::stringstream ss(line);
+        std::string e;
+        while (std::getline(ss, e, ',')) v.push_back(e);
+        if (line[0] == '#') {
+            if (v.size() >= 2 && v[0] == "#Touchstone format") fmt = v[1];
+            if (v.size() >= 2 && v[0] == "#frequency unit") unit = v[1];
+            if (v.size() >= 2 && v[0] == "#number of ports" && !parse_int(v[1], N)) return OPEM_ERR_ARG;
+            continue;
+        }
+        const double sc = unit_scale(unit);
+        if (sc == 0 || N < 1 || v.size() != (size_t)(1 + 2 * N * N)) return OPEM_ERR_ARG;
+        double f;
+        if (!parse_double(v[0], f)) return OPEM_ERR_ARG;
+        std::vector<cd> vals(N * N);
+        for (int k = 0; k < N * N; ++k) {
+            double a, b;
+            if (!parse_double(v[1 + 2 * k], a) || !parse_double(v[2 + 2 * k], b)) return OPEM_ERR_ARG;
+            vals[k] = cd(a, b);
+        }
+        results.push_back({f / sc, vals});
+    }
+    // evaluation
+    int np = 0;
+    for (TestCase& c : cases) {
+        c.passed = false;
+        c.found = 0;
+        const std::vector<cd>* R = nullptr;
+        for (auto& r : results)
+            if (same_value(r.first, c.freq, 1e-12)) { R = &r.second; break; }
+        if (R && c.out >= 1 && c.out <= N && c.in >= 1 && c.in <= N) {
+            // pair k = (portIn - 1) N + (portOut - 1): the driven port outer, as the header orders S(row;col)
+            const cd pr = (*R)[(c.in - 1) * N + (c.out - 1)];
+            double db = pr.real(), deg = pr.imag();
+            if (fmt == "RI") { db = 20 * std::log10(std::abs(pr)); deg = std::arg(pr) * 180 / M_PI; }
+            if (fmt == "MA") { db = 20 * std::log10(pr.real()); }
+            if (c.var == "magS(dB)") {
+                c.found = db;
+                if (c.fn == "equal") {
+                    c.error = c.value == 0 ? std::fabs(c.found) : std::fabs((c.found - c.value) / c.value);
+                    c.passed = c.error <= c.tol;
+                } else if (c.fn == "lessthan") c.passed = c.found <= c.value;
+                else c.passed = c.found >= c.value;
+            } else {
+                c.found = deg;
+                if (c.fn == "equal") {
+                    if (c.value == 0) c.error = std::fabs(c.found);
+                    else {
+                        const double e1 = std::fabs((c.found - c.value) / c.value);
+                        const double e2 = std::fabs((c.found + 360 - c.value) / c.value);
+                        const double e3 = std::fabs((c.found - 360 - c.value) / c.value);
+                        c.error = std::min(std::min(e1, e2), e3);
+                    }
+                    c.passed = c.error <= c.tol;
+                } else {
+                    while (c.found >= 180) c.found -= 360;
+                    while (c.found <= -180) c.found += 360;
+                    c.passed = c.fn == "lessthan" ? c.found <= c.value : c.found >= c.value;
+                }
+            }
+        }
+        if (c.passed) ++np;
+    }
+    // the reference's ordering (TestCaseDatabase::sort, process3D.cpp:390-422)
+    const size_t n = cases.size();
+    auto key = [&](size_t k) { return std::fabs(cases[k].fn == "equal" ? cases[k].error : cases[k].found); };
+    std::vector<size_t> idx(n);
+    for (size_t i = 0; i < n; ++i) idx[i] = i;
+    for (size_t i = 0; i + 1 < n; ++i) {
+        bool found = true;
+        while (found) {
+            found = false;
+            for (size_t j = i + 1; j < n; ++j)
+                if (key(idx[i]) < key(idx[j])) {
+                    found = true;
+                    std::swap(idx[i], idx[j]);
+                }
+        }
+    }
+    FILE* f = std::fopen(out_path, "w");
+    if (!f) return OPEM_ERR_ARG;
+    std::fprintf(f, "# name,status,frequency,portOut,portIn,testVariable,testFunction,[equal:expectedValue,]"
+                    "foundValue,[equal:error,tolerance | lessthan:threshold | greaterthan:threshold\n");
+    for (size_t k : idx) {
+        const TestCase& c = cases[k];
+        std::fprintf(f, "%s,%s,%.15g,%d,%d,%s,%s,", c.name.c_str(), c.passed ? "pass" : "FAIL", c.freq, c.out, c.in,
+                     c.var.c_str(), c.fn.c_str());
+        if (c.fn == "equal") std::fprintf(f, "%.15g,", c.value);
+        std::fprintf(f, "%.15g,", c.found);
+        if (c.fn == "equal") std::fprintf(f, "%.15g,%.15g,\n", c.error, c.tol);
+        else std::fprintf(f, "%.15g,\n", c.value);
+    }
+    const bool ok = std::ferror(f) == 0;
+    std::fclose(f);
+    if (ncases) *ncases = (int)n;
+    if (npassed) *npassed = np;
     return ok ? OPEM_OK : OPEM_ERR_ARG;
 }
 

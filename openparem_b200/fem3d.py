@@ -456,3 +456,25 @@ def write_touchstone2(path, freqs, S, zref=50.0, fmt="RI", unit="GHz", pairs=())
                                            len(pr), pr.ctypes.data_as(C.POINTER(C.c_int)))
     if rc != _lib.OK:
         raise OpemError(rc, "opem_write_touchstone2")
+
+
+def write_results_csv(path, freqs, S, zref=50.0, fmt="DB", unit="GHz"):
+    """The reference's _results.csv layout (opem_write_results_csv); zref <= 0 marks
+    S as not renormalised."""
+    freqs = np.ascontiguousarray(freqs, dtype=np.float64)
+    S = np.ascontiguousarray(S, dtype=np.complex128)
+    rc = _lib.lib().opem_write_results_csv(str(path).encode(), len(freqs), _dp(freqs), S.shape[1],
+                                           _dp(S.view(np.float64).ravel()), float(zref), fmt.encode(), unit.encode())
+    if rc != _lib.OK:
+        raise OpemError(rc, "opem_write_results_csv")
+
+
+def evaluate_test_cases(test_cases, results_csv, out_path):
+    """The reference's regression comparator (opem_evaluate_test_cases) ->
+    (number of cases, number passed); the evaluation is written to out_path."""
+    nc, npass = C.c_int(), C.c_int()
+    rc = _lib.lib().opem_evaluate_test_cases(str(test_cases).encode(), str(results_csv).encode(),
+                                             str(out_path).encode(), C.byref(nc), C.byref(npass))
+    if rc != _lib.OK:
+        raise OpemError(rc, "opem_evaluate_test_cases")
+    return nc.value, npass.value

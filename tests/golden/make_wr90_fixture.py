@@ -20,6 +20,12 @@ and, for the project-reader pins, from
   tests/golden/wr90_projects.json       their ports files (paths, boundaries, ports)
                                         as data, mesh order, frequency points and
                                         the database entries of their materials
+  tests/golden/wr90_regression.json     for the comparator: the test cases of the
+                                        straight, straight-lossy, straight-loaded,
+                                        shorted and opened projects (*_test_cases.csv
+                                        rows) and the reference's evaluation of them
+                                        (the first block of each in
+                                        regression_results.csv.current, in order)
 
 Run once in a container that has the reference tree; the outputs are
 committed so the tests never need the reference at run time.
@@ -198,6 +204,40 @@ def read_material(paths, name):
     return out
 
 
+def read_test_cases(path):
+    """Rows (field lists) of a *_test_cases.csv (comments dropped)."""
+    rows = []
+    with open(path) as f:
+        for ln in f:
+            ln = ln.strip()
+            if not ln or ln.startswith("#"):
+                continue
+            rows.append(ln.split("//")[0].split(","))
+    return rows
+
+
+def read_first_block(path, project):
+    """The rows (field lists, trailing empty field dropped) of the first block of
+    a project in regression_results.csv.current."""
+    rows, inside = [], False
+    with open(path) as f:
+        for ln in f:
+            ln = ln.rstrip("\n")
+            if ln.startswith("#./"):
+                if inside:
+                    break
+                inside = ln[1:].split()[0] == project
+                continue
+            if inside and ln and not ln.startswith("#"):
+                t = ln.split(",")
+                rows.append(t[:-1] if t[-1] == "" else t)
+    return rows
+
+
+REGRESSION = {"straight": "straight", "straight-lossy": "straight", "straight-loaded": "straight-loaded",
+              "shorted": "shorted", "opened": "opened"}
+
+
 PROJECTS = {"straight-flipped": "straight-flipped", "straight-rotated-xyz": "straight-rotated",
             "shorted": "shorted", "opened": "opened", "straight-loaded": "straight-loaded"}
 
@@ -229,6 +269,13 @@ def main(ref):
                        "ports_file": read_ports_file(os.path.join(pd, pj["port.definition.file"]))}
         keep[f"./WR90/{d}/{stem}.proj"] = res[f"./WR90/{d}/{stem}.proj"]
     np.savez_compressed(os.path.join(HERE, "wr90_projects.npz"), **arrays)
+    reg = {}
+    rpath = os.path.join(ref, "regression", "OpenParEM3D", "regression_results.csv.current")
+    for d, stem in REGRESSION.items():
+        reg[d] = {"test_cases": read_test_cases(os.path.join(wr, d, stem + "_test_cases.csv")),
+                  "evaluation": read_first_block(rpath, f"./WR90/{d}/{stem}.proj")}
+    with open(os.path.join(HERE, "wr90_regression.json"), "w") as f:
+        json.dump({"source": "regression/OpenParEM3D", "projects": reg}, f, indent=0)
     with open(os.path.join(HERE, "wr90_projects.json"), "w") as f:
         json.dump({"source": "regression/OpenParEM3D/WR90", "projects": projects}, f, indent=1, sort_keys=True)
     meta = {
