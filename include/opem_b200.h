@@ -260,6 +260,23 @@ int  opem_write_results_csv(const char* path, int nfreq, const double* freqs, in
  * antenna-metric cases.                                                          */
 int  opem_evaluate_test_cases(const char* test_cases_path, const char* results_csv_path, const char* out_path,
                               int* ncases, int* npassed);
+/* Largest column 2-norm of S_cur^-1 (S_prev - S_cur): the reference's change of S
+ * between adaptive passes (ResultDatabase::calculate_maxRelativeError,
+ * results.cpp:714-768), compared with refinement.relative.tolerance.            */
+int  opem_s_relative_change(int nports, const double* S_prev, const double* S_cur, double* out);
+
+/* ---- mesh refinement (host only) ---------------------------------------------
+ * Conforming refinement of the marked tetrahedra (the reference refines what its
+ * error indicator marks with MFEM GeneralRefinement, fem3D::refineMesh,
+ * fem3D.cpp:1426-1447): each marked tetrahedron is bisected at its longest edge
+ * and the mesh closed by longest-edge bisection; regions and boundary attributes
+ * carry over, boundary triangles are split to match.  counts = {vertices, tets,
+ * boundary triangles} of the refined mesh; the output arrays may be NULL (size
+ * query).  OPEM_ERR_MESH if a boundary triangle is not a face of the mesh.      */
+int  opem_refine_mesh(int64_t nverts, const double* verts, int64_t ntets, const int64_t* tets,
+                      const int32_t* region, int64_t nbdr, const int64_t* bdr_tris, const int32_t* bdr_attr,
+                      int64_t nmarked, const int64_t* marked, int64_t* counts, double* verts_out,
+                      int64_t* tets_out, int32_t* region_out, int64_t* bdr_out, int32_t* attr_out);
 
 /* ---- serving loop (no counterpart in the reference: it solves one project per
  * process, OpenParEM3D.cpp:494-555) -------------------------------------------

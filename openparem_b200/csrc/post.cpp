@@ -7,6 +7,7 @@
 // <RI|MA|DB> R <Zref>", 1- and 2-port data with S11 S21 S12 S22 (column by
 // column) on one line per frequency, more ports row by row with at most four
 // pairs per line and a "!row i" comment, 15 significant digits.
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -270,6 +271,29 @@ int opem_write_touchstone(const char* path, int nfreq, const double* freqs, int 
     const bool ok = std::ferror(f) == 0;
     std::fclose(f);
     return ok ? OPEM_OK : OPEM_ERR_ARG;
+}
+
+// Change of S between two adaptive passes (ResultDatabase::
+// calculate_maxRelativeError, results.cpp:714-768): the largest column 2-norm of
+// S_cur^-1 (S_prev - S_cur).
+int opem_s_relative_change(int nports, const double* S_prev, const double* S_cur, double* out) {
+    if (nports < 1 || !S_prev || !S_cur || !out) return OPEM_ERR_ARG;
+    const int n = nports;
+    std::vector<cd> inv((size_t)n * n), d((size_t)n * n);
+    for (int i = 0; i < n * n; ++i) {
+        inv[i] = cd(S_cur[2 * i], S_cur[2 * i + 1]);
+        d[i] = cd(S_prev[2 * i], S_prev[2 * i + 1]) - inv[i];
+    }
+    if (!invert(n, inv)) return OPEM_ERR_BREAKDOWN;
+    const std::vector<cd> e = matmul(n, inv, d);
+    double best = 0;
+    for (int c = 0; c < n; ++c) {
+        double s = 0;
+        for (int r = 0; r < n; ++r) s += std::norm(e[(size_t)r * n + c]);
+        best = std::max(best, std::sqrt(s));
+    }
+    *out = best;
+    return OPEM_OK;
 }
 
 // Results CSV (ResultDatabase::saveCSV, results.cpp:940-1052, and

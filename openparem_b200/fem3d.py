@@ -478,3 +478,84 @@ def evaluate_test_cases(test_cases, results_csv, out_path):
     if rc != _lib.OK:
         raise OpemError(rc, "opem_evaluate_test_cases")
     return nc.value, npass.value
+
+
+def s_relative_change(S_prev, S_cur):
+    """Largest column 2-norm of S_cur^-1 (S_prev - S_cur) (opem_s_relative_change)."""
+    a = np.ascontiguousarray(S_prev, dtype=np.complex128)
+    b = np.ascontiguousarray(S_cur, dtype=np.complex128)
+    out = C.c_double()
+    rc = _lib.lib().opem_s_relative_change(a.shape[0], _dp(a.view(np.float64).ravel()),
+                                           _dp(b.view(np.float64).ravel()), C.byref(out))
+    if rc != _lib.OK:
+        raise OpemError(rc, "opem_s_relative_change")
+    return out.value
+
+
+def refine_problem(prob, marked):
+    """A copy of a problem dict with the marked tetrahedra refined
+    (opem_refine_mesh: longest-edge bisection with conforming closure)."""
+    verts = np.ascontiguousarray(prob["verts"], dtype=np.float64)
+    tets = np.ascontiguousarray(prob["tets"], dtype=np.int64)
+    reg = np.ascontiguousarray(prob.get("tet_region", np.zeros(len(tets))), dtype=np.int32)
+    tris = np.ascontiguousarray(prob["bdr_tris"], dtype=np.int64)
+    attr = np.ascontiguousarray(prob["bdr_attr"], dtype=np.int32)
+    mk = np.ascontiguousarray(marked, dtype=np.int64)
+    L = _lib.lib()
+    cnt = np.zeros(3, dtype=np.int64)
+    args = (len(verts), _dp(verts), len(tets), tets.ctypes.data_as(_lib.I64P), reg.ctypes.data_as(_lib.I32P),
+            len(tris), tris.ctypes.data_as(_lib.I64P), attr.ctypes.data_as(_lib.I32P), len(mk),
+            mk.ctypes.data_as(_lib.I64P), cnt.ctypes.data_as(_lib.I64P))
+    rc = L.opem_refine_mesh(*args, None, None, None, None, None)
+    if rc != _lib.OK:
+        raise OpemError(rc, "opem_refine_mesh")
+    nv, nt, nb = (int(c) for c in cnt)
+    V = np.zeros((nv, 3)); T = np.zeros((nt, 4), dtype=np.int64); R = np.zeros(nt, dtype=np.int32)
+    B = np.zeros((nb, 3), dtype=np.int64); A = np.zeros(nb, dtype=np.int32)
+    rc = L.opem_refine_mesh(*args, _dp(V), T.ctypes.data_as(_lib.I64P), R.ctypes.data_as(_lib.I32P),
+                            B.ctypes.data_as(_lib.I64P), A.ctypes.data_as(_lib.I32P))
+    if rc != _lib.OK:
+        raise OpemError(rc, "opem_refine_mesh")
+    out = dict(prob)
+    out.update(verts=V, tets=T, tet_region=R.astype(np.int64), bdr_tris=B, bdr_attr=A.astype(np.int64))
+    return out
+
+
+def adaptive_solve(prob, step, fraction=0.005, variable="SandH", rel_tol=0.02, abs_tol=1e-6, iter_min=1,
+                   iter_max=10, passes=1):
+    """The reference's adaptive loop for one frequency point (OpenParEM3D.cpp:442-630,
+    is_converged project.c:344-364, isSequentialConverged results.cpp:828-843):
+    step(prob) -> (S, max mesh error, marked elements) solves and estimates; the
+    change of S between passes (s_relative_change) and/or the max mesh error are
+    tested against rel_tol / abs_tol ("S", "SorH", "SandH"), iterations below
+    iter_min never converge, the loop stops after `passes` converged passes in a
+    row or iter_max passes, and otherwise refines the marked elements
+    (refine_problem).  Returns (S, final problem, history of per-pass dicts)."""
+    history, S_prev, conv_run = [], None, 0
+    for it in range(iter_max):
+        S, max_err, marked = step(prob)
+        rel = s_relative_change(S_prev, S) if S_prev is not None else -1.0
+        ok_rel = 0 <= rel <= rel_tol
+        ok_abs = 0 <= max_err <= abs_tol
+        conv = {"S": ok_rel, "SorH": ok_rel or ok_abs, "SandH": ok_rel and ok_abs}[variable]
+        if it < iter_min - 1:
+            conv = False
+        conv_run = conv_run + 1 if conv else 0
+        history.append({"iteration": it + 1, "tets": len(prob["tets"]), "S": S, "relative_error": rel,
+                        "max_mesh_error": max_err, "converged": conv})
+        if conv_run >= passes or it == iter_max - 1:
+            return S, prob, history
+        prob = refine_problem(prob, marked)
+        S_prev = S
+    return S, prob, history
+
+
+def device_step(freq, fraction=0.005, opts=None, context=None):
+    """A step for adaptive_solve on the device: assemble, opem_solve_frequency,
+    opem_mesh_errors."""
+    def step(prob):
+        F = Fem3D(prob, context=context).assemble()
+        S, _, _ = F.solve(freq, opts)
+        _, marked, mx = F.mesh_errors(fraction)
+        return S, mx, marked
+    return step
