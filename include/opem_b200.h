@@ -175,6 +175,10 @@ int  opem_profile_batch_kernels(opem_problem prob, double freq, int nsys, int re
  * freqs (up to max_freqs) and its length to *nfreq.                            */
 int  opem_project_load(opem_context ctx, const char* proj_path, int order, opem_problem* out, int* nfreq,
                        double* freqs, int max_freqs);
+/* The last value of a key of a .proj file ("refinement.relative.tolerance",
+ * "mesh.3D.refinement.fraction", ...), "//" comment removed, into buf (len bytes
+ * with the terminator); OPEM_ERR_ARG if the file or the key is missing.         */
+int  opem_project_value(const char* proj_path, const char* key, char* buf, int len);
 /* The same reading without a device (host only): info[0]=vertices, [1]=tets,
  * [2]=regions, [3]=exterior faces, [4]=port faces, [5]=Boundary-block faces,
  * [6]=PEC faces, [7]=ports, [8]=frequency points, [9]=order; msg receives the

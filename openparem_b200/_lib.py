@@ -75,6 +75,7 @@ SIGNATURES = [
     ("opem_selftest_wait_timeout", C.c_int, [P, C.c_int]),
     ("opem_project_load", C.c_int, [P, C.c_char_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_int), DP, C.c_int]),
     ("opem_project_info", C.c_int, [C.c_char_p, C.c_int, I64P, C.c_int, DP, C.c_int, C.c_char_p, C.c_int]),
+    ("opem_project_value", C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int]),
     ("opem_project_read", C.c_int, [C.c_char_p, C.c_int, I64P, DP, I64P, I32P, DP, I64P, I32P, I32P, DP, DP, I32P,
                                      DP, C.c_char_p, C.c_int]),
     ("opem_port_mode_2d", C.c_int, [C.c_int64, DP, C.c_int64, I64P, DP, DP, C.c_double, DP, I64P, I64P, DP, DP]),

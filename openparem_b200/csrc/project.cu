@@ -448,6 +448,23 @@ void build(const std::string& proj_path, int order_override, Project& P) {
 
 extern "C" {
 
+int opem_project_value(const char* proj_path, const char* key, char* buf, int len) {
+    if (!proj_path || !key || !buf || len < 1) return OPEM_ERR_ARG;
+    buf[0] = 0;
+    Project P;
+    try {
+        parse_proj(proj_path, P);
+    } catch (const std::exception&) {
+        return OPEM_ERR_ARG;
+    }
+    auto it = P.kv.find(key);
+    if (it == P.kv.end() || it->second.empty()) return OPEM_ERR_ARG;
+    const std::string v = trim(it->second.back().substr(0, it->second.back().find("//")));
+    if ((int)v.size() >= len) return OPEM_ERR_ARG;
+    std::memcpy(buf, v.c_str(), v.size() + 1);
+    return OPEM_OK;
+}
+
 int opem_project_info(const char* proj_path, int order, int64_t* info, int ninfo, double* freqs, int max_freqs,
                       char* msg, int msg_len) {
     if (!proj_path || !info) return OPEM_ERR_ARG;

@@ -559,3 +559,25 @@ def device_step(freq, fraction=0.005, opts=None, context=None):
         _, marked, mx = F.mesh_errors(fraction)
         return S, mx, marked
     return step
+
+
+# the reference's defaults for the adaptive keys (project.c:555-567)
+REFINEMENT_DEFAULTS = {"mesh.3D.refinement.fraction": 0.005, "refinement.frequency": "highlow",
+                       "refinement.iteration.min": 1, "refinement.iteration.max": 10,
+                       "refinement.required.passes": 1, "refinement.relative.tolerance": 0.02,
+                       "refinement.absolute.tolerance": 1e-6, "refinement.variable": "SandH"}
+
+
+def project_refinement(proj_path):
+    """The adaptive settings of a project (opem_project_value), the reference's
+    defaults where a key is absent, as keyword arguments of adaptive_solve plus
+    "frequency" (none | high | low | highlow | all | plan)."""
+    buf = C.create_string_buffer(256)
+    v = {}
+    for k, d in REFINEMENT_DEFAULTS.items():
+        rc = _lib.lib().opem_project_value(str(proj_path).encode(), k.encode(), buf, 256)
+        v[k] = type(d)(buf.value.decode()) if rc == _lib.OK else d
+    return {"fraction": v["mesh.3D.refinement.fraction"], "variable": v["refinement.variable"],
+            "rel_tol": v["refinement.relative.tolerance"], "abs_tol": v["refinement.absolute.tolerance"],
+            "iter_min": v["refinement.iteration.min"], "iter_max": v["refinement.iteration.max"],
+            "passes": v["refinement.required.passes"], "frequency": v["refinement.frequency"]}

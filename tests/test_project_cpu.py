@@ -41,3 +41,16 @@ def test_reference_wr90_straight_project():
     assert info["tets"] == 282 and info["ports"] == 2 and info["order"] == 6
     assert info["port_faces"] > 0 and info["pec_faces"] > 0
     assert np.allclose(fr, [9e9, 9.999999999e9, 11e9])
+
+
+def test_project_refinement_settings(tmp_path):
+    from openparem_b200.fem3d import project_refinement
+    proj = write_guide_project(str(tmp_path))
+    r = project_refinement(proj)
+    assert r == {"fraction": 0.005, "variable": "SandH", "rel_tol": 0.02, "abs_tol": 1e-6, "iter_min": 1,
+                 "iter_max": 10, "passes": 1, "frequency": "highlow"}
+    with open(proj, "a") as f:
+        f.write("refinement.variable            S   // on S only\nrefinement.iteration.max       30\n"
+                "refinement.relative.tolerance  0.001\nmesh.3D.refinement.fraction    0.05\n")
+    r = project_refinement(proj)
+    assert (r["variable"], r["iter_max"], r["rel_tol"], r["fraction"]) == ("S", 30, 0.001, 0.05)
