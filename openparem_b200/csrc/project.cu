@@ -424,8 +424,22 @@ void build(const std::string& proj_path, int order_override, Project& P) {
         const int nsub = (int)std::lround(std::sqrt(1024.0 / (double)std::max<int64_t>(1, port_nface[p])));
         P.port_nsub.push_back(port_mixed[p] ? std::min(16, std::max(1, nsub)) : 0);
     }
-    // boundary conditions: attribute 1 PEC, ports 2.., the Boundary blocks after them
-    P.bdr.push_back({OPEM_BDR_PEC, {0, 0, 0}});
+    // boundary conditions: attribute 1 the faces no port or Boundary block claims
+    // (PEC, or the surface impedance of materials.default.boundary, as
+    // BoundaryDatabase::createDefaultBoundary does, port.cpp:7047-7078), ports
+    // 2.., the Boundary blocks after them
+    std::string dflt = kv1(P, "materials.default.boundary", "PEC");
+    dflt = trim(dflt.substr(0, dflt.find("//")));
+    if (dflt.empty()) dflt = "PEC";
+    if (dflt == "PEC") {
+        P.bdr.push_back({OPEM_BDR_PEC, {0, 0, 0}});
+    } else {
+        auto it = db.find(dflt);
+        if (it == db.end()) throw std::runtime_error("default boundary material " + dflt + " not found");
+        P.bdr.push_back({OPEM_BDR_IMPEDANCE, {it->second.sigma, it->second.Rz, it->second.mur}});
+        P.n_bdr_faces += P.n_pec_faces;
+        P.n_pec_faces = 0;
+    }
     for (int p = 0; p < np; ++p) P.bdr.push_back({OPEM_BDR_PORT, {(double)p, 0, 0}});
     for (auto& bd : bdrs) {
         if (bd.type == "surface_impedance") {

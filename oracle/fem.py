@@ -364,7 +364,9 @@ def solve_frequency(ops, freq, return_fields=False, reciprocal=True):
         b = -(A @ x0)
         b[pd] = x0[pd]
         A = eliminate(A, pd)
-        e = spla.splu(A.tocsc(), permc_spec="MMD_AT_PLUS_A").solve(b)
+        # threshold partial pivoting (0.1) keeps the minimum-degree order: without it the
+        # lossy ND6 systems fill in 3x and factor 9x slower, at the same residual
+        e = spla.splu(A.tocsc(), permc_spec="MMD_AT_PLUS_A", options=dict(DiagPivotThresh=0.1)).solve(b)
         qe = (ops.Q_mu @ e) / (w * MU0)
         h = 1j * (Plu.solve(qe.real) + 1j * Plu.solve(qe.imag))
         for k in range(N):

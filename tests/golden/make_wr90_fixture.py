@@ -176,7 +176,7 @@ def read_proj(path):
             elif t[0] == "frequency.plan.point":
                 out["freqs"].append(float(t[1]))
             elif t[0] in ("mesh.file", "port.definition.file", "materials.global.path", "materials.global.name",
-                          "materials.local.path", "materials.local.name"):
+                          "materials.local.path", "materials.local.name", "materials.default.boundary"):
                 out[t[0]] = t[1]
     return out
 
@@ -239,7 +239,8 @@ REGRESSION = {"straight": "straight", "straight-lossy": "straight", "straight-lo
 
 
 PROJECTS = {"straight-flipped": "straight-flipped", "straight-rotated-xyz": "straight-rotated",
-            "shorted": "shorted", "opened": "opened", "straight-loaded": "straight-loaded"}
+            "shorted": "shorted", "opened": "opened", "straight-loaded": "straight-loaded",
+            "straight-lossy": "straight", "straight-loaded-lossy": "straight-loaded"}
 
 
 def main(ref):
@@ -263,9 +264,12 @@ def main(ref):
         names = read_physical_names(os.path.join(pd, pj["mesh.file"]))
         mdb = [os.path.join(pd, pj.get("materials.local.path", "./"), pj.get("materials.local.name", "-")),
                os.path.join(pd, pj["materials.global.path"], pj["materials.global.name"])]
+        dflt = pj.get("materials.default.boundary", "PEC")
+        mats = sorted(set(names.values()) | ({dflt} if dflt != "PEC" else set()))
         projects[d] = {"stem": stem, "npz_key": key, "order": pj["order"], "freqs": pj["freqs"],
                        "physical_names": {str(k): v for k, v in names.items()},
-                       "materials": {v: read_material(mdb, v) for v in sorted(set(names.values()))},
+                       "default_boundary": dflt,
+                       "materials": {v: read_material(mdb, v) for v in mats},
                        "ports_file": read_ports_file(os.path.join(pd, pj["port.definition.file"]))}
         keep[f"./WR90/{d}/{stem}.proj"] = res[f"./WR90/{d}/{stem}.proj"]
     np.savez_compressed(os.path.join(HERE, "wr90_projects.npz"), **arrays)

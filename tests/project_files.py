@@ -76,7 +76,7 @@ def write_materials(path, mats):
                     f"   Source\n   EndSource\nEndMaterial\n\n")
 
 
-def write_project(d, stem, verts, tets, phys, names, ports_spec, materials, order, freqs):
+def write_project(d, stem, verts, tets, phys, names, ports_spec, materials, order, freqs, default_boundary="PEC"):
     """A complete project in directory d (stem.proj, stem.msh, stem_ports.txt,
     materials.txt); returns the .proj path."""
     write_gmsh22(os.path.join(d, stem + ".msh"), verts, tets, tag=phys, names=names)
@@ -89,6 +89,8 @@ def write_project(d, stem, verts, tets, phys, names, ports_spec, materials, orde
         f.write(f"port.definition.file           {stem}_ports.txt\n")
         f.write("materials.global.path          ./\nmaterials.global.name          materials.txt\n")
         f.write("materials.local.path           ./\nmaterials.local.name           //local_materials.txt\n")
+        if default_boundary != "PEC":
+            f.write(f"materials.default.boundary     {default_boundary}\n")
         for fr in freqs:
             f.write(f"frequency.plan.point           {fr!r}\n")
         f.write("solution.3D.tolerance          1e-14\n")
@@ -106,7 +108,8 @@ def reference_project(d, name):
     k = rec["npz_key"]
     names = {int(t): v for t, v in rec["physical_names"].items()}
     proj = write_project(d, rec["stem"], z[k + "_verts"], z[k + "_tets"], z[k + "_phys"], names,
-                         rec["ports_file"], rec["materials"], rec["order"], rec["freqs"])
+                         rec["ports_file"], rec["materials"], rec["order"], rec["freqs"],
+                         rec.get("default_boundary", "PEC"))
     return proj, rec
 
 

@@ -84,3 +84,21 @@ def test_one_port_nd6_pin(tmp_path, name):
     assert S.shape == (1, 1)
     assert abs(np.angle(S[0, 0], deg=True) - found(name, name, "argS(deg)", 1, 1)) < 1e-6
     assert abs(20 * np.log10(abs(S[0, 0]))) < 1e-9          # total reflection
+
+
+@pytest.mark.parametrize("name,stem,tol_deg", [("straight-lossy", "straight", 1e-5),
+                                               ("straight-loaded-lossy", "straight-loaded", 1e-5)])
+def test_default_boundary_lossy_nd6_pin(tmp_path, name, stem, tol_deg):
+    """materials.default.boundary copper: the walls no port or Boundary block
+    claims are copper surface impedance (sigma 5.813e7).  The slab-loaded one is
+    also driven by the ports' own second-order 2D modes.  The oracle on what the
+    reader produced reproduces the reference's found arg S21 to ~3e-6 deg and
+    |S21| (the copper loss, ~0.012 dB) to ~1e-8 dB."""
+    proj, rec = reference_project(str(tmp_path), name)
+    prob, fr = project_problem(proj)
+    assert prob["boundaries"][1] == {"type": "impedance", "sigma": 5.813e7, "Rz": 0.0, "mu_r": 1.0}
+    f = fr[0]
+    S = fem.solve_frequency(fem.Operators(prob), f)["S"]
+    assert abs(np.angle(S[1, 0], deg=True) - found(name, stem, "argS(deg)", 2, 1, f)) < tol_deg
+    assert abs(20 * np.log10(abs(S[1, 0])) - found(name, stem, "magS(dB)", 2, 1, f)) < 5e-8
+    assert abs(20 * np.log10(abs(S[0, 0])) - found(name, stem, "magS(dB)", 1, 1, f)) < 0.01
