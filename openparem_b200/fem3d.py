@@ -581,3 +581,10 @@ def project_refinement(proj_path):
             "rel_tol": v["refinement.relative.tolerance"], "abs_tol": v["refinement.absolute.tolerance"],
             "iter_min": v["refinement.iteration.min"], "iter_max": v["refinement.iteration.max"],
             "passes": v["refinement.required.passes"], "frequency": v["refinement.frequency"]}
+
+
+def project_value(proj_path, key, default=None):
+    """The last value of a .proj key as a string (opem_project_value), or default."""
+    buf = C.create_string_buffer(256)
+    rc = _lib.lib().opem_project_value(str(proj_path).encode(), key.encode(), buf, 256)
+    return buf.value.decode() if rc == _lib.OK else default

@@ -133,10 +133,10 @@ def read_ports_file(path):
                 continue
             if block is None or block["kind"] == "File":
                 continue
-            if ln == "Line":
-                port_line = {"Sport": None, "integration": []}
+            if ln in ("Line", "Mode"):
+                port_line = {"Sport": None, "integration": [], "block": ln}
                 continue
-            if ln == "EndLine":
+            if ln in ("EndLine", "EndMode"):
                 block["lines"].append(port_line)
                 port_line = None
                 continue
@@ -175,6 +175,10 @@ def read_proj(path):
                 out["order"] = int(t[1])
             elif t[0] == "frequency.plan.point":
                 out["freqs"].append(float(t[1]))
+            elif t[0] == "frequency.plan.linear":
+                out.setdefault("freq_linear", []).append(t[1])
+            elif t[0] == "reference.impedance":
+                out["reference.impedance"] = float(t[1])
             elif t[0] in ("mesh.file", "port.definition.file", "materials.global.path", "materials.global.name",
                           "materials.local.path", "materials.local.name", "materials.default.boundary"):
                 out[t[0]] = t[1]
@@ -238,6 +242,13 @@ REGRESSION = {"straight": "straight", "straight-lossy": "straight", "straight-lo
               "shorted": "shorted", "opened": "opened"}
 
 
+# further regression projects with rectangular ports, outside WR90/: fixture name -> (directory, stem)
+OTHER = {"partially-filled-lossless": ("partially_filled_rect_waveguide/partially_filled_rect_waveguide_lossless",
+                                       "part"),
+         "partially-filled-lossy": ("partially_filled_rect_waveguide/partially_filled_rect_waveguide_lossy", "part"),
+         "tee": ("WR90/tee", "tee"),
+         "t-junction": ("WR75/T-Junction", "T-Junction")}
+
 PROJECTS = {"straight-flipped": "straight-flipped", "straight-rotated-xyz": "straight-rotated",
             "shorted": "shorted", "opened": "opened", "straight-loaded": "straight-loaded",
             "straight-lossy": "straight", "straight-loaded-lossy": "straight-loaded"}
@@ -255,8 +266,9 @@ def main(ref):
                  "./WR90/straight-loaded/straight-loaded.proj"):
         keep[proj] = res[proj]
     arrays, projects = {}, {}
-    for d, stem in PROJECTS.items():
-        pd = os.path.join(wr, d)
+    todo = [(d, f"WR90/{d}", stem) for d, stem in PROJECTS.items()] + [(d, r, s) for d, (r, s) in OTHER.items()]
+    for d, rel, stem in todo:
+        pd = os.path.join(ref, "regression", "OpenParEM3D", rel)
         pj = read_proj(os.path.join(pd, stem + ".proj"))
         xyz, tets, phys = read_gmsh22(os.path.join(pd, pj["mesh.file"]))
         key = d.replace("-", "_")
@@ -265,13 +277,17 @@ def main(ref):
         mdb = [os.path.join(pd, pj.get("materials.local.path", "./"), pj.get("materials.local.name", "-")),
                os.path.join(pd, pj["materials.global.path"], pj["materials.global.name"])]
         dflt = pj.get("materials.default.boundary", "PEC")
-        mats = sorted(set(names.values()) | ({dflt} if dflt != "PEC" else set()))
+        ports_file = read_ports_file(os.path.join(pd, pj["port.definition.file"]))
+        bmats = {b["material"] for b in ports_file["boundaries"] if b.get("material")}
+        mats = sorted(set(names.values()) | ({dflt} if dflt != "PEC" else set()) | bmats)
         projects[d] = {"stem": stem, "npz_key": key, "order": pj["order"], "freqs": pj["freqs"],
                        "physical_names": {str(k): v for k, v in names.items()},
-                       "default_boundary": dflt,
+                       "default_boundary": dflt, "freq_linear": pj.get("freq_linear", []),
+                       "reference_impedance": pj.get("reference.impedance", 0.0),
+                       "results_key": f"./{rel}/{stem}.proj",
                        "materials": {v: read_material(mdb, v) for v in mats},
-                       "ports_file": read_ports_file(os.path.join(pd, pj["port.definition.file"]))}
-        keep[f"./WR90/{d}/{stem}.proj"] = res[f"./WR90/{d}/{stem}.proj"]
+                       "ports_file": ports_file}
+        keep[f"./{rel}/{stem}.proj"] = res[f"./{rel}/{stem}.proj"]
     np.savez_compressed(os.path.join(HERE, "wr90_projects.npz"), **arrays)
     reg = {}
     rpath = os.path.join(ref, "regression", "OpenParEM3D", "regression_results.csv.current")

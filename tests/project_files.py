@@ -54,12 +54,13 @@ def write_ports_file(path, spec):
             if p.get(k):
                 out.append(f"   {k}={p[k]}")
         for ln in p["lines"]:
-            out += ["   Line", f"      Sport={ln['Sport']}"]
+            blk = ln.get("block", "Line")
+            out += [f"   {blk}", f"      Sport={ln['Sport']}"]
             for ip in ln["integration"]:
                 out += ["      IntegrationPath", f"         type={ip['type']}"]
                 out += [f"         path={q}" for q in ip["paths"]]
                 out.append("      EndIntegrationPath")
-            out.append("   EndLine")
+            out.append(f"   End{blk}")
         out += ["EndPort", ""]
     with open(path, "w") as f:
         f.write("\n".join(out) + "\n")
@@ -76,7 +77,8 @@ def write_materials(path, mats):
                     f"   Source\n   EndSource\nEndMaterial\n\n")
 
 
-def write_project(d, stem, verts, tets, phys, names, ports_spec, materials, order, freqs, default_boundary="PEC"):
+def write_project(d, stem, verts, tets, phys, names, ports_spec, materials, order, freqs, default_boundary="PEC",
+                  freq_linear=(), reference_impedance=0.0):
     """A complete project in directory d (stem.proj, stem.msh, stem_ports.txt,
     materials.txt); returns the .proj path."""
     write_gmsh22(os.path.join(d, stem + ".msh"), verts, tets, tag=phys, names=names)
@@ -93,6 +95,9 @@ def write_project(d, stem, verts, tets, phys, names, ports_spec, materials, orde
             f.write(f"materials.default.boundary     {default_boundary}\n")
         for fr in freqs:
             f.write(f"frequency.plan.point           {fr!r}\n")
+        for lin in freq_linear:
+            f.write(f"frequency.plan.linear          {lin}\n")
+        f.write(f"reference.impedance            {reference_impedance!r}\n")
         f.write("solution.3D.tolerance          1e-14\n")
     return proj
 
@@ -109,7 +114,8 @@ def reference_project(d, name):
     names = {int(t): v for t, v in rec["physical_names"].items()}
     proj = write_project(d, rec["stem"], z[k + "_verts"], z[k + "_tets"], z[k + "_phys"], names,
                          rec["ports_file"], rec["materials"], rec["order"], rec["freqs"],
-                         rec.get("default_boundary", "PEC"))
+                         rec.get("default_boundary", "PEC"), rec.get("freq_linear", ()),
+                         rec.get("reference_impedance", 0.0))
     return proj, rec
 
 

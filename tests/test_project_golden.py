@@ -102,3 +102,39 @@ def test_default_boundary_lossy_nd6_pin(tmp_path, name, stem, tol_deg):
     assert abs(np.angle(S[1, 0], deg=True) - found(name, stem, "argS(deg)", 2, 1, f)) < tol_deg
     assert abs(20 * np.log10(abs(S[1, 0])) - found(name, stem, "magS(dB)", 2, 1, f)) < 5e-8
     assert abs(20 * np.log10(abs(S[0, 0])) - found(name, stem, "magS(dB)", 1, 1, f)) < 0.01
+
+
+@pytest.mark.parametrize("name,tol_deg,tol_db", [
+    ("partially-filled-lossless", 1e-4, 2e-6),   # half-height dielectric: the ports' own 2D modes
+    ("partially-filled-lossy", 1e-4, 2e-6),      # the same with copper Boundary blocks on the walls
+    ("tee", 1e-6, 5e-7),                         # 3 ports in three planes, S renormalised to 50 ohm
+    ("t-junction", 2e-5, 1e-6),                  # WR75 T-junction, ND4, 3 ports, modal impedance blocks
+])
+def test_more_reference_projects(tmp_path, name, tol_deg, tol_db):
+    """Further regression projects of the reference with rectangular ports,
+    read by the C++ reader and solved by the oracle at their own order; every
+    value the reference recorded at the first frequency is reproduced (S
+    renormalised with opem_s_renormalize where the project sets
+    reference.impedance).  Reflections below -60 dB (discretisation level) are
+    held to 1 dB."""
+    from openparem_b200.fem3d import project_value, renormalize
+    proj, rec = reference_project(str(tmp_path), name)
+    prob, fr = project_problem(proj)
+    with open(os.path.join(HERE, "golden", "wr90_expected.json")) as f:
+        rows = json.load(f)["cases"][rec["results_key"]]
+    f0 = min(v["frequency"] for v in rows.values())
+    r = fem.solve_frequency(fem.Operators(prob), f0)
+    z0 = float(project_value(proj, "reference.impedance", "0"))
+    S = renormalize(r["S"], r["Z"], z0) if z0 > 0 else r["S"]
+    n = 0
+    for v in rows.values():
+        if v["frequency"] != f0:
+            continue
+        s = S[v["portOut"] - 1, v["portIn"] - 1]
+        if v["variable"] == "argS(deg)":
+            assert abs(np.angle(s, deg=True) - v["found"]) < tol_deg, v
+        else:
+            tol = 1.0 if v["found"] < -60 else tol_db
+            assert abs(20 * np.log10(abs(s)) - v["found"]) < tol, v
+        n += 1
+    assert n >= 6
