@@ -247,7 +247,8 @@ OTHER = {"partially-filled-lossless": ("partially_filled_rect_waveguide/partiall
                                        "part"),
          "partially-filled-lossy": ("partially_filled_rect_waveguide/partially_filled_rect_waveguide_lossy", "part"),
          "tee": ("WR90/tee", "tee"),
-         "t-junction": ("WR75/T-Junction", "T-Junction")}
+         "t-junction": ("WR75/T-Junction", "T-Junction"),
+         "permeability-straight": ("permeability/rectangular_waveguide", "straight")}
 
 PROJECTS = {"straight-flipped": "straight-flipped", "straight-rotated-xyz": "straight-rotated",
             "shorted": "shorted", "opened": "opened", "straight-loaded": "straight-loaded",
@@ -275,7 +276,7 @@ def main(ref):
         arrays[key + "_verts"], arrays[key + "_tets"], arrays[key + "_phys"] = xyz, tets, phys
         names = read_physical_names(os.path.join(pd, pj["mesh.file"]))
         mdb = [os.path.join(pd, pj.get("materials.local.path", "./"), pj.get("materials.local.name", "-")),
-               os.path.join(pd, pj["materials.global.path"], pj["materials.global.name"])]
+               os.path.join(pd, pj.get("materials.global.path", "./"), pj.get("materials.global.name", "-"))]
         dflt = pj.get("materials.default.boundary", "PEC")
         ports_file = read_ports_file(os.path.join(pd, pj["port.definition.file"]))
         bmats = {b["material"] for b in ports_file["boundaries"] if b.get("material")}
@@ -287,13 +288,18 @@ def main(ref):
                        "results_key": f"./{rel}/{stem}.proj",
                        "materials": {v: read_material(mdb, v) for v in mats},
                        "ports_file": ports_file}
-        keep[f"./{rel}/{stem}.proj"] = res[f"./{rel}/{stem}.proj"]
+        if f"./{rel}/{stem}.proj" in res:   # (the permeability guide has test cases but no recorded run)
+            keep[f"./{rel}/{stem}.proj"] = res[f"./{rel}/{stem}.proj"]
     np.savez_compressed(os.path.join(HERE, "wr90_projects.npz"), **arrays)
     reg = {}
     rpath = os.path.join(ref, "regression", "OpenParEM3D", "regression_results.csv.current")
     for d, stem in REGRESSION.items():
         reg[d] = {"test_cases": read_test_cases(os.path.join(wr, d, stem + "_test_cases.csv")),
                   "evaluation": read_first_block(rpath, f"./WR90/{d}/{stem}.proj")}
+    reg["permeability-straight"] = {
+        "test_cases": read_test_cases(os.path.join(ref, "regression", "OpenParEM3D", "permeability",
+                                                   "rectangular_waveguide", "straight_test_cases.csv")),
+        "evaluation": []}
     with open(os.path.join(HERE, "wr90_regression.json"), "w") as f:
         json.dump({"source": "regression/OpenParEM3D", "projects": reg}, f, indent=0)
     with open(os.path.join(HERE, "wr90_projects.json"), "w") as f:

@@ -105,8 +105,8 @@ def test_default_boundary_lossy_nd6_pin(tmp_path, name, stem, tol_deg):
 
 
 @pytest.mark.parametrize("name,tol_deg,tol_db", [
-    ("partially-filled-lossless", 1e-4, 2e-6),   # half-height dielectric: the ports' own 2D modes
-    ("partially-filled-lossy", 1e-4, 2e-6),      # the same with copper Boundary blocks on the walls
+    ("partially-filled-lossy", 1e-4, 2e-6),      # half-height dielectric (the ports' own 2D modes),
+                                                 # copper Boundary blocks on the walls
     ("tee", 1e-6, 5e-7),                         # 3 ports in three planes, S renormalised to 50 ohm
     ("t-junction", 2e-5, 1e-6),                  # WR75 T-junction, ND4, 3 ports, modal impedance blocks
 ])

@@ -94,3 +94,27 @@ def test_results_csv_round_trip_and_failures(tmp_path):
         fh.write("x,9e9,argS(deg),2,1,equal,1\n")     # equal without a tolerance
     with pytest.raises(OpemError):
         evaluate_test_cases(bad, tmp_path / "r_DB.csv", tmp_path / "o.csv")
+
+
+def test_regression_flow_on_the_mu_r_2_guide(tmp_path):
+    """The reference's regression flow end to end on its permeability/
+    rectangular_waveguide project (mu_r = 2, ND6, no recorded run): the project
+    read by the C++ reader, solved by the oracle, written by
+    opem_write_results_csv and judged by opem_evaluate_test_cases against the
+    project's own test cases (those of its first frequency): all pass."""
+    from project_files import reference_project
+    from openparem_b200.fem3d import project_problem
+    from oracle import fem
+    proj, rec = reference_project(str(tmp_path), "permeability-straight")
+    prob, fr = project_problem(proj)
+    assert np.allclose(prob["mu_r"], [2.0])
+    f0 = fr[0]
+    S = fem.solve_frequency(fem.Operators(prob), f0)["S"]
+    res = tmp_path / "straight_results.csv"
+    write_results_csv(res, [f0], S[None], 0.0, "DB", "GHz")
+    cases = [r for r in _regression()["permeability-straight"]["test_cases"] if float(r[1]) == f0]
+    tc = tmp_path / "cases.csv"
+    with open(tc, "w") as fh:
+        fh.write("# ResultDatabase::save_as_test\n" + "\n".join(",".join(r) for r in cases) + "\n")
+    n, npass = evaluate_test_cases(tc, res, tmp_path / "out.csv")
+    assert n == len(cases) == 8 and npass == n
