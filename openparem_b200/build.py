@@ -26,7 +26,7 @@ def build(verbose=False, extra=()):
         deps.append(os.path.join(HERE, "..", "include", "opem_b200.h"))
         if not os.path.exists(obj) or any(os.path.getmtime(d) > os.path.getmtime(obj) for d in deps):
             fl = list(FLAGS)
-            if s == "dense.cpp":
+            if s in ("dense.cpp", "port2d.cpp"):
                 # small dense complex LA: plain complex arithmetic, no C99 inf/NaN recovery
                 fl[fl.index("-fPIC,-fopenmp,-O3")] = "-fPIC,-fopenmp,-O3,-fcx-limited-range"
             cmd = [NVCC] + fl + list(extra) + ["-x", "cu" if s.endswith(".cu") else "c++", "-c", src, "-o", obj]

@@ -8,9 +8,11 @@
 //     [S - k0^2 T_eps  0] x = -beta^2 [T_mu  -G; -G^T  Kz] x,
 //
 // and the fundamental mode (largest beta^2) is found by inverse iteration with
-// the shift -k0^2 max Re(eps_r mu_r).  The shifted matrix is factorised once by
-// banded LU with partial pivoting after a reverse Cuthill-McKee ordering (2D
-// meshes keep the band near sqrt(n)).
+// the shift -k0^2 max Re(eps_r mu_r), moved onto the Rayleigh quotient once
+// that has settled to ~1e-6.  The shifted matrix is factorised (twice) by
+// banded LU with partial pivoting, updated column by column, after the
+// narrowest of a few reverse Cuthill-McKee orderings (2D meshes keep the band
+// near sqrt(n)).
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -56,11 +58,14 @@ struct Banded {
             if (p != j)
                 for (int k = j; k <= jmax; ++k) std::swap(at(j, k), at(p, k));
             const cd d = 1.0 / at(j, j);
-            for (int i = j + 1; i <= imax; ++i) {
-                cd& l = at(i, j);
-                l *= d;
-                if (l == 0.0) continue;
-                for (int k = j + 1; k <= jmax; ++k) at(i, k) -= l * at(j, k);
+            for (int i = j + 1; i <= imax; ++i) at(i, j) *= d;
+            // rank-1 update column by column: within a column the band rows are contiguous
+            const cd* lj = &at(j + 1, j);
+            for (int k = j + 1; k <= jmax; ++k) {
+                const cd u = at(j, k);
+                if (u == 0.0) continue;
+                cd* ck = &at(j + 1, k);
+                for (int i = 0; i < imax - j; ++i) ck[i] -= lj[i] * u;
             }
         }
         return true;
@@ -80,14 +85,14 @@ struct Banded {
 };
 
 // reverse Cuthill-McKee order of a symmetric sparsity pattern
-std::vector<int> rcm(int n, const std::vector<std::vector<int>>& adj) {
+std::vector<int> rcm(int n, const std::vector<std::vector<int>>& adj, int start = -1) {
     std::vector<int> order, deg(n);
     for (int i = 0; i < n; ++i) deg[i] = (int)adj[i].size();
     std::vector<char> seen(n, 0);
-    for (int root0 = 0; root0 < n; ++root0) {
+    for (int root0 = (start >= 0 ? start : 0), first = 1; root0 < n; root0 = first ? 0 : root0 + 1, first = 0) {
         if (seen[root0]) continue;
         int root = root0;   // a pseudo-peripheral start: lowest degree in the component's first BFS level set
-        for (int pass = 0; pass < 2; ++pass) {
+        for (int pass = 0; pass < (first && start >= 0 ? 0 : 2); ++pass) {
             std::vector<int> lvl(n, -1);
             std::queue<int> q;
             q.push(root);
@@ -136,16 +141,44 @@ int solve_pencil(int n, const std::vector<Triplet>& A, const std::vector<Triplet
         for (auto& x : *T)
             if (x.r != x.c) adj[x.r].push_back(x.c);
     for (auto& a : adj) { std::sort(a.begin(), a.end()); a.erase(std::unique(a.begin(), a.end()), a.end()); }
-    std::vector<int> ord = rcm(n, adj), pos(n);
+    // the band of the reverse Cuthill-McKee order from the pseudo-peripheral start
+    // and from a few lowest-degree starts: the narrowest one is kept (the LU costs
+    // n bw^2)
+    auto band = [&](const std::vector<int>& ord) {
+        std::vector<int> ps(n);
+        for (int i = 0; i < n; ++i) ps[ord[i]] = i;
+        int b = 0;
+        for (int i = 0; i < n; ++i)
+            for (int j : adj[i]) b = std::max(b, std::abs(ps[i] - ps[j]));
+        return b;
+    };
+    std::vector<int> ord = rcm(n, adj);
+    int bw = band(ord);
+    {
+        std::vector<int> cand(n);
+        for (int i = 0; i < n; ++i) cand[i] = i;
+        const int K = std::min(n, 8);
+        std::partial_sort(cand.begin(), cand.begin() + K, cand.end(), [&](int a, int b) {
+            return adj[a].size() < adj[b].size() || (adj[a].size() == adj[b].size() && a < b);
+        });
+        for (int k = 0; k < K; ++k) {
+            std::vector<int> o2 = rcm(n, adj, cand[k]);
+            const int b2 = band(o2);
+            if (b2 < bw) { bw = b2; ord.swap(o2); }
+        }
+    }
+    std::vector<int> pos(n);
     for (int i = 0; i < n; ++i) pos[ord[i]] = i;
-    int bw = 0;
-    for (int i = 0; i < n; ++i)
-        for (int j : adj[i]) bw = std::max(bw, std::abs(pos[i] - pos[j]));
     Banded M;
-    M.init(n, bw, bw);
-    for (auto& x : A) M.at(pos[x.r], pos[x.c]) += x.v;
-    for (auto& x : Bm) M.at(pos[x.r], pos[x.c]) -= sigma * x.v;
-    if (!M.factor()) return OPEM_ERR_BREAKDOWN;
+    auto factor_at = [&](cd shift) {
+        M.init(n, bw, bw);
+        for (auto& x : A) M.at(pos[x.r], pos[x.c]) += x.v;
+        for (auto& x : Bm) M.at(pos[x.r], pos[x.c]) -= shift * x.v;
+        return M.factor();
+    };
+    cd shift = sigma;
+    if (!factor_at(shift)) return OPEM_ERR_BREAKDOWN;
+    bool refreshed = false;
     // inverse iteration: y = (A - sigma B)^-1 B x; its dominant eigenvalue mu gives lambda = sigma + 1/mu
     auto Bmul = [&](const std::vector<cd>& x, std::vector<cd>& y) {
         std::fill(y.begin(), y.end(), 0.0);
@@ -173,10 +206,23 @@ int solve_pencil(int n, const std::vector<Triplet>& A, const std::vector<Triplet
         if (!(nrm > 0) || den == 0.0) return OPEM_ERR_BREAKDOWN;
         for (int i = 0; i < n; ++i) x[i] = y[i] / nrm;
         const cd mu = num / den;
-        lam = sigma + 1.0 / mu;
+        lam = shift + 1.0 / mu;
         // converged when the eigenvalue has settled and the unit eigenvector stops
         // moving (up to phase): the eigenvalue settles about twice as fast, and
         // small components such as e_z of a TE-like mode need the vector itself
+        // once the eigenvalue is known to ~1e-6, move the shift onto it (one more
+        // factorisation): the remaining steps then converge in a few iterations
+        if (!refreshed && it > 3 && std::abs(lam - lam_prev) <= 1e-6 * std::abs(lam)) {
+            refreshed = true;
+            const cd s2 = lam;
+            if (factor_at(s2)) {
+                shift = s2;
+                lam_prev = 0;
+                lam_done = 0;
+                continue;
+            }
+            if (!factor_at(shift)) return OPEM_ERR_BREAKDOWN;   // exactly singular: keep the first shift
+        }
         if (it > 3 && std::abs(lam - lam_prev) <= 1e-14 * std::abs(lam)) ++lam_done;
         if (lam_done) {
             cd c = 0;
@@ -184,7 +230,7 @@ int solve_pencil(int n, const std::vector<Triplet>& A, const std::vector<Triplet
             const cd ph = std::abs(c) > 0 ? c / std::abs(c) : cd(1.0);
             double dx = 0;
             for (int i = 0; i < n; ++i) dx += std::norm(x[i] - ph * xold[i]);
-            if (std::sqrt(dx) <= 1e-13 || lam_done > 200) { ok = true; break; }
+            if (std::sqrt(dx) <= 1e-12 || lam_done > 20) { ok = true; break; }
         }
         lam_prev = lam;
     }
