@@ -77,3 +77,22 @@ def test_loaded_project_2d_mode_ports_match_oracle(tmp_path):
     Sm, stm = F.sweep(fr, default_opts(precision=_lib.PREC_MIXED, rtol=1e-10))
     for i in range(len(fr)):
         assert np.abs(Sm[i] - refs[i]).max() <= 1e-6
+
+
+def test_default_copper_walls_project_matches_oracle(tmp_path):
+    """The reference's straight-lossy project: materials.default.boundary copper
+    makes every wall no port claims a copper surface impedance.  ND2 on the
+    device against the oracle on the problem the same reader produced
+    (|dS| <= 1e-8, solver rtol 1e-12)."""
+    from oracle import fem
+    from openparem_b200.fem3d import project_problem
+    from project_files import reference_project
+    proj, _ = reference_project(str(tmp_path), "straight-lossy")
+    F, fr = Fem3D.from_project(proj, order=2, context=Context(0))
+    F.assemble()
+    prob, _ = project_problem(proj, order=2)
+    assert prob["boundaries"][1]["type"] == "impedance"
+    S, _, st = F.solve(fr[0], default_opts(rtol=1e-12, restart=200, maxits=6000, h_rtol=1e-13))
+    assert st["converged"] == 1
+    ref = fem.solve_frequency(fem.Operators(prob), fr[0])["S"]
+    assert np.abs(S - ref).max() <= 1e-8
