@@ -54,3 +54,11 @@ def test_project_refinement_settings(tmp_path):
                 "refinement.relative.tolerance  0.001\nmesh.3D.refinement.fraction    0.05\n")
     r = project_refinement(proj)
     assert (r["variable"], r["iter_max"], r["rel_tol"], r["fraction"]) == ("S", 30, 0.001, 0.05)
+
+
+def test_project_value_missing(tmp_path):
+    from openparem_b200.fem3d import project_value
+    proj = write_guide_project(str(tmp_path))
+    assert project_value(proj, "mesh.order") == "1"
+    assert project_value(proj, "no.such.key", "x") == "x"
+    assert project_value(os.path.join(str(tmp_path), "none.proj"), "mesh.order") is None

@@ -92,3 +92,15 @@ def test_adaptive_loop_with_oracle_step():
     assert len(h2) == 2 and h2[-1]["converged"]
     _, _, h3 = adaptive_solve(prob, step, fraction=0.1, variable="S", rel_tol=1.0, iter_min=3, iter_max=5)
     assert len(h3) == 3 and not h3[1]["converged"] and h3[2]["converged"]
+
+
+def test_refine_rejects_bad_input():
+    from openparem_b200.fem3d import OpemError
+    from openparem_b200 import _lib
+    prob = meshgen.waveguide_problem(meshgen.WR_A, meshgen.WR_B, 50e-3, 2, 1, 2, 1)
+    with pytest.raises(OpemError) as e:
+        refine_problem(prob, [len(prob["tets"])])          # no such tetrahedron
+    assert e.value.code == _lib.ERR_ARG
+    bad = dict(prob, bdr_tris=np.array([[0, 1, 10 ** 6]]), bdr_attr=np.array([1]))
+    with pytest.raises(OpemError):
+        refine_problem(bad, [0])                            # vertex out of range

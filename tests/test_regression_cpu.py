@@ -118,3 +118,17 @@ def test_regression_flow_on_the_mu_r_2_guide(tmp_path):
         fh.write("# ResultDatabase::save_as_test\n" + "\n".join(",".join(r) for r in cases) + "\n")
     n, npass = evaluate_test_cases(tc, res, tmp_path / "out.csv")
     assert n == len(cases) == 8 and npass == n
+
+
+def test_comparator_rejects_antenna_cases_and_missing_files(tmp_path):
+    from openparem_b200 import _lib
+    tc = tmp_path / "ant.csv"
+    with open(tc, "w") as fh:
+        fh.write("# PatternDatabase::save_as_test\ng,9e9,gain,1,equal,5,0.1\n")
+    res = tmp_path / "r.csv"
+    write_results_csv(res, [9e9], np.eye(1)[None].astype(complex) * 0.5, 50.0)
+    with pytest.raises(OpemError) as e:
+        evaluate_test_cases(tc, res, tmp_path / "o.csv")
+    assert e.value.code == _lib.ERR_UNSUPPORTED
+    with pytest.raises(OpemError):
+        evaluate_test_cases(tmp_path / "missing.csv", res, tmp_path / "o.csv")
