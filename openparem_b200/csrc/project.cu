@@ -7,7 +7,8 @@
 // (the wide side of the port rectangle is the mode's a dimension; the voltage
 // integration path of the port's Line block sets the mode voltage), boundary
 // types surface_impedance, perfect_electric_conductor, perfect_magnetic_conductor
-// and radiation, frequency plans of point / point.refine / linear entries.
+// and radiation, frequency plans of point / linear / log entries (and their
+// .refine forms).
 // Exterior faces in no port or boundary path are PEC (the reference's default).
 #include <algorithm>
 #include <array>
@@ -318,18 +319,32 @@ void build(const std::string& proj_path, int order_override, Project& P) {
         if (it != P.kv.end())
             for (auto& v : it->second) P.freqs.push_back(std::stod(v));
     }
-    auto lin = P.kv.find("frequency.plan.linear");
-    if (lin != P.kv.end())
-        for (auto v : lin->second) {
+    // linear plans: start, stop, step, the step added repeatedly; log plans: start,
+    // stop, points per decade, the factor 10^(1/points) applied repeatedly; both up
+    // to stop (1 + 1e-12) (FrequencyPlan, OpenParEMCommon/frequencyPlan.cpp:137-197;
+    // the .refine forms give the same points)
+    for (auto k : {"frequency.plan.linear", "frequency.plan.linear.refine", "frequency.plan.log",
+                   "frequency.plan.log.refine"}) {
+        auto it = P.kv.find(k);
+        if (it == P.kv.end()) continue;
+        const bool lg = std::string(k).find(".log") != std::string::npos;
+        for (auto v : it->second) {
+            v = v.substr(0, v.find("//"));
             for (char& c : v) if (c == ',') c = ' ';
             std::istringstream is(v);
-            double a, b, st;
-            is >> a >> b >> st;
-            if (!(st > 0)) throw std::runtime_error("bad frequency.plan.linear");
-            for (double f = a; f <= b * (1 + 1e-12); f += st) P.freqs.push_back(f);
+            double a = 0, b = 0, st = 0;
+            if (!(is >> a >> b >> st) || !(a > 0) || !(st > 0)) throw std::runtime_error(std::string("bad ") + k);
+            const double factor = lg ? std::pow(10.0, 1.0 / st) : 0.0;
+            for (double f = a; f <= b * (1 + 1e-12); f = lg ? f * factor : f + st) {
+                P.freqs.push_back(f);
+                if (P.freqs.size() > 10000000) throw std::runtime_error(std::string("too many points in ") + k);
+            }
         }
+    }
     std::sort(P.freqs.begin(), P.freqs.end());
-    P.freqs.erase(std::unique(P.freqs.begin(), P.freqs.end()), P.freqs.end());
+    P.freqs.erase(std::unique(P.freqs.begin(), P.freqs.end(),
+                              [](double x, double y) { return std::fabs(y - x) <= 1e-12 * std::fabs(y); }),
+                  P.freqs.end());
     // exterior faces with the opposite vertex of their tet
     const int64_t ne = (int64_t)P.tets.size() / 4;
     struct FaceUse { int count = 0; int64_t second = -1, tet = -1; };   // uses, opposite vertex, owning tet

@@ -62,3 +62,16 @@ def test_project_value_missing(tmp_path):
     assert project_value(proj, "mesh.order") == "1"
     assert project_value(proj, "no.such.key", "x") == "x"
     assert project_value(os.path.join(str(tmp_path), "none.proj"), "mesh.order") is None
+
+
+def test_frequency_plans(tmp_path):
+    """linear, linear.refine, log and point entries expand as the reference's
+    FrequencyPlan does (repeated step / repeated factor up to stop (1 + 1e-12))."""
+    proj = write_guide_project(str(tmp_path))
+    with open(proj, "a") as f:
+        f.write("frequency.plan.log             1e9,1e10,4\n"
+                "frequency.plan.linear.refine   20e9,22e9,1e9   // refined\n")
+    _, fr = project_info(proj)
+    logs = [1e9 * 10 ** (k / 4) for k in range(5)]
+    expect = sorted(set([9e9, 10e9, 10.5e9, 11e9, 20e9, 21e9, 22e9]) | set(logs))
+    assert len(fr) == len(expect) and np.allclose(fr, expect, rtol=1e-12)
