@@ -730,7 +730,10 @@ static int noalloc_scratch(int device, double2** out, std::string& err) {
     return OPEM_OK;
 }
 
-// system_coefficients without host containers: the port terms only need gamma.
+// system_coefficients into a fixed-size array: the port terms only need gamma.
+// gamma comes from port_gamma_Z_V for every port kind, so a port driven by its
+// own 2D mode (kind 1) gets the gamma of that mode, solved on the host (host
+// memory only; no device allocation).  May throw OpemError from the 2D solve.
 static int coefficients_fixed(const Problem& P, double freq, int d, VolCoef& vc, BCoef* bc, int cap) {
     if ((int)P.groups.size() > cap) return -1;
     double w = 2 * M_PI * freq, k0 = w * std::sqrt(MU0 * EPS0), k02 = k0 * k0;
@@ -742,12 +745,8 @@ static int coefficients_fixed(const Problem& P, double freq, int d, VolCoef& vc,
         BCoef c;
         std::memset(&c, 0, sizeof(c));
         if (G.type == OPEM_BDR_PORT && G.port != d) {
-            const double* dd = P.modes[G.port].desc;
-            int r = port_region(P, G.port);
-            cd epsc = P.eps_r[r] * cd(1.0, -P.tand[r]) - cd(0.0, P.sigma[r] / (w * EPS0));
-            double kc2 = std::pow(dd[14] * M_PI / dd[12], 2) + std::pow(dd[15] * M_PI / dd[13], 2);
-            cd gamma = std::sqrt(cd(kc2, 0) - k02 * epsc * P.mu_r[r]);
-            if (gamma.real() < 0) gamma = -gamma;
+            cd gamma, Z, V;
+            port_gamma_Z_V(P, G.port, freq, gamma, Z, V);
             cd ig = 1.0 / gamma;
             cd ce = -k02 * ig, ct = cd(0, k02) * ig, cs = cd(0, w * MU0) * ig;
             c.c_cc = make_double2(ig.real(), ig.imag());
@@ -1161,13 +1160,14 @@ int opem_system_matrix_noalloc(opem_problem prob, double freq, int d, double* va
         return OPEM_ERR_ARG;
     }
     const int CAP = 64;
-    BCoef bc[CAP];
-    VolCoef vc;
-    if (coefficients_fixed(P, freq, d, vc, bc, CAP) < 0) {
+    if ((int)P.groups.size() > CAP) {
         P.ctx->last_error = "opem_system_matrix_noalloc: more than 64 boundary groups";
         return OPEM_ERR_ARG;
     }
     return guarded(P.ctx, [&] {
+        BCoef bc[CAP];
+        VolCoef vc;
+        coefficients_fixed(P, freq, d, vc, bc, CAP);
         OPEM_CUDA(cudaSetDevice(P.ctx->device));
         double2* scratch = nullptr;
         std::string err;

@@ -475,13 +475,16 @@ __global__ void __launch_bounds__(512, TR == 1 ? 2 : 1) patch_apply1_batch_kerne
 #pragma unroll
         for (int q = 0; q < RC; ++q) { re[r][q] = 0.f; im[r][q] = 0.f; }
     }
+    // Every thread waits (bounded) for the stage; whether the whole CTA goes on
+    // is decided at the end-of-panel barrier by __syncthreads_or, so all threads
+    // take the same branch and none leaves while others are still in a barrier.
     bool ok = true;
     int p = 0;
     for (; p < npanel; ++p) {
-        if (!mbar_wait(&bar[p % NS], (uint32_t)((p / NS) & 1))) { ok = false; break; }
+        const bool got = mbar_wait(&bar[p % NS], (uint32_t)((p / NS) & 1));
         const int b0 = p * PW, pw = min(PW, s - b0);
         const float2* panel = ring + (size_t)(p % NS) * PW * smax;
-        if (work) {
+        if (work && got) {
             // one block column: TR row entries against the group's RC staged inputs
             auto step = [&](const float2* __restrict__ col, const float4* __restrict__ xr) {
                 float2 m[TR];
@@ -512,7 +515,9 @@ __global__ void __launch_bounds__(512, TR == 1 ? 2 : 1) patch_apply1_batch_kerne
                 for (int bb = 0; bb < pw; ++bb, col += s, xr += xstride) step(col, xr);
             }
         }
-        __syncthreads();   // every thread is done with this stage
+        // every thread is done with this stage; a stage that did not complete for
+        // any thread stops the whole CTA
+        if (__syncthreads_or(!got)) { ok = false; break; }
         if (threadIdx.x == 0 && p + NS < npanel) pa_issue(p + NS, NS, PW, s, smax, Bv, ring, bar);
     }
     if (!ok) {
@@ -1213,6 +1218,8 @@ static void launch_patch_apply1(Problem& P, cudaStream_t s, const PatchSet32& ps
         // concurrent launches with other ring shapes or patch sizes cannot lower it
         int optin = 0;
         OPEM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, P.ctx->device));
+        if (smem > (size_t)optin - 1024)
+            throw OpemError(OPEM_ERR_UNSUPPORTED, "vertex patch too large for the batched block apply's ring");
         OPEM_CUDA(cudaFuncSetAttribute(patch_apply1_batch_kernel<RC, TR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        optin - 1024));
     }
@@ -1222,6 +1229,7 @@ static void launch_patch_apply1(Problem& P, cudaStream_t s, const PatchSet32& ps
     patch_apply1_batch_kernel<RC, TR><<<P.npatch, threads, smem, s>>>(P.npatch, smax, ring.ns, ring.pw,
                                                                       P.d_patch_ptr.p, P.d_patch_dofs.p, ps.off32.p,
                                                                       ps.B.p, x_il, R, r0, Rd, t, err);
+    OPEM_CUDA(cudaGetLastError());
     ++P.ctx->launches;
 }
 

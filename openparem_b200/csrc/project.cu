@@ -333,7 +333,20 @@ void build(const std::string& proj_path, int order_override, Project& P) {
             for (char& c : v) if (c == ',') c = ' ';
             std::istringstream is(v);
             double a = 0, b = 0, st = 0;
-            if (!(is >> a >> b >> st) || !(a > 0) || !(st > 0)) throw std::runtime_error(std::string("bad ") + k);
+            std::string third, extra;
+            if (!(is >> a >> b >> third) || (is >> extra) || !(a > 0)) throw std::runtime_error(std::string("bad ") + k);
+            if (lg) {
+                // points per decade is an integer (project.c reads it with is_int/atoi)
+                size_t q = (third[0] == '+') ? 1 : 0;
+                if (q == third.size() || third.find_first_not_of("0123456789", q) != std::string::npos)
+                    throw std::runtime_error(std::string("bad ") + k + ": points per decade must be an integer");
+                st = std::atof(third.c_str());
+            } else {
+                char* end = nullptr;
+                st = std::strtod(third.c_str(), &end);
+                if (!end || *end) throw std::runtime_error(std::string("bad ") + k);
+            }
+            if (!(st > 0)) throw std::runtime_error(std::string("bad ") + k);
             const double factor = lg ? std::pow(10.0, 1.0 / st) : 0.0;
             for (double f = a; f <= b * (1 + 1e-12); f = lg ? f * factor : f + st) {
                 P.freqs.push_back(f);
@@ -341,9 +354,11 @@ void build(const std::string& proj_path, int order_override, Project& P) {
             }
         }
     }
+    // duplicates: relative difference below 1e-14 (FrequencyPlan::eliminateDuplicates,
+    // OpenParEMCommon/frequencyPlan.cpp:60-84)
     std::sort(P.freqs.begin(), P.freqs.end());
     P.freqs.erase(std::unique(P.freqs.begin(), P.freqs.end(),
-                              [](double x, double y) { return std::fabs(y - x) <= 1e-12 * std::fabs(y); }),
+                              [](double x, double y) { return std::fabs(y - x) < 1e-14 * std::fabs(y); }),
                   P.freqs.end());
     // exterior faces with the opposite vertex of their tet
     const int64_t ne = (int64_t)P.tets.size() / 4;

@@ -1,7 +1,7 @@
 """Generate the WR90 golden fixtures from the OpenParEM source tree.
 
-Reads, from the reference tree given on the command line (default
-/root/reference):
+Reads, from the reference tree given on the command line (default: the
+directory named by the OPEM_REFERENCE_ROOT environment variable):
   regression/OpenParEM3D/WR90/straight/straight.msh      (gmsh 2.2 mesh, 282 tets)
   regression/OpenParEM3D/WR90/straight-loaded/straight-loaded.msh
   regression/OpenParEM3D/regression_results.csv.current  (the reference's own
@@ -318,4 +318,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("OPEM_REFERENCE_ROOT", "")
+    if not root:
+        sys.exit("usage: make_wr90_fixture.py REFERENCE_ROOT (or set OPEM_REFERENCE_ROOT)")
+    main(root)

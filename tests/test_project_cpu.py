@@ -30,10 +30,13 @@ def test_project_errors(tmp_path):
         project_info(os.path.join(str(tmp_path), "missing.proj"))
 
 
-REF = "/root/reference/regression/OpenParEM3D/WR90/straight/straight.proj"
+# The reference's OpenParEM source tree, when one is mounted: its location comes
+# from OPEM_REFERENCE_ROOT (unset: the test is skipped).
+_ROOT = os.environ.get("OPEM_REFERENCE_ROOT", "")
+REF = os.path.join(_ROOT, "regression/OpenParEM3D/WR90/straight/straight.proj") if _ROOT else ""
 
 
-@pytest.mark.skipif(not os.path.exists(REF), reason="the reference tree is not mounted here")
+@pytest.mark.skipif(not REF or not os.path.exists(REF), reason="the reference tree is not mounted here")
 def test_reference_wr90_straight_project():
     """The reference's own regression project reads: 282 tets, two TE10 ports,
     its three frequency points, mesh order 6."""
@@ -75,3 +78,26 @@ def test_frequency_plans(tmp_path):
     logs = [1e9 * 10 ** (k / 4) for k in range(5)]
     expect = sorted(set([9e9, 10e9, 10.5e9, 11e9, 20e9, 21e9, 22e9]) | set(logs))
     assert len(fr) == len(expect) and np.allclose(fr, expect, rtol=1e-12)
+
+
+def test_frequency_plan_duplicates_and_integer_points_per_decade(tmp_path):
+    """Points whose relative difference is below 1e-14 are one point, points
+    1e-13 apart stay two (FrequencyPlan::eliminateDuplicates); a log plan's
+    points per decade must be an integer, as the reference's project parser
+    requires."""
+    proj = write_guide_project(str(tmp_path))
+    with open(proj, "a") as f:
+        f.write("frequency.plan.point           12e9\n"
+                f"frequency.plan.point           {12e9 * (1 + 2e-16)!r}\n"
+                f"frequency.plan.point           {13e9 * (1 + 1e-13)!r}\n"
+                "frequency.plan.point           13e9\n")
+    _, fr = project_info(proj)
+    assert np.sum(np.abs(np.asarray(fr) - 12e9) < 1e3) == 1
+    assert np.sum(np.abs(np.asarray(fr) - 13e9) < 1e3) == 2
+    d2 = tmp_path / "b"
+    d2.mkdir()
+    proj2 = write_guide_project(str(d2))
+    with open(proj2, "a") as f:
+        f.write("frequency.plan.log             1e9,1e10,2.5\n")
+    with pytest.raises(Exception):
+        project_info(proj2)

@@ -9,7 +9,10 @@ static 16 MiB device array, so it is limited to OPEM_NOALLOC_MAX_NNZ nonzeros.
 
 The test goes through the C ABI (ctypes) and compares two calls in a row with
 the allocating entry point opem_get_system_matrix, at the 1e-12 relative
-tolerance the operator parity tests use.  This file sorts last so a run that
+tolerance the operator parity tests use.  The cases cover analytic TE ports,
+copper walls with a lossy slab, and ports driven by their own 2D mode (the
+slab-loaded WR90 project through the project reader), whose propagation
+constant comes from the 2D mode solve rather than the TE formula.  This file sorts last so a run that
 stops at the first failure has already run every other test.
 """
 import ctypes as C
@@ -29,15 +32,23 @@ def _noalloc(F, freq, d, nnz):
     return rc, out[0::2] + 1j * out[1::2]
 
 
-@pytest.mark.parametrize("case", ["c1_nd1", "slab_nd2_copper"])
-def test_noalloc_matches_allocating_entry_point(case):
+@pytest.mark.parametrize("case", ["c1_nd1", "slab_nd2_copper", "loaded_2d_mode_ports"])
+def test_noalloc_matches_allocating_entry_point(case, tmp_path):
     ctx = Context(0)
-    if case == "c1_nd1":
-        prob = meshgen.config1()[0]
+    if case == "loaded_2d_mode_ports":
+        from openparem_b200.fem3d import project_problem
+        from project_files import reference_project
+        proj, _ = reference_project(str(tmp_path), "straight-loaded")
+        assert [p["mode"]["kind"] for p in project_problem(proj, order=2)[0]["ports"]] == ["FEM2D", "FEM2D"]
+        F, _ = Fem3D.from_project(proj, order=2, context=ctx)
+        F.assemble()
     else:
-        prob = meshgen.waveguide_problem(meshgen.WR_A, meshgen.WR_B, 20e-3, 3, 2, 6, 2, wall="impedance",
-                                         wall_sigma=5.8e7, wall_Rz=0.5e-6, slab=(5e-3, 12e-3, 4.4, 0.02))
-    F = Fem3D(prob, context=ctx).assemble()
+        if case == "c1_nd1":
+            prob = meshgen.config1()[0]
+        else:
+            prob = meshgen.waveguide_problem(meshgen.WR_A, meshgen.WR_B, 20e-3, 3, 2, 6, 2, wall="impedance",
+                                             wall_sigma=5.8e7, wall_Rz=0.5e-6, slab=(5e-3, 12e-3, 4.4, 0.02))
+        F = Fem3D(prob, context=ctx).assemble()
     nnz = F.info()["nnz"]
     assert nnz <= _lib.NOALLOC_MAX_NNZ
     for freq, d in [(9.3e9, 0), (11.1e9, 1)]:
