@@ -156,9 +156,21 @@ int  opem_context_launches(opem_context ctx, int64_t* out);
 int  opem_profile_kernels(opem_problem prob, double freq, int reps, double* out, int nout);
 /* The same for the batched sweep solver's kernels, nsys (1..32) systems near
  * freq on driving set 0; out receives 15 doubles, kernels 0 = FP32 block apply
- * for nsys systems, 1 = batched SpMV with FP32 operators and vectors, 2 = FP64
- * operators and FP32 vectors, 3 = FP64 operators and vectors, 4 = patch sum.     */
+ * for nsys systems (the kernel the solver picks), 1 = batched SpMV with FP32
+ * operators and vectors, 2 = FP64 operators and FP32 vectors, 3 = FP64 operators
+ * and vectors, 4 = patch sum; with nout >= 21 also 5 = the FP32 FMA block apply
+ * and 6 = the tensor-core block apply (ms = -1 where it does not apply).         */
 int  opem_profile_batch_kernels(opem_problem prob, double freq, int nsys, int reps, double* out, int nout);
+/* Checks the batched block apply (the preconditioner that replaces the
+ * reference's direct PCLU, solveComplexLinearSystem.c:153-161): the FP32 block
+ * set of driving set 0 at freq, nsys interleaved systems of deterministic
+ * inputs, systems [r0, r0+nd) applied by the FP32 FMA kernel and by the
+ * tensor-core kernel, both compared with an FP64 host product of the same FP32
+ * blocks.  out (5 doubles): [0] max error of the tensor-core kernel relative to
+ * the largest result (-1 if it does not apply), [1] the same for the FMA kernel,
+ * [2] the kernel the solver uses for this case (2 tensor core, 1 FMA),
+ * [3] max |tensor - FMA| relative, [4] 1 if a bounded wait ran out.            */
+int  opem_check_block_apply(opem_problem prob, double freq, int nsys, int r0, int nd, double* out, int nout);
 
 /* ---- OpenParEM3D project input (project.c, mesh.cpp:449-588, port.cpp:6369-7078,
  * OpenParEMmaterials.cpp) --------------------------------------------------------

@@ -66,6 +66,7 @@ SIGNATURES = [
     ("opem_context_launches", C.c_int, [P, I64P]),
     ("opem_profile_kernels", C.c_int, [P, C.c_double, C.c_int, DP, C.c_int]),
     ("opem_profile_batch_kernels", C.c_int, [P, C.c_double, C.c_int, C.c_int, DP, C.c_int]),
+    ("opem_check_block_apply", C.c_int, [P, C.c_double, C.c_int, C.c_int, C.c_int, DP, C.c_int]),
     ("opem_server_create", C.c_int, [C.c_int, C.c_int, C.c_int64, C.POINTER(C.c_void_p)]),
     ("opem_server_destroy", C.c_int, [P]),
     ("opem_server_submit", C.c_int, [P, P, C.c_int, DP, P, C.POINTER(C.c_int64)]),

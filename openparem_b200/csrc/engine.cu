@@ -1131,7 +1131,18 @@ int opem_profile_batch_kernels(opem_problem prob, double freq, int nsys, int rep
     if (!P.assembled) return OPEM_ERR_STATE;
     return guarded(P.ctx, [&] {
         OPEM_CUDA(cudaSetDevice(P.ctx->device));
-        profile_batch(P, freq, nsys, reps, out);
+        profile_batch(P, freq, nsys, reps, out, nout);
+    });
+}
+
+int opem_check_block_apply(opem_problem prob, double freq, int nsys, int r0, int nd, double* out, int nout) {
+    if (!prob || !out || nout < 5 || !(freq > 0) || nsys < 1 || nsys > 32 || r0 < 0 || nd < 1 || r0 + nd > nsys)
+        return OPEM_ERR_ARG;
+    Problem& P = prob->p;
+    if (!P.assembled) return OPEM_ERR_STATE;
+    return guarded(P.ctx, [&] {
+        OPEM_CUDA(cudaSetDevice(P.ctx->device));
+        check_block_apply(P, freq, nsys, r0, nd, out);
     });
 }
 

@@ -162,7 +162,8 @@ SolveResult solve_mass_cg(Problem& P, const double2* b, double2* x, double rtol,
 void spmv_real_complex(Problem& P, const double* vals, const double2* x, double2* y, double scale_re, double scale_im);
 void spmv_complex(Problem& P, const double2* A, const double2* x, double2* y, const uint8_t* zero_rows);
 void profile_fp64(Problem& P, const double2* A, const uint8_t* dmask, int reps, double* out);
-void profile_batch(Problem& P, double f, int R, int reps, double* out);
+void profile_batch(Problem& P, double f, int R, int reps, double* out, int nout);
+void check_block_apply(Problem& P, double f, int R, int r0, int Rd, double* out);
 void patch_blocks_fp64(Problem& P, const double2* A, const uint8_t* dmask, DBuf<double2>& B);
 
 // ---- engine helpers shared with the mixed path (engine.cu)
