@@ -13,17 +13,22 @@
 // RP = Rd rounded up to 16 or 32), P = C [Xr | Xi] gives
 //   Re T[a][r] = P[2a][r] - P[2a+1][RP + r],  Im T[a][r] = P[2a][RP + r] + P[2a+1][r].
 // P is one tcgen05.mma.kind::tf32 product per 128-row tile (M = 128) and K step
-// of 8.  TF32 keeps 10 mantissa bits, too few for these inverted blocks, so both
+// of 8.  TF32 keeps 10 mantissa bits, too few for these inverted blocks (block
+// Jacobi with TF32-rounded blocks took the config-2 sweep from 66-91 Krylov
+// steps per batch to 91-104, and one batch to the 3000-step limit), so both
 // operands are split, hi = the value with the low 13 mantissa bits cleared (an
-// exact TF32 number) and lo = value - hi (exact in FP32): three products
-// hi(C) hi(X) + lo(C) hi(X) + hi(C) lo(X) accumulate in FP32 in tensor memory,
-// the dropped lo(C) lo(X) term being 2^-22 relative.
+// exact TF32 number) and lo = value - hi (exact in FP32); the dropped lo(C) lo(X)
+// term is 2^-22 relative.  The split inputs sit side by side as one K x 2N
+// operand [hi(X) | lo(X)], so two products per K step, hi(C) [hi(X) | lo(X)]
+// (N = 2N columns) and lo(C) hi(X) accumulated onto its first N columns, give
+// P = D[:, :N] + D[:, N:] in FP32 in tensor memory.
 //
 // One persistent CTA per SM walks its patches (v = blockIdx.x, + gridDim.x, ...)
 // with warp-specialised roles connected by mbarriers:
 //   warp 0          TMA producer: streams each patch's block in panels of KC = 16
 //                   columns (contiguous in HBM) with cp.async.bulk.tensor 2D
-//                   boxes of BH 128-byte rows into an NS-stage ring;
+//                   boxes of BH 128-byte rows into an NS-stage ring, the boxes
+//                   of a panel issued by as many lanes at once;
 //   warp 1          MMA issuer (one thread): tcgen05.mma with A (the split block
 //                   panel) in tensor memory and B (the split inputs) in shared
 //                   memory, tcgen05.commit to release each stage;
@@ -60,7 +65,7 @@ namespace tc {
 constexpr int KC = 16;        // block columns per panel
 constexpr int BH = 16;        // 128-byte rows per TMA box
 constexpr int AS = 4;         // tensor-memory staging slots for the split panel
-constexpr int AB = 2;         // accumulator buffers
+constexpr int AB_MAX = 2;     // accumulator buffers (two for up to 16 systems, one above)
 constexpr int XB = 3;         // split-input buffers
 constexpr int NS_MAX = 8;     // ring stages
 constexpr int THREADS = 640;
@@ -72,7 +77,7 @@ constexpr uint32_t POLL_LIMIT = 1u << 22;
 struct Bars {
     uint64_t full[NS_MAX], empty[NS_MAX];
     uint64_t tfull[AS], tempty[AS];
-    uint64_t afull[AB], aempty[AB];
+    uint64_t afull[AB_MAX], aempty[AB_MAX];
     uint64_t xfull[XB], xempty[XB];
     uint64_t drain;
     uint32_t tmem_base;
@@ -201,19 +206,23 @@ struct Args {
     int* err;
 };
 
-// Bytes of one split-input buffer part (hi or lo) for patches of up to smax
-// DOFs: K rows rounded up to 8, N = 2 RP columns of 4 bytes.
-inline int xpart_bytes(int smax, int RP) { return ((smax + 7) / 8 * 8) * (2 * RP) * 4; }
+// Bytes of one split-input buffer [hi | lo] for patches of up to smax DOFs: K
+// rows rounded up to 8, 2 x 2 RP columns of 4 bytes.
+inline int xbuf_bytes(int smax, int RP) { return ((smax + 7) / 8 * 8) * (4 * RP) * 4; }
+// accumulator buffers for RP (tensor memory: 4 x 2 x 32 staging + AB x 2 x 4RP columns <= 512)
+__host__ __device__ constexpr int acc_buffers(int RP) { return RP <= 16 ? 2 : 1; }
 
 template <int RP>
 __global__ void __launch_bounds__(THREADS, 1) patch_apply_tc_kernel(const __grid_constant__ CUtensorMap tmap, Args g) {
-    constexpr int NA = 2 * RP;   // accumulator / input columns
+    constexpr int NA = 2 * RP;   // columns of [Xr | Xi] and of P
+    constexpr int NB = 2 * NA;   // columns of the split inputs [hi | lo] and of the accumulators
+    constexpr int AB = acc_buffers(RP);
     __shared__ __align__(8) Bars S;
     extern __shared__ __align__(1024) unsigned char dsm_raw[];
     // the launch adds 1024 bytes so the ring can start on a 1024-byte boundary
     unsigned char* dsm = dsm_raw + ((1024u - (su32(dsm_raw) & 1023u)) & 1023u);
     unsigned char* ring = dsm;
-    unsigned char* xbuf = dsm + (size_t)g.NS * g.slot_bytes;   // XB x (hi, lo)
+    unsigned char* xbuf = dsm + (size_t)g.NS * g.slot_bytes;   // XB x [hi | lo]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int MT = g.MT;
     const uint32_t colD0 = (uint32_t)(AS * MT * 2 * KC);
@@ -251,37 +260,38 @@ __global__ void __launch_bounds__(THREADS, 1) patch_apply_tc_kernel(const __grid
     const uint32_t tbase = S.tmem_base;
 
     if (warp == W_TMA) {
-        if (lane == 0) {
-            asm volatile("prefetch.tensormap [%0];" ::"l"(&tmap) : "memory");
-            int gp = 0;
-            bool ok = true;
-            for (int v = blockIdx.x; v < g.npatch && ok; v += gridDim.x) {
-                const int s = g.pptr[v + 1] - g.pptr[v];
-                const int npan = (s + KC - 1) / KC;
-                const int64_t vrow = g.off32[v];
-                for (int p = 0; p < npan; ++p, ++gp) {
-                    const int slot = gp % g.NS;
-                    if (gp >= g.NS && !bar_wait(S, &S.empty[slot], (uint32_t)(((gp / g.NS) + 1) & 1), g.err)) {
-                        ok = false;
-                        break;
-                    }
-                    const int b0 = p * KC, pw = min(KC, s - b0);
-                    const int rows = (pw * s + 15) / 16;   // 128-byte rows of the panel
-                    const int nbox = (rows + BH - 1) / BH;
-                    const int row0 = (int)((vrow + (int64_t)b0 * s) / 16);
-                    bar_expect_tx(&S.full[slot], (uint32_t)(nbox * BH * 128));
-                    unsigned char* dst = ring + (size_t)slot * g.slot_bytes;
-                    for (int j = 0; j < nbox; ++j) tma_load_2d(dst + j * BH * 128, &tmap, 0, row0 + j * BH, &S.full[slot]);
+        if (lane == 0) asm volatile("prefetch.tensormap [%0];" ::"l"(&tmap) : "memory");
+        int gp = 0;
+        bool ok = true;
+        for (int v = blockIdx.x; v < g.npatch && ok; v += gridDim.x) {
+            const int s = g.pptr[v + 1] - g.pptr[v];
+            const int npan = (s + KC - 1) / KC;
+            const int64_t vrow = g.off32[v];
+            for (int p = 0; p < npan; ++p, ++gp) {
+                const int slot = gp % g.NS;
+                if (gp >= g.NS && !bar_wait_warp(S, &S.empty[slot], (uint32_t)(((gp / g.NS) + 1) & 1), g.err)) {
+                    ok = false;
+                    break;
                 }
+                const int b0 = p * KC, pw = min(KC, s - b0);
+                const int rows = (pw * s + 15) / 16;   // 128-byte rows of the panel
+                const int nbox = (rows + BH - 1) / BH;   // at most 32 (slot sizing)
+                const int row0 = (int)((vrow + (int64_t)b0 * s) / 16);
+                if (lane == 0) bar_expect_tx(&S.full[slot], (uint32_t)(nbox * BH * 128));
+                __syncwarp();
+                if (lane < nbox)
+                    tma_load_2d(ring + (size_t)slot * g.slot_bytes + lane * BH * 128, &tmap, 0, row0 + lane * BH,
+                                &S.full[slot]);
             }
-            // every copy issued has landed before the CTA may exit (bounded)
-            for (int q = max(0, gp - g.NS); q < gp; ++q) bar_wait_drain(&S.full[q % g.NS], (uint32_t)((q / g.NS) & 1));
         }
+        // every copy issued has landed before the CTA may exit (bounded)
+        if (lane == 0)
+            for (int q = max(0, gp - g.NS); q < gp; ++q) bar_wait_drain(&S.full[q % g.NS], (uint32_t)((q / g.NS) & 1));
     } else if (warp == W_MMA) {
         if (lane == 0) {
-            constexpr uint32_t IDESC = idesc_tf32(NA);
-            constexpr uint32_t LBO = (uint32_t)(NA / 8) * 128u, SBO = 128u;
-            constexpr uint64_t KSTEP = (uint64_t)(8 * NA * 4 / 16);   // 8 K rows, in 16-byte descriptor units
+            constexpr uint32_t IDESC_W = idesc_tf32(NB), IDESC_N = idesc_tf32(NA);
+            constexpr uint32_t LBO = (uint32_t)(NB / 8) * 128u, SBO = 128u;
+            constexpr uint64_t KSTEP = (uint64_t)(8 * NB * 4 / 16);   // 8 K rows, in 16-byte descriptor units
             int gp = 0, i = 0;
             bool ok = true;
             for (int v = blockIdx.x; v < g.npatch && ok; v += gridDim.x, ++i) {
@@ -291,9 +301,8 @@ __global__ void __launch_bounds__(THREADS, 1) patch_apply_tc_kernel(const __grid
                 if (!bar_wait(S, &S.xfull[xb], (uint32_t)((i / XB) & 1), g.err)) break;
                 if (i >= AB && !bar_wait(S, &S.aempty[ab], (uint32_t)(((i / AB) + 1) & 1), g.err)) break;
                 tc_fence_after();
-                const uint64_t dh0 = desc_kmajor(su32(xbuf + (size_t)(2 * xb) * g.xbytes), LBO, SBO);
-                const uint64_t dl0 = desc_kmajor(su32(xbuf + (size_t)(2 * xb + 1) * g.xbytes), LBO, SBO);
-                const uint32_t d0 = tbase + colD0 + (uint32_t)(ab * MT * NA);
+                const uint64_t dx0 = desc_kmajor(su32(xbuf + (size_t)xb * g.xbytes), LBO, SBO);
+                const uint32_t d0 = tbase + colD0 + (uint32_t)(ab * MT * NB);
                 for (int p = 0; p < npan; ++p, ++gp) {
                     const int ts = gp % AS;
                     if (!bar_wait(S, &S.tfull[ts], (uint32_t)((gp / AS) & 1), g.err)) {
@@ -307,16 +316,15 @@ __global__ void __launch_bounds__(THREADS, 1) patch_apply_tc_kernel(const __grid
 #pragma unroll
                     for (int mt = 0; mt < 2; ++mt) {
                         if (mt >= mtv) break;
-                        const uint32_t d = d0 + (uint32_t)(mt * NA);
+                        const uint32_t d = d0 + (uint32_t)(mt * NB);
                         const uint32_t ahi = a0 + (uint32_t)(mt * 2 * KC);
 #pragma unroll
                         for (int ks = 0; ks < KC / 8; ++ks) {
                             if (ks >= nks) break;
-                            const uint64_t bh = dh0 + kb + ks * KSTEP, bl = dl0 + kb + ks * KSTEP;
+                            const uint64_t bx = dx0 + kb + ks * KSTEP;
                             const uint32_t a = ahi + 8u * ks;
-                            umma_tf32_ts(d, a, bh, IDESC, (p > 0 || ks > 0) ? 1u : 0u);
-                            umma_tf32_ts(d, a + KC, bh, IDESC, 1u);
-                            umma_tf32_ts(d, a, bl, IDESC, 1u);
+                            umma_tf32_ts(d, a, bx, IDESC_W, (p > 0 || ks > 0) ? 1u : 0u);   // hi(C) [hi(X) | lo(X)]
+                            umma_tf32_ts(d, a + KC, bx, IDESC_N, 1u);                     // + lo(C) hi(X)
                         }
                     }
                     umma_commit(&S.tempty[ts]);
@@ -337,8 +345,7 @@ __global__ void __launch_bounds__(THREADS, 1) patch_apply_tc_kernel(const __grid
             const int xb = i % XB;
             if (i >= XB && !bar_wait(S, &S.xempty[xb], (uint32_t)(((i / XB) + 1) & 1), g.err)) break;
             const int p0 = g.pptr[v], s = g.pptr[v + 1] - p0, SP = (s + 7) / 8 * 8;
-            float* xh = reinterpret_cast<float*>(xbuf + (size_t)(2 * xb) * g.xbytes);
-            float* xl = reinterpret_cast<float*>(xbuf + (size_t)(2 * xb + 1) * g.xbytes);
+            float* xs = reinterpret_cast<float*>(xbuf + (size_t)xb * g.xbytes);
             const int tot = SP * RP;
             for (int e0 = tid; e0 < tot; e0 += X_THREADS * X_UNROLL) {
                 // all index loads, then all value loads, in flight together
@@ -362,15 +369,14 @@ __global__ void __launch_bounds__(THREADS, 1) patch_apply_tc_kernel(const __grid
                     uint32_t h0, l0, h1, l1;
                     split_tf32(xv[u].x, h0, l0);
                     split_tf32(xv[u].y, h1, l1);
-                    // element (k = b, n) of a K-major operand: core matrix (k / 4, n / 8)
-                    const int base = (b >> 2) * (NA / 8) * 32 + (b & 3);   // in floats
-                    const int nr = r, ni = RP + r;
-                    const int ore = base + (nr >> 3) * 32 + (nr & 7) * 4;
-                    const int oim = base + (ni >> 3) * 32 + (ni & 7) * 4;
-                    xh[ore] = __uint_as_float(h0);
-                    xl[ore] = __uint_as_float(l0);
-                    xh[oim] = __uint_as_float(h1);
-                    xl[oim] = __uint_as_float(l1);
+                    // element (k = b, n) of a K-major operand: core matrix (k / 4, n / 8);
+                    // columns: hi re r, hi im RP + r, lo re NA + r, lo im NA + RP + r
+                    const int base = (b >> 2) * (NB / 8) * 32 + (b & 3);   // in floats
+                    auto at = [&](int n) { return base + (n >> 3) * 32 + (n & 7) * 4; };
+                    xs[at(r)] = __uint_as_float(h0);
+                    xs[at(RP + r)] = __uint_as_float(h1);
+                    xs[at(NA + r)] = __uint_as_float(l0);
+                    xs[at(NA + RP + r)] = __uint_as_float(l1);
                 }
             }
             fence_async_smem();
@@ -431,27 +437,29 @@ __global__ void __launch_bounds__(THREADS, 1) patch_apply_tc_kernel(const __grid
             tc_fence_after();
             const int p0 = g.pptr[v], s = g.pptr[v + 1] - p0, mtv = (2 * s + 127) / 128;
             for (int mt = 0; mt < mtv; ++mt) {
-                const uint32_t col = colD0 + (uint32_t)((ab * MT + mt) * NA);
+                const uint32_t col = colD0 + (uint32_t)((ab * MT + mt) * NB);
                 float val[RP];
 #pragma unroll
                 for (int h = 0; h < NA / 32; ++h) {
-                    uint32_t d[32];
+                    uint32_t d[32], e[32];
                     tmem_ld32(tbase + lane_off + col + 32u * h, d);
+                    tmem_ld32(tbase + lane_off + col + NA + 32u * h, e);
                     tmem_wait_ld();
-                    // this lane holds row m of P: columns [0, RP) = C Xr, [RP, 2RP) = C Xi;
-                    // the even row of a pair needs the odd row's C Xi, the odd row the
-                    // even row's C Xi (same column indices, one xor shuffle)
+                    // this lane holds row m of P = D[:, :NA] + D[:, NA:]: columns [0, RP)
+                    // = C Xr, [RP, 2RP) = C Xi; the even row of a pair needs the odd
+                    // row's C Xi, the odd row the even row's C Xi (one xor shuffle)
 #pragma unroll
                     for (int c = 0; c < 32; ++c) {
                         const int n = 32 * h + c;
+                        const float pn = __uint_as_float(d[c]) + __uint_as_float(e[c]);
                         if (n >= RP) {
-                            const float mine = __uint_as_float(d[c]);
+                            const float mine = pn;
                             const float other = __shfl_xor_sync(0xffffffffu, mine, 1);
                             const int r = n - RP;
                             if (lane & 1) val[r] += other;    // Im T = P[2a][RP+r] + P[2a+1][r]
                             else val[r] -= other;             // Re T = P[2a][r] - P[2a+1][RP+r]
                         } else {
-                            val[n] = __uint_as_float(d[c]);
+                            val[n] = pn;
                         }
                     }
                 }
@@ -530,14 +538,14 @@ void patch_apply1_batch_tc(const PatchTcLaunch& L, cudaStream_t stream) {
     g.npatch = L.npatch;
     g.MT = MT;
     g.slot_bytes = slot_rows * 128;
-    g.xbytes = xpart_bytes(L.smax, RP);
+    g.xbytes = xbuf_bytes(L.smax, RP);
     int optin = 0;
     OPEM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, L.device));
     const int dyn_max = optin - 2048;   // static barriers and the alignment slack stay below 2 KB
-    const int budget = dyn_max - 1024 - 2 * XB * g.xbytes;
+    const int budget = dyn_max - 1024 - XB * g.xbytes;
     g.NS = std::min(NS_MAX, budget / g.slot_bytes);
     if (g.NS < 2) throw OpemError(OPEM_ERR_UNSUPPORTED, "tensor-core block apply: shared memory");
-    uint32_t cols = (uint32_t)(AS * MT * 2 * KC + AB * MT * 2 * RP), c = 32;
+    uint32_t cols = (uint32_t)(AS * MT * 2 * KC + acc_buffers(RP) * MT * 4 * RP), c = 32;
     while (c < cols) c <<= 1;
     g.tmem_cols = c;
     if (c > 512) throw OpemError(OPEM_ERR_UNSUPPORTED, "tensor-core block apply: tensor memory");
@@ -550,7 +558,7 @@ void patch_apply1_batch_tc(const PatchTcLaunch& L, cudaStream_t stream) {
     g.Rd = L.Rd;
     g.t = reinterpret_cast<float*>(L.t);
     g.err = L.err;
-    const size_t smem = 1024 + (size_t)g.NS * g.slot_bytes + (size_t)2 * XB * g.xbytes;
+    const size_t smem = 1024 + (size_t)g.NS * g.slot_bytes + (size_t)XB * g.xbytes;
     const int grid = std::max(1, std::min(L.npatch, L.sm_count));
     // the maximum dynamic shared memory is a process-wide function attribute:
     // always the same device-wide value, so concurrent launches cannot lower it
