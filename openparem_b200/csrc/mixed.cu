@@ -550,6 +550,7 @@ static inline int patch_rc(int Rd) {
     return (Rd + G - 1) / G;
 }
 
+// FP64 row-major blocks -> FP32 column-major blocks at off32 (one CTA per patch)
 __global__ void blocks_to_f32_colmajor_kernel(int npatch, const int32_t* __restrict__ pptr,
                                               const int64_t* __restrict__ poff, const int64_t* __restrict__ off32,
                                               const double2* __restrict__ in, float2* __restrict__ out) {
