@@ -252,7 +252,8 @@ def run_ours(args, rank, world, local_rank):
     N = F.nports
     if args.kernels:
         if rank == 0:
-            kern = kernel_profile(F, float(freqs[len(freqs) // 2]), args.batch, max(1, args.steps), _lib)
+            kern = kernel_profile(F, float(freqs[len(freqs) // 2]), min(32, args.batch * max(1, N)),
+                                  max(1, args.steps), _lib)
             print(json.dumps({"mesh": args.mesh, "ndofs": info["ndofs"], "nnz": info["nnz"],
                               "systems": args.batch, "kernels": kern}), flush=True)
         return
@@ -358,7 +359,10 @@ def run_ours(args, rank, world, local_rank):
                     for f, Sf in zip(fr, S):
                         res["mixed"]["S"][float(f)] = Sf
                     res["mixed"]["conv"] += [x["converged"] for x in st]
-    kern = kernel_profile(F, float(freqs[len(freqs) // 2]), args.batch, 20, _lib)
+    # the batched path applies the blocks of patches away from the ports to the
+    # systems of both driving sets at once: profile that launch (2 x batch systems)
+    nsys_apply = min(32, args.batch * max(1, N))
+    kern = kernel_profile(F, float(freqs[len(freqs) // 2]), nsys_apply, 20, _lib)
     if rank != 0:
         return
     peak, peak_kind = peaks()

@@ -130,6 +130,10 @@ struct Problem {
     DBuf<int32_t> d_patch_ptr, d_patch_dofs, d_d2p_ptr, d_d2p_idx;
     DBuf<int64_t> d_patch_off;
     int npatch = 0;
+    // patches with no DOF on any port face (their blocks are the same for every
+    // driving set) and the others; built on first use by the batched solver
+    DBuf<int32_t> d_plist_shared, d_plist_port;
+    int n_plist_shared = -1, n_plist_port = 0;
     // last fields per driving set
     std::vector<std::vector<double>> last_e, last_h;
     int64_t device_bytes() const;

@@ -420,12 +420,12 @@ template <int RC, int TR>
 __global__ void __launch_bounds__(512, TR == 1 ? 2 : 1) patch_apply1_batch_kernel(
     int npatch, int smax, int NS, int PW, const int32_t* __restrict__ pptr, const int32_t* __restrict__ pdofs,
     const int64_t* __restrict__ off32, const float2* __restrict__ B, const float2* __restrict__ x, int R, int r0, int Rd,
-    float2* __restrict__ t, int* __restrict__ err) {
+    float2* __restrict__ t, int* __restrict__ err, const int32_t* __restrict__ plist, int ldt) {
     constexpr int RCP = (RC + 1) & ~1;   // group stride in shared memory (16-byte aligned groups)
     constexpr int NV = RCP / 2;          // float4 loads per input row and group
     __shared__ __align__(8) uint64_t bar[PA_NS_MAX];
     extern __shared__ float4 smem4[];
-    const int v = blockIdx.x;
+    const int v = plist ? plist[blockIdx.x] : blockIdx.x;
     const int32_t p0 = pptr[v];
     const int s = pptr[v + 1] - p0;
     const int G = (Rd + RC - 1) / RC;
@@ -535,7 +535,7 @@ __global__ void __launch_bounds__(512, TR == 1 ? 2 : 1) patch_apply1_batch_kerne
         for (int r = 0; r < TR; ++r) {
             const int a = j + r * SA;
             if (a < s) {
-                float2* out = t + (int64_t)(p0 + a) * Rd + g * RC;
+                float2* out = t + (int64_t)(p0 + a) * ldt + g * RC;
 #pragma unroll
                 for (int q = 0; q < RC; ++q)
                     if (q < nc) out[q] = make_float2(re[r][q], im[r][q]);
@@ -565,10 +565,12 @@ __global__ void blocks_to_f32_colmajor_kernel(int npatch, const int32_t* __restr
     }
 }
 
+// y[:, r0 + l] = sum over the patch entries of each DOF of t (row stride ldt), for
+// the Rd systems of driving set d (Dirichlet rows zero)
 __global__ void patch_apply2_batch_kernel(int64_t n, const int32_t* __restrict__ d2p_ptr,
-                                          const int32_t* __restrict__ d2p_idx, const float2* __restrict__ t, int R,
-                                          int r0, int Rd, const uint8_t* __restrict__ pec, const uint8_t* __restrict__ pm,
-                                          int d, float2* __restrict__ y) {
+                                          const int32_t* __restrict__ d2p_idx, const float2* __restrict__ t, int ldt,
+                                          int R, int r0, int Rd, const uint8_t* __restrict__ pec,
+                                          const uint8_t* __restrict__ pm, int d, float2* __restrict__ y) {
     int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (e >= n * Rd) return;
     int64_t i = e / Rd;
@@ -576,7 +578,7 @@ __global__ void patch_apply2_batch_kernel(int64_t n, const int32_t* __restrict__
     float re = 0.f, im = 0.f;
     if (!(pec[i] || ((pm[i] >> d) & 1)))
         for (int32_t q = d2p_ptr[i]; q < d2p_ptr[i + 1]; ++q) {
-            float2 v = t[(int64_t)d2p_idx[q] * Rd + l];
+            float2 v = t[(int64_t)d2p_idx[q] * ldt + l];
             re += v.x;
             im += v.y;
         }
@@ -1207,9 +1209,17 @@ static void build_patchset(Batch& B, double f, int d, PatchSet32& ps) {
 
 struct Ring { int ns, pw; };
 
+// Patches a block apply covers: plist[0..nlist) (all patches when plist is null),
+// T written with row stride ldt systems (Rd when 0).
+struct PatchSel {
+    const int32_t* plist = nullptr;
+    int nlist = 0;
+    int ldt = 0;
+};
+
 template <int RC, int TR>
 static void launch_patch_apply1(Problem& P, cudaStream_t s, const PatchSet32& ps, const float2* x_il, int R, int r0,
-                                int Rd, float2* t, int* err, Ring ring) {
+                                int Rd, float2* t, int* err, Ring ring, const PatchSel& sel) {
     const int G = (Rd + RC - 1) / RC;
     const int RCP = (RC + 1) & ~1;
     const int smax = P.topo.max_patch;
@@ -1227,9 +1237,11 @@ static void launch_patch_apply1(Problem& P, cudaStream_t s, const PatchSet32& ps
     const int items = (smax + TR - 1) / TR * G;
     const int threads = std::max(32, (items + 31) / 32 * 32);
     if (threads > 512) throw OpemError(OPEM_ERR_UNSUPPORTED, "vertex patch too large for the batched block apply");
-    patch_apply1_batch_kernel<RC, TR><<<P.npatch, threads, smem, s>>>(P.npatch, smax, ring.ns, ring.pw,
-                                                                      P.d_patch_ptr.p, P.d_patch_dofs.p, ps.off32.p,
-                                                                      ps.B.p, x_il, R, r0, Rd, t, err);
+    const int grid = sel.plist ? sel.nlist : P.npatch;
+    if (grid < 1) return;
+    patch_apply1_batch_kernel<RC, TR><<<grid, threads, smem, s>>>(P.npatch, smax, ring.ns, ring.pw, P.d_patch_ptr.p,
+                                                                  P.d_patch_dofs.p, ps.off32.p, ps.B.p, x_il, R, r0, Rd,
+                                                                  t, err, sel.plist, sel.ldt > 0 ? sel.ldt : Rd);
     OPEM_CUDA(cudaGetLastError());
     ++P.ctx->launches;
 }
@@ -1282,26 +1294,26 @@ static Ring tune_ring(Problem& P, cudaStream_t s, int Rd, int RC, int G, Launch&
 
 template <int RC, int TR>
 static void launch_patch_apply1_tuned(Problem& P, cudaStream_t s, const PatchSet32& ps, const float2* x_il, int R,
-                                      int r0, int Rd, float2* t, int* err) {
+                                      int r0, int Rd, float2* t, int* err, const PatchSel& sel) {
     const int G = (Rd + RC - 1) / RC;
     const Ring ring = tune_ring(P, s, Rd, RC, G, [&](Ring c) {
-        launch_patch_apply1<RC, TR>(P, s, ps, x_il, R, r0, Rd, t, err, c);
+        launch_patch_apply1<RC, TR>(P, s, ps, x_il, R, r0, Rd, t, err, c, sel);
     });
-    launch_patch_apply1<RC, TR>(P, s, ps, x_il, R, r0, Rd, t, err, ring);
+    launch_patch_apply1<RC, TR>(P, s, ps, x_il, R, r0, Rd, t, err, ring, sel);
 }
 
 template <int TR>
 static void patch_apply1_batch_tr(Problem& P, cudaStream_t s, const PatchSet32& ps, const float2* x_il, int R, int r0,
-                                  int Rd, float2* t, int* err) {
+                                  int Rd, float2* t, int* err, const PatchSel& sel) {
     switch (patch_rc(Rd)) {
-        case 1: launch_patch_apply1_tuned<1, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
-        case 2: launch_patch_apply1_tuned<2, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
-        case 3: launch_patch_apply1_tuned<3, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
-        case 4: launch_patch_apply1_tuned<4, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
-        case 5: launch_patch_apply1_tuned<5, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
-        case 6: launch_patch_apply1_tuned<6, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
-        case 7: launch_patch_apply1_tuned<7, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
-        default: launch_patch_apply1_tuned<8, TR>(P, s, ps, x_il, R, r0, Rd, t, err); break;
+        case 1: launch_patch_apply1_tuned<1, TR>(P, s, ps, x_il, R, r0, Rd, t, err, sel); break;
+        case 2: launch_patch_apply1_tuned<2, TR>(P, s, ps, x_il, R, r0, Rd, t, err, sel); break;
+        case 3: launch_patch_apply1_tuned<3, TR>(P, s, ps, x_il, R, r0, Rd, t, err, sel); break;
+        case 4: launch_patch_apply1_tuned<4, TR>(P, s, ps, x_il, R, r0, Rd, t, err, sel); break;
+        case 5: launch_patch_apply1_tuned<5, TR>(P, s, ps, x_il, R, r0, Rd, t, err, sel); break;
+        case 6: launch_patch_apply1_tuned<6, TR>(P, s, ps, x_il, R, r0, Rd, t, err, sel); break;
+        case 7: launch_patch_apply1_tuned<7, TR>(P, s, ps, x_il, R, r0, Rd, t, err, sel); break;
+        default: launch_patch_apply1_tuned<8, TR>(P, s, ps, x_il, R, r0, Rd, t, err, sel); break;
     }
 }
 
@@ -1310,10 +1322,10 @@ static void patch_apply1_batch_tr(Problem& P, cudaStream_t s, const PatchSet32& 
 enum { PA_AUTO = 0, PA_FMA = 1, PA_TENSOR = 2 };
 
 static void patch_apply1_batch_fma(Problem& P, cudaStream_t s, const PatchSet32& ps, const float2* x_il, int R, int r0,
-                                   int Rd, float2* t, int* err);
+                                   int Rd, float2* t, int* err, const PatchSel& sel);
 
 static void patch_apply1_batch_tensor(Problem& P, cudaStream_t s, const PatchSet32& ps, const float2* x_il, int R,
-                                      int r0, int Rd, float2* t, int* err) {
+                                      int r0, int Rd, float2* t, int* err, const PatchSel& sel) {
     PatchTcLaunch L;
     L.device = P.ctx->device;
     L.sm_count = P.ctx->sm_count;
@@ -1329,6 +1341,9 @@ static void patch_apply1_batch_tensor(Problem& P, cudaStream_t s, const PatchSet
     L.r0 = r0;
     L.Rd = Rd;
     L.t = t;
+    L.ldt = sel.ldt;
+    L.plist = sel.plist;
+    L.nlist = sel.nlist;
     L.err = err;
     patch_apply1_batch_tc(L, s);
     ++P.ctx->launches;
@@ -1337,13 +1352,13 @@ static void patch_apply1_batch_tensor(Problem& P, cudaStream_t s, const PatchSet
 // Variant chooser: on the first call for a (device, largest patch, systems)
 // combination where the tensor-core kernel applies, both kernels run once to
 // warm up and twice timed (CUDA events on the caller's stream, the call's own
-// inputs; both overwrite their output) and the faster is kept for the life of
-// the process.
+// inputs and patches; both overwrite their output) and the faster is kept for
+// the life of the process.
 static std::mutex g_pa_mu;
 static std::map<std::tuple<int, int, int>, int> g_pa_choice;
 
 static int patch_apply_variant(Problem& P, cudaStream_t s, const PatchSet32& ps, const float2* x_il, int R, int r0,
-                               int Rd, float2* t, int* err) {
+                               int Rd, float2* t, int* err, const PatchSel& sel) {
     if (!patch_tc_supported(P.ctx->device, P.topo.max_patch, Rd)) return PA_FMA;
     const auto key = std::make_tuple(P.ctx->device, P.topo.max_patch, Rd);
     {
@@ -1357,8 +1372,8 @@ static int patch_apply_variant(Problem& P, cudaStream_t s, const PatchSet32& ps,
     float ms[3] = {0, 0, 0};
     for (int v = PA_FMA; v <= PA_TENSOR; ++v) {
         auto run = [&] {
-            if (v == PA_TENSOR) patch_apply1_batch_tensor(P, s, ps, x_il, R, r0, Rd, t, err);
-            else patch_apply1_batch_fma(P, s, ps, x_il, R, r0, Rd, t, err);
+            if (v == PA_TENSOR) patch_apply1_batch_tensor(P, s, ps, x_il, R, r0, Rd, t, err, sel);
+            else patch_apply1_batch_fma(P, s, ps, x_il, R, r0, Rd, t, err, sel);
         };
         run();
         OPEM_CUDA(cudaEventRecord(e0, s));
@@ -1378,33 +1393,88 @@ static int patch_apply_variant(Problem& P, cudaStream_t s, const PatchSet32& ps,
 
 // t = blocks (x restricted to the patches) for systems [r0, r0+Rd) of x_il (R systems)
 static void patch_apply1_batch(Problem& P, cudaStream_t s, const PatchSet32& ps, const float2* x_il, int R, int r0,
-                               int Rd, float2* t, int* err, int variant = PA_AUTO) {
-    if (variant == PA_AUTO) variant = patch_apply_variant(P, s, ps, x_il, R, r0, Rd, t, err);
-    if (variant == PA_TENSOR) patch_apply1_batch_tensor(P, s, ps, x_il, R, r0, Rd, t, err);
-    else patch_apply1_batch_fma(P, s, ps, x_il, R, r0, Rd, t, err);
+                               int Rd, float2* t, int* err, int variant = PA_AUTO, const PatchSel& sel = PatchSel{}) {
+    if (variant == PA_AUTO) variant = patch_apply_variant(P, s, ps, x_il, R, r0, Rd, t, err, sel);
+    if (variant == PA_TENSOR) patch_apply1_batch_tensor(P, s, ps, x_il, R, r0, Rd, t, err, sel);
+    else patch_apply1_batch_fma(P, s, ps, x_il, R, r0, Rd, t, err, sel);
 }
 
 static void patch_apply1_batch_fma(Problem& P, cudaStream_t s, const PatchSet32& ps, const float2* x_il, int R, int r0,
-                                   int Rd, float2* t, int* err) {
+                                   int Rd, float2* t, int* err, const PatchSel& sel) {
     int tr = 1;   // rows per thread: 1 unless the patch needs more than 512 threads
     const int G = (Rd + patch_rc(Rd) - 1) / patch_rc(Rd);
     while (tr < 4 && (P.topo.max_patch + tr - 1) / tr * G > 512) tr *= 2;   // one work item per thread
     switch (tr) {
-        case 1: patch_apply1_batch_tr<1>(P, s, ps, x_il, R, r0, Rd, t, err); break;
-        case 4: patch_apply1_batch_tr<4>(P, s, ps, x_il, R, r0, Rd, t, err); break;
-        default: patch_apply1_batch_tr<2>(P, s, ps, x_il, R, r0, Rd, t, err); break;
+        case 1: patch_apply1_batch_tr<1>(P, s, ps, x_il, R, r0, Rd, t, err, sel); break;
+        case 4: patch_apply1_batch_tr<4>(P, s, ps, x_il, R, r0, Rd, t, err, sel); break;
+        default: patch_apply1_batch_tr<2>(P, s, ps, x_il, R, r0, Rd, t, err, sel); break;
     }
 }
 
+// Splits the vertex patches into those with no DOF on any port face and the
+// others.  The system matrices of the driving sets differ only in port terms
+// (the driven port's Dirichlet rows, the other ports' boundary terms), which
+// sit on port-face DOFs, so the first kind has the same inverted block for
+// every driving set.
+static void ensure_patch_lists(Problem& P, cudaStream_t s) {
+    if (P.n_plist_shared >= 0) return;
+    const Topology& T = P.topo;
+    std::vector<int32_t> sh, pt;
+    for (int v = 0; v < P.npatch; ++v) {
+        bool port = false;
+        for (int32_t q = T.patch_ptr[v]; q < T.patch_ptr[v + 1] && !port; ++q)
+            port = P.h_portmask[T.patch_dofs[q]] != 0;
+        (port ? pt : sh).push_back(v);
+    }
+    P.d_plist_shared.upload(sh, s);
+    P.d_plist_port.upload(pt, s);
+    OPEM_CUDA(cudaStreamSynchronize(s));
+    P.n_plist_shared = (int)sh.size();
+    P.n_plist_port = (int)pt.size();
+}
+
+// y = block Jacobi (x) for every system of the batch.  Patch outputs t have row
+// stride R (all systems).  With more than one driving set, the patches away from
+// the ports are applied once for all R systems (one block read, every system in
+// the tensor-core N dimension); the port patches per driving set with its blocks.
 static void patch_apply_batch(Batch& B, const std::vector<PatchSet32>& sets, DBuf<float2>& t, const float2* x_il,
                               float2* y_il) {
     Problem& P = B.P;
+    const int R = B.R;
+    int first = -1, active = 0;
+    for (int d = 0; d < B.N; ++d)
+        if (B.Rd[d] > 0) { if (first < 0) first = d; ++active; }
+    if (first < 0) return;
+    ensure_patch_lists(P, B.s);
+    if (active > 1 && P.n_plist_shared > 0) {
+        PatchSel sh;
+        sh.plist = P.d_plist_shared.p;
+        sh.nlist = P.n_plist_shared;
+        sh.ldt = R;
+        patch_apply1_batch(P, B.s, sets[first], x_il, R, 0, R, t.p, B.err.p, PA_AUTO, sh);
+        if (P.n_plist_port > 0)
+            for (int d = 0; d < B.N; ++d) {
+                if (B.Rd[d] == 0) continue;
+                PatchSel pt;
+                pt.plist = P.d_plist_port.p;
+                pt.nlist = P.n_plist_port;
+                pt.ldt = R;
+                patch_apply1_batch(P, B.s, sets[d], x_il, R, B.r0[d], B.Rd[d], t.p + B.r0[d], B.err.p, PA_AUTO, pt);
+            }
+    } else {
+        for (int d = 0; d < B.N; ++d) {
+            if (B.Rd[d] == 0) continue;
+            PatchSel all;
+            all.ldt = R;
+            patch_apply1_batch(P, B.s, sets[d], x_il, R, B.r0[d], B.Rd[d], t.p + B.r0[d], B.err.p, PA_AUTO, all);
+        }
+    }
     for (int d = 0; d < B.N; ++d) {
         if (B.Rd[d] == 0) continue;
-        patch_apply1_batch(P, B.s, sets[d], x_il, B.R, B.r0[d], B.Rd[d], t.p, B.err.p);
         int64_t work = B.n * B.Rd[d];
         patch_apply2_batch_kernel<<<(unsigned)((work + 255) / 256), 256, 0, B.s>>>(
-            B.n, P.d_d2p_ptr.p, P.d_d2p_idx.p, t.p, B.R, B.r0[d], B.Rd[d], P.d_pec.p, P.d_portmask.p, d, y_il);
+            B.n, P.d_d2p_ptr.p, P.d_d2p_idx.p, t.p + B.r0[d], R, B.R, B.r0[d], B.Rd[d], P.d_pec.p, P.d_portmask.p, d,
+            y_il);
         ++P.ctx->launches;
     }
     OPEM_CUDA(cudaGetLastError());
@@ -1919,7 +1989,6 @@ static void solve_batch(Problem& P, const std::vector<System>& systems, const op
     InnerWork W;
     const int64_t ldV = (int64_t)(m + 1) * n;
     const int nbm = md_blocks_sys(P.ctx->sm_count, R, n);
-    const int maxRd = std::max(1, *std::max_element(B.Rd.begin(), B.Rd.end()));
     W.V.alloc((size_t)R * ldV);
     W.Z.alloc((size_t)R * ldV);
     W.w.alloc(nR);
@@ -1927,7 +1996,7 @@ static void solve_batch(Problem& P, const std::vector<System>& systems, const op
     W.z_il64.alloc(nR);
     W.x_il32.alloc(nR);
     W.z_il32.alloc(nR);
-    W.t.alloc(P.topo.patch_dofs.size() * (size_t)maxRd);
+    W.t.alloc(P.topo.patch_dofs.size() * (size_t)R);   // patch outputs of every system (row stride R)
     W.h.alloc((size_t)R * (m + 1));
     W.part.alloc((size_t)R * (m + 1) * nbm);
     W.yd.alloc((size_t)R * m);
@@ -2213,7 +2282,7 @@ void profile_batch(Problem& P, double f, int R, int reps, double* out, int nout)
     out[10] = ebe ? ebe_bytes(16) : csr + nnz * 8.0 * nops + 2.0 * nR * 16;
     out[12] = timeit([&] {
         patch_apply2_batch_kernel<<<(unsigned)((nR + 255) / 256), 256, 0, B.s>>>(
-            n, P.d_d2p_ptr.p, P.d_d2p_idx.p, t.p, R, 0, R, P.d_pec.p, P.d_portmask.p, 0, y32.p);
+            n, P.d_d2p_ptr.p, P.d_d2p_idx.p, t.p, R, R, 0, R, P.d_pec.p, P.d_portmask.p, 0, y32.p);
         ++P.ctx->launches;
     });
     out[13] = (double)sum_s * (R * 8 + 4) + 4.0 * (n + 1) + 2.0 * n + nR * 8.0;
@@ -2307,7 +2376,7 @@ void check_block_apply(Problem& P, double f, int R, int r0, int Rd, double* out)
     if (!(scale > 0)) scale = 1;
     out[0] = tc ? e2 / scale : -1.0;
     out[1] = e1 / scale;
-    out[2] = patch_apply_variant(P, B.s, set, x.p, R, r0, Rd, t1.p, B.err.p) == PA_TENSOR ? 2.0 : 1.0;
+    out[2] = patch_apply_variant(P, B.s, set, x.p, R, r0, Rd, t1.p, B.err.p, PatchSel{}) == PA_TENSOR ? 2.0 : 1.0;
     out[3] = tc ? e12 / scale : -1.0;
     out[4] = herr ? 1.0 : 0.0;
 }

@@ -23,7 +23,8 @@
 // (N = 2N columns) and lo(C) hi(X) accumulated onto its first N columns, give
 // P = D[:, :N] + D[:, N:] in FP32 in tensor memory.
 //
-// One persistent CTA per SM walks its patches (v = blockIdx.x, + gridDim.x, ...)
+// One persistent CTA per SM walks its share of the selected patches (selection
+// entries blockIdx.x, + gridDim.x, ...)
 // with warp-specialised roles connected by mbarriers:
 //   warp 0          TMA producer: streams each patch's block in panels of KC = 16
 //                   columns (contiguous in HBM) with cp.async.bulk.tensor 2D
@@ -195,7 +196,9 @@ __device__ __forceinline__ void split_tf32(float a, uint32_t& hi, uint32_t& lo) 
 }
 
 struct Args {
-    int npatch, MT, NS, slot_bytes, xbytes;
+    int nsel, MT, NS, slot_bytes, xbytes;
+    const int32_t* plist;   // the patches to apply (nsel of them), or all patches when null
+    int ldt;                // row stride of T in systems (>= Rd)
     uint32_t tmem_cols;
     const int32_t* pptr;
     const int32_t* pdofs;
@@ -263,7 +266,8 @@ __global__ void __launch_bounds__(THREADS, 1) patch_apply_tc_kernel(const __grid
         if (lane == 0) asm volatile("prefetch.tensormap [%0];" ::"l"(&tmap) : "memory");
         int gp = 0;
         bool ok = true;
-        for (int v = blockIdx.x; v < g.npatch && ok; v += gridDim.x) {
+        for (int k = blockIdx.x; k < g.nsel && ok; k += gridDim.x) {
+            const int v = g.plist ? g.plist[k] : k;
             const int s = g.pptr[v + 1] - g.pptr[v];
             const int npan = (s + KC - 1) / KC;
             const int64_t vrow = g.off32[v];
@@ -294,7 +298,8 @@ __global__ void __launch_bounds__(THREADS, 1) patch_apply_tc_kernel(const __grid
             constexpr uint64_t KSTEP = (uint64_t)(8 * NB * 4 / 16);   // 8 K rows, in 16-byte descriptor units
             int gp = 0, i = 0;
             bool ok = true;
-            for (int v = blockIdx.x; v < g.npatch && ok; v += gridDim.x, ++i) {
+            for (int k = blockIdx.x; k < g.nsel && ok; k += gridDim.x, ++i) {
+                const int v = g.plist ? g.plist[k] : k;
                 const int s = g.pptr[v + 1] - g.pptr[v];
                 const int npan = (s + KC - 1) / KC, mtv = (2 * s + 127) / 128;
                 const int ab = i % AB, xb = i % XB;
@@ -341,7 +346,8 @@ __global__ void __launch_bounds__(THREADS, 1) patch_apply_tc_kernel(const __grid
         // input stager: X rows of the patch, split, canonical K-major layout
         const int tid = (warp < W_CV ? warp - 2 : warp - (W_EP + 4) + 2) * 32 + lane;
         int i = 0;
-        for (int v = blockIdx.x; v < g.npatch; v += gridDim.x, ++i) {
+        for (int k = blockIdx.x; k < g.nsel; k += gridDim.x, ++i) {
+            const int v = g.plist ? g.plist[k] : k;
             const int xb = i % XB;
             if (i >= XB && !bar_wait(S, &S.xempty[xb], (uint32_t)(((i / XB) + 1) & 1), g.err)) break;
             const int p0 = g.pptr[v], s = g.pptr[v + 1] - p0, SP = (s + 7) / 8 * 8;
@@ -389,7 +395,8 @@ __global__ void __launch_bounds__(THREADS, 1) patch_apply_tc_kernel(const __grid
         const uint32_t lane_off = (uint32_t)(q * 32) << 16;
         int gp = 0;
         bool ok = true;
-        for (int v = blockIdx.x; v < g.npatch && ok; v += gridDim.x) {
+        for (int k = blockIdx.x; k < g.nsel && ok; k += gridDim.x) {
+            const int v = g.plist ? g.plist[k] : k;
             const int s = g.pptr[v + 1] - g.pptr[v];
             const int npan = (s + KC - 1) / KC, mtv = (2 * s + 127) / 128;
             for (int p = 0; p < npan; ++p, ++gp) {
@@ -431,7 +438,8 @@ __global__ void __launch_bounds__(THREADS, 1) patch_apply_tc_kernel(const __grid
         const int q = warp & 3;
         const uint32_t lane_off = (uint32_t)(q * 32) << 16;
         int i = 0;
-        for (int v = blockIdx.x; v < g.npatch; v += gridDim.x, ++i) {
+        for (int k = blockIdx.x; k < g.nsel; k += gridDim.x, ++i) {
+            const int v = g.plist ? g.plist[k] : k;
             const int ab = i % AB;
             if (!bar_wait_warp(S, &S.afull[ab], (uint32_t)((i / AB) & 1), g.err)) break;
             tc_fence_after();
@@ -465,7 +473,7 @@ __global__ void __launch_bounds__(THREADS, 1) patch_apply_tc_kernel(const __grid
                 }
                 const int m = mt * 128 + q * 32 + lane;
                 if (m < 2 * s) {
-                    float* out = g.t + ((int64_t)(p0 + (m >> 1)) * g.Rd) * 2 + (lane & 1);
+                    float* out = g.t + ((int64_t)(p0 + (m >> 1)) * g.ldt) * 2 + (lane & 1);
 #pragma unroll
                     for (int r = 0; r < RP; ++r)
                         if (r < g.Rd) out[2 * r] = val[r];
@@ -535,7 +543,9 @@ void patch_apply1_batch_tc(const PatchTcLaunch& L, cudaStream_t stream) {
     const int MT = (2 * L.smax + 127) / 128;
     const int slot_rows = ((KC * L.smax + 15) / 16 + BH - 1) / BH * BH;
     Args g;
-    g.npatch = L.npatch;
+    g.nsel = L.plist ? L.nlist : L.npatch;
+    g.plist = L.plist;
+    g.ldt = L.ldt > 0 ? L.ldt : L.Rd;
     g.MT = MT;
     g.slot_bytes = slot_rows * 128;
     g.xbytes = xbuf_bytes(L.smax, RP);
@@ -559,7 +569,8 @@ void patch_apply1_batch_tc(const PatchTcLaunch& L, cudaStream_t stream) {
     g.t = reinterpret_cast<float*>(L.t);
     g.err = L.err;
     const size_t smem = 1024 + (size_t)g.NS * g.slot_bytes + (size_t)XB * g.xbytes;
-    const int grid = std::max(1, std::min(L.npatch, L.sm_count));
+    if (g.nsel < 1) return;
+    const int grid = std::max(1, std::min(g.nsel, L.sm_count));
     // the maximum dynamic shared memory is a process-wide function attribute:
     // always the same device-wide value, so concurrent launches cannot lower it
     if (RP == 16) {

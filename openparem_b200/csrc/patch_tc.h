@@ -10,7 +10,8 @@ namespace opem {
 // of the interleaved inputs x (element (dof, r) at dof*R + r).  B holds the FP32
 // column-major blocks (block v at off32[v] float2 elements, a multiple of 16;
 // total_f2 elements in all, a multiple of 16).  T is written per patch entry:
-// t[(pptr[v] + a) * Rd + r].
+// t[(pptr[v] + a) * ldt + r] (ldt = Rd when 0).  With plist, only the nlist
+// patches plist[0..nlist) are applied.
 struct PatchTcLaunch {
     int device = 0, sm_count = 148;
     int npatch = 0, smax = 0;
@@ -22,6 +23,9 @@ struct PatchTcLaunch {
     const float2* x = nullptr;
     int R = 0, r0 = 0, Rd = 0;
     float2* t = nullptr;
+    int ldt = 0;
+    const int32_t* plist = nullptr;
+    int nlist = 0;
     int* err = nullptr;   // set to 1 when a bounded wait ran out
 };
 
