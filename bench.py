@@ -255,7 +255,7 @@ def run_ours(args, rank, world, local_rank):
             kern = kernel_profile(F, float(freqs[len(freqs) // 2]), min(32, args.batch * max(1, N)),
                                   max(1, args.steps), _lib)
             print(json.dumps({"mesh": args.mesh, "ndofs": info["ndofs"], "nnz": info["nnz"],
-                              "systems": args.batch, "kernels": kern}), flush=True)
+                              "systems": min(32, args.batch * max(1, N)), "kernels": kern}), flush=True)
         return
     plain_o = default_opts(rtol=args.rtol, restart=args.restart, deflate=args.deflate, maxits=5000)
     mixed_o = default_opts(rtol=args.rtol, restart=args.restart, deflate=args.deflate, maxits=3000,
@@ -368,7 +368,7 @@ def run_ours(args, rank, world, local_rank):
     peak, peak_kind = peaks()
     if modes[0] == "mixed":
         # the batched path's dominant kernel: FP32 block apply for one driving set of `batch` systems
-        dom, dom_label, ratio = ("patch_apply1_batch", f"patch_apply1_batch_kernel (FP32 blocks x {args.batch} systems)",
+        dom, dom_label, ratio = ("patch_apply1_batch", f"batched block apply (FP32 blocks x {nsys_apply} systems)",
                                  TRAFFIC_RATIO_PATCH_BATCH)
         traffic_src = ("ncu dram__bytes_read+write of the same kernel on the 16x8x40-hex ND2 case, "
                        "scaled by algorithmic bytes")
@@ -381,7 +381,7 @@ def run_ours(args, rank, world, local_rank):
     if dom == "patch_apply1_batch" and kern[dom].get("ms"):
         sum_s2 = float(info["sum_patch_sq"]) if "sum_patch_sq" in info else None
         if sum_s2:
-            fl = sum_s2 * args.batch * 8.0
+            fl = sum_s2 * nsys_apply * 8.0
             tf = fl / (kern[dom]["ms"] * 1e-3) / 1e12
             fp32 = {"flops_per_launch": fl, "tflops": tf, "peak_tflops_nominal": FP32_PEAK_TFLOPS,
                     "frac": tf / FP32_PEAK_TFLOPS}
