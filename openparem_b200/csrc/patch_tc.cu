@@ -26,30 +26,34 @@
 // One persistent CTA per SM walks its share of the selected patches (selection
 // entries blockIdx.x, + gridDim.x, ...)
 // with warp-specialised roles connected by mbarriers:
-//   warp 0          TMA producer: streams each patch's block in panels of KC = 16
-//                   columns (contiguous in HBM) with cp.async.bulk.tensor 2D
-//                   boxes of BH 128-byte rows into an NS-stage ring, the boxes
-//                   of a panel issued by as many lanes at once;
+//   warp 0          TMA producer (one thread): streams each patch's block in
+//                   panels of KC = 16 columns (contiguous in HBM), one bulk copy
+//                   (cp.async.bulk, the TMA engine) per panel into an NS-stage
+//                   ring.  Bulk copies, not tensor-map boxes: with the panels
+//                   seen as a 2D map of 128-byte rows, boxes of 16 rows held one
+//                   CTA per SM to 2.9 TB/s in a streaming probe on B200, while one
+//                   bulk copy per 12.8 KB panel reached 6.0 TB/s;
 //   warp 1          MMA issuer (one thread): tcgen05.mma with A (the split block
 //                   panel) in tensor memory and B (the split inputs) in shared
 //                   memory, tcgen05.commit to release each stage;
-//   warps 2-3, 16-19 input stager: gathers the patch's X rows (X_UNROLL index and
-//                   value loads in flight per thread: the gather is latency-
-//                   bound), splits them and writes them in the canonical K-major
+//   warps 2-3, 20-21 input stager: a warp gathers chunks of the patch's X rows
+//                   (one coalesced index load, then per row one coalesced load of
+//                   its Rd systems, RP lanes per row, 16 loads in flight per
+//                   lane), splits them and writes them in the canonical K-major
 //                   (no swizzle) layout, XB buffers;
 //   warps 4-7, 8-11 converter, two warpgroups taking alternate panels: reads a
 //                   ring stage (thread = one of the 128 lanes of an M tile,
 //                   consecutive rows, conflict-free), splits each entry into
 //                   hi/lo and stores them into tensor memory with tcgen05.st
 //                   (AS staging slots);
-//   warps 12-15     epilogue: tcgen05.ld of the accumulators (AB buffers), the
-//                   re/im recombination of neighbouring rows by one shuffle, and
-//                   the stores of T.
+//   warps 12-19     epilogue, warpgroup E draining M tile E of each patch (both
+//                   tiles at once, so the accumulators free up sooner): tcgen05.ld
+//                   (AB buffers), the re/im recombination of neighbouring rows by
+//                   one shuffle, and the stores of T.
 // Every wait is bounded: a wait that runs out sets *err and a shared abort flag
 // that stops every role; the producer then waits (bounded) for its copies in
 // flight, the MMA thread for its products, and the CTA frees its tensor memory.
-// The tensor map covers only this GPU's own block array; no load multicasts.
-#include <cuda.h>
+// The bulk copies read only this GPU's own block array; no load multicasts.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -64,15 +68,14 @@ namespace opem {
 namespace tc {
 
 constexpr int KC = 16;        // block columns per panel
-constexpr int BH = 16;        // 128-byte rows per TMA box
 constexpr int AS = 4;         // tensor-memory staging slots for the split panel
 constexpr int AB_MAX = 2;     // accumulator buffers (two for up to 16 systems, one above)
 constexpr int XB = 3;         // split-input buffers
 constexpr int NS_MAX = 8;     // ring stages
-constexpr int THREADS = 640;
-constexpr int W_TMA = 0, W_MMA = 1, W_CV = 4, W_EP = 12;
-constexpr int X_THREADS = 192, CV_WARPS = 4, EP_THREADS = 128;
-constexpr int X_UNROLL = 12;  // input elements per stager thread with loads in flight together
+constexpr int THREADS = 704;
+constexpr int W_TMA = 0, W_MMA = 1, W_CV = 4, W_EP = 12, W_X2 = 20;
+constexpr int X_WARPS = 4, X_THREADS = 128, CV_WARPS = 4, EP_THREADS = 256;
+constexpr int X_ITERS = 16;   // row loads in flight per stager lane (a chunk is 16 x (32 / RP) rows)
 constexpr uint32_t POLL_LIMIT = 1u << 22;
 
 struct Bars {
@@ -127,12 +130,13 @@ __device__ __forceinline__ void bar_wait_drain(uint64_t* b, uint32_t parity) {
         if (bar_try(b, parity)) return;
 }
 
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int c0, int c1, uint64_t* b) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-            su32(dst)),
-        "l"(map), "r"(c0), "r"(c1), "r"(su32(b))
-        : "memory");
+// global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16)
+// completing on mbarrier b
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* b) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     su32(dst)),
+                 "l"(src), "r"(bytes), "r"(su32(b))
+                 : "memory");
 }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -196,6 +200,7 @@ __device__ __forceinline__ void split_tf32(float a, uint32_t& hi, uint32_t& lo) 
 }
 
 struct Args {
+    const float2* B;        // FP32 blocks (column-major, block v at off32[v])
     int nsel, MT, NS, slot_bytes, xbytes;
     const int32_t* plist;   // the patches to apply (nsel of them), or all patches when null
     int ldt;                // row stride of T in systems (>= Rd)
@@ -216,7 +221,7 @@ inline int xbuf_bytes(int smax, int RP) { return ((smax + 7) / 8 * 8) * (4 * RP)
 __host__ __device__ constexpr int acc_buffers(int RP) { return RP <= 16 ? 2 : 1; }
 
 template <int RP>
-__global__ void __launch_bounds__(THREADS, 1) patch_apply_tc_kernel(const __grid_constant__ CUtensorMap tmap, Args g) {
+__global__ void __launch_bounds__(THREADS, 1) patch_apply_tc_kernel(Args g) {
     constexpr int NA = 2 * RP;   // columns of [Xr | Xi] and of P
     constexpr int NB = 2 * NA;   // columns of the split inputs [hi | lo] and of the accumulators
     constexpr int AB = acc_buffers(RP);
@@ -263,34 +268,31 @@ __global__ void __launch_bounds__(THREADS, 1) patch_apply_tc_kernel(const __grid
     const uint32_t tbase = S.tmem_base;
 
     if (warp == W_TMA) {
-        if (lane == 0) asm volatile("prefetch.tensormap [%0];" ::"l"(&tmap) : "memory");
-        int gp = 0;
-        bool ok = true;
-        for (int k = blockIdx.x; k < g.nsel && ok; k += gridDim.x) {
-            const int v = g.plist ? g.plist[k] : k;
-            const int s = g.pptr[v + 1] - g.pptr[v];
-            const int npan = (s + KC - 1) / KC;
-            const int64_t vrow = g.off32[v];
-            for (int p = 0; p < npan; ++p, ++gp) {
-                const int slot = gp % g.NS;
-                if (gp >= g.NS && !bar_wait_warp(S, &S.empty[slot], (uint32_t)(((gp / g.NS) + 1) & 1), g.err)) {
-                    ok = false;
-                    break;
+        if (lane == 0) {
+            int gp = 0;
+            bool ok = true;
+            for (int k = blockIdx.x; k < g.nsel && ok; k += gridDim.x) {
+                const int v = g.plist ? g.plist[k] : k;
+                const int s = g.pptr[v + 1] - g.pptr[v];
+                const int npan = (s + KC - 1) / KC;
+                const float2* Bv = g.B + g.off32[v];
+                for (int p = 0; p < npan; ++p, ++gp) {
+                    const int slot = gp % g.NS;
+                    if (gp >= g.NS && !bar_wait(S, &S.empty[slot], (uint32_t)(((gp / g.NS) + 1) & 1), g.err)) {
+                        ok = false;
+                        break;
+                    }
+                    // the panel's columns are contiguous; the size is rounded up to 16
+                    // bytes (at most 8 bytes past the block: the array ends with slack)
+                    const int b0 = p * KC, pw = min(KC, s - b0);
+                    const uint32_t bytes = (uint32_t)(((int64_t)pw * s * 8 + 15) & ~15ll);
+                    bar_expect_tx(&S.full[slot], bytes);
+                    bulk_g2s(ring + (size_t)slot * g.slot_bytes, Bv + (int64_t)b0 * s, bytes, &S.full[slot]);
                 }
-                const int b0 = p * KC, pw = min(KC, s - b0);
-                const int rows = (pw * s + 15) / 16;   // 128-byte rows of the panel
-                const int nbox = (rows + BH - 1) / BH;   // at most 32 (slot sizing)
-                const int row0 = (int)((vrow + (int64_t)b0 * s) / 16);
-                if (lane == 0) bar_expect_tx(&S.full[slot], (uint32_t)(nbox * BH * 128));
-                __syncwarp();
-                if (lane < nbox)
-                    tma_load_2d(ring + (size_t)slot * g.slot_bytes + lane * BH * 128, &tmap, 0, row0 + lane * BH,
-                                &S.full[slot]);
             }
-        }
-        // every copy issued has landed before the CTA may exit (bounded)
-        if (lane == 0)
+            // every copy issued has landed before the CTA may exit (bounded)
             for (int q = max(0, gp - g.NS); q < gp; ++q) bar_wait_drain(&S.full[q % g.NS], (uint32_t)((q / g.NS) & 1));
+        }
     } else if (warp == W_MMA) {
         if (lane == 0) {
             constexpr uint32_t IDESC_W = idesc_tf32(NB), IDESC_N = idesc_tf32(NA);
@@ -342,9 +344,9 @@ __global__ void __launch_bounds__(THREADS, 1) patch_apply_tc_kernel(const __grid
             umma_commit(&S.drain);
             bar_wait_drain(&S.drain, 0);
         }
-    } else if (warp < W_CV || warp >= W_EP + 4) {
+    } else if (warp < W_CV || warp >= W_X2) {
         // input stager: X rows of the patch, split, canonical K-major layout
-        const int tid = (warp < W_CV ? warp - 2 : warp - (W_EP + 4) + 2) * 32 + lane;
+        const int sw = warp < W_CV ? warp - 2 : warp - W_X2 + 2;
         int i = 0;
         for (int k = blockIdx.x; k < g.nsel; k += gridDim.x, ++i) {
             const int v = g.plist ? g.plist[k] : k;
@@ -352,29 +354,24 @@ __global__ void __launch_bounds__(THREADS, 1) patch_apply_tc_kernel(const __grid
             if (i >= XB && !bar_wait(S, &S.xempty[xb], (uint32_t)(((i / XB) + 1) & 1), g.err)) break;
             const int p0 = g.pptr[v], s = g.pptr[v + 1] - p0, SP = (s + 7) / 8 * 8;
             float* xs = reinterpret_cast<float*>(xbuf + (size_t)xb * g.xbytes);
-            const int tot = SP * RP;
-            for (int e0 = tid; e0 < tot; e0 += X_THREADS * X_UNROLL) {
-                // all index loads, then all value loads, in flight together
-                int32_t dof[X_UNROLL];
+            constexpr int RPW = 32 / RP, CH = X_ITERS * RPW;   // rows per warp load, rows per chunk
+            const int r = lane % RP, hg = lane / RP;
+            for (int b0 = sw * CH; b0 < SP; b0 += X_WARPS * CH) {
+                int mydof = -1;
+                if (lane < CH && b0 + lane < s) mydof = g.pdofs[p0 + b0 + lane];
+                float2 xv[X_ITERS];
 #pragma unroll
-                for (int u = 0; u < X_UNROLL; ++u) {
-                    const int e = e0 + u * X_THREADS, b = e / RP, r = e - b * RP;
-                    dof[u] = (e < tot && b < s && r < g.Rd) ? g.pdofs[p0 + b] : -1;
-                }
-                float2 xv[X_UNROLL];
-#pragma unroll
-                for (int u = 0; u < X_UNROLL; ++u) {
-                    const int e = e0 + u * X_THREADS, r = e % RP;
-                    xv[u] = dof[u] >= 0 ? g.x[(int64_t)dof[u] * g.R + g.r0 + r] : make_float2(0.f, 0.f);
+                for (int j = 0; j < X_ITERS; ++j) {
+                    const int dj = __shfl_sync(0xffffffffu, mydof, j * RPW + hg);
+                    xv[j] = (dj >= 0 && r < g.Rd) ? g.x[(int64_t)dj * g.R + g.r0 + r] : make_float2(0.f, 0.f);
                 }
 #pragma unroll
-                for (int u = 0; u < X_UNROLL; ++u) {
-                    const int e = e0 + u * X_THREADS;
-                    if (e >= tot) break;
-                    const int b = e / RP, r = e - b * RP;
+                for (int j = 0; j < X_ITERS; ++j) {
+                    const int b = b0 + j * RPW + hg;
+                    if (b >= SP) break;
                     uint32_t h0, l0, h1, l1;
-                    split_tf32(xv[u].x, h0, l0);
-                    split_tf32(xv[u].y, h1, l1);
+                    split_tf32(xv[j].x, h0, l0);
+                    split_tf32(xv[j].y, h1, l1);
                     // element (k = b, n) of a K-major operand: core matrix (k / 4, n / 8);
                     // columns: hi re r, hi im RP + r, lo re NA + r, lo im NA + RP + r
                     const int base = (b >> 2) * (NB / 8) * 32 + (b & 3);   // in floats
@@ -434,8 +431,8 @@ __global__ void __launch_bounds__(THREADS, 1) patch_apply_tc_kernel(const __grid
             }
         }
     } else {
-        // epilogue: accumulators -> T (lane quarter q)
-        const int q = warp & 3;
+        // epilogue group E drains M tile E of each patch (lane quarter q)
+        const int E = (warp - W_EP) >> 2, q = warp & 3;
         const uint32_t lane_off = (uint32_t)(q * 32) << 16;
         int i = 0;
         for (int k = blockIdx.x; k < g.nsel; k += gridDim.x, ++i) {
@@ -444,43 +441,47 @@ __global__ void __launch_bounds__(THREADS, 1) patch_apply_tc_kernel(const __grid
             if (!bar_wait_warp(S, &S.afull[ab], (uint32_t)((i / AB) & 1), g.err)) break;
             tc_fence_after();
             const int p0 = g.pptr[v], s = g.pptr[v + 1] - p0, mtv = (2 * s + 127) / 128;
-            for (int mt = 0; mt < mtv; ++mt) {
-                const uint32_t col = colD0 + (uint32_t)((ab * MT + mt) * NB);
-                float val[RP];
+            if (E >= mtv) {
+                tc_fence_before();
+                bar_arrive(&S.aempty[ab]);
+                continue;
+            }
+            const int mt = E;
+            const uint32_t col = colD0 + (uint32_t)((ab * MT + mt) * NB);
+            float val[RP];
 #pragma unroll
-                for (int h = 0; h < NA / 32; ++h) {
-                    uint32_t d[32], e[32];
-                    tmem_ld32(tbase + lane_off + col + 32u * h, d);
-                    tmem_ld32(tbase + lane_off + col + NA + 32u * h, e);
-                    tmem_wait_ld();
-                    // this lane holds row m of P = D[:, :NA] + D[:, NA:]: columns [0, RP)
-                    // = C Xr, [RP, 2RP) = C Xi; the even row of a pair needs the odd
-                    // row's C Xi, the odd row the even row's C Xi (one xor shuffle)
+            for (int h = 0; h < NA / 32; ++h) {
+                uint32_t d[32], e[32];
+                tmem_ld32(tbase + lane_off + col + 32u * h, d);
+                tmem_ld32(tbase + lane_off + col + NA + 32u * h, e);
+                tmem_wait_ld();
+                // this lane holds row m of P = D[:, :NA] + D[:, NA:]: columns [0, RP)
+                // = C Xr, [RP, 2RP) = C Xi; the even row of a pair needs the odd
+                // row's C Xi, the odd row the even row's C Xi (one xor shuffle)
 #pragma unroll
-                    for (int c = 0; c < 32; ++c) {
-                        const int n = 32 * h + c;
-                        const float pn = __uint_as_float(d[c]) + __uint_as_float(e[c]);
-                        if (n >= RP) {
-                            const float mine = pn;
-                            const float other = __shfl_xor_sync(0xffffffffu, mine, 1);
-                            const int r = n - RP;
-                            if (lane & 1) val[r] += other;    // Im T = P[2a][RP+r] + P[2a+1][r]
-                            else val[r] -= other;             // Re T = P[2a][r] - P[2a+1][RP+r]
-                        } else {
-                            val[n] = pn;
-                        }
+                for (int c = 0; c < 32; ++c) {
+                    const int n = 32 * h + c;
+                    const float pn = __uint_as_float(d[c]) + __uint_as_float(e[c]);
+                    if (n >= RP) {
+                        const float other = __shfl_xor_sync(0xffffffffu, pn, 1);
+                        const int r = n - RP;
+                        if (lane & 1) val[r] += other;    // Im T = P[2a][RP+r] + P[2a+1][r]
+                        else val[r] -= other;             // Re T = P[2a][r] - P[2a+1][RP+r]
+                    } else {
+                        val[n] = pn;
                     }
                 }
-                const int m = mt * 128 + q * 32 + lane;
-                if (m < 2 * s) {
-                    float* out = g.t + ((int64_t)(p0 + (m >> 1)) * g.ldt) * 2 + (lane & 1);
-#pragma unroll
-                    for (int r = 0; r < RP; ++r)
-                        if (r < g.Rd) out[2 * r] = val[r];
-                }
             }
+            // the accumulator tile is read: release it before the stores
             tc_fence_before();
             bar_arrive(&S.aempty[ab]);
+            const int m = mt * 128 + q * 32 + lane;
+            if (m < 2 * s) {
+                float* out = g.t + ((int64_t)(p0 + (m >> 1)) * g.ldt) * 2 + (lane & 1);
+#pragma unroll
+                for (int r = 0; r < RP; ++r)
+                    if (r < g.Rd) out[2 * r] = val[r];
+            }
         }
     }
     tc_fence_before();
@@ -494,23 +495,6 @@ __global__ void __launch_bounds__(THREADS, 1) patch_apply_tc_kernel(const __grid
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-static EncodeTiled encode_fn() {
-    static std::once_flag once;
-    static EncodeTiled fn = nullptr;
-    std::call_once(once, [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiled>(p);
-    });
-    return fn;
-}
-
 }  // namespace tc
 
 bool patch_tc_supported(int device, int smax, int Rd) {
@@ -518,36 +502,25 @@ bool patch_tc_supported(int device, int smax, int Rd) {
     int major = 0, minor = 0;
     if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess) return false;
     if (cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device) != cudaSuccess) return false;
-    return major == 10 && minor == 0 && tc::encode_fn() != nullptr;
+    return major == 10 && minor == 0;
 }
 
 void patch_apply1_batch_tc(const PatchTcLaunch& L, cudaStream_t stream) {
     using namespace tc;
     if (!patch_tc_supported(L.device, L.smax, L.Rd)) throw OpemError(OPEM_ERR_UNSUPPORTED, "tensor-core block apply");
-    // the block array seen as 128-byte rows (32 floats); every block and every
-    // 16-column panel starts on a row, and the array ends on a row
-    if (L.total_f2 % 16 != 0) throw OpemError(OPEM_ERR_ARG, "block array not a whole number of 128-byte rows");
-    const int64_t rows = L.total_f2 / 16;
-    if (rows + BH >= ((int64_t)1 << 31)) throw OpemError(OPEM_ERR_UNSUPPORTED, "block array too large for the tensor map");
-    CUtensorMap map;
-    std::memset(&map, 0, sizeof(map));
-    const cuuint64_t gdim[2] = {32, (cuuint64_t)rows};
-    const cuuint64_t gstride[1] = {128};
-    const cuuint32_t box[2] = {32, (cuuint32_t)BH};
-    const cuuint32_t estride[2] = {1, 1};
-    CUresult cr = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float2*>(L.B), gdim, gstride, box,
-                              estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (cr != CUDA_SUCCESS) throw OpemError(OPEM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    // every block and every 16-column panel starts 16-byte aligned (off32 a
+    // multiple of 16 elements), and the array ends with 16 elements of slack
+    if (L.total_f2 % 16 != 0 || (reinterpret_cast<uintptr_t>(L.B) & 15))
+        throw OpemError(OPEM_ERR_ARG, "block array not 16-byte aligned with slack");
     const int RP = L.Rd <= 16 ? 16 : 32;
     const int MT = (2 * L.smax + 127) / 128;
-    const int slot_rows = ((KC * L.smax + 15) / 16 + BH - 1) / BH * BH;
     Args g;
     g.nsel = L.plist ? L.nlist : L.npatch;
     g.plist = L.plist;
+    g.B = L.B;
     g.ldt = L.ldt > 0 ? L.ldt : L.Rd;
     g.MT = MT;
-    g.slot_bytes = slot_rows * 128;
+    g.slot_bytes = (KC * L.smax * 8 + 127) / 128 * 128;
     g.xbytes = xbuf_bytes(L.smax, RP);
     int optin = 0;
     OPEM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, L.device));
@@ -575,10 +548,10 @@ void patch_apply1_batch_tc(const PatchTcLaunch& L, cudaStream_t stream) {
     // always the same device-wide value, so concurrent launches cannot lower it
     if (RP == 16) {
         OPEM_CUDA(cudaFuncSetAttribute(patch_apply_tc_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_max));
-        patch_apply_tc_kernel<16><<<grid, THREADS, smem, stream>>>(map, g);
+        patch_apply_tc_kernel<16><<<grid, THREADS, smem, stream>>>(g);
     } else {
         OPEM_CUDA(cudaFuncSetAttribute(patch_apply_tc_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_max));
-        patch_apply_tc_kernel<32><<<grid, THREADS, smem, stream>>>(map, g);
+        patch_apply_tc_kernel<32><<<grid, THREADS, smem, stream>>>(g);
     }
     OPEM_CUDA(cudaGetLastError());
 }
