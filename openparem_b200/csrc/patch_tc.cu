@@ -36,7 +36,7 @@
 //   warp 1          MMA issuer (one thread): tcgen05.mma with A (the split block
 //                   panel) in tensor memory and B (the split inputs) in shared
 //                   memory, tcgen05.commit to release each stage;
-//   warps 2-3, 20-21 input stager: a warp gathers chunks of the patch's X rows
+//   warps 2-3, 20-23 input stager: a warp gathers chunks of the patch's X rows
 //                   (one coalesced index load, then per row one coalesced load of
 //                   its Rd systems, RP lanes per row, 16 loads in flight per
 //                   lane), splits them and writes them in the canonical K-major
@@ -72,9 +72,9 @@ constexpr int AS = 4;         // tensor-memory staging slots for the split panel
 constexpr int AB_MAX = 2;     // accumulator buffers (two for up to 16 systems, one above)
 constexpr int XB = 3;         // split-input buffers
 constexpr int NS_MAX = 8;     // ring stages
-constexpr int THREADS = 704;
+constexpr int THREADS = 768;
 constexpr int W_TMA = 0, W_MMA = 1, W_CV = 4, W_EP = 12, W_X2 = 20;
-constexpr int X_WARPS = 4, X_THREADS = 128, CV_WARPS = 4, EP_THREADS = 256;
+constexpr int X_WARPS = 6, X_THREADS = 192, CV_WARPS = 4, EP_THREADS = 256;
 constexpr int X_ITERS = 16;   // row loads in flight per stager lane (a chunk is 16 x (32 / RP) rows)
 constexpr uint32_t POLL_LIMIT = 1u << 22;
 
