@@ -8,6 +8,8 @@ Tolerances
   server vs a direct FP64 sweep on the caller's stream: |dS| <= 1e-12
   server vs a direct batched (mixed) sweep: |dS| <= 1e-8 (the server caps the
       batched workspace, which may split the sweep into other batches)
+  mixed-precision requests run concurrently vs the same requests alone:
+      |dS| <= 1e-8 (same reason)
 """
 import numpy as np
 import pytest
@@ -73,6 +75,31 @@ def test_results_alone_equal_results_in_the_mix(ctx):
             assert np.abs(S - a).max() <= 1e-12, name
     finally:
         srv.close()
+
+
+def test_concurrent_mixed_requests_equal_alone(ctx):
+    """Three mixed-precision (batched sweep) requests of different orders and
+    sizes submitted at once, with no budget limit: their run intervals overlap on
+    the GPU and each S equals the same request run alone (|dS| <= 1e-8), all
+    systems converged."""
+    probs = _problems()[:3]
+    fems = [Fem3D(p, context=ctx).assemble() for _, p, _ in probs]
+    opts = default_opts(rtol=1e-10, precision=_lib.PREC_MIXED, poly_degree=8)
+    srv = Server(0, slots=3)
+    try:
+        alone = []
+        for F, (_, _, fr) in zip(fems, probs):
+            S, st, _ = srv.wait(srv.submit(F, fr, opts))
+            assert all(s["converged"] == 1 for s in st)
+            alone.append(S)
+        ids = [srv.submit(F, fr, opts) for F, (_, _, fr) in zip(fems, probs)]
+        res = [srv.wait(r) for r in ids]
+    finally:
+        srv.close()
+    assert _overlaps([r[2] for r in res]), "no two mixed requests ran at the same time"
+    for (name, _, _), a, (S, st, _) in zip(probs, alone, res):
+        assert all(s["converged"] == 1 for s in st), name
+        assert np.abs(S - a).max() <= 1e-8, name
 
 
 def test_budget_serialises_and_mixed_requests(ctx):
