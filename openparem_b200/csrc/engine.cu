@@ -774,6 +774,9 @@ using namespace opem;
 
 template <class F>
 static int guarded(Context* ctx, F&& f) {
+    // a runtime error left by an earlier, unrelated call on this thread must not
+    // be reported by this call's launch checks
+    (void)cudaGetLastError();
     try {
         f();
         return OPEM_OK;
@@ -848,6 +851,7 @@ int opem_problem_create(opem_context ctx, int64_t nverts, const double* verts, i
     auto* p = new (std::nothrow) opem_problem_s;
     if (!p) return OPEM_ERR_NOMEM;
     p->p.ctx = &ctx->c;
+    p->device = ctx->c.device;
     int rc = guarded(&ctx->c, [&] {
         OPEM_CUDA(cudaSetDevice(ctx->c.device));
         std::string err;
@@ -861,8 +865,9 @@ int opem_problem_create(opem_context ctx, int64_t nverts, const double* verts, i
 
 int opem_problem_destroy(opem_problem prob) {
     if (!prob) return OPEM_ERR_ARG;
-    cudaSetDevice(prob->p.ctx->device);
+    cudaSetDevice(prob->device);   // not through the context, which may be gone
     delete prob;
+    (void)cudaGetLastError();
     return OPEM_OK;
 }
 

@@ -188,4 +188,7 @@ int selftest_wait_timeout(Context& C, int polls);
 
 // opaque handles of the C ABI
 struct opem_context_s { opem::Context c; };
-struct opem_problem_s { opem::Problem p; };
+struct opem_problem_s {
+    opem::Problem p;
+    int device = 0;   // the context's device, kept for teardown without the context
+};

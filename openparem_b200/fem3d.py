@@ -10,6 +10,7 @@ carrying the ABI status code, the way the reference returns a PetscErrorCode
 or ``true`` on failure.
 """
 import ctypes as C
+import weakref
 
 import numpy as np
 import scipy.sparse as sp
@@ -39,12 +40,17 @@ class Context:
 
     def __init__(self, device=0):
         self.h = C.c_void_p()
+        self._problems = weakref.WeakSet()   # problems created on this context
         rc = _lib.lib().opem_context_create(int(device), C.byref(self.h))
         if rc != _lib.OK:
             raise OpemError(rc, "opem_context_create")
 
     def close(self):
+        """Destroys the context; problems created on it are closed first (a
+        problem must not outlive its context)."""
         if self.h:
+            for F in list(getattr(self, "_problems", ())):
+                F.close()
             _lib.lib().opem_context_destroy(self.h)
             self.h = C.c_void_p()
 
@@ -176,6 +182,7 @@ class Fem3D:
 
     def __init__(self, prob, context=None, device=0):
         self.ctx = context if context is not None else Context(device)
+        self.ctx._problems.add(self)
         self.prob = prob
         self._ne = len(prob["tets"])
         L = _lib.lib()
@@ -226,6 +233,7 @@ class Fem3D:
         info, freqs = project_info(proj_path, order)
         self = cls.__new__(cls)
         self.ctx = context if context is not None else Context(device)
+        self.ctx._problems.add(self)
         self.prob = None
         self.h = C.c_void_p()
         nf = C.c_int()
