@@ -54,6 +54,11 @@ def parse():
     ap.add_argument("--poly", type=int, default=16, help="GMRES-polynomial preconditioner degree of the batched path")
     ap.add_argument("--restart", type=int, default=100)
     ap.add_argument("--deflate", type=int, default=30)
+    ap.add_argument("--config", type=int, default=2, choices=[2, 3],
+                    help="2: the 24x12x60 slab guide, 51 points (headline); 3: the 40x20x100 copper-walled guide with "
+                         "per-element eps_r, 101 points")
+    ap.add_argument("--plain-points", type=int, default=0,
+                    help="points of the sweep the FP64 comparison arm solves (0: all)")
     ap.add_argument("--mesh", default="24,12,60",
                     help="hex grid nx,ny,nz of the same box/slab/ND2 problem (profiling runs use a smaller one)")
     ap.add_argument("--rtol", type=float, default=1e-10)
@@ -224,9 +229,15 @@ def run_reference(args, rank, world, budget_s=200.0):
 
 
 def config_dict(args):
-    return {"workload": "WR90 guide 24x12x60 hex (103,680 tets), eps_r 4.4/tan_d 0.02 slab, ND2 "
-                        "(681,312 DOF), 2 wave ports, 51-point 8-12 GHz sweep",
-            "order": 2, "ndof": C2_NDOF, "nnz": 28969152, "mode": args.mode,
+    if getattr(args, "config", 2) == 3:
+        wl, nd, nz = ("WR90 guide 40x20x100 hex (480,000 tets), copper walls sigma 5.8e7 with 0.5 um roughness, "
+                      "per-element eps_r ~ lognormal(ln 3, 0.1), ND2 (3,108,320 DOF), 2 wave ports, 101-point "
+                      "8-12 GHz sweep", 3108320, 133589440)
+    else:
+        wl, nd, nz = ("WR90 guide 24x12x60 hex (103,680 tets), eps_r 4.4/tan_d 0.02 slab, ND2 "
+                      "(681,312 DOF), 2 wave ports, 51-point 8-12 GHz sweep", C2_NDOF, 28969152)
+    return {"workload": wl,
+            "order": 2, "ndof": nd, "nnz": nz, "mode": args.mode, "plain_points": args.plain_points or "all",
             "step": (f"mixed: one batch of {args.batch} frequency points x 2 driving sets; plain: one point"
                      if args.mode != "plain" else "one frequency point (2 driving sets)"),
             "mesh": args.mesh, "gmres_restart": args.restart, "gmres_deflate": args.deflate, "rtol": args.rtol,
@@ -263,7 +274,9 @@ def run_ours(args, rank, world, local_rank):
     dev = local_rank
     torch.cuda.set_device(dev)
     nx, ny, nz = (int(v) for v in args.mesh.split(","))
-    if (nx, ny, nz) == (24, 12, 60):
+    if args.config == 3:
+        prob, freqs = meshgen.config3()
+    elif (nx, ny, nz) == (24, 12, 60):
         prob, freqs = meshgen.config2()
     else:
         prob = meshgen.waveguide_problem(meshgen.WR_A, meshgen.WR_B, 50e-3, nx, ny, nz, 2,
@@ -325,9 +338,12 @@ def run_ours(args, rank, world, local_rank):
         if mode == modes[0]:
             steps, warm = args.steps, args.warmup
         else:
-            # the FP64 comparison arm solves every point of this rank's sweep, so
-            # |dS| mixed vs FP64 is stated for every result
+            # the FP64 comparison arm solves every point of this rank's sweep (or
+            # --plain-points of them, spread over it), so |dS| mixed vs FP64 is
+            # stated for those results
             steps, warm = len(my_freqs), 1
+            if args.plain_points and args.plain_points < len(my_freqs):
+                steps = args.plain_points
         for i in range(warm):
             note(f"{mode} warmup {i}")
             if mode == "mixed":
@@ -353,7 +369,11 @@ def run_ours(args, rank, world, local_rank):
                     for f, Sf in zip(fr, S):
                         Sd[float(f)] = Sf
                 else:
-                    f = float(my_freqs[i % len(my_freqs)]) if "mixed" in res else my_freqs[(warm + i) % len(my_freqs)]
+                    if "mixed" in res:
+                        stride = max(1, len(my_freqs) // steps)
+                        f = float(my_freqs[(i * stride) % len(my_freqs)])
+                    else:
+                        f = my_freqs[(warm + i) % len(my_freqs)]
                     S, st, wall = plain_step(f)
                     dev_s.append(st["seconds"])
                     wall_s.append(wall)

@@ -7,8 +7,10 @@
 // preconditioned by overlapping vertex-patch block Jacobi (additive Schwarz
 // on the dofs of each vertex star), which keeps the discrete-gradient kernel
 // of curl-curl local to each block.  Orthogonalisation is classical Gram-
-// Schmidt with one reorthogonalisation (CGS2); the Hessenberg least-squares
-// (Givens rotations, back substitution) runs on the device in FP64.
+// Schmidt with one reorthogonalisation (CGS2).  The small (m+1) x m Hessenberg
+// least-squares problem (Givens rotations, back substitution) and the harmonic
+// Ritz eigenproblem of each restart run on the host in FP64 (dense.cpp), one
+// Hessenberg column copied back per Arnoldi step.
 #include <algorithm>
 #include <cmath>
 
