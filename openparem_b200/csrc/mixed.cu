@@ -565,24 +565,25 @@ __global__ void blocks_to_f32_colmajor_kernel(int npatch, const int32_t* __restr
     }
 }
 
-// y[:, r0 + l] = sum over the patch entries of each DOF of t (row stride ldt), for
-// the Rd systems of driving set d (Dirichlet rows zero)
-__global__ void patch_apply2_batch_kernel(int64_t n, const int32_t* __restrict__ d2p_ptr,
-                                          const int32_t* __restrict__ d2p_idx, const float2* __restrict__ t, int ldt,
-                                          int R, int r0, int Rd, const uint8_t* __restrict__ pec,
-                                          const uint8_t* __restrict__ pm, int d, float2* __restrict__ y) {
-    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (e >= n * Rd) return;
-    int64_t i = e / Rd;
-    int l = (int)(e % Rd);
+// y[i, r] = sum over the patch entries of DOF i of t (row stride R), for every
+// system r; system r belongs to driving set dsys[r] (its Dirichlet rows zero).
+// One launch for all systems, every thread group reading whole R-system rows of t.
+__global__ void patch_sum_all_kernel(int64_t n, const int32_t* __restrict__ d2p_ptr,
+                                     const int32_t* __restrict__ d2p_idx, const float2* __restrict__ t, int R,
+                                     const uint8_t* __restrict__ pec, const uint8_t* __restrict__ pm,
+                                     const uint8_t* __restrict__ dsys, float2* __restrict__ y) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n * R) return;
+    const int64_t i = e / R;
+    const int r = (int)(e - i * R);
     float re = 0.f, im = 0.f;
-    if (!(pec[i] || ((pm[i] >> d) & 1)))
+    if (!(pec[i] || ((pm[i] >> dsys[r]) & 1)))
         for (int32_t q = d2p_ptr[i]; q < d2p_ptr[i + 1]; ++q) {
-            float2 v = t[(int64_t)d2p_idx[q] * ldt + l];
+            const float2 v = t[(int64_t)d2p_idx[q] * R + r];
             re += v.x;
             im += v.y;
         }
-    y[i * R + r0 + l] = make_float2(re, im);
+    y[e] = make_float2(re, im);
 }
 
 // ---------------------------------------------------------------------------
@@ -1469,14 +1470,10 @@ static void patch_apply_batch(Batch& B, const std::vector<PatchSet32>& sets, DBu
             patch_apply1_batch(P, B.s, sets[d], x_il, R, B.r0[d], B.Rd[d], t.p + B.r0[d], B.err.p, PA_AUTO, all);
         }
     }
-    for (int d = 0; d < B.N; ++d) {
-        if (B.Rd[d] == 0) continue;
-        int64_t work = B.n * B.Rd[d];
-        patch_apply2_batch_kernel<<<(unsigned)((work + 255) / 256), 256, 0, B.s>>>(
-            B.n, P.d_d2p_ptr.p, P.d_d2p_idx.p, t.p + B.r0[d], R, B.R, B.r0[d], B.Rd[d], P.d_pec.p, P.d_portmask.p, d,
-            y_il);
-        ++P.ctx->launches;
-    }
+    const int64_t work = B.n * R;
+    patch_sum_all_kernel<<<(unsigned)((work + 255) / 256), 256, 0, B.s>>>(
+        B.n, P.d_d2p_ptr.p, P.d_d2p_idx.p, t.p, R, P.d_pec.p, P.d_portmask.p, B.dsys.p, y_il);
+    ++P.ctx->launches;
     OPEM_CUDA(cudaGetLastError());
 }
 
@@ -2216,7 +2213,7 @@ void solve_sweep_mixed(Problem& P, int nfreq, const double* freqs, const opem_so
 //   k = 1  batched SpMV, FP32 operators and vectors (polynomial products)
 //   k = 2  batched SpMV, FP64 operators, FP32 vectors
 //   k = 3  batched SpMV, FP64 operators and vectors (Arnoldi products)
-//   k = 4  patch sum of the block apply (patch_apply2_batch_kernel)
+//   k = 4  patch sum of the block apply (patch_sum_all_kernel)
 // The SpMV entries include the boundary-group kernels of the same product.
 void profile_batch(Problem& P, double f, int R, int reps, double* out, int nout) {
     if (R < 1 || R > RMAX) throw OpemError(OPEM_ERR_ARG, "profile_batch: 1 <= nsys <= 32");
@@ -2281,8 +2278,8 @@ void profile_batch(Problem& P, double f, int R, int reps, double* out, int nout)
     out[9] = timeit([&] { spmv_batch<double2, double>(B, P.d_K.p, P.d_Meps.p, Mt, Ms, B.vc64.p, bp64, x64.p, y64.p); });
     out[10] = ebe ? ebe_bytes(16) : csr + nnz * 8.0 * nops + 2.0 * nR * 16;
     out[12] = timeit([&] {
-        patch_apply2_batch_kernel<<<(unsigned)((nR + 255) / 256), 256, 0, B.s>>>(
-            n, P.d_d2p_ptr.p, P.d_d2p_idx.p, t.p, R, R, 0, R, P.d_pec.p, P.d_portmask.p, 0, y32.p);
+        patch_sum_all_kernel<<<(unsigned)((nR + 255) / 256), 256, 0, B.s>>>(
+            n, P.d_d2p_ptr.p, P.d_d2p_idx.p, t.p, R, P.d_pec.p, P.d_portmask.p, B.dsys.p, y32.p);
         ++P.ctx->launches;
     });
     out[13] = (double)sum_s * (R * 8 + 4) + 4.0 * (n + 1) + 2.0 * n + nR * 8.0;
