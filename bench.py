@@ -34,8 +34,8 @@ C2_NDOF = 681312
 # ncu dram__bytes_read+write / algorithmic bytes of the FP64 block apply, measured on the
 # 16x8x40-hex ND2 case (traffic grows with the patches, so the ratio carries to 24x12x60)
 TRAFFIC_RATIO_PATCH = 726.0 / 727.1
-# the same for the batched block apply, 13 systems, 16x8x40-hex ND2 case
-TRAFFIC_RATIO_PATCH_BATCH = (376.8448 + 43.41632) / 459.063756
+# the same for the batched block apply (tensor-core kernel, 26 systems), 16x8x40-hex ND2 case
+TRAFFIC_RATIO_PATCH_BATCH = (396.159488 + 83.910656) / 561.419724
 # nominal FP32 FMA rate: 148 SMs x 128 lanes x 2 flops x 1.965 GHz
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 BATCH_KERNELS = ["patch_apply1_batch", "spmv_batch_f32", "spmv_batch_f64op_f32vec", "spmv_batch_f64",
