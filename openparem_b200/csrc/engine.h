@@ -168,7 +168,10 @@ void spmv_complex(Problem& P, const double2* A, const double2* x, double2* y, co
 void profile_fp64(Problem& P, const double2* A, const uint8_t* dmask, int reps, double* out);
 void profile_batch(Problem& P, double f, int R, int reps, double* out, int nout);
 void check_block_apply(Problem& P, double f, int R, int r0, int Rd, double* out);
-void patch_blocks_fp64(Problem& P, const double2* A, const uint8_t* dmask, DBuf<double2>& B);
+// Inverted FP64 vertex-patch blocks of A (Dirichlet rows/columns from dmask); with
+// plist, only the nlist listed patches are computed (the others are left as they are).
+void patch_blocks_fp64(Problem& P, const double2* A, const uint8_t* dmask, DBuf<double2>& B,
+                       const int32_t* plist = nullptr, int nlist = 0);
 
 // ---- engine helpers shared with the mixed path (engine.cu)
 void make_dmask(Problem& P, int d, uint8_t* dm);

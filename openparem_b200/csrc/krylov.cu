@@ -387,8 +387,9 @@ __device__ inline int32_t find_col(const int32_t* __restrict__ c, int32_t lo, in
 __global__ void patch_extract_kernel(int npatch, const int32_t* __restrict__ pptr, const int32_t* __restrict__ pdofs,
                                      const int64_t* __restrict__ poff, const int32_t* __restrict__ rowptr,
                                      const int32_t* __restrict__ cols, const double2* __restrict__ A,
-                                     const uint8_t* __restrict__ dmask, double2* __restrict__ B) {
-    int v = blockIdx.x;
+                                     const uint8_t* __restrict__ dmask, double2* __restrict__ B,
+                                     const int32_t* __restrict__ plist) {
+    int v = plist ? plist[blockIdx.x] : blockIdx.x;   // plist: only the listed patches
     if (v >= npatch) return;
     int32_t p0 = pptr[v];
     int s = pptr[v + 1] - p0;
@@ -411,13 +412,14 @@ __global__ void patch_extract_kernel(int npatch, const int32_t* __restrict__ ppt
 // The block is staged in shared memory when it fits, otherwise worked on in
 // global memory (L2 resident).
 __global__ void patch_invert_kernel(int npatch, const int32_t* __restrict__ pptr, const int64_t* __restrict__ poff,
-                                    double2* __restrict__ B, int smem_max_s, int* __restrict__ status) {
+                                    double2* __restrict__ B, int smem_max_s, int* __restrict__ status,
+                                    const int32_t* __restrict__ plist) {
     extern __shared__ double2 sm[];
     __shared__ int piv_row;
     __shared__ double piv_abs[32];
     __shared__ int piv_idx[32];
     __shared__ int ipiv[512];
-    int v = blockIdx.x;
+    int v = plist ? plist[blockIdx.x] : blockIdx.x;   // plist: only the listed patches
     if (v >= npatch) return;
     int s = pptr[v + 1] - pptr[v];
     double2* G = B + poff[v];
@@ -616,7 +618,8 @@ struct PatchPrec {
     DBuf<int> status;
 };
 
-static void patch_setup(Problem& P, PatchPrec& pc, const double2* A, const uint8_t* dmask) {
+static void patch_setup(Problem& P, PatchPrec& pc, const double2* A, const uint8_t* dmask,
+                        const int32_t* plist = nullptr, int nlist = 0) {
     cudaStream_t s = P.ctx->stream;
     const Topology& T = P.topo;
     size_t tot = (size_t)T.patch_off.back();
@@ -624,8 +627,10 @@ static void patch_setup(Problem& P, PatchPrec& pc, const double2* A, const uint8
     if (pc.t.n < T.patch_dofs.size()) pc.t.alloc(T.patch_dofs.size());
     if (pc.status.n < 1) pc.status.alloc(1);
     pc.status.zero(s);
-    patch_extract_kernel<<<P.npatch, 256, 0, s>>>(P.npatch, P.d_patch_ptr.p, P.d_patch_dofs.p, P.d_patch_off.p,
-                                                  P.d_rowptr.p, P.d_cols.p, A, dmask, pc.B.p); ++P.ctx->launches;
+    const unsigned grid = plist ? (unsigned)nlist : (unsigned)P.npatch;
+    if (grid == 0) return;
+    patch_extract_kernel<<<grid, 256, 0, s>>>(P.npatch, P.d_patch_ptr.p, P.d_patch_dofs.p, P.d_patch_off.p,
+                                              P.d_rowptr.p, P.d_cols.p, A, dmask, pc.B.p, plist); ++P.ctx->launches;
     OPEM_CUDA(cudaGetLastError());
     int smax = 0;
     size_t smem = 0;
@@ -639,14 +644,16 @@ static void patch_setup(Problem& P, PatchPrec& pc, const double2* A, const uint8
     // every call (concurrent problems with other patch sizes must not lower it)
     OPEM_CUDA(cudaFuncSetAttribute(patch_invert_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)budget));
     if (T.max_patch > 512) throw OpemError(OPEM_ERR_UNSUPPORTED, "vertex patch larger than 512 dofs");
-    patch_invert_kernel<<<P.npatch, 256, smem, s>>>(P.npatch, P.d_patch_ptr.p, P.d_patch_off.p, pc.B.p, smax, pc.status.p); ++P.ctx->launches;
+    patch_invert_kernel<<<grid, 256, smem, s>>>(P.npatch, P.d_patch_ptr.p, P.d_patch_off.p, pc.B.p, smax, pc.status.p,
+                                                plist); ++P.ctx->launches;
     OPEM_CUDA(cudaGetLastError());
 }
 
 // FP64 inverted vertex-patch blocks of A (for the mixed path, which rounds them to FP32).
-void patch_blocks_fp64(Problem& P, const double2* A, const uint8_t* dmask, DBuf<double2>& B) {
+void patch_blocks_fp64(Problem& P, const double2* A, const uint8_t* dmask, DBuf<double2>& B, const int32_t* plist,
+                       int nlist) {
     PatchPrec pc;
-    patch_setup(P, pc, A, dmask);
+    patch_setup(P, pc, A, dmask, plist, nlist);
     B = std::move(pc.B);
 }
 

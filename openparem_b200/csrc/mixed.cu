@@ -553,8 +553,9 @@ static inline int patch_rc(int Rd) {
 // FP64 row-major blocks -> FP32 column-major blocks at off32 (one CTA per patch)
 __global__ void blocks_to_f32_colmajor_kernel(int npatch, const int32_t* __restrict__ pptr,
                                               const int64_t* __restrict__ poff, const int64_t* __restrict__ off32,
-                                              const double2* __restrict__ in, float2* __restrict__ out) {
-    const int v = blockIdx.x;
+                                              const double2* __restrict__ in, float2* __restrict__ out,
+                                              const int32_t* __restrict__ plist) {
+    const int v = plist ? plist[blockIdx.x] : blockIdx.x;   // plist: only the listed patches
     const int s = pptr[v + 1] - pptr[v];
     const double2* src = in + poff[v];
     float2* dst = out + off32[v];
@@ -1184,8 +1185,10 @@ static std::vector<int64_t> block_offsets32(const Topology& T) {
     return off;
 }
 
-// FP32 block-Jacobi blocks for driving set d at frequency f (FP64 inversion, then rounded)
-static void build_patchset(Batch& B, double f, int d, PatchSet32& ps) {
+// FP32 block-Jacobi blocks for driving set d at frequency f (FP64 inversion, then
+// rounded).  With `port_only`, only the patches that touch a port face are built:
+// the others are the same for every driving set and are read from another set.
+static void build_patchset(Batch& B, double f, int d, PatchSet32& ps, bool port_only = false) {
     Problem& P = B.P;
     const int64_t nnz = (int64_t)P.topo.cols.size();
     DBuf<double2> A(nnz);
@@ -1195,16 +1198,20 @@ static void build_patchset(Batch& B, double f, int d, PatchSet32& ps) {
     system_coefficients(P, f, d, vc, bc);
     form_system_matrix(P, vc, bc, A.p);
     make_dmask(P, d, dm.p);
+    const int32_t* plist = port_only ? P.d_plist_port.p : nullptr;
+    const int nlist = port_only ? P.n_plist_port : P.npatch;
     DBuf<double2> B64;
-    patch_blocks_fp64(P, A.p, dm.p, B64);
+    patch_blocks_fp64(P, A.p, dm.p, B64, plist, port_only ? nlist : 0);
     std::vector<int64_t> off = block_offsets32(P.topo);
     ps.B.alloc((size_t)off.back());
     OPEM_CUDA(cudaMemsetAsync(ps.B.p, 0, ps.B.bytes(), B.s));
     off.pop_back();
     ps.off32.upload(off, B.s);
-    blocks_to_f32_colmajor_kernel<<<P.npatch, 256, 0, B.s>>>(P.npatch, P.d_patch_ptr.p, P.d_patch_off.p, ps.off32.p,
-                                                            B64.p, ps.B.p);
-    ++P.ctx->launches;
+    if (nlist > 0) {
+        blocks_to_f32_colmajor_kernel<<<nlist, 256, 0, B.s>>>(P.npatch, P.d_patch_ptr.p, P.d_patch_off.p, ps.off32.p,
+                                                              B64.p, ps.B.p, plist);
+        ++P.ctx->launches;
+    }
     OPEM_CUDA(cudaStreamSynchronize(B.s));
 }
 
@@ -1973,8 +1980,15 @@ static void solve_batch(Problem& P, const std::vector<System>& systems, const op
         for (auto& sy : systems) { lo = std::min(lo, sy.freq); hi = std::max(hi, sy.freq); }
         fmid = 0.5 * (lo + hi);
     }
+    // the first active driving set gets every block; the others only those of the
+    // patches touching a port face (patch_apply_batch reads the rest from the first)
+    ensure_patch_lists(P, B.s);
+    int first = -1;
     for (int d = 0; d < N; ++d)
-        if (B.Rd[d] > 0) build_patchset(B, fmid, d, sets[d]);
+        if (B.Rd[d] > 0) {
+            build_patchset(B, fmid, d, sets[d], first >= 0 && P.n_plist_shared > 0);
+            if (first < 0) first = d;
+        }
     // right-hand sides b_r = -(A_r x0_r) with Dirichlet rows 0  (FP64)
     DBuf<double2> x0(nR), x0_il(nR), y_il(nR), b(nR), x(nR), r64(nR);
     const unsigned gy = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, P.ctx->sm_count * 2));
