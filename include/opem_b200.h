@@ -259,6 +259,16 @@ int  opem_write_touchstone(const char* path, int nfreq, const double* freqs, int
  * (Zo = 2 zref).  Zo_out (nports complex, may be NULL) receives the new impedances.  */
 int  opem_s_mixed_mode(int nports, const double* S, int npairs, const int* pairs, double zref, double* S_out,
                        double* Zo_out);
+/* Modal to single-ended conversion (fem3D::build_Mc_Ms with conversion 0,
+ * fem3D.cpp:1586-1900; Result::SparameterConversion, results.cpp:587-630): S the
+ * modal S-parameters (nports x nports complex, row = portOut), Zmode the modes'
+ * impedances (nports complex), Tv and Ti (nports x nports complex, row-major) the
+ * maps from single-ended line voltages / currents to modal ones, each port's block
+ * on the diagonal in S-port order (the Tv, Ti a multi-conductor port's 2D solve
+ * gives).  S_out: single-ended S at zref on every S-port; Zo_out (may be NULL) = zref.
+ * OPEM_ERR_BREAKDOWN if Tv, Ti or Ms + Mc S is singular.                         */
+int  opem_s_single_ended(int nports, const double* S, const double* Zmode, const double* Tv, const double* Ti,
+                         double zref, double* S_out, double* Zo_out);
 /* Touchstone 2.0 (the reference's mixed-mode writer, results.cpp:1210-1372): as
  * opem_write_touchstone plus the 2.0 keywords and, with pairs, [Mixed-Mode Order]. */
 int  opem_write_touchstone2(const char* path, int nfreq, const double* freqs, int nports, const double* S,

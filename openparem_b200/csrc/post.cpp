@@ -158,6 +158,50 @@ int opem_s_mixed_mode(int nports, const double* S, int npairs, const int* pairs,
     return OPEM_OK;
 }
 
+// Modal to single-ended conversion, fem3D::build_Mc_Ms with conversion = 0
+// (src/OpenParEM3D/fem3D.cpp:1586-1900) and Result::SparameterConversion
+// (results.cpp:587-630): S holds the modal S-parameters of the ports' modes
+// (S-port order), Zmode their impedances; Tv and Ti map the single-ended line
+// voltages / currents of each port to its modal ones (the port's Tv, Ti
+// blocks on the diagonal, S-port order).  Kv = Tv^-1, Ki = Ti^-1 take modal to
+// single-ended; za = Zmode, zb = zref on every S-port; then term1, term2, Ms,
+// Mc and S_b as in the mixed-mode conversion above.
+int opem_s_single_ended(int nports, const double* S, const double* Zmode, const double* Tv, const double* Ti,
+                        double zref, double* S_out, double* Zo_out) {
+    if (nports < 1 || !S || !Zmode || !Tv || !Ti || !(zref > 0) || !S_out) return OPEM_ERR_ARG;
+    const int n = nports;
+    std::vector<cd> Kv((size_t)n * n), Ki((size_t)n * n), rza(n);
+    for (int i = 0; i < n * n; ++i) {
+        Kv[i] = cd(Tv[2 * i], Tv[2 * i + 1]);
+        Ki[i] = cd(Ti[2 * i], Ti[2 * i + 1]);
+    }
+    if (!invert(n, Kv) || !invert(n, Ki)) return OPEM_ERR_BREAKDOWN;
+    for (int j = 0; j < n; ++j) {
+        const cd z(Zmode[2 * j], Zmode[2 * j + 1]);
+        if (!(std::abs(z) > 0)) return OPEM_ERR_ARG;
+        rza[j] = std::sqrt(z);
+    }
+    const double rzb = std::sqrt(zref);
+    std::vector<cd> Ms((size_t)n * n), Mc((size_t)n * n);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            const cd t1 = Kv[(size_t)i * n + j] * rza[j] / rzb;
+            const cd t2 = Ki[(size_t)i * n + j] * rzb / rza[j];
+            Ms[(size_t)i * n + j] = 0.5 * (t1 + t2);
+            Mc[(size_t)i * n + j] = 0.5 * (t1 - t2);
+        }
+    std::vector<cd> Sa((size_t)n * n);
+    for (int i = 0; i < n * n; ++i) Sa[i] = cd(S[2 * i], S[2 * i + 1]);
+    std::vector<cd> num = matmul(n, Ms, Sa), den = matmul(n, Mc, Sa);
+    for (int i = 0; i < n * n; ++i) { num[i] += Mc[i]; den[i] += Ms[i]; }
+    if (!invert(n, den)) return OPEM_ERR_BREAKDOWN;
+    std::vector<cd> Sb = matmul(n, num, den);
+    for (int i = 0; i < n * n; ++i) { S_out[2 * i] = Sb[i].real(); S_out[2 * i + 1] = Sb[i].imag(); }
+    if (Zo_out)
+        for (int i = 0; i < n; ++i) { Zo_out[2 * i] = zref; Zo_out[2 * i + 1] = 0.0; }
+    return OPEM_OK;
+}
+
 // Touchstone 2.0 (the reference's saveTouchstone branch for mixed-mode data,
 // results.cpp:1210-1372): "[Version] 2.0", the option line, "[Number of Ports]",
 // "[Two-Port Data Order] 21_12" for two ports, "[Number of Frequencies]",

@@ -3,9 +3,11 @@
 // materials (mesh.cpp:449-588), the ports file (Path / Port / Boundary blocks,
 // port.cpp:6369-7078) and the materials databases (OpenParEMmaterials.cpp),
 // turned into the inputs of opem_problem_create / set_regions / set_boundary /
-// set_port_te.  Supported subset: rectangular ports driven by their TE10 mode
-// (the wide side of the port rectangle is the mode's a dimension; the voltage
-// integration path of the port's Line block sets the mode voltage), boundary
+// set_port_te.  Supported subset: ports on any planar closed path; a rectangle
+// whose faces see one material is driven by its TE10 mode (the wide side is
+// the mode's a dimension), every other port by the fundamental mode of its own
+// faces (set_port_fem2d); the voltage integration path of the port's Line
+// block sets the mode voltage; boundary
 // types surface_impedance, perfect_electric_conductor, perfect_magnetic_conductor
 // and radiation, frequency plans of point / linear / log entries (and their
 // .refine forms).
@@ -294,6 +296,18 @@ struct Poly {
     }
 };
 
+// four corners with right angles (within tol of the longer side)
+bool is_rectangle(const std::vector<V3>& pts, double tol) {
+    if (pts.size() != 4) return false;
+    for (int i = 0; i < 4; ++i) {
+        const V3 e1 = sub(pts[(i + 1) % 4], pts[i]), e2 = sub(pts[(i + 3) % 4], pts[i]);
+        const double l1 = norm(e1), l2 = norm(e2);
+        if (!(l1 > 0 && l2 > 0)) return false;
+        if (std::fabs(dot(e1, e2)) > tol * std::max(l1, l2)) return false;
+    }
+    return true;
+}
+
 void build(const std::string& proj_path, int order_override, Project& P) {
     const size_t sl = proj_path.find_last_of('/');
     P.dir = sl == std::string::npos ? std::string() : proj_path.substr(0, sl);
@@ -386,11 +400,13 @@ void build(const std::string& proj_path, int order_override, Project& P) {
     read_ports(join(P.dir, kv1(P, "port.definition.file")), paths, ports, bdrs);
     std::sort(ports.begin(), ports.end(), [](const PortDef& a, const PortDef& b) { return a.sport < b.sport; });
     std::vector<Poly> port_poly;
+    std::vector<int> port_rect;   // 1: a rectangle (driven by TE10 where its faces see one material)
     for (auto& pd : ports) {
         bool closed = false;
         auto pts = path_points(paths, pd.path, &closed);
-        if (!closed || pts.size() != 4) throw std::runtime_error("port " + pd.name + ": only rectangular ports are supported");
+        if (!closed) throw std::runtime_error("port " + pd.name + ": the port path must be closed");
         port_poly.emplace_back(pts, tol);
+        port_rect.push_back(is_rectangle(pts, tol) ? 1 : 0);
     }
     std::vector<std::vector<Poly>> bdr_poly(bdrs.size());
     for (size_t j = 0; j < bdrs.size(); ++j)
@@ -425,14 +441,34 @@ void build(const std::string& proj_path, int order_override, Project& P) {
         else if (a < 2 + np) ++P.n_port_faces;
         else ++P.n_bdr_faces;
     }
-    // port modes: TE10 on the port rectangle, a along the wide side, outward normal
+    // port frames: on a rectangle TE10's, a along the wide side; on any other
+    // polygon u along its first edge, v in its plane, a x b its bounding box
+    // in (u, v); outward normal
     for (int p = 0; p < np; ++p) {
         if (port_opp[p] < 0) throw std::runtime_error("port " + ports[p].name + " covers no boundary face");
         auto pts = path_points(paths, ports[p].path);
-        V3 o = pts[0], e1 = sub(pts[1], pts[0]), e2 = sub(pts[3], pts[0]);
-        if (norm(e2) > norm(e1)) std::swap(e1, e2);
-        const double a = norm(e1), b = norm(e2);
-        const V3 u = scale(e1, 1.0 / a), v = scale(e2, 1.0 / b);
+        V3 o = pts[0], u, v;
+        double a, b;
+        if (port_rect[p]) {
+            V3 e1 = sub(pts[1], pts[0]), e2 = sub(pts[3], pts[0]);
+            if (norm(e2) > norm(e1)) std::swap(e1, e2);
+            a = norm(e1);
+            b = norm(e2);
+            u = scale(e1, 1.0 / a);
+            v = scale(e2, 1.0 / b);
+        } else {
+            const Poly& pg = port_poly[p];
+            u = pg.u;
+            v = pg.v;
+            double lo_u = 1e300, hi_u = -1e300, lo_v = 1e300, hi_v = -1e300;
+            for (auto& q : pg.q) {
+                lo_u = std::min(lo_u, q[0]); hi_u = std::max(hi_u, q[0]);
+                lo_v = std::min(lo_v, q[1]); hi_v = std::max(hi_v, q[1]);
+            }
+            for (int i = 0; i < 3; ++i) o[i] = pg.o[i] + lo_u * u[i] + lo_v * v[i];   // bounding-box corner
+            a = hi_u - lo_u;
+            b = hi_v - lo_v;
+        }
         V3 n = cross(u, v);
         if (dot(sub(vtx(port_opp[p]), vtx(port_face0[p])), n) > 0) n = scale(n, -1.0);   // point out of the mesh
         std::array<double, 22> d{};
@@ -451,8 +487,9 @@ void build(const std::string& proj_path, int order_override, Project& P) {
         // a port whose faces see more than one material is driven by its own 2D
         // mode (as the reference drives every port), with second-order 2D elements
         // on a split that keeps the 2D mesh near 1024 triangles
+        // (and every port that is not a rectangle, which has no analytic mode here)
         const int nsub = (int)std::lround(std::sqrt(1024.0 / (double)std::max<int64_t>(1, port_nface[p])));
-        P.port_nsub.push_back(port_mixed[p] ? std::min(16, std::max(1, nsub)) : 0);
+        P.port_nsub.push_back(port_mixed[p] || !port_rect[p] ? std::min(16, std::max(1, nsub)) : 0);
     }
     // boundary conditions: attribute 1 the faces no port or Boundary block claims
     // (PEC, or the surface impedance of materials.default.boundary, as

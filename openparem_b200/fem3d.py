@@ -453,6 +453,26 @@ def mixed_mode(S, pairs, zref=50.0):
     return out, zo
 
 
+def single_ended(S, Zmode, Tv, Ti, zref=50.0):
+    """Single-ended S at zref of modal S (N, N) (opem_s_single_ended): Zmode (N,)
+    the modes' impedances, Tv and Ti (N, N) the single-ended -> modal voltage and
+    current maps (each port's block on the diagonal, S-port order)."""
+    S = np.ascontiguousarray(S, dtype=np.complex128)
+    n = S.shape[0]
+    zm = np.ascontiguousarray(Zmode, dtype=np.complex128)
+    tv = np.ascontiguousarray(Tv, dtype=np.complex128)
+    ti = np.ascontiguousarray(Ti, dtype=np.complex128)
+    if zm.shape != (n,) or tv.shape != (n, n) or ti.shape != (n, n):
+        raise OpemError(_lib.ERR_ARG, "single_ended: shapes")
+    out = np.zeros((n, n), dtype=np.complex128)
+    rc = _lib.lib().opem_s_single_ended(n, _dp(S.view(np.float64).ravel()), _dp(zm.view(np.float64).ravel()),
+                                        _dp(tv.view(np.float64).ravel()), _dp(ti.view(np.float64).ravel()),
+                                        float(zref), _dp(out.view(np.float64).ravel()), None)
+    if rc != _lib.OK:
+        raise OpemError(rc, "opem_s_single_ended")
+    return out
+
+
 def write_touchstone2(path, freqs, S, zref=50.0, fmt="RI", unit="GHz", pairs=()):
     """Touchstone 2.0 file (opem_write_touchstone2); pairs mark mixed-mode S-ports."""
     freqs = np.ascontiguousarray(freqs, dtype=np.float64)

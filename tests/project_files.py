@@ -168,3 +168,29 @@ def write_guide_project(d, nx=6, ny=3, nz=15, L=50e-3, order=1, copper_wall=Fals
         f.write("frequency.plan.linear          9e9,11e9,1e9\nfrequency.plan.point           10.5e9\n")
         f.write("frequency.plan.point           10e9\nsolution.3D.tolerance          1e-10\n")
     return proj
+
+
+def write_lguide_project(d, nx=6, ny=4, nz=10, L=40e-3, order=1, freqs=(8e9, 8.5e9)):
+    """An air-filled guide of L-shaped cross-section (the a x b = 24 x 16 mm box
+    without its x > 0, y > 0 quadrant, whole Kuhn hexes removed), length L, as a
+    project in directory d: the port paths are the six-point L outline at z = 0
+    and z = L, the voltage paths cross the tall arm at x = -a/4.  Returns the
+    .proj path."""
+    a, b = 24e-3, 16e-3
+    verts, tets = meshgen.box_kuhn(a, b, L, nx, ny, nz)
+    cen = verts[tets].mean(axis=1)
+    tets = tets[~((cen[:, 0] > 0) & (cen[:, 1] > 0))]
+    used = np.unique(tets)
+    remap = -np.ones(len(verts), dtype=np.int64)
+    remap[used] = np.arange(len(used))
+    verts, tets = verts[used], remap[tets]
+    outline = [(-a / 2, -b / 2), (a / 2, -b / 2), (a / 2, 0.0), (0.0, 0.0), (0.0, b / 2), (-a / 2, b / 2)]
+    spec = {"paths": [], "boundaries": [], "ports": []}
+    for k, z in ((1, 0.0), (2, L)):
+        spec["paths"].append({"name": f"port{k}", "points": [(x, y, z) for x, y in outline], "closed": True})
+        spec["paths"].append({"name": f"V{k}", "points": [(-a / 4, -b / 2, z), (-a / 4, b / 2, z)], "closed": False})
+        spec["ports"].append({"name": str(k), "paths": [f"+port{k}"], "impedance_definition": "PV",
+                              "impedance_calculation": "line",
+                              "lines": [{"Sport": k, "integration": [{"type": "voltage", "paths": [f"+V{k}"]}]}]})
+    return write_project(d, "lguide", verts, tets, 1, {1: "air"}, spec,
+                         {"air": {"er": 1.0, "mur": 1.0, "tand": 0.0, "Rz": 0.0}}, order, list(freqs))

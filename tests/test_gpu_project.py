@@ -96,3 +96,26 @@ def test_default_copper_walls_project_matches_oracle(tmp_path):
     assert st["converged"] == 1
     ref = fem.solve_frequency(fem.Operators(prob), fr[0])["S"]
     assert np.abs(S - ref).max() <= 1e-8
+
+
+def test_polygon_port_project_matches_oracle(tmp_path):
+    """A guide of L-shaped cross-section whose port paths are six-point
+    outlines: the reader drives both ports by their own 2D modes.  ND1 on the
+    device, plain FP64 and the batched mixed sweep, against the oracle on the
+    problem the same reader produced (|dS| <= 1e-8 plain with solver rtol
+    1e-12; <= 1e-6 mixed); the straight guide passes the wave (|S21| > 0.99)."""
+    from oracle import fem
+    from openparem_b200 import _lib
+    from openparem_b200.fem3d import project_problem
+    from project_files import write_lguide_project
+    proj = write_lguide_project(str(tmp_path))
+    F, fr = Fem3D.from_project(proj, context=Context(0))
+    F.assemble()
+    prob, _ = project_problem(proj)
+    ref = fem.solve_frequency(fem.Operators(prob), fr[0])["S"]
+    S, _, st = F.solve(fr[0], default_opts(rtol=1e-12, restart=200, maxits=6000, h_rtol=1e-13))
+    assert st["converged"] == 1
+    assert np.abs(S - ref).max() <= 1e-8, (S, ref)
+    assert abs(S[1, 0]) > 0.99
+    Sm, _ = F.sweep([fr[0]], default_opts(precision=_lib.PREC_MIXED, rtol=1e-10))
+    assert np.abs(Sm[0] - ref).max() <= 1e-6

@@ -101,3 +101,22 @@ def test_frequency_plan_duplicates_and_integer_points_per_decade(tmp_path):
         f.write("frequency.plan.log             1e9,1e10,2.5\n")
     with pytest.raises(Exception):
         project_info(proj2)
+
+
+def test_polygon_port_paths(tmp_path):
+    """Port paths that are not rectangles (the six-point outline of an L-shaped
+    guide) are read: their faces are the port's, and the port is driven by the
+    fundamental mode of its own faces, with an outward normal."""
+    from openparem_b200.fem3d import project_problem
+    from project_files import write_lguide_project
+    proj = write_lguide_project(str(tmp_path))
+    info, fr = project_info(proj)
+    assert info["tets"] == 1080 and info["ports"] == 2
+    assert info["port_faces"] == 2 * 18 * 2                 # 3/4 of the 6 x 4 cross-section, two triangles a quad
+    assert info["pec_faces"] == info["exterior_faces"] - info["port_faces"]
+    prob, _ = project_problem(proj)
+    modes = [p["mode"] for p in prob["ports"]]
+    assert [m["kind"] for m in modes] == ["FEM2D", "FEM2D"] and all(m["nsub"] > 0 for m in modes)
+    assert np.allclose(modes[0]["normal"], [0, 0, -1]) and np.allclose(modes[1]["normal"], [0, 0, 1])
+    assert np.allclose([modes[0]["a"], modes[0]["b"]], [24e-3, 16e-3])   # the outline's bounding box
+    assert np.allclose(modes[1]["vpath"][0], [-6e-3, -8e-3, 40e-3])
