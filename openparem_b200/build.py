@@ -9,7 +9,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libopem_b200.so")
-SOURCES = ["basis.cpp", "topology.cpp", "dense.cpp", "assemble.cu", "krylov.cu", "mixed.cu", "patch_tc.cu", "engine.cu",
+SOURCES = ["basis.cpp", "topology.cpp", "dense.cpp", "assemble.cu", "krylov.cu", "lsq.cu", "mixed.cu", "patch_tc.cu", "engine.cu",
            "server.cu", "post.cpp", "project.cu", "port2d.cpp", "portfem.cpp", "estimate.cu", "refine.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",

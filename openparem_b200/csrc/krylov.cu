@@ -8,14 +8,16 @@
 // on the dofs of each vertex star), which keeps the discrete-gradient kernel
 // of curl-curl local to each block.  Orthogonalisation is classical Gram-
 // Schmidt with one reorthogonalisation (CGS2).  The small (m+1) x m Hessenberg
-// least-squares problem (Givens rotations, back substitution) and the harmonic
-// Ritz eigenproblem of each restart run on the host in FP64 (dense.cpp), one
-// Hessenberg column copied back per Arnoldi step.
+// least-squares problem (Givens rotations, back substitution) runs on the
+// device in FP64 (lsq.cu), the host reading one residual estimate per Arnoldi
+// step; the harmonic Ritz eigenproblem of each restart runs on the host in
+// FP64 (dense.cpp).
 #include <algorithm>
 #include <cmath>
 
 #include "dense.h"
 #include "engine.h"
+#include "lsq.h"
 
 namespace opem {
 
@@ -703,9 +705,9 @@ __global__ void basis_rotate_kernel(int64_t n, int nin, int nout, const double2*
 // the basis (Morgan's GMRES-DR), so restarts do not throw away the slow
 // modes.  k = 0 gives plain GMRES(m).  Solves the free block A_FF x_F = b_F;
 // rows/cols in dmask are identity and every Krylov vector is zero there.
-// The device runs the Arnoldi steps (SpMV, block Jacobi, CGS2); the host keeps
-// the (m+1) x m Hessenberg least-squares problem and the per-restart
-// harmonic-Ritz eigenproblem in FP64.
+// The device runs the Arnoldi steps (SpMV, block Jacobi, CGS2) and the
+// Hessenberg least squares; the host the per-restart harmonic-Ritz
+// eigenproblem, in FP64.
 // ---------------------------------------------------------------------------
 SolveResult solve_plain_fp64(Problem& P, const double2* A, const uint8_t* dmask, const double2* b, double2* x,
                              const opem_solver_opts& o) {
@@ -726,8 +728,11 @@ SolveResult solve_plain_fp64(Problem& P, const double2* A, const uint8_t* dmask,
     if (bnorm == 0.0) { res.converged = 1; return res; }
     OPEM_CUDA(cudaMemcpyAsync(w.p, b, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
     std::vector<cd> Hh((size_t)(m + 1) * m, 0.0), c(m + 1, 0.0), y;
-    std::vector<double2> colbuf(m + 2);
-    GivensLsq L;
+    LsqWork lsq;
+    lsq.alloc(1, m, kd, s);
+    DBuf<uint8_t> one;
+    one.upload(std::vector<uint8_t>(1, 1), s);
+    DBuf<int> ncd(1);
     double beta = bnorm;
     int start = 0, its = 0;
     bool fresh = true;
@@ -742,9 +747,12 @@ SolveResult solve_plain_fp64(Problem& P, const double2* A, const uint8_t* dmask,
             c[0] = beta;
             start = 0;
         }
-        L.reset(m, c);
-        double est = 0;
-        for (int j = 0; j < start; ++j) est = L.add_column(j, &Hh[(size_t)j * (m + 1)], start);
+        std::vector<double2> c0(m + 1);
+        for (int i = 0; i <= m; ++i) c0[i] = make_double2(c[i].real(), c[i].imag());
+        std::vector<double> e1(1, 0.0);
+        lsq.start_cycle(std::vector<uint8_t>(1, 1), c0, std::vector<int>(1, start), H.p, s, e1);
+        ++P.ctx->launches;
+        double est = e1[0];
         int ncol = start;
         for (int j = start; j < m; ++j) {
             double2* Vj = V.p + (int64_t)j * n;
@@ -760,22 +768,21 @@ SolveResult solve_plain_fp64(Problem& P, const double2* A, const uint8_t* dmask,
             normalize_kernel<<<vgrid(P), 256, 0, s>>>(n, scal.p + 2, w.p, V.p + (int64_t)(j + 1) * n, Hcol + j + 1);
             ++P.ctx->launches;
             OPEM_CUDA(cudaGetLastError());
-            OPEM_CUDA(cudaMemcpyAsync(colbuf.data(), Hcol, (j + 2) * sizeof(double2), cudaMemcpyDeviceToHost, s));
-            OPEM_CUDA(cudaStreamSynchronize(s));
+            lsq.step(j, one.p, H.p, s, e1);
+            ++P.ctx->launches;
             if (P.cancel.load(std::memory_order_relaxed)) throw OpemError(OPEM_ERR_CANCELLED, "request cancelled");
-            for (int i = 0; i <= j + 1; ++i) Hh[i + (size_t)j * (m + 1)] = cd(colbuf[i].x, colbuf[i].y);
-            est = L.add_column(j, &Hh[(size_t)j * (m + 1)], j + 1);
+            est = e1[0];
             ++its;
             ncol = j + 1;
             if (!std::isfinite(est)) { res.code = OPEM_ERR_BREAKDOWN; break; }
             if (est / bnorm <= o.rtol || its >= o.maxits) break;
         }
         if (res.code != OPEM_OK) break;
-        // x += M^-1 (V y)
-        L.solve(ncol, y);
-        std::vector<double2> yh(ncol);
-        for (int i = 0; i < ncol; ++i) yh[i] = make_double2(y[i].real(), y[i].imag());
-        OPEM_CUDA(cudaMemcpyAsync(yd.p, yh.data(), ncol * sizeof(double2), cudaMemcpyHostToDevice, s));
+        // x += M^-1 (V y), y from the device least squares
+        lsq.check(s);
+        ncd.upload(&ncol, 1, s);
+        lsq.solve(ncd.p, one.p, yd.p, m, s);
+        ++P.ctx->launches;
         combo_kernel<<<vgrid(P), 256, ncol * sizeof(double2), s>>>(n, ncol, V.p, n, yd.p, w.p);
         ++P.ctx->launches;
         patch_apply(P, pc, w.p, z.p, dmask);
@@ -792,7 +799,21 @@ SolveResult solve_plain_fp64(Problem& P, const double2* A, const uint8_t* dmask,
         if (its >= o.maxits) break;
         fresh = true;
         if (kd == 0 || ncol < m) continue;
-        // ---- deflated restart (harmonic Ritz vectors of the m x m problem)
+        // ---- deflated restart (harmonic Ritz vectors of the m x m problem), from
+        // the cycle's H (zero outside each column's rows) and y
+        {
+            std::vector<double2> hh((size_t)(m + 1) * m), yh(m);
+            OPEM_CUDA(cudaMemcpyAsync(hh.data(), H.p, hh.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
+            OPEM_CUDA(cudaMemcpyAsync(yh.data(), yd.p, m * sizeof(double2), cudaMemcpyDeviceToHost, s));
+            OPEM_CUDA(cudaStreamSynchronize(s));
+            for (int j = 0; j < m; ++j) {
+                const int top = j < start ? start : j + 1;
+                for (int i = 0; i <= m; ++i)
+                    Hh[i + (size_t)j * (m + 1)] = i <= top ? cd(hh[i + (size_t)j * (m + 1)].x, hh[i + (size_t)j * (m + 1)].y) : cd(0.0);
+            }
+            y.assign(m, 0.0);
+            for (int i = 0; i < m; ++i) y[i] = cd(yh[i].x, yh[i].y);
+        }
         std::vector<cd> Pm, Hn, cn;
         if (!gmres_dr_deflate(m, kd, Hh, c, y, Pm, Hn, cn)) continue;
         // device: V[:, :kd+1] = V Pm
@@ -802,8 +823,13 @@ SolveResult solve_plain_fp64(Problem& P, const double2* A, const uint8_t* dmask,
         basis_rotate_kernel<<<vgrid(P), 256, 0, s>>>(n, m + 1, kd + 1, V.p, n, Qd.p, Wd.p, n);
         ++P.ctx->launches;
         OPEM_CUDA(cudaMemcpyAsync(V.p, Wd.p, (size_t)(kd + 1) * n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+        // the restart block becomes the first kd columns of the next cycle's H
+        {
+            std::vector<double2> hn(Hn.size());
+            for (size_t t = 0; t < hn.size(); ++t) hn[t] = make_double2(Hn[t].real(), Hn[t].imag());
+            OPEM_CUDA(cudaMemcpyAsync(H.p, hn.data(), hn.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
+        }
         OPEM_CUDA(cudaStreamSynchronize(s));
-        Hh = Hn;
         c = cn;
         start = kd;
         fresh = false;

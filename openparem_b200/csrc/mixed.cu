@@ -12,8 +12,8 @@
 //   overlaps and S: FP64, as in the FP64 path.
 // (An FP32-Krylov inner solve was measured first and dropped: FP32 vectors cap
 // each inner solve's contraction of the FP64 residual near u32 * cond.)
-// The Hessenberg least-squares and the deflation eigenproblem of every system
-// are kept on the host in FP64.
+// The Hessenberg least squares of every system runs on the device in FP64
+// (lsq.cu); the deflation eigenproblem and the polynomial's roots on the host.
 //
 // Layouts: vectors that feed the shared-matrix kernels (SpMV, block apply) are
 // interleaved, element (k, r) at k*R + r, so one row's gather for all systems
@@ -28,6 +28,7 @@
 #include <tuple>
 
 #include "dense.h"
+#include "lsq.h"
 #include "engine.h"
 #include "patch_tc.h"
 
@@ -1522,6 +1523,7 @@ struct InnerWork {
     DBuf<double> nrm, npart, nrm0;
     DBuf<uint8_t> act2;   // systems whose second Gram-Schmidt pass is needed
     DBuf<int> ncols;
+    LsqWork lsq;   // the systems' Hessenberg least squares (device, FP64)
 };
 
 // Leja ordering of polynomial roots (largest first, then maximising the product of distances)
@@ -1580,12 +1582,29 @@ static int inner_solve(Batch& B, InnerWork& W, const std::vector<PatchSet32>& se
     OPEM_CUDA(cudaMemsetAsync(W.d.p, 0, W.d.bytes(), B.s));
     OPEM_CUDA(cudaMemcpyAsync(W.w.p, W.rhs.p, (size_t)n * R * sizeof(double2), cudaMemcpyDeviceToDevice, B.s));
     std::vector<std::vector<cd>> Hh(R, std::vector<cd>((size_t)(m + 1) * m)), c(R, std::vector<cd>(m + 1));
-    std::vector<GivensLsq> L(R);
     std::vector<int> start(R, 0), ncol(R, 0);
     std::vector<char> fresh(R, 1);
-    std::vector<double> beta(R, 1.0), est(R, 1.0), hnrm(R);
-    std::vector<double2> hcol((size_t)R * (m + 2));
+    std::vector<double> beta(R, 1.0), est(R, 1.0), hnrm(R), hest(R);
     std::vector<std::vector<cd>> ys(R);
+    // the Hessenberg least squares runs on the device (W.lsq); the host reads
+    // the residual estimates per step, and H itself only where it forms the
+    // polynomial's roots and the deflated restarts
+    auto download_H = [&]() {   // W.H -> Hh of the systems still running, zero outside each column's rows
+        std::vector<double2> hh((size_t)R * ldH);
+        OPEM_CUDA(cudaMemcpyAsync(hh.data(), W.H.p, hh.size() * sizeof(double2), cudaMemcpyDeviceToHost, B.s));
+        OPEM_CUDA(cudaStreamSynchronize(B.s));
+        for (int r = 0; r < R; ++r) {
+            if (done[r]) continue;
+            for (int j = 0; j < m; ++j) {
+                const int top = j < start[r] ? start[r] : j + 1;
+                for (int i = 0; i <= m; ++i) {
+                    const double2 v = i <= top && j < std::max(ncol[r], start[r]) ? hh[(size_t)r * ldH + (size_t)j * (m + 1) + i]
+                                                                                  : make_double2(0, 0);
+                    Hh[r][i + (size_t)j * (m + 1)] = cd(v.x, v.y);
+                }
+            }
+        }
+    };
     int its = 0;
     int npoly = 0;   // degree of the polynomial preconditioner in use (0: block Jacobi alone)
     auto upload_act = [&](const std::vector<uint8_t>& a) {
@@ -1605,24 +1624,28 @@ static int inner_solve(Batch& B, InnerWork& W, const std::vector<PatchSet32>& se
         OPEM_CUDA(cudaMemcpyAsync(hnrm.data(), W.nrm.p, R * sizeof(double), cudaMemcpyDeviceToHost, B.s));
         OPEM_CUDA(cudaStreamSynchronize(B.s));
         int jmin = m;
+        std::vector<double2> hc0((size_t)R * (m + 1), make_double2(0, 0));
+        std::vector<uint8_t> rst(R, 0);
         for (int r = 0; r < R; ++r) {
             if (done[r]) continue;
             if (fresh[r]) {
                 beta[r] = hnrm[r];
-                std::fill(Hh[r].begin(), Hh[r].end(), 0.0);
                 std::fill(c[r].begin(), c[r].end(), 0.0);
                 c[r][0] = beta[r];
                 start[r] = 0;
                 if (!(beta[r] > 0)) { done[r] = 1; continue; }
             }
-            L[r].reset(m, c[r]);
-            for (int j = 0; j < start[r]; ++j) est[r] = L[r].add_column(j, &Hh[r][(size_t)j * (m + 1)], start[r]);
+            rst[r] = 1;
+            for (int i = 0; i <= m; ++i) hc0[(size_t)r * (m + 1) + i] = make_double2(c[r][i].real(), c[r][i].imag());
             ncol[r] = start[r];
             jmin = std::min(jmin, start[r]);
         }
         bool any = false;
         for (int r = 0; r < R; ++r) any |= !done[r];
         if (!any) break;
+        // least-squares state of the cycle: g = c, the restart block's columns
+        W.lsq.start_cycle(rst, hc0, start, W.H.p, B.s, est);
+        ++P.ctx->launches;
         std::vector<uint8_t> cyc(R, 0);
         for (int r = 0; r < R; ++r) cyc[r] = !done[r];
         for (int j = jmin; j < m; ++j) {
@@ -1680,20 +1703,18 @@ static int inner_solve(Batch& B, InnerWork& W, const std::vector<PatchSet32>& se
                                                                 W.H.p + (int64_t)j * (m + 1) + j + 1, ldH);
             ++P.ctx->launches;
             OPEM_CUDA(cudaGetLastError());
-            OPEM_CUDA(cudaMemcpy2DAsync(hcol.data(), (m + 2) * sizeof(double2), W.H.p + (int64_t)j * (m + 1),
-                                        ldH * sizeof(double2), (j + 2) * sizeof(double2), R, cudaMemcpyDeviceToHost, B.s));
-            OPEM_CUDA(cudaStreamSynchronize(B.s));
+            W.lsq.step(j, B.act.p, W.H.p, B.s, hest);
+            ++P.ctx->launches;
             if (P.cancel.load(std::memory_order_relaxed)) throw OpemError(OPEM_ERR_CANCELLED, "request cancelled");
             ++its;
             for (int r = 0; r < R; ++r) {
                 if (!iact[r]) continue;
-                for (int i = 0; i <= j + 1; ++i)
-                    Hh[r][i + (size_t)j * (m + 1)] = cd(hcol[(size_t)r * (m + 2) + i].x, hcol[(size_t)r * (m + 2) + i].y);
-                est[r] = L[r].add_column(j, &Hh[r][(size_t)j * (m + 1)], j + 1);
+                est[r] = hest[r];
                 ncol[r] = j + 1;
                 if (!std::isfinite(est[r]) || est[r] <= tol) cyc[r] = 0;
             }
             if (poly_deg > 1 && npoly == 0 && j + 1 == poly_deg) {
+                download_H();
                 // harmonic Ritz values of the first poly_deg steps of every system -> GMRES polynomial roots
                 const int dg = poly_deg;
                 std::vector<float2> hc((size_t)dg * R, make_float2(0.f, 0.f));
@@ -1729,22 +1750,21 @@ static int inner_solve(Batch& B, InnerWork& W, const std::vector<PatchSet32>& se
             }
             if (its >= maxits) break;
         }
-        // d += Z y
-        std::vector<double2> yh((size_t)R * m, make_double2(0, 0));
+        // d += Z y, y from the device least squares
         std::vector<int> nc(R, 0);
         int ymax = 0;
         for (int r = 0; r < R; ++r) {
             iact[r] = (!done[r] && ncol[r] > 0) ? 1 : 0;
             if (!iact[r]) continue;
-            L[r].solve(ncol[r], ys[r]);
-            for (int i = 0; i < ncol[r]; ++i) yh[(size_t)r * m + i] = make_double2(ys[r][i].real(), ys[r][i].imag());
             nc[r] = ncol[r];
             ymax = std::max(ymax, ncol[r]);
         }
+        W.lsq.check(B.s);
         if (ymax > 0) {
             upload_act(iact);
-            OPEM_CUDA(cudaMemcpyAsync(W.yd.p, yh.data(), yh.size() * sizeof(double2), cudaMemcpyHostToDevice, B.s));
             OPEM_CUDA(cudaMemcpyAsync(W.ncols.p, nc.data(), R * sizeof(int), cudaMemcpyHostToDevice, B.s));
+            W.lsq.solve(W.ncols.p, B.act.p, W.yd.p, m, B.s);
+            ++P.ctx->launches;
             combo_add_sys_kernel<<<dim3(gy, R), 256, ymax * sizeof(double2), B.s>>>(n, W.Z.p, ldV, W.yd.p, m, W.ncols.p,
                                                                                    B.act.p, W.d.p);
             ++P.ctx->launches;
@@ -1765,7 +1785,20 @@ static int inner_solve(Batch& B, InnerWork& W, const std::vector<PatchSet32>& se
             sub_sys_kernel<<<(unsigned)((n * R + 255) / 256), 256, 0, B.s>>>(n, R, W.rhs.p, W.w.p, W.w.p);
             ++P.ctx->launches;
         }
-        // deflated restarts (host FP64, systems in parallel)
+        // deflated restarts (host FP64, systems in parallel) from the cycle's H and y
+        bool want_def = false;
+        for (int r = 0; r < R; ++r) want_def |= (!done[r] && kd > 0 && ncol[r] == m);
+        if (want_def) {
+            download_H();
+            std::vector<double2> yh((size_t)R * m);
+            OPEM_CUDA(cudaMemcpyAsync(yh.data(), W.yd.p, yh.size() * sizeof(double2), cudaMemcpyDeviceToHost, B.s));
+            OPEM_CUDA(cudaStreamSynchronize(B.s));
+            for (int r = 0; r < R; ++r) {
+                if (done[r] || ncol[r] != m) continue;
+                ys[r].assign(m, 0.0);
+                for (int i = 0; i < m; ++i) ys[r][i] = cd(yh[(size_t)r * m + i].x, yh[(size_t)r * m + i].y);
+            }
+        }
         std::vector<std::vector<cd>> Pm(R), Hn(R), cn(R);
         std::vector<char> ok(R, 0);
 #pragma omp parallel for schedule(dynamic, 1)
@@ -1808,7 +1841,11 @@ static int inner_solve(Batch& B, InnerWork& W, const std::vector<PatchSet32>& se
             OPEM_CUDA(cudaStreamSynchronize(B.s));
             for (int r = 0; r < R; ++r) {
                 if (!iact[r]) continue;
-                Hh[r] = Hn[r];
+                // the restart block becomes the first kd columns of the next cycle's H
+                std::vector<double2> hn((size_t)ldH);
+                for (size_t t2 = 0; t2 < hn.size(); ++t2) hn[t2] = make_double2(Hn[r][t2].real(), Hn[r][t2].imag());
+                OPEM_CUDA(cudaMemcpyAsync(W.H.p + r * ldH, hn.data(), hn.size() * sizeof(double2), cudaMemcpyHostToDevice, B.s));
+                OPEM_CUDA(cudaStreamSynchronize(B.s));
                 c[r] = cn[r];
                 start[r] = kd;
                 fresh[r] = 0;
@@ -2029,6 +2066,7 @@ static void solve_batch(Problem& P, const std::vector<System>& systems, const op
     W.rhs.alloc(nR);
     W.d.alloc(nR);
     W.H.alloc((size_t)R * (m + 1) * m);
+    W.lsq.alloc(R, m, kd, B.s);
     W.nrm.alloc(RMAX);
     W.nrm0.alloc(RMAX);
     W.act2.alloc(RMAX);
