@@ -147,6 +147,48 @@ def test_mixed_mode_of_two_uncoupled_lines():
         mixed_mode(S, [(1, 1)], 50.0)
 
 
+def test_single_ended_identity_maps_renormalise():
+    """With Tv = Ti = I the modal to single-ended conversion only changes the
+    reference impedance of every S-port from the mode's to zref: it equals the
+    reference's renormalisation (S2Z / Z2S) to zref."""
+    from openparem_b200.fem3d import single_ended
+    rng = np.random.default_rng(13)
+    for n in (1, 2, 4):
+        S = _random_s(n, rng)
+        Zm = 60 + 20 * rng.random(n) + 1j * 5 * rng.normal(size=n)
+        out = single_ended(S, Zm, np.eye(n), np.eye(n), 50.0)
+        assert np.abs(out - _ref_renorm(S, Zm, 50.0)).max() < 1e-12
+
+
+def test_single_ended_from_line_voltages_and_currents():
+    """Two two-conductor ports (four S-ports): modal waves a_m, b_m = S a_m give
+    modal line voltages V = sqrt(Zm)(a + b) and currents I = (a - b)/sqrt(Zm); the
+    single-ended ones are Tv^-1 V and Ti^-1 I, whose waves at zref,
+    (V/sqrt(zref) +- sqrt(zref) I)/2, must satisfy b_s = S_out a_s for every a_m."""
+    from openparem_b200.fem3d import single_ended
+    rng = np.random.default_rng(17)
+    n = 4
+    S = _random_s(n, rng)
+    Zm = np.array([30 + 2j, 70 - 3j, 28 + 1j, 75 + 0j])
+    Tv = np.zeros((n, n), dtype=complex)
+    Ti = np.zeros((n, n), dtype=complex)
+    for b in (0, 2):   # one 2 x 2 block per port
+        Tv[b:b + 2, b:b + 2] = rng.normal(size=(2, 2)) + 0.1j * rng.normal(size=(2, 2)) + 2 * np.eye(2)
+        Ti[b:b + 2, b:b + 2] = rng.normal(size=(2, 2)) + 0.1j * rng.normal(size=(2, 2)) + 2 * np.eye(2)
+    zref = 50.0
+    out = single_ended(S, Zm, Tv, Ti, zref)
+    am = rng.normal(size=(n, 3)) + 1j * rng.normal(size=(n, 3))
+    bm = S @ am
+    V = np.sqrt(Zm)[:, None] * (am + bm)
+    I = (am - bm) / np.sqrt(Zm)[:, None]
+    Vs, Is = np.linalg.solve(Tv, V), np.linalg.solve(Ti, I)
+    a_s = (Vs / np.sqrt(zref) + np.sqrt(zref) * Is) / 2
+    b_s = (Vs / np.sqrt(zref) - np.sqrt(zref) * Is) / 2
+    assert np.abs(out @ a_s - b_s).max() < 1e-12
+    with pytest.raises(OpemError):
+        single_ended(S, Zm, np.zeros((n, n)), Ti, zref)   # Tv singular
+
+
 def test_touchstone2_layout(tmp_path):
     from openparem_b200.fem3d import write_touchstone2
     rng = np.random.default_rng(5)
