@@ -834,7 +834,7 @@ __global__ void sub_sys_kernel(int64_t n, int R, const double2* __restrict__ a, 
 }
 
 // polynomial preconditioner steps on interleaved FP32 vectors, c[r] = 1/theta_i of system r:
-//   y += c u   (first = 1: y = c u)      and      u -= c t
+//   y += c u   (first = 1: y = c u)
 __global__ void poly_acc_kernel(int64_t cnt, int R, const float2* __restrict__ c, const float2* __restrict__ u,
                                 float2* __restrict__ y, int first) {
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < cnt; e += (int64_t)gridDim.x * blockDim.x) {
@@ -844,11 +844,17 @@ __global__ void poly_acc_kernel(int64_t cnt, int R, const float2* __restrict__ c
         else y[e] = make_float2(y[e].x + p.x, y[e].y + p.y);
     }
 }
-__global__ void poly_sub_kernel(int64_t cnt, int R, const float2* __restrict__ c, const float2* __restrict__ t,
-                                float2* __restrict__ u) {
+// one polynomial step in one pass: u = src - c t (src may be u), then y += cn u
+__global__ void poly_step_kernel(int64_t cnt, int R, const float2* __restrict__ c, const float2* __restrict__ cn,
+                                 const float2* src, const float2* __restrict__ t, float2* u, float2* __restrict__ y) {
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < cnt; e += (int64_t)gridDim.x * blockDim.x) {
-        float2 cc = c[e % R], tt = t[e];
-        u[e] = make_float2(u[e].x - (cc.x * tt.x - cc.y * tt.y), u[e].y - (cc.x * tt.y + cc.y * tt.x));
+        const int r = (int)(e % R);
+        const float2 cc = c[r], tt = t[e], ss = src[e];
+        const float2 uu = make_float2(ss.x - (cc.x * tt.x - cc.y * tt.y), ss.y - (cc.x * tt.y + cc.y * tt.x));
+        u[e] = uu;
+        const float2 c2 = cn[r];
+        const float2 p = make_float2(c2.x * uu.x - c2.y * uu.y, c2.x * uu.y + c2.y * uu.x);
+        y[e] = make_float2(y[e].x + p.x, y[e].y + p.y);
     }
 }
 
@@ -1660,18 +1666,18 @@ static int inner_solve(Batch& B, InnerWork& W, const std::vector<PatchSet32>& se
             if (npoly > 0) {
                 const int64_t cnt = n * R;
                 const unsigned gp = (unsigned)std::min<int64_t>((cnt + 255) / 256, P.ctx->sm_count * 16);
-                // y = q(A M^-1) v with Leja-ordered roots: y += u/theta_i ; u -= (A M^-1 u)/theta_i
-                OPEM_CUDA(cudaMemcpyAsync(W.pu.p, W.x_il32.p, cnt * sizeof(float2), cudaMemcpyDeviceToDevice, B.s));
-                for (int i = 0; i < npoly; ++i) {
-                    poly_acc_kernel<<<gp, 256, 0, B.s>>>(cnt, R, W.pc.p + (size_t)i * R, W.pu.p, W.py.p, i == 0);
+                // y = q(A M^-1) v with Leja-ordered roots: u_0 = v, y = u_0/theta_0, then
+                // u_{i+1} = u_i - (A M^-1 u_i)/theta_i and y += u_{i+1}/theta_{i+1} in one pass
+                poly_acc_kernel<<<gp, 256, 0, B.s>>>(cnt, R, W.pc.p, W.x_il32.p, W.py.p, 1);
+                ++P.ctx->launches;
+                for (int i = 0; i + 1 < npoly; ++i) {
+                    const float2* src = i == 0 ? W.x_il32.p : W.pu.p;
+                    patch_apply_batch(B, sets, W.t, src, W.pt.p);
+                    spmv_batch<float2, float>(B, P.f_K.p, P.f_Meps.p, P.has_tand ? P.f_Mtand.p : nullptr,
+                                              P.has_sig ? P.f_Msig.p : nullptr, B.vc32.p, bc32, W.pt.p, W.pt2.p);
+                    poly_step_kernel<<<gp, 256, 0, B.s>>>(cnt, R, W.pc.p + (size_t)i * R, W.pc.p + (size_t)(i + 1) * R,
+                                                          src, W.pt2.p, W.pu.p, W.py.p);
                     ++P.ctx->launches;
-                    if (i + 1 < npoly) {
-                        patch_apply_batch(B, sets, W.t, W.pu.p, W.pt.p);
-                        spmv_batch<float2, float>(B, P.f_K.p, P.f_Meps.p, P.has_tand ? P.f_Mtand.p : nullptr,
-                                                  P.has_sig ? P.f_Msig.p : nullptr, B.vc32.p, bc32, W.pt.p, W.pt2.p);
-                        poly_sub_kernel<<<gp, 256, 0, B.s>>>(cnt, R, W.pc.p + (size_t)i * R, W.pt2.p, W.pu.p);
-                        ++P.ctx->launches;
-                    }
                 }
                 patch_apply_batch(B, sets, W.t, W.py.p, W.z_il32.p);
             } else {
