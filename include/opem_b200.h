@@ -45,6 +45,11 @@ extern "C" {
 #define OPEM_BDR_IMPEDANCE  4   /* surface impedance; params = {sigma S/m, Rz m, mu_r}        */
 #define OPEM_BDR_RADIATION  5   /* 1st-order RBC; params[0] = wave impedance ohm (<=0: eta0)  */
 
+/* ---- port impedance definitions (the port file's impedance_definition) ---- */
+#define OPEM_Z_PV           0   /* Z = V V* / (2 Pz*)   (voltage path)                        */
+#define OPEM_Z_VI           1   /* Z = V / I            (voltage and current paths)           */
+#define OPEM_Z_PI           2   /* Z = 2 Pz / (I I*)    (current path)                        */
+
 /* ---- precision modes ----------------------------------------------------- */
 #define OPEM_PREC_FP64      0   /* plain FP64 GMRES (the drop-in)                             */
 #define OPEM_PREC_MIXED     1   /* FP32 inner GMRES + polynomial/block-Jacobi, FP64 refinement */
@@ -107,6 +112,16 @@ int  opem_problem_set_port_te(opem_problem prob, int port, const double* desc);
  * quadratic nodal e_z (beta converges at fourth order in the split).  desc as for
  * opem_problem_set_port_te; its a, b, m, n are not used.                       */
 int  opem_problem_set_port_fem2d(opem_problem prob, int port, const double* desc, int nsub, int order);
+/* Impedance definition of a port driven by its own 2D mode (after
+ * opem_problem_set_port_fem2d; the reference's impedance_definition and current
+ * IntegrationPath, Mode::calculateImpedance in OpenParEM2D fem2D.cpp:1803-1824):
+ * definition OPEM_Z_PV (default) | OPEM_Z_VI | OPEM_Z_PI; path: npath >= 2 points
+ * (xyz) of the current integration path in the port plane, I = sum over its
+ * segments of int H . dl (a closed path also takes the segment from the last
+ * point back to the first).  VI and PI need the path.  OPEM_ERR_UNSUPPORTED for a
+ * port driven by an analytic TE mode.                                          */
+int  opem_problem_set_port_impedance(opem_problem prob, int port, int definition, int npath, const double* path,
+                                     int closed);
 /* Builds DOF numbering, CSR pattern, vertex patches, and assembles the frequency-
  * independent operators on the device.                                         */
 int  opem_problem_assemble(opem_problem prob);
@@ -238,6 +253,12 @@ int  opem_port_mode_faces(int64_t nverts, const double* verts, int64_t nface, co
                           const double* eps_face, const double* mu_face, const double* desc, int nsub, int order,
                           double freq, double* metrics, int64_t npts, const int64_t* pt_face, const double* pt_s,
                           double* E_out, double* Hy_out);
+/* The same metrics under an impedance definition (as opem_problem_set_port_impedance):
+ * metrics = {gamma, Z, V, Pz, I} (5 complex; I = 0 without a current path).     */
+int  opem_port_mode_faces_z(int64_t nverts, const double* verts, int64_t nface, const int64_t* face_verts,
+                            const double* eps_face, const double* mu_face, const double* desc, int nsub, int order,
+                            double freq, int definition, int npath, const double* path, int closed,
+                            double* metrics);
 
 /* ---- S-parameter post-processing (host only, no GPU needed) -----------------
  * Renormalises S (nports x nports complex, interleaved, row = portOut) from the

@@ -55,6 +55,7 @@ SIGNATURES = [
     ("opem_problem_set_boundary", C.c_int, [P, C.c_int, C.c_int, DP, C.c_int]),
     ("opem_problem_set_port_te", C.c_int, [P, C.c_int, DP]),
     ("opem_problem_set_port_fem2d", C.c_int, [P, C.c_int, DP, C.c_int, C.c_int]),
+    ("opem_problem_set_port_impedance", C.c_int, [P, C.c_int, C.c_int, C.c_int, DP, C.c_int]),
     ("opem_mesh_errors", C.c_int, [P, C.c_double, DP, I64P, C.c_int64, I64P, DP]),
     ("opem_problem_assemble", C.c_int, [P]),
     ("opem_problem_info", C.c_int, [P, I64P, C.c_int]),
@@ -82,6 +83,8 @@ SIGNATURES = [
     ("opem_port_mode_2d", C.c_int, [C.c_int64, DP, C.c_int64, I64P, DP, DP, C.c_double, DP, I64P, I64P, DP, DP]),
     ("opem_port_mode_faces", C.c_int, [C.c_int64, DP, C.c_int64, I64P, DP, DP, DP, C.c_int, C.c_int, C.c_double, DP,
                                         C.c_int64, I64P, DP, DP, DP]),
+    ("opem_port_mode_faces_z", C.c_int, [C.c_int64, DP, C.c_int64, I64P, DP, DP, DP, C.c_int, C.c_int, C.c_double,
+                                          C.c_int, C.c_int, DP, C.c_int, DP]),
     ("opem_s_renormalize", C.c_int, [C.c_int, DP, DP, C.c_double, C.c_double, DP]),
     ("opem_write_touchstone", C.c_int, [C.c_char_p, C.c_int, DP, C.c_int, DP, C.c_double, C.c_char_p, C.c_char_p]),
     ("opem_s_mixed_mode", C.c_int, [C.c_int, DP, C.c_int, C.POINTER(C.c_int), C.c_double, DP, DP]),

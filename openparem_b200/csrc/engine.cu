@@ -104,7 +104,9 @@ static std::shared_ptr<const PortFem2D> port_fem2d(const Problem& P, int k, doub
     auto sol = std::make_shared<PortFem2D>();
     std::string err;
     int rc = port_fem2d_solve(T.verts.data(), (int64_t)fv.size() / 3, fv.data(), eps.data(), mu.data(), pm.desc,
-                              pm.nsub, pm.order2d, freq, mu[0].real(), *sol, err);
+                              pm.nsub, pm.order2d, freq, mu[0].real(), *sol, err, pm.zdef,
+                              pm.ipath.empty() ? nullptr : pm.ipath.data(), (int)(pm.ipath.size() / 3),
+                              pm.ipath_closed);
     if (rc != OPEM_OK) throw OpemError(rc, err);
     pm.fem->sols.emplace_back(freq, sol);
     if (pm.fem->sols.size() > 8) pm.fem->sols.erase(pm.fem->sols.begin());
@@ -912,6 +914,8 @@ int opem_problem_set_port_te(opem_problem prob, int port, const double* desc) {
     if ((int)P.modes.size() <= port) P.modes.resize(port + 1);
     P.modes[port].set = true;
     P.modes[port].kind = 0;
+    P.modes[port].zdef = OPEM_Z_PV;
+    P.modes[port].ipath.clear();
     P.modes[port].fem.reset();
     std::memcpy(P.modes[port].desc, desc, 22 * sizeof(double));
     P.assembled = false;
@@ -929,8 +933,29 @@ int opem_problem_set_port_fem2d(opem_problem prob, int port, const double* desc,
     m.kind = 1;
     m.nsub = nsub;
     m.order2d = order;
+    m.zdef = OPEM_Z_PV;
+    m.ipath.clear();
     m.fem = std::make_shared<PortFemCache>();
     std::memcpy(m.desc, desc, 22 * sizeof(double));
+    P.assembled = false;
+    return OPEM_OK;
+}
+
+int opem_problem_set_port_impedance(opem_problem prob, int port, int definition, int npath, const double* path,
+                                    int closed) {
+    if (!prob || port < 0 || definition < OPEM_Z_PV || definition > OPEM_Z_PI || npath < 0 || (npath > 0 && !path))
+        return OPEM_ERR_ARG;
+    if (definition != OPEM_Z_PV && npath < 2) return OPEM_ERR_ARG;
+    for (int i = 0; i < 3 * npath; ++i)
+        if (!std::isfinite(path[i])) return OPEM_ERR_ARG;
+    Problem& P = prob->p;
+    if ((int)P.modes.size() <= port || !P.modes[port].set) return OPEM_ERR_STATE;
+    PortMode& m = P.modes[port];
+    if (m.kind != 1) return definition == OPEM_Z_PV && npath == 0 ? OPEM_OK : OPEM_ERR_UNSUPPORTED;
+    m.zdef = definition;
+    m.ipath.assign(path ? path : nullptr, path ? path + 3 * npath : nullptr);
+    m.ipath_closed = closed != 0;
+    m.fem = std::make_shared<PortFemCache>();   // solved again with the new definition
     P.assembled = false;
     return OPEM_OK;
 }

@@ -89,6 +89,9 @@ struct PortMode {
     int kind = 0;    // 0: analytic TE_mn (desc), 1: 2D mode of the port faces
     int nsub = 0;    // kind 1: split of each port face
     int order2d = 1; // kind 1: 2D element order
+    int zdef = 0;    // kind 1: OPEM_Z_PV / VI / PI
+    std::vector<double> ipath;   // kind 1: current path points (xyz)
+    bool ipath_closed = true;
     std::shared_ptr<PortFemCache> fem;
 };
 

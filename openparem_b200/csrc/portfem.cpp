@@ -16,7 +16,10 @@
 //     analytic TE modes) H_t = n x (gamma e_t + grad_t e_z) / (j w mu);
 //   * V = -int E . dl along the voltage path (composite 4-point Gauss on
 //     16 nsub pieces), Pz = 1/2 int (E x H*) . n (edge-midpoint rule, exact for
-//     the piecewise-quadratic integrand), Z = V V* / (2 Pz*) (the PV definition).
+//     the piecewise-quadratic integrand), and along the current path, where one
+//     is given, I = int H . dl (the same Gauss rule per segment);
+//   * Z by the port's impedance definition (OpenParEM2D Mode::calculateImpedance,
+//     fem2D.cpp:1803-1824): PV V V* / (2 Pz*), VI V / I, PI 2 Pz / (I I*).
 // The 3D port trace is then the moment interpolation of this field on each
 // port face (engine.cu port_traces), as for the analytic modes.
 #include "portfem.h"
@@ -130,7 +133,11 @@ int64_t PortFem2D::locate(const double X[3]) const {
 
 int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* fv, const cd* eps_face, const cd* mu_face,
                      const double* desc, int nsub, int order, double freq, double mu_port, PortFem2D& M,
-                     std::string& err) {
+                     std::string& err, int zdef, const double* ipath, int npath, bool closed) {
+    if (zdef < 0 || zdef > 2 || (zdef != 0 && (!ipath || npath < 2))) {
+        err = "impedance definition: VI and PI need a current path of at least two points";
+        return OPEM_ERR_ARG;
+    }
     if (nface < 1 || nsub < 1 || nsub > 64 || order < 1 || order > 2 || !(freq > 0)) {
         err = "port mode: bad arguments";
         return OPEM_ERR_ARG;
@@ -342,11 +349,66 @@ int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* fv, cons
         }
         M.Pz = 0.5 * pz;
     }
-    M.Z = 0.5 * M.V * std::conj(M.V) / std::conj(M.Pz);
+    // I = int H . dl along the current path, H = y Hy
+    M.I = 0.0;
+    if (ipath && npath >= 2) {
+        const double w = 2 * M_PI * freq;
+        const cd y = M.gamma / cd(0.0, w * MU0 * mu_port);
+        std::vector<double> x, wq;
+        gauss_legendre01(4, x, wq);
+        const int K = 16 * N;
+        const int nseg = closed ? npath : npath - 1;
+        cd iint = 0.0;
+        for (int sgi = 0; sgi < nseg; ++sgi) {
+            const double* p0 = ipath + 3 * sgi;
+            const double* p1 = ipath + 3 * ((sgi + 1) % npath);
+            const double dl[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+            for (int k = 0; k < K; ++k)
+                for (int q = 0; q < 4; ++q) {
+                    const double s = (k + x[q]) / K;
+                    const double X[3] = {p0[0] + s * dl[0], p0[1] + s * dl[1], p0[2] + s * dl[2]};
+                    cd E[3], Hy[3];
+                    M.eval_tri(M.locate(X), X, E, Hy);
+                    iint += (wq[q] / K) * (Hy[0] * dl[0] + Hy[1] * dl[1] + Hy[2] * dl[2]);
+                }
+        }
+        M.I = y * iint;
+    }
+    if (zdef == OPEM_Z_VI) M.Z = M.V / M.I;
+    else if (zdef == OPEM_Z_PI) M.Z = 2.0 * M.Pz / (M.I * std::conj(M.I));
+    else M.Z = 0.5 * M.V * std::conj(M.V) / std::conj(M.Pz);
+    if (!std::isfinite(M.Z.real()) || !std::isfinite(M.Z.imag())) {
+        err = "port impedance is not finite (zero current or voltage on its path)";
+        return OPEM_ERR_BREAKDOWN;
+    }
     return OPEM_OK;
 }
 
 }  // namespace opem
+
+extern "C" int opem_port_mode_faces_z(int64_t nverts, const double* verts, int64_t nface, const int64_t* face_verts,
+                                      const double* eps_face, const double* mu_face, const double* desc, int nsub,
+                                      int order, double freq, int definition, int npath, const double* path,
+                                      int closed, double* metrics) {
+    using cd = std::complex<double>;
+    if (nverts < 3 || !verts || nface < 1 || !face_verts || !eps_face || !desc || !metrics) return OPEM_ERR_ARG;
+    if (npath < 0 || (npath > 0 && !path)) return OPEM_ERR_ARG;
+    for (int64_t i = 0; i < 3 * nface; ++i)
+        if (face_verts[i] < 0 || face_verts[i] >= nverts) return OPEM_ERR_ARG;
+    std::vector<cd> eps(nface), mu(nface, cd(1.0));
+    for (int64_t f = 0; f < nface; ++f) {
+        eps[f] = cd(eps_face[2 * f], eps_face[2 * f + 1]);
+        if (mu_face) mu[f] = cd(mu_face[2 * f], mu_face[2 * f + 1]);
+    }
+    opem::PortFem2D M;
+    std::string err;
+    int rc = opem::port_fem2d_solve(verts, nface, face_verts, eps.data(), mu.data(), desc, nsub, order, freq, mu[0].real(), M,
+                                    err, definition, npath > 0 ? path : nullptr, npath, closed != 0);
+    if (rc != OPEM_OK) return rc;
+    const cd m5[5] = {M.gamma, M.Z, M.V, M.Pz, M.I};
+    for (int i = 0; i < 5; ++i) { metrics[2 * i] = m5[i].real(); metrics[2 * i + 1] = m5[i].imag(); }
+    return OPEM_OK;
+}
 
 extern "C" int opem_port_mode_faces(int64_t nverts, const double* verts, int64_t nface, const int64_t* face_verts,
                                     const double* eps_face, const double* mu_face, const double* desc, int nsub,

@@ -24,7 +24,7 @@ struct PortFem2D {
     int64_t nface = 0;
     double o[3], u[3], v[3], n[3];    // unit frame of the port plane; n = outward normal
     double freq = 0, mu_port = 1;
-    cd gamma, V, Z, Pz;
+    cd gamma, V, Z, Pz, I;            // I: current along the current path (0 without one)
     std::vector<double> xy;           // 2D nodes
     std::vector<int64_t> st;          // 3 sorted node ids per sub-triangle
     std::vector<double> P0, Jinv, g;  // per sub-triangle: first node (2), J^-1 (4), grad lambda (3x2)
@@ -46,9 +46,12 @@ struct PortFem2D {
 // permittivity / permeability per face (from the owning tetrahedron);
 // desc: the 22-double port descriptor (origin, u, v, outward normal, a, b, m, n,
 // voltage path); order: 2D element order (1 or 2); mu_port: mu_r used to scale
-// H_t / y.  Returns an OPEM_* code.
+// H_t / y; zdef: OPEM_Z_PV / VI / PI; ipath: the current path's points (xyz,
+// npath of them, closed: with the segment back to the first).  Returns an
+// OPEM_* code.
 int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* face_verts,
                      const std::complex<double>* eps_face, const std::complex<double>* mu_face, const double* desc,
-                     int nsub, int order, double freq, double mu_port, PortFem2D& out, std::string& err);
+                     int nsub, int order, double freq, double mu_port, PortFem2D& out, std::string& err,
+                     int zdef = 0, const double* ipath = nullptr, int npath = 0, bool closed = true);
 
 }  // namespace opem

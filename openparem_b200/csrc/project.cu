@@ -29,7 +29,12 @@ namespace {
 
 struct Mat { double er = 1, mur = 1, tand = 0, sigma = 0, Rz = 0; };
 struct Path { std::vector<std::array<double, 3>> pts; bool closed = false; };
-struct PortDef { std::string name, path, vpath; int sport = 0; };
+struct PortDef {
+    std::string name, path, vpath, ipath, zdef = "PV";
+    int sport = 0;
+    int nmodes = 0;           // Line / Mode blocks (one per S-port of the port)
+    bool composite = false;   // an integration path summed from several paths or scaled
+};
 struct BdrDef { std::string name, type, material; std::vector<std::string> paths; };
 
 struct Project {
@@ -45,6 +50,9 @@ struct Project {
     std::vector<int64_t> tri_opp;     // vertex of the owning tet opposite the face
     std::vector<std::array<double, 22>> port_desc;
     std::vector<int> port_nsub;       // 0: analytic TE10; > 0: the port's own 2D mode on faces split nsub x nsub
+    std::vector<int> port_zdef;       // OPEM_Z_PV / VI / PI
+    std::vector<std::vector<double>> port_ipath;   // current path points (xyz)
+    std::vector<int> port_ipath_closed;
     std::vector<std::pair<int, std::array<double, 3>>> bdr;   // attr -> (type, params)
     std::vector<double> freqs;
     int order = 1;
@@ -196,7 +204,20 @@ void read_ports(const std::string& path, std::map<std::string, Path>& paths, std
             block = ln; cur = Path(); pname.clear(); pd = PortDef(); bd = BdrDef(); continue;
         }
         if (ln == "EndPath") { paths[pname] = cur; block.clear(); continue; }
-        if (ln == "EndPort") { ports.push_back(pd); block.clear(); continue; }
+        if (ln == "EndPort") {
+            // ports with several conductors (several modes, composite integration
+            // paths) need the multi-mode 2D solve, which is not built
+            if (pd.nmodes > 1)
+                throw std::runtime_error("port " + pd.name + " has " + std::to_string(pd.nmodes) +
+                                         " modes: multi-conductor ports are not supported");
+            if (pd.composite)
+                throw std::runtime_error("port " + pd.name +
+                                         ": integration paths summed from several paths or scaled are not supported");
+            ports.push_back(pd);
+            block.clear();
+            continue;
+        }
+        if (block == "Port" && (ln == "Line" || ln == "Mode")) { ++pd.nmodes; continue; }
         if (ln == "EndBoundary") { bdrs.push_back(bd); block.clear(); continue; }
         if (ln == "EndFile") { block.clear(); continue; }
         if (ln == "IntegrationPath") { itype.clear(); in_ipath = true; continue; }
@@ -218,13 +239,17 @@ void read_ports(const std::string& path, std::map<std::string, Path>& paths, std
         } else if (block == "Port") {
             if (in_ipath) {
                 if (k == "type") itype = v;
+                else if (k == "path+" || k == "path-" || k == "scale") pd.composite = true;
                 else if (k == "path" && itype == "voltage" && pd.vpath.empty()) pd.vpath = v;
+                else if (k == "path" && itype == "current" && pd.ipath.empty()) pd.ipath = v;
             } else if (k == "name") {
                 pd.name = v;
             } else if (k == "path") {
                 pd.path = v;
             } else if (k == "Sport") {
                 pd.sport = std::stoi(v);
+            } else if (k == "impedance_definition") {
+                pd.zdef = v;
             }
         } else if (block == "Boundary") {
             if (k == "name") bd.name = v;
@@ -415,6 +440,7 @@ void build(const std::string& proj_path, int order_override, Project& P) {
     const int np = (int)ports.size(), nb = (int)bdrs.size();
     std::vector<int64_t> port_opp(np, -1), port_face0(np, -1), port_nface(np, 0);
     std::vector<int> port_mixed(np, 0), port_reg0(np, -1);   // faces of more than one material behind the port
+    std::vector<double> port_area(np, 0.0);                  // area of the port's faces
     auto same_mat = [&](int r0, int r1) {
         const Mat &A = P.region_mat[r0], &B = P.region_mat[r1];
         return A.er == B.er && A.tand == B.tand && A.sigma == B.sigma && A.mur == B.mur;
@@ -431,6 +457,7 @@ void build(const std::string& proj_path, int order_override, Project& P) {
                 if (port_reg0[p] < 0) port_reg0[p] = r;
                 else if (!same_mat(port_reg0[p], r)) port_mixed[p] = 1;
                 ++port_nface[p];
+                port_area[p] += 0.5 * norm(cross(sub(vtx(k[1]), vtx(k[0])), sub(vtx(k[2]), vtx(k[0]))));
             }
         for (int j = 0; j < nb && a == 1; ++j)
             for (auto& poly : bdr_poly[j])
@@ -489,7 +516,40 @@ void build(const std::string& proj_path, int order_override, Project& P) {
         // on a split that keeps the 2D mesh near 1024 triangles
         // (and every port that is not a rectangle, which has no analytic mode here)
         const int nsub = (int)std::lround(std::sqrt(1024.0 / (double)std::max<int64_t>(1, port_nface[p])));
-        P.port_nsub.push_back(port_mixed[p] || !port_rect[p] ? std::min(16, std::max(1, nsub)) : 0);
+        // faces that leave part of the port polygon uncovered (a conductor inside
+        // the cross-section is a hole in them): no analytic mode either
+        double parea = 0.0;
+        {
+            const auto& q = port_poly[p].q;
+            for (size_t i = 0; i < q.size(); ++i) {
+                const auto& a0 = q[i];
+                const auto& a1 = q[(i + 1) % q.size()];
+                parea += 0.5 * (a0[0] * a1[1] - a1[0] * a0[1]);
+            }
+            parea = std::fabs(parea);
+        }
+        const bool holes = port_area[p] < (1.0 - 1e-9) * parea;
+        // impedance definition and current path (a port that uses its current
+        // is driven by its own 2D mode, where the current is integrated)
+        const std::string& zd = ports[p].zdef;
+        int zdef = OPEM_Z_PV;
+        if (zd == "VI") zdef = OPEM_Z_VI;
+        else if (zd == "PI") zdef = OPEM_Z_PI;
+        else if (zd != "PV") throw std::runtime_error("port " + ports[p].name + ": impedance_definition must be VI, PV or PI");
+        std::vector<double> ip;
+        int ipc = 1;
+        if (!ports[p].ipath.empty()) {
+            bool cl = false;
+            for (auto& q : path_points(paths, ports[p].ipath, &cl)) ip.insert(ip.end(), q.begin(), q.end());
+            ipc = cl ? 1 : 0;
+        }
+        if (zdef != OPEM_Z_PV && ip.size() < 6)
+            throw std::runtime_error("port " + ports[p].name + ": impedance_definition " + zd + " needs a current path");
+        P.port_zdef.push_back(zdef);
+        P.port_ipath.push_back(ip);
+        P.port_ipath_closed.push_back(ipc);
+        P.port_nsub.push_back(port_mixed[p] || !port_rect[p] || holes || zdef != OPEM_Z_PV ? std::min(16, std::max(1, nsub))
+                                                                                           : 0);
     }
     // boundary conditions: attribute 1 the faces no port or Boundary block claims
     // (PEC, or the surface impedance of materials.default.boundary, as
@@ -642,9 +702,13 @@ int opem_project_load(opem_context ctx, const char* proj_path, int order, opem_p
         const int np = type == OPEM_BDR_PORT ? 1 : (type == OPEM_BDR_IMPEDANCE ? 3 : (type == OPEM_BDR_RADIATION ? 1 : 0));
         rc = opem_problem_set_boundary(prob, (int)a + 1, type, np ? P.bdr[a].second.data() : nullptr, np);
     }
-    for (size_t p = 0; rc == OPEM_OK && p < P.port_desc.size(); ++p)
+    for (size_t p = 0; rc == OPEM_OK && p < P.port_desc.size(); ++p) {
         rc = P.port_nsub[p] > 0 ? opem_problem_set_port_fem2d(prob, (int)p, P.port_desc[p].data(), P.port_nsub[p], 2)
                                 : opem_problem_set_port_te(prob, (int)p, P.port_desc[p].data());
+        if (rc == OPEM_OK && P.port_nsub[p] > 0 && !P.port_ipath[p].empty())
+            rc = opem_problem_set_port_impedance(prob, (int)p, P.port_zdef[p], (int)(P.port_ipath[p].size() / 3),
+                                                 P.port_ipath[p].data(), P.port_ipath_closed[p]);
+    }
     if (rc != OPEM_OK) {
         opem_problem_destroy(prob);
         return rc;

@@ -99,6 +99,31 @@ def project_info(proj_path, order=0):
     return info, fr[:min(info["frequencies"], len(fr))]
 
 
+_ZDEF = {"PV": 0, "VI": 1, "PI": 2}
+
+
+def port_mode_faces_z(verts, face_verts, eps_face, mode, nsub, freq, zdef="PV", ipath=None, closed=True,
+                      mu_face=None, order=2):
+    """The 2D mode's metrics under an impedance definition (opem_port_mode_faces_z,
+    host only): zdef "PV" | "VI" | "PI", ipath (k, 3) the current path's points
+    -> {gamma, Z, V, Pz, I}."""
+    verts = np.ascontiguousarray(verts, dtype=np.float64)
+    fv = np.ascontiguousarray(face_verts, dtype=np.int64)
+    eps = np.ascontiguousarray(np.stack([np.real(eps_face), np.imag(eps_face)], axis=1), dtype=np.float64)
+    mu = None if mu_face is None else np.ascontiguousarray(np.stack([np.real(mu_face), np.imag(mu_face)], axis=1))
+    d = te_descriptor(mode)
+    ip = None if ipath is None else np.ascontiguousarray(ipath, dtype=np.float64).reshape(-1, 3)
+    m = np.zeros(10)
+    rc = _lib.lib().opem_port_mode_faces_z(len(verts), _dp(verts), len(fv), fv.ctypes.data_as(_lib.I64P), _dp(eps),
+                                           None if mu is None else _dp(mu), _dp(d), int(nsub), int(order),
+                                           float(freq), _ZDEF[zdef], 0 if ip is None else len(ip),
+                                           None if ip is None else _dp(ip), int(closed), _dp(m))
+    if rc != _lib.OK:
+        raise OpemError(rc, "opem_port_mode_faces_z")
+    c = m[0::2] + 1j * m[1::2]
+    return {"gamma": c[0], "Z": c[1], "V": c[2], "Pz": c[3], "I": c[4]}
+
+
 def port_mode_faces(verts, face_verts, eps_face, mode, nsub, freq, pt_face=None, pt_s=None, mu_face=None, order=1):
     """The 2D mode of a port given by its faces (opem_port_mode_faces, host only):
     -> (metrics {gamma, Z, V, Pz}, E_t (npts,3), H_t / y (npts,3)) at the points
@@ -220,6 +245,12 @@ class Fem3D:
                 _chk(self.ctx.h, L.opem_problem_set_port_fem2d(self.h, k, _dp(d), int(port["mode"]["nsub"]),
                                                                int(port["mode"].get("order2d", 1))),
                      "set_port_fem2d")
+                ip = port["mode"].get("ipath")
+                if ip is not None:   # impedance definition with a current path
+                    ip = np.ascontiguousarray(ip, dtype=np.float64).reshape(-1, 3)
+                    _chk(self.ctx.h, L.opem_problem_set_port_impedance(
+                        self.h, k, _ZDEF[port["mode"].get("zdef", "PV")], len(ip), _dp(ip),
+                        int(port["mode"].get("ipath_closed", True))), "set_port_impedance")
             else:
                 _chk(self.ctx.h, L.opem_problem_set_port_te(self.h, k, _dp(d)), "set_port_te")
         self.nports = len(prob["ports"])

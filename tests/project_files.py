@@ -194,3 +194,56 @@ def write_lguide_project(d, nx=6, ny=4, nz=10, L=40e-3, order=1, freqs=(8e9, 8.5
                               "lines": [{"Sport": k, "integration": [{"type": "voltage", "paths": [f"+V{k}"]}]}]})
     return write_project(d, "lguide", verts, tets, 1, {1: "air"}, spec,
                          {"air": {"er": 1.0, "mur": 1.0, "tand": 0.0, "Rz": 0.0}}, order, list(freqs))
+
+
+def coax_mesh(nx=6, ny=4, nz=6, L=24e-3):
+    """An air-filled rectangular coaxial line: the 24 x 16 mm box without the
+    8 x 8 mm inner conductor about its axis (whole Kuhn hexes removed), length L
+    along z.  Returns (verts, tets)."""
+    a, b = 24e-3, 16e-3
+    verts, tets = meshgen.box_kuhn(a, b, L, nx, ny, nz)
+    cen = verts[tets].mean(axis=1)
+    tets = tets[~((np.abs(cen[:, 0]) < 4e-3) & (np.abs(cen[:, 1]) < 4e-3))]
+    used = np.unique(tets)
+    remap = -np.ones(len(verts), dtype=np.int64)
+    remap[used] = np.arange(len(used))
+    return verts[used], remap[tets]
+
+
+def faces_at_z(verts, tets, z):
+    """The exterior faces of a tetrahedral mesh whose three vertices lie on the
+    plane z (vertex triples in the owning tetrahedron's local order)."""
+    from collections import Counter
+    loc = ((0, 1, 2), (0, 1, 3), (0, 2, 3), (1, 2, 3))
+    cnt = Counter(tuple(sorted(t[list(l)])) for t in tets for l in loc)
+    out = []
+    for t in tets:
+        for l in loc:
+            f = t[list(l)]
+            if cnt[tuple(sorted(f))] == 1 and np.all(np.abs(verts[f, 2] - z) < 1e-12):
+                out.append(f)
+    return np.array(out, dtype=np.int64)
+
+
+def write_coax_project(d, zdef="PI", with_current=True, freqs=(3e9,)):
+    """The rectangular coaxial line of coax_mesh as a project in directory d:
+    ports on the 24 x 16 mm outline at z = 0 and z = L (the inner conductor a hole
+    in their faces), voltage paths from the inner conductor to the outer wall
+    along +x, current paths a loop about the inner conductor; impedance_definition
+    zdef.  Returns the .proj path."""
+    L = 24e-3
+    verts, tets = coax_mesh(L=L)
+    outline = [(-12e-3, -8e-3), (12e-3, -8e-3), (12e-3, 8e-3), (-12e-3, 8e-3)]
+    loop = [(-8e-3, -6e-3), (8e-3, -6e-3), (8e-3, 6e-3), (-8e-3, 6e-3)]
+    spec = {"paths": [], "boundaries": [], "ports": []}
+    for k, z in ((1, 0.0), (2, L)):
+        spec["paths"].append({"name": f"port{k}", "points": [(x, y, z) for x, y in outline], "closed": True})
+        spec["paths"].append({"name": f"V{k}", "points": [(4e-3, 0.0, z), (12e-3, 0.0, z)], "closed": False})
+        spec["paths"].append({"name": f"I{k}", "points": [(x, y, z) for x, y in loop], "closed": True})
+        integ = [{"type": "voltage", "paths": [f"+V{k}"]}]
+        if with_current:
+            integ.append({"type": "current", "paths": [f"+I{k}"]})
+        spec["ports"].append({"name": str(k), "paths": [f"+port{k}"], "impedance_definition": zdef,
+                              "impedance_calculation": "line", "lines": [{"Sport": k, "integration": integ}]})
+    return write_project(d, "coax", verts, tets, 1, {1: "air"}, spec,
+                         {"air": {"er": 1.0, "mur": 1.0, "tand": 0.0, "Rz": 0.0}}, 1, list(freqs))
