@@ -227,6 +227,12 @@ int  opem_project_read(const char* proj_path, int order, int64_t* counts, double
                        double* bdr_params, double* port_desc, int32_t* port_nsub, double* freqs, char* msg,
                        int msg_len);
 
+/* Impedance definition of port `port` of a project as the reader takes it
+ * (host only): definition OPEM_Z_PV / VI / PI, the current path's point count
+ * and up to cap of its points (xyz), closed = 1 when the path is closed.       */
+int  opem_project_port_impedance(const char* proj_path, int port, int* definition, int* closed, int* npath,
+                                 double* path, int cap, char* msg, int msg_len);
+
 /* ---- port eigenmode of a cross-section (host only; the modal problem the
  * reference hands to OpenParEM2D, port.cpp:5081-5176) ----------------------------
  * Fundamental mode of a guide with PEC walls on a triangle mesh: nodes xy

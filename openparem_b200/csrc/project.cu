@@ -671,6 +671,25 @@ int opem_project_read(const char* proj_path, int order, int64_t* counts, double*
     return OPEM_OK;
 }
 
+int opem_project_port_impedance(const char* proj_path, int port, int* definition, int* closed, int* npath,
+                                double* path, int cap, char* msg, int msg_len) {
+    if (!proj_path || port < 0 || !definition || !closed || !npath || cap < 0 || (cap > 0 && !path))
+        return OPEM_ERR_ARG;
+    Project P;
+    try {
+        build(proj_path, 0, P);
+    } catch (const std::exception& e) {
+        if (msg && msg_len > 0) { std::strncpy(msg, e.what(), msg_len - 1); msg[msg_len - 1] = 0; }
+        return OPEM_ERR_ARG;
+    }
+    if (port >= (int)P.port_zdef.size()) return OPEM_ERR_ARG;
+    *definition = P.port_zdef[port];
+    *closed = P.port_ipath_closed[port];
+    *npath = (int)(P.port_ipath[port].size() / 3);
+    for (int i = 0; i < 3 * std::min(cap, *npath); ++i) path[i] = P.port_ipath[port][i];
+    return OPEM_OK;
+}
+
 int opem_project_load(opem_context ctx, const char* proj_path, int order, opem_problem* out, int* nfreq,
                       double* freqs, int max_freqs) {
     if (!ctx || !proj_path || !out) return OPEM_ERR_ARG;

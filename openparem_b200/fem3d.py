@@ -195,6 +195,15 @@ def project_problem(proj_path, order=0):
                 "normal": d[9:12].tolist(), "vpath": (d[16:19].tolist(), d[19:22].tolist())}
         if ns[k] > 0:   # the port's own 2D mode (the reader uses second-order 2D elements)
             mode.update(kind="FEM2D", nsub=int(ns[k]), order2d=2)
+            zd, cl, npth = C.c_int(0), C.c_int(1), C.c_int(0)
+            pbuf = np.zeros((64, 3))
+            rc = L.opem_project_port_impedance(path, k, C.byref(zd), C.byref(cl), C.byref(npth), _dp(pbuf), 64, msg,
+                                               512)
+            if rc != _lib.OK:
+                raise OpemError(rc, f"opem_project_port_impedance: {msg.value.decode()}")
+            if npth.value > 0:   # the impedance definition and its current path
+                mode.update(zdef={0: "PV", 1: "VI", 2: "PI"}[zd.value], ipath=pbuf[:min(npth.value, 64)].copy(),
+                            ipath_closed=bool(cl.value))
         ports.append({"mode": mode})
     prob = {"verts": verts, "tets": tets, "tet_region": reg.astype(np.int64), "bdr_tris": tris,
             "bdr_attr": attr.astype(np.int64), "order": p, "eps_r": mat[:, 0], "tand": mat[:, 1],

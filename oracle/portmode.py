@@ -17,7 +17,12 @@ that chain for one mode per port:
   analytic modes), H_t = n x (gamma e_t + grad_t e_z) / (j w mu);
 * V = -int E . dl along the voltage path (composite 4-point Gauss on 16 nsub
   pieces), Pz = 1/2 int (E x H*) . n over the sub-triangles (exact rule for the
-  piecewise-quadratic integrand), Z = V V* / (2 Pz*) (the PV definition).
+  piecewise-quadratic integrand), and where the mode gives a current path
+  ("ipath", closed unless "ipath_closed" is False) I = int H . dl along it (the
+  same composite rule per segment);
+* Z by the mode's impedance definition ("zdef", OpenParEM2D
+  Mode::calculateImpedance, src/OpenParEM2D/fem2D.cpp:1803-1824): PV
+  V V* / (2 Pz*) (the default), VI V / I, PI 2 Pz / (I I*).
 """
 import numpy as np
 
@@ -140,7 +145,21 @@ class Fem2DMode:
         E, H = self._eval(tt, X2)
         # weights sum to 1/2 on the unit triangle: int = 2 area sum(w f)
         self.Pz = 0.5 * np.sum(2 * self.area[tt] * np.tile(wq, T) * (np.cross(E, np.conj(H)) @ nh))
-        self.Z = 0.5 * self.V * np.conj(self.V) / np.conj(self.Pz)
+        self.I = 0j
+        ip = mode.get("ipath")
+        if ip is not None:
+            ip = np.asarray(ip, dtype=np.float64).reshape(-1, 3)
+            nseg = len(ip) if mode.get("ipath_closed", True) else len(ip) - 1
+            for k in range(nseg):
+                a, b = ip[k], ip[(k + 1) % len(ip)]
+                self.I += np.sum(ws * (self.Ht(a[None, :] + s[:, None] * (b - a)[None, :]) @ (b - a)))
+        zdef = mode.get("zdef", "PV")
+        if zdef == "VI":
+            self.Z = self.V / self.I
+        elif zdef == "PI":
+            self.Z = 2 * self.Pz / (self.I * np.conj(self.I))
+        else:
+            self.Z = 0.5 * self.V * np.conj(self.V) / np.conj(self.Pz)
 
     def _locate(self, X2):
         """Sub-triangle of each 2D point: the one it is deepest inside."""
@@ -219,4 +238,5 @@ class Fem2DMode:
             def at_face(self, f, S12, X):
                 return mode._eval(mode.face_tri(f, S12), mode._xy(X))[self.which]
 
-        return {"gamma": self.gamma, "Z": self.Z, "V": self.V, "Pz": self.Pz, "Et": _Field(0), "Ht": _Field(1)}
+        return {"gamma": self.gamma, "Z": self.Z, "V": self.V, "Pz": self.Pz, "I": self.I, "Et": _Field(0),
+                "Ht": _Field(1)}

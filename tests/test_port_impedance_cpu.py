@@ -91,3 +91,31 @@ def test_multi_conductor_ports_rejected(tmp_path):
     with pytest.raises(OpemError) as e:
         project_info(proj)
     assert "multi-conductor" in str(e.value)
+
+
+def test_library_equals_oracle_definitions(tmp_path):
+    """The library's current and impedance under each definition equal the
+    oracle's restatement (oracle/portmode.py) on the coaxial project's port, as
+    read by the project reader (its current path included)."""
+    from oracle import fem
+    from oracle.materials import relative_eps
+    from oracle.nd_basis import FACES
+    from oracle.portmode import Fem2DMode
+    from openparem_b200.fem3d import project_problem
+    from project_files import write_coax_project
+    prob, fr = project_problem(write_coax_project(str(tmp_path), "PI"))
+    mode = prob["ports"][0]["mode"]
+    assert mode["zdef"] == "PI" and mode["ipath"].shape == (4, 3) and mode["ipath_closed"]
+    ops = fem.Operators(prob)
+    topo, faces = ops.topo, ops.ports[0]["faces"]
+    fv = np.array([topo.tets[topo.face_owner[x]][list(FACES[topo.face_lface[x]])] for x in faces])
+    reg = np.asarray(prob["tet_region"])[topo.face_owner[faces]]
+    f = fr[0]
+    eps = relative_eps(f, prob["eps_r"][reg], prob["tand"][reg], prob["sigma"][reg])
+    for zdef in ("PV", "VI", "PI"):
+        m = dict(mode, zdef=zdef)
+        om = Fem2DMode(prob, topo, faces, m, f)
+        lib = port_mode_faces_z(prob["verts"], fv, eps, m, m["nsub"], f, zdef, m["ipath"], order=2)
+        assert abs(lib["Z"] - om.Z) <= 1e-10 * abs(om.Z), (zdef, lib["Z"], om.Z)
+        # V and I scale with the mode's normalisation; their ratio does not
+        assert abs(lib["V"] / lib["I"] - om.V / om.I) <= 1e-10 * abs(om.V / om.I)
