@@ -118,7 +118,9 @@ int  opem_problem_set_port_fem2d(opem_problem prob, int port, const double* desc
  * definition OPEM_Z_PV (default) | OPEM_Z_VI | OPEM_Z_PI; path: npath >= 2 points
  * (xyz) of the current integration path in the port plane, I = sum over its
  * segments of int H . dl (a closed path also takes the segment from the last
- * point back to the first).  VI and PI need the path.  OPEM_ERR_UNSUPPORTED for a
+ * point back to the first).  VI and PI need the path.  The mode's sign is set by
+ * its voltage, so I takes the sign of the path's orientation: as in the reference's
+ * port files, orient it so that V / I is positive.  OPEM_ERR_UNSUPPORTED for a
  * port driven by an analytic TE mode.                                          */
 int  opem_problem_set_port_impedance(opem_problem prob, int port, int definition, int npath, const double* path,
                                      int closed);

@@ -229,8 +229,10 @@ def write_coax_project(d, zdef="PI", with_current=True, freqs=(3e9,)):
     """The rectangular coaxial line of coax_mesh as a project in directory d:
     ports on the 24 x 16 mm outline at z = 0 and z = L (the inner conductor a hole
     in their faces), voltage paths from the inner conductor to the outer wall
-    along +x, current paths a loop about the inner conductor; impedance_definition
-    zdef.  Returns the .proj path."""
+    along +x, current paths a loop about the inner conductor, clockwise seen from
+    outside each port (so the port's current has the sign of its voltage, as the
+    reference's own port files orient them); impedance_definition zdef.  Returns
+    the .proj path."""
     L = 24e-3
     verts, tets = coax_mesh(L=L)
     outline = [(-12e-3, -8e-3), (12e-3, -8e-3), (12e-3, 8e-3), (-12e-3, 8e-3)]
@@ -239,7 +241,8 @@ def write_coax_project(d, zdef="PI", with_current=True, freqs=(3e9,)):
     for k, z in ((1, 0.0), (2, L)):
         spec["paths"].append({"name": f"port{k}", "points": [(x, y, z) for x, y in outline], "closed": True})
         spec["paths"].append({"name": f"V{k}", "points": [(4e-3, 0.0, z), (12e-3, 0.0, z)], "closed": False})
-        spec["paths"].append({"name": f"I{k}", "points": [(x, y, z) for x, y in loop], "closed": True})
+        lp = loop if k == 1 else loop[::-1]   # outward normals -z and +z
+        spec["paths"].append({"name": f"I{k}", "points": [(x, y, z) for x, y in lp], "closed": True})
         integ = [{"type": "voltage", "paths": [f"+V{k}"]}]
         if with_current:
             integ.append({"type": "current", "paths": [f"+I{k}"]})
