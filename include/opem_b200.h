@@ -109,8 +109,11 @@ int  opem_problem_set_port_te(opem_problem prob, int port, const double* desc);
  * the tetrahedra behind them (the 2D solve the reference spawns per frequency,
  * port.cpp:5081-5176).  order 1: lowest-order edge elements for e_t and linear
  * nodal e_z (opem_port_mode_2d's solve); order 2: degree-2 edge elements and
- * quadratic nodal e_z (beta converges at fourth order in the split).  desc as for
- * opem_problem_set_port_te; its a, b, m, n are not used.                       */
+ * quadratic nodal e_z (beta converges at fourth order in the split); order p up
+ * to 8: first-kind edge elements of order p and degree-p nodal e_z, the spaces of
+ * the reference's 2D solver at mesh.order p (with nsub 1 and p the 3D order the
+ * mode lies in the 3D port trace space).  desc as for opem_problem_set_port_te;
+ * its a, b, m, n are not used.                                                 */
 int  opem_problem_set_port_fem2d(opem_problem prob, int port, const double* desc, int nsub, int order);
 /* Impedance definition of a port driven by its own 2D mode (after
  * opem_problem_set_port_fem2d; the reference's impedance_definition and current
@@ -221,8 +224,11 @@ int  opem_project_info(const char* proj_path, int order, int64_t* info, int ninf
  * (eps_r, tan_d, sigma, mu_r per region), tris (3 per face), attr (per face,
  * 1-based), bdr_type and bdr_params (3 per attribute: port index | sigma, Rz,
  * mu_r | eta), port_desc (22 per port, as opem_problem_set_port_te), port_nsub
- * (per port: 0 = analytic TE10, n > 0 = its own 2D mode with faces split n x n,
- * chosen for ports whose faces see more than one material), freqs.
+ * (per port: 0 = analytic TE10, n > 0 = its own 2D mode with faces split n x n
+ * and 2D elements of the problem's order (n = 1: the reference's own 2D problem),
+ * chosen for ports whose faces see more than one material or leave part of the
+ * port polygon uncovered, ports that are not rectangles and ports whose impedance
+ * definition uses the current), freqs.
  * Call once with only counts to size the buffers.                              */
 int  opem_project_read(const char* proj_path, int order, int64_t* counts, double* verts, int64_t* tets,
                        int32_t* region, double* region_mat, int64_t* tris, int32_t* attr, int32_t* bdr_type,

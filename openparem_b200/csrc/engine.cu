@@ -923,7 +923,7 @@ int opem_problem_set_port_te(opem_problem prob, int port, const double* desc) {
 }
 
 int opem_problem_set_port_fem2d(opem_problem prob, int port, const double* desc, int nsub, int order) {
-    if (!prob || !desc || port < 0 || port > 7 || nsub < 1 || nsub > 64 || order < 1 || order > 2) return OPEM_ERR_ARG;
+    if (!prob || !desc || port < 0 || port > 7 || nsub < 1 || nsub > 64 || order < 1 || order > 8) return OPEM_ERR_ARG;
     for (int i = 0; i < 22; ++i)
         if (!std::isfinite(desc[i])) return OPEM_ERR_ARG;
     Problem& P = prob->p;

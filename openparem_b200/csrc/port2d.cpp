@@ -19,6 +19,9 @@
 #include <complex>
 #include <cstring>
 #include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
 #include <numeric>
 #include <queue>
 #include <vector>
@@ -547,6 +550,371 @@ int port_mode_2d_p2(int64_t nnodes, const double* xy, int64_t ntri, const int64_
         for (int i = 0; i < 6; ++i) {
             const int m = zmap[zdof[6 * t + i]];
             cz[6 * t + i] = m >= 0 ? -cd(0, 1) * beta * xs[m] * sc : cd(0.0);   // e_z = -j beta psi
+        }
+    }
+    return OPEM_OK;
+}
+
+}  // namespace opem
+
+// ---------------------------------------------------------------------------
+// Order-p elements (the spaces of the reference's 2D solver at mesh.order p,
+// MFEM ND_FECollection(p) and H1_FECollection(p), OpenParEM2D fem2D.cpp:2188-2191)
+// ---------------------------------------------------------------------------
+namespace opem {
+
+namespace {
+// inverse of a dense real n x n matrix (row-major) by Gauss-Jordan with partial pivoting
+bool invert_real(int n, std::vector<double>& A) {
+    std::vector<double> I((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i) I[(size_t)i * n + i] = 1.0;
+    for (int c = 0; c < n; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < n; ++r)
+            if (std::fabs(A[(size_t)r * n + c]) > std::fabs(A[(size_t)piv * n + c])) piv = r;
+        if (!(std::fabs(A[(size_t)piv * n + c]) > 0)) return false;
+        if (piv != c)
+            for (int k = 0; k < n; ++k) {
+                std::swap(A[(size_t)piv * n + k], A[(size_t)c * n + k]);
+                std::swap(I[(size_t)piv * n + k], I[(size_t)c * n + k]);
+            }
+        const double d = 1.0 / A[(size_t)c * n + c];
+        for (int k = 0; k < n; ++k) { A[(size_t)c * n + k] *= d; I[(size_t)c * n + k] *= d; }
+        for (int r = 0; r < n; ++r) {
+            if (r == c) continue;
+            const double f = A[(size_t)r * n + c];
+            if (f == 0.0) continue;
+            for (int k = 0; k < n; ++k) {
+                A[(size_t)r * n + k] -= f * A[(size_t)c * n + k];
+                I[(size_t)r * n + k] -= f * I[(size_t)c * n + k];
+            }
+        }
+    }
+    A.swap(I);
+    return true;
+}
+
+double ipow(double x, int a) {
+    double r = 1.0;
+    for (int i = 0; i < a; ++i) r *= x;
+    return r;
+}
+
+RefSpaces2D build_ref_spaces(int p) {
+    RefSpaces2D R;
+    R.p = p;
+    for (int d = 0; d <= p; ++d)
+        for (int a = d; a >= 0; --a) { R.mono.push_back(a); R.mono.push_back(d - a); }
+    R.nm = (int)R.mono.size() / 2;
+    auto idx = [&](int a, int b) {
+        for (int m = 0; m < R.nm; ++m)
+            if (R.mono[2 * m] == a && R.mono[2 * m + 1] == b) return m;
+        throw std::runtime_error("monomial out of range");
+    };
+    // spanning set of R_p: P_{p-1}^2, then (-y, x) x^a y^(p-1-a)
+    std::vector<std::vector<double>> FX, FY;
+    for (int d = 0; d <= p - 1; ++d)
+        for (int a = d; a >= 0; --a) {
+            std::vector<double> e(R.nm, 0.0), z(R.nm, 0.0);
+            e[idx(a, d - a)] = 1.0;
+            FX.push_back(e); FY.push_back(z);
+            FX.push_back(z); FY.push_back(e);
+        }
+    for (int a = 0; a < p; ++a) {
+        const int b = p - 1 - a;
+        std::vector<double> ex(R.nm, 0.0), ey(R.nm, 0.0);
+        ex[idx(a, b + 1)] = -1.0;
+        ey[idx(a + 1, b)] = 1.0;
+        FX.push_back(ex); FY.push_back(ey);
+    }
+    const int nf = (int)FX.size();
+    if (nf != p * (p + 2)) throw std::runtime_error("edge space dimension");
+    R.nf = nf;
+    auto poly = [&](const std::vector<double>& c, double x, double y) {
+        double s = 0;
+        for (int m = 0; m < R.nm; ++m)
+            if (c[m] != 0.0) s += c[m] * ipow(x, R.mono[2 * m]) * ipow(y, R.mono[2 * m + 1]);
+        return s;
+    };
+    // degrees of freedom of the spanning functions: D (nf x nf), row = DOF
+    std::vector<double> D((size_t)nf * nf, 0.0);
+    std::vector<double> s, ws;
+    gauss_legendre01(p + 2, s, ws);
+    static const double VR[3][2] = {{0, 0}, {1, 0}, {0, 1}};
+    static const int LPr[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+    int row = 0;
+    for (auto& lp : LPr) {
+        const double ax = VR[lp[0]][0], ay = VR[lp[0]][1];
+        const double tx = VR[lp[1]][0] - ax, ty = VR[lp[1]][1] - ay;
+        for (int k = 0; k < p; ++k, ++row)
+            for (int j = 0; j < nf; ++j) {
+                double acc = 0;
+                for (size_t q = 0; q < s.size(); ++q) {
+                    const double x = ax + s[q] * tx, y = ay + s[q] * ty;
+                    acc += ws[q] * shifted_legendre(k, s[q]) * (poly(FX[j], x, y) * tx + poly(FY[j], x, y) * ty);
+                }
+                D[(size_t)row * nf + j] = acc;
+            }
+    }
+    if (p >= 2) {
+        std::vector<int> m2;
+        const std::vector<double> T2 = tri_test_polys(p - 2, m2);
+        const int nq2 = (int)m2.size() / 2;
+        std::vector<double> q1, q2, qw;
+        tri_rule(2 * p + 2, q1, q2, qw);
+        for (int r = 0; r < nq2; ++r)
+            for (int comp = 0; comp < 2; ++comp, ++row)
+                for (int j = 0; j < nf; ++j) {
+                    double acc = 0;
+                    for (size_t q = 0; q < qw.size(); ++q) {
+                        double tv = 0;
+                        for (int c = 0; c < nq2; ++c)
+                            tv += T2[(size_t)r * nq2 + c] * ipow(q1[q], m2[2 * c]) * ipow(q2[q], m2[2 * c + 1]);
+                        acc += qw[q] * tv * (comp ? poly(FY[j], q1[q], q2[q]) : poly(FX[j], q1[q], q2[q]));
+                    }
+                    D[(size_t)row * nf + j] = acc;
+                }
+    }
+    if (row != nf || !invert_real(nf, D)) throw std::runtime_error("edge degrees of freedom not unisolvent");
+    // nodal function i = sum_j F_j Dinv[j][i]
+    R.CX.assign((size_t)R.nm * nf, 0.0);
+    R.CY.assign((size_t)R.nm * nf, 0.0);
+    for (int j = 0; j < nf; ++j)
+        for (int i = 0; i < nf; ++i) {
+            const double c = D[(size_t)j * nf + i];
+            if (c == 0.0) continue;
+            for (int m = 0; m < R.nm; ++m) {
+                R.CX[(size_t)m * nf + i] += c * FX[j][m];
+                R.CY[(size_t)m * nf + i] += c * FY[j][m];
+            }
+        }
+    // Lagrange nodes and the inverse Vandermonde
+    std::vector<std::array<double, 2>> nodes = {{0, 0}, {1, 0}, {0, 1}};
+    for (auto& lp : LPr)
+        for (int k = 1; k < p; ++k)
+            nodes.push_back({VR[lp[0]][0] + (double)k / p * (VR[lp[1]][0] - VR[lp[0]][0]),
+                             VR[lp[0]][1] + (double)k / p * (VR[lp[1]][1] - VR[lp[0]][1])});
+    for (int j = 1; j < p; ++j)
+        for (int i = 1; i < p - j; ++i) nodes.push_back({(double)i / p, (double)j / p});
+    R.nl = (int)nodes.size();
+    if (R.nl != R.nm) throw std::runtime_error("Lagrange node count");
+    std::vector<double> V((size_t)R.nl * R.nm);
+    for (int r = 0; r < R.nl; ++r)
+        for (int m = 0; m < R.nm; ++m) V[(size_t)r * R.nm + m] = ipow(nodes[r][0], R.mono[2 * m]) * ipow(nodes[r][1], R.mono[2 * m + 1]);
+    if (!invert_real(R.nm, V)) throw std::runtime_error("Lagrange nodes not unisolvent");
+    R.CL = V;   // (V^-1)[m][i]: coefficient of monomial m in Lagrange function i
+    return R;
+}
+}  // namespace
+
+void RefSpaces2D::nd(double x, double y, double* N, double* curl) const {
+    for (int i = 0; i < nf; ++i) { N[2 * i] = N[2 * i + 1] = 0.0; curl[i] = 0.0; }
+    for (int m = 0; m < nm; ++m) {
+        const int a = mono[2 * m], b = mono[2 * m + 1];
+        const double v = ipow(x, a) * ipow(y, b);
+        const double dx = a > 0 ? a * ipow(x, a - 1) * ipow(y, b) : 0.0;
+        const double dy = b > 0 ? b * ipow(x, a) * ipow(y, b - 1) : 0.0;
+        const double* cx = &CX[(size_t)m * nf];
+        const double* cy = &CY[(size_t)m * nf];
+        for (int i = 0; i < nf; ++i) {
+            N[2 * i] += cx[i] * v;
+            N[2 * i + 1] += cy[i] * v;
+            curl[i] += cy[i] * dx - cx[i] * dy;
+        }
+    }
+}
+
+void RefSpaces2D::h1(double x, double y, double* L, double* gL) const {
+    for (int i = 0; i < nl; ++i) { L[i] = 0.0; gL[2 * i] = gL[2 * i + 1] = 0.0; }
+    for (int m = 0; m < nm; ++m) {
+        const int a = mono[2 * m], b = mono[2 * m + 1];
+        const double v = ipow(x, a) * ipow(y, b);
+        const double dx = a > 0 ? a * ipow(x, a - 1) * ipow(y, b) : 0.0;
+        const double dy = b > 0 ? b * ipow(x, a) * ipow(y, b - 1) : 0.0;
+        const double* c = &CL[(size_t)m * nl];
+        for (int i = 0; i < nl; ++i) {
+            L[i] += c[i] * v;
+            gL[2 * i] += c[i] * dx;
+            gL[2 * i + 1] += c[i] * dy;
+        }
+    }
+}
+
+const RefSpaces2D& ref_spaces_2d(int p) {
+    static std::mutex mu;
+    static std::map<int, std::unique_ptr<RefSpaces2D>> cache;
+    if (p < 1 || p > 8) throw std::runtime_error("2D element order must be 1..8");
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(p);
+    if (it == cache.end()) it = cache.emplace(p, std::make_unique<RefSpaces2D>(build_ref_spaces(p))).first;
+    return *it->second;
+}
+
+}  // namespace opem
+
+namespace opem {
+
+int port_mode_2d_pp(int64_t nnodes, const double* xy, int64_t ntri, const int64_t* tris, const cd* eps_r,
+                    const cd* mu_r, double freq, int p, cd& beta, std::vector<cd>& ct, std::vector<cd>& cz,
+                    std::vector<int64_t>& st) {
+    if (nnodes < 3 || !xy || ntri < 1 || !tris || !eps_r || !(freq > 0) || p < 1 || p > 8) return OPEM_ERR_ARG;
+    for (int64_t t = 0; t < 3 * ntri; ++t)
+        if (tris[t] < 0 || tris[t] >= nnodes) return OPEM_ERR_ARG;
+    const RefSpaces2D& R = ref_spaces_2d(p);
+    static const int LP[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+    const double k0 = 2 * M_PI * freq * std::sqrt(MU0 * EPS0);
+    st.resize(3 * ntri);
+    std::map<std::pair<int64_t, int64_t>, int> eid;
+    for (int64_t t = 0; t < ntri; ++t) {
+        int64_t v[3] = {tris[3 * t], tris[3 * t + 1], tris[3 * t + 2]};
+        std::sort(v, v + 3);
+        for (int k = 0; k < 3; ++k) st[3 * t + k] = v[k];
+        for (auto& lp : LP) eid[{v[lp[0]], v[lp[1]]}] = 0;
+    }
+    int ne = 0;
+    std::vector<std::pair<int64_t, int64_t>> edges;
+    for (auto& kv : eid) { kv.second = ne++; edges.push_back(kv.first); }
+    // global numbering: e_t = [edge moments (p per edge), interior (p (p-1) per triangle)],
+    // e_z = [vertex (nnodes), edge nodes (p-1 per edge), interior ((p-1)(p-2)/2 per triangle)]
+    const int nf = R.nf, nl = R.nl, nint = p * (p - 1), nle = p - 1, nli = (p - 1) * (p - 2) / 2;
+    const int64_t net = (int64_t)ne * p + ntri * nint, nz = nnodes + (int64_t)ne * nle + ntri * nli;
+    std::vector<int64_t> tdof((size_t)nf * ntri), zdof((size_t)nl * ntri);
+    std::vector<int> ecount(ne, 0);
+    for (int64_t t = 0; t < ntri; ++t) {
+        int64_t* td = &tdof[(size_t)nf * t];
+        int64_t* zd = &zdof[(size_t)nl * t];
+        for (int i = 0; i < 3; ++i) {
+            const int e = eid[{st[3 * t + LP[i][0]], st[3 * t + LP[i][1]]}];
+            ++ecount[e];
+            for (int k = 0; k < p; ++k) td[p * i + k] = (int64_t)e * p + k;
+            for (int k = 0; k < nle; ++k) zd[3 + nle * i + k] = nnodes + (int64_t)e * nle + k;
+            zd[i] = st[3 * t + i];
+        }
+        for (int j = 0; j < nint; ++j) td[3 * p + j] = (int64_t)ne * p + t * nint + j;
+        for (int j = 0; j < nli; ++j) zd[3 + 3 * nle + j] = nnodes + (int64_t)ne * nle + t * nli + j;
+    }
+    if (net > INT32_MAX / 2 || nz > INT32_MAX / 2) return OPEM_ERR_ARG;
+    // reference bases at the quadrature points (exact for the degree-2p products)
+    std::vector<double> q1, q2, qw;
+    tri_rule(2 * p + 1, q1, q2, qw);
+    const int nq = (int)qw.size();
+    std::vector<double> Nh((size_t)nq * nf * 2), Ch((size_t)nq * nf), Lh((size_t)nq * nl), Gh((size_t)nq * nl * 2);
+    for (int q = 0; q < nq; ++q) {
+        R.nd(q1[q], q2[q], &Nh[(size_t)q * nf * 2], &Ch[(size_t)q * nf]);
+        R.h1(q1[q], q2[q], &Lh[(size_t)q * nl], &Gh[(size_t)q * nl * 2]);
+    }
+    std::vector<Triplet> Aee, Bee, Ben, Bnn;
+    double emax = 0;
+    std::vector<double> M((size_t)nf * nf), C((size_t)nf * nf), Gm((size_t)nf * nl), Kg((size_t)nl * nl),
+        Ml((size_t)nl * nl), Np((size_t)nf * 2), Gp((size_t)nl * 2);
+    for (int64_t t = 0; t < ntri; ++t) {
+        const double* p0 = xy + 2 * st[3 * t];
+        const double* p1 = xy + 2 * st[3 * t + 1];
+        const double* p2 = xy + 2 * st[3 * t + 2];
+        const double J00 = p1[0] - p0[0], J01 = p2[0] - p0[0], J10 = p1[1] - p0[1], J11 = p2[1] - p0[1];
+        const double det = J00 * J11 - J01 * J10;
+        if (!(std::fabs(det) > 0)) return OPEM_ERR_ARG;
+        // J^-T = [[J11, -J10], [-J01, J00]] / det
+        const double a00 = J11 / det, a01 = -J10 / det, a10 = -J01 / det, a11 = J00 / det;
+        const cd er = eps_r[t], mr = mu_r ? mu_r[t] : cd(1.0), im = 1.0 / mr;
+        emax = std::max(emax, std::real(er * mr));
+        std::fill(M.begin(), M.end(), 0.0);
+        std::fill(C.begin(), C.end(), 0.0);
+        std::fill(Gm.begin(), Gm.end(), 0.0);
+        std::fill(Kg.begin(), Kg.end(), 0.0);
+        std::fill(Ml.begin(), Ml.end(), 0.0);
+        for (int q = 0; q < nq; ++q) {
+            const double w = qw[q] * std::fabs(det);
+            const double* nh = &Nh[(size_t)q * nf * 2];
+            const double* ch = &Ch[(size_t)q * nf];
+            const double* lh = &Lh[(size_t)q * nl];
+            const double* gh = &Gh[(size_t)q * nl * 2];
+            for (int i = 0; i < nf; ++i) {
+                Np[2 * i] = a00 * nh[2 * i] + a01 * nh[2 * i + 1];
+                Np[2 * i + 1] = a10 * nh[2 * i] + a11 * nh[2 * i + 1];
+            }
+            for (int i = 0; i < nl; ++i) {
+                Gp[2 * i] = a00 * gh[2 * i] + a01 * gh[2 * i + 1];
+                Gp[2 * i + 1] = a10 * gh[2 * i] + a11 * gh[2 * i + 1];
+            }
+            for (int i = 0; i < nf; ++i) {
+                const double ci = ch[i] / det;
+                for (int j = 0; j < nf; ++j) {
+                    M[(size_t)i * nf + j] += w * (Np[2 * i] * Np[2 * j] + Np[2 * i + 1] * Np[2 * j + 1]);
+                    C[(size_t)i * nf + j] += w * ci * (ch[j] / det);
+                }
+                for (int j = 0; j < nl; ++j)
+                    Gm[(size_t)i * nl + j] += w * (Np[2 * i] * Gp[2 * j] + Np[2 * i + 1] * Gp[2 * j + 1]);
+            }
+            for (int i = 0; i < nl; ++i)
+                for (int j = 0; j < nl; ++j) {
+                    Kg[(size_t)i * nl + j] += w * (Gp[2 * i] * Gp[2 * j] + Gp[2 * i + 1] * Gp[2 * j + 1]);
+                    Ml[(size_t)i * nl + j] += w * lh[i] * lh[j];
+                }
+        }
+        const int64_t* td = &tdof[(size_t)nf * t];
+        const int64_t* zd = &zdof[(size_t)nl * t];
+        for (int i = 0; i < nf; ++i) {
+            for (int j = 0; j < nf; ++j) {
+                Aee.push_back({(int)td[i], (int)td[j], im * C[(size_t)i * nf + j] - k0 * k0 * er * M[(size_t)i * nf + j]});
+                Bee.push_back({(int)td[i], (int)td[j], im * M[(size_t)i * nf + j]});
+            }
+            for (int j = 0; j < nl; ++j) Ben.push_back({(int)td[i], (int)zd[j], -im * Gm[(size_t)i * nl + j]});
+        }
+        for (int i = 0; i < nl; ++i)
+            for (int j = 0; j < nl; ++j)
+                Bnn.push_back({(int)zd[i], (int)zd[j], im * Kg[(size_t)i * nl + j] - k0 * k0 * er * Ml[(size_t)i * nl + j]});
+    }
+    // PEC: every DOF of a boundary edge (its moments, its edge nodes) and its vertices
+    std::vector<int> tmap(net, -1), zmap(nz, -1);
+    std::vector<char> bnode(nnodes, 0), bedge(ne, 0);
+    for (int e = 0; e < ne; ++e)
+        if (ecount[e] == 1) { bedge[e] = 1; bnode[edges[e].first] = 1; bnode[edges[e].second] = 1; }
+    int nu = 0;
+    for (int64_t i = 0; i < net; ++i) {
+        const bool drop = i < (int64_t)ne * p && bedge[i / p];
+        if (!drop) tmap[i] = nu++;
+    }
+    const int nut = nu;
+    std::vector<char> used(nnodes, 0);
+    for (int64_t t = 0; t < 3 * ntri; ++t) used[tris[t]] = 1;
+    for (int64_t i = 0; i < nz; ++i) {
+        bool drop = false;
+        if (i < nnodes) drop = !used[i] || bnode[i];
+        else if (i < nnodes + (int64_t)ne * nle) drop = bedge[(i - nnodes) / nle];
+        if (!drop) zmap[i] = nu++;
+    }
+    const int n = nu;
+    if (nut == 0) return OPEM_ERR_ARG;
+    std::vector<Triplet> A, Bm;
+    for (auto& x : Aee) if (tmap[x.r] >= 0 && tmap[x.c] >= 0) A.push_back({tmap[x.r], tmap[x.c], x.v});
+    for (auto& x : Bee) if (tmap[x.r] >= 0 && tmap[x.c] >= 0) Bm.push_back({tmap[x.r], tmap[x.c], x.v});
+    for (auto& x : Ben)
+        if (tmap[x.r] >= 0 && zmap[x.c] >= 0) {
+            Bm.push_back({tmap[x.r], zmap[x.c], x.v});
+            Bm.push_back({zmap[x.c], tmap[x.r], x.v});
+        }
+    for (auto& x : Bnn) if (zmap[x.r] >= 0 && zmap[x.c] >= 0) Bm.push_back({zmap[x.r], zmap[x.c], x.v});
+    cd lam = 0;
+    std::vector<cd> xs;
+    int rc = solve_pencil(n, A, Bm, -k0 * k0 * emax, lam, xs);
+    if (rc != OPEM_OK) return rc;
+    beta = std::sqrt(-lam);
+    if (beta.real() < 0) beta = -beta;
+    cd big = 0.0;
+    for (int64_t i = 0; i < (int64_t)ne * p; ++i)
+        if (tmap[i] >= 0 && std::abs(xs[tmap[i]]) > std::abs(big)) big = xs[tmap[i]];
+    const cd sc = std::abs(big) > 0 ? 1.0 / big : cd(1.0);
+    ct.assign((size_t)nf * ntri, 0.0);
+    cz.assign((size_t)nl * ntri, 0.0);
+    for (int64_t t = 0; t < ntri; ++t) {
+        for (int i = 0; i < nf; ++i) {
+            const int m = tmap[tdof[(size_t)nf * t + i]];
+            ct[(size_t)nf * t + i] = m >= 0 ? xs[m] * sc : cd(0.0);
+        }
+        for (int i = 0; i < nl; ++i) {
+            const int m = zmap[zdof[(size_t)nl * t + i]];
+            cz[(size_t)nl * t + i] = m >= 0 ? -cd(0, 1) * beta * xs[m] * sc : cd(0.0);   // e_z = -j beta psi
         }
     }
     return OPEM_OK;

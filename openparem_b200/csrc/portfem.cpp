@@ -63,7 +63,22 @@ void PortFem2D::eval_tri(int64_t t, const double X[3], cd E[3], cd Hy[3]) const 
     const double lam[3] = {1 - l1 - l2, l1, l2};
     const double* gg = &g[6 * t];
     cd ex = 0.0, ey = 0.0, zx, zy;
-    if (order == 2) {
+    if (order >= 3) {
+        // reference bases at (l1, l2), covariant map J^-T (J^-1 = Ji row-major)
+        const int nf = ref->nf, nl = ref->nl;
+        std::vector<double> N(2 * nf), cu(nf), L(nl), gL(2 * nl);
+        ref->nd(l1, l2, N.data(), cu.data());
+        ref->h1(l1, l2, L.data(), gL.data());
+        cd rx = 0.0, ry = 0.0, gx = 0.0, gy = 0.0;
+        const cd* c = &ct[(size_t)nf * t];
+        for (int i = 0; i < nf; ++i) { rx += c[i] * N[2 * i]; ry += c[i] * N[2 * i + 1]; }
+        const cd* z = &cz[(size_t)nl * t];
+        for (int i = 0; i < nl; ++i) { gx += z[i] * gL[2 * i]; gy += z[i] * gL[2 * i + 1]; }
+        ex = Ji[0] * rx + Ji[2] * ry;
+        ey = Ji[1] * rx + Ji[3] * ry;
+        zx = Ji[0] * gx + Ji[2] * gy;
+        zy = Ji[1] * gx + Ji[3] * gy;
+    } else if (order == 2) {
         // W_ab, G_ab = grad(l_a l_b) per edge, then l_2 W_01 and l_0 W_12; e_z quadratic
         zx = 0.0;
         zy = 0.0;
@@ -138,7 +153,7 @@ int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* fv, cons
         err = "impedance definition: VI and PI need a current path of at least two points";
         return OPEM_ERR_ARG;
     }
-    if (nface < 1 || nsub < 1 || nsub > 64 || order < 1 || order > 2 || !(freq > 0)) {
+    if (nface < 1 || nsub < 1 || nsub > 64 || order < 1 || order > 8 || !(freq > 0)) {
         err = "port mode: bad arguments";
         return OPEM_ERR_ARG;
     }
@@ -228,12 +243,24 @@ int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* fv, cons
     int64_t ne = 0;
     std::vector<int64_t> edges;
     std::vector<double> et, ez;
-    if (order == 2) {
+    if (order >= 2) {
         std::vector<cd> epsc(T), muc(T);
         for (int64_t t = 0; t < T; ++t) { epsc[t] = cd(eps2[2 * t], eps2[2 * t + 1]); muc[t] = M.mu[t]; }
         cd b2;
         std::vector<int64_t> st2;
-        int rc = port_mode_2d_p2(nn, M.xy.data(), T, tris.data(), epsc.data(), muc.data(), freq, b2, M.ct, M.cz, st2);
+        int rc;
+        if (order == 2) {
+            rc = port_mode_2d_p2(nn, M.xy.data(), T, tris.data(), epsc.data(), muc.data(), freq, b2, M.ct, M.cz, st2);
+        } else {
+            try {
+                M.ref = &ref_spaces_2d(order);
+            } catch (const std::exception& e) {
+                err = e.what();
+                return OPEM_ERR_ARG;
+            }
+            rc = port_mode_2d_pp(nn, M.xy.data(), T, tris.data(), epsc.data(), muc.data(), freq, order, b2, M.ct,
+                                 M.cz, st2);
+        }
         if (rc != OPEM_OK) { err = "port mode: 2D eigensolve failed"; return rc; }
         beta[0] = b2.real();
         beta[1] = b2.imag();
@@ -277,7 +304,7 @@ int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* fv, cons
             M.g[6 * t + 2 * k] = Ji[0] * r[k][0] + Ji[2] * r[k][1];
             M.g[6 * t + 2 * k + 1] = Ji[1] * r[k][0] + Ji[3] * r[k][1];
         }
-        if (order == 2) continue;   // coefficients per triangle already (ct, cz)
+        if (order >= 2) continue;   // coefficients per triangle already (ct, cz)
         for (int i = 0; i < 3; ++i) {
             const int64_t e = eid.at({s[LP[i][0]], s[LP[i][1]]});
             M.ce[3 * t + i] = cd(et[2 * e], et[2 * e + 1]);
@@ -315,10 +342,10 @@ int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* fv, cons
         const double w = 2 * M_PI * freq;
         const cd y = M.gamma / cd(0.0, w * MU0 * mu_port);
         // edge-midpoint rule (exact for the quadratic integrand of order 1), or
-        // the degree-4 triangle rule (order 2: quartic integrand)
+        // the degree-2p triangle rule (order p >= 2: integrand of degree 2p)
         std::vector<double> r1, r2, rw;
-        if (order == 2) {
-            tri_rule(4, r1, r2, rw);
+        if (order >= 2) {
+            tri_rule(2 * order, r1, r2, rw);
             for (double& x : rw) x *= 6.0;   // weights of the midpoint form: area/3 * sum -> sum_q 2 w_q area
         } else {
             r1 = {0.5, 0.0, 0.5};

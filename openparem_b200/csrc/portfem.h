@@ -17,10 +17,37 @@ int port_mode_2d_p2(int64_t nnodes, const double* xy, int64_t ntri, const int64_
                     std::complex<double>& beta, std::vector<std::complex<double>>& ct,
                     std::vector<std::complex<double>>& cz, std::vector<int64_t>& st);
 
+// Nodal bases of order p on the unit triangle (x, y >= 0, x + y <= 1), with the
+// triangle's vertices in increasing global order: the first-kind Nedelec space
+// R_p = P_{p-1}^2 + (-y, x) P~_{p-1} (p (p+2) functions, degrees of freedom the
+// edge moments against shifted Legendre L_0..L_{p-1} along each edge from its
+// lower to its higher vertex, then interior moments against P_{p-2}^2) and the
+// Lagrange space of degree p (equispaced nodes: vertices, edge nodes from the
+// edge's lower vertex, interior), both as coefficients over the monomials
+// x^a y^b of degree <= p.
+struct RefSpaces2D {
+    int p = 0, nm = 0, nf = 0, nl = 0;
+    std::vector<int> mono;            // 2 nm exponents
+    std::vector<double> CX, CY, CL;   // nm x nf, nm x nf, nm x nl (row m, column i)
+    // values N (nf x 2) and scalar curls (nf) of the edge functions at (x, y)
+    void nd(double x, double y, double* N, double* curl) const;
+    // values (nl) and gradients (nl x 2) of the Lagrange functions at (x, y)
+    void h1(double x, double y, double* L, double* gL) const;
+};
+const RefSpaces2D& ref_spaces_2d(int p);   // cached; throws std::runtime_error for p < 1 or p > 8
+
+// The fundamental mode with order-p elements of RefSpaces2D (the spaces of the
+// reference's 2D solver at mesh.order p): per triangle nf e_t and nl e_z
+// coefficients on the reference bases, and the sorted vertex ids.
+int port_mode_2d_pp(int64_t nnodes, const double* xy, int64_t ntri, const int64_t* tris,
+                    const std::complex<double>* eps_r, const std::complex<double>* mu_r, double freq, int p,
+                    std::complex<double>& beta, std::vector<std::complex<double>>& ct,
+                    std::vector<std::complex<double>>& cz, std::vector<int64_t>& st);
+
 struct PortFem2D {
     using cd = std::complex<double>;
     int nsub = 0;
-    int order = 1;                    // 2D element order (1 or 2)
+    int order = 1;                    // 2D element order (1 .. 8)
     int64_t nface = 0;
     double o[3], u[3], v[3], n[3];    // unit frame of the port plane; n = outward normal
     double freq = 0, mu_port = 1;
@@ -29,7 +56,8 @@ struct PortFem2D {
     std::vector<int64_t> st;          // 3 sorted node ids per sub-triangle
     std::vector<double> P0, Jinv, g;  // per sub-triangle: first node (2), J^-1 (4), grad lambda (3x2)
     std::vector<cd> ce, gz, mu;       // order 1: edge coefficients (3), grad e_z (2); mu_r (1)
-    std::vector<cd> ct, cz;           // order 2: e_t (8) and e_z (6) coefficients
+    std::vector<cd> ct, cz;           // order 2: e_t (8) and e_z (6) coefficients; order >= 3: nf and nl
+    const RefSpaces2D* ref = nullptr; // order >= 3: the reference bases
     std::vector<int64_t> sub;         // per face: (i, j, upper) -> sub-triangle
 
     // E_t and H_t / y (y = gamma / (j w mu0 mu_port)) at the 3D point X of

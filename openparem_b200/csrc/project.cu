@@ -512,10 +512,11 @@ void build(const std::string& proj_path, int order_override, Project& P) {
         for (int i = 0; i < 3; ++i) { d[16 + i] = vs[i]; d[19 + i] = ve[i]; }
         P.port_desc.push_back(d);
         // a port whose faces see more than one material is driven by its own 2D
-        // mode (as the reference drives every port), with second-order 2D elements
-        // on a split that keeps the 2D mesh near 1024 triangles
+        // mode (as the reference drives every port), solved as the reference's 2D
+        // solver does: on the port faces themselves (no split) with elements of the
+        // problem's order, so the mode lies in the 3D port trace space
         // (and every port that is not a rectangle, which has no analytic mode here)
-        const int nsub = (int)std::lround(std::sqrt(1024.0 / (double)std::max<int64_t>(1, port_nface[p])));
+        const int nsub = 1;
         // faces that leave part of the port polygon uncovered (a conductor inside
         // the cross-section is a hole in them): no analytic mode either
         double parea = 0.0;
@@ -548,8 +549,7 @@ void build(const std::string& proj_path, int order_override, Project& P) {
         P.port_zdef.push_back(zdef);
         P.port_ipath.push_back(ip);
         P.port_ipath_closed.push_back(ipc);
-        P.port_nsub.push_back(port_mixed[p] || !port_rect[p] || holes || zdef != OPEM_Z_PV ? std::min(16, std::max(1, nsub))
-                                                                                           : 0);
+        P.port_nsub.push_back(port_mixed[p] || !port_rect[p] || holes || zdef != OPEM_Z_PV ? nsub : 0);
     }
     // boundary conditions: attribute 1 the faces no port or Boundary block claims
     // (PEC, or the surface impedance of materials.default.boundary, as
@@ -722,7 +722,8 @@ int opem_project_load(opem_context ctx, const char* proj_path, int order, opem_p
         rc = opem_problem_set_boundary(prob, (int)a + 1, type, np ? P.bdr[a].second.data() : nullptr, np);
     }
     for (size_t p = 0; rc == OPEM_OK && p < P.port_desc.size(); ++p) {
-        rc = P.port_nsub[p] > 0 ? opem_problem_set_port_fem2d(prob, (int)p, P.port_desc[p].data(), P.port_nsub[p], 2)
+        rc = P.port_nsub[p] > 0 ? opem_problem_set_port_fem2d(prob, (int)p, P.port_desc[p].data(), P.port_nsub[p],
+                                                              std::min(8, P.order))
                                 : opem_problem_set_port_te(prob, (int)p, P.port_desc[p].data());
         if (rc == OPEM_OK && P.port_nsub[p] > 0 && !P.port_ipath[p].empty())
             rc = opem_problem_set_port_impedance(prob, (int)p, P.port_zdef[p], (int)(P.port_ipath[p].size() / 3),

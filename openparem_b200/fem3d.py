@@ -193,8 +193,8 @@ def project_problem(proj_path, order=0):
         mode = {"kind": "TE", "m": int(d[14]), "n": int(d[15]), "a": d[12], "b": d[13],
                 "origin": d[0:3].tolist(), "u": d[3:6].tolist(), "v": d[6:9].tolist(),
                 "normal": d[9:12].tolist(), "vpath": (d[16:19].tolist(), d[19:22].tolist())}
-        if ns[k] > 0:   # the port's own 2D mode (the reader uses second-order 2D elements)
-            mode.update(kind="FEM2D", nsub=int(ns[k]), order2d=2)
+        if ns[k] > 0:   # the port's own 2D mode (the reader: 2D elements of the problem's order)
+            mode.update(kind="FEM2D", nsub=int(ns[k]), order2d=min(8, int(p)))
             zd, cl, npth = C.c_int(0), C.c_int(1), C.c_int(0)
             pbuf = np.zeros((64, 3))
             rc = L.opem_project_port_impedance(path, k, C.byref(zd), C.byref(cl), C.byref(npth), _dp(pbuf), 64, msg,

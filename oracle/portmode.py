@@ -30,6 +30,7 @@ from .materials import MU0, EPS0, relative_eps
 from .modes import _frame
 from .nd_basis import FACES
 from .port2d import solve_mode, solve_mode_p2, LP2
+from .port2d_pp import solve_mode_pp, ref_spaces
 from .quadrature import tri_rule
 
 
@@ -100,7 +101,13 @@ class Fem2DMode:
                            np.asarray(prob["sigma"], dtype=np.float64)[reg])
         mu = np.asarray(prob["mu_r"], dtype=np.float64)[reg].astype(np.complex128)
         self.order = int(mode.get("order2d", 1))
-        if self.order == 2:
+        if self.order >= 3:   # order-p edge / Lagrange elements (oracle.port2d_pp)
+            beta, ct, cz, _ = solve_mode_pp(xy, tris, freq, eps, mu, self.order)
+            e0 = ct[:, :3 * self.order].ravel()
+            big = e0[np.argmax(np.abs(e0))]
+            self.ctp, self.czp = ct / big, cz / big
+            self.ref = ref_spaces(self.order)
+        elif self.order == 2:
             beta, ct, cz, _ = solve_mode_p2(xy, tris, freq, eps, mu)
             big = ct[:, :3].ravel()[np.argmax(np.abs(ct[:, :3]).ravel())]   # largest Whitney coefficient
             self.ct, self.cz2 = ct / big, cz / big
@@ -137,7 +144,7 @@ class Fem2DMode:
         ws = np.tile(0.5 * wg / K, K)
         Xp = p0[None, :] + s[:, None] * (p1 - p0)[None, :]
         self.V = -np.sum(ws * (self.Et(Xp) @ (p1 - p0)))
-        q, wq = tri_rule(4)
+        q, wq = tri_rule(max(4, 2 * self.order))   # exact for the degree-2p integrand
         T, nq = len(st), len(wq)
         tt = np.repeat(np.arange(T), nq)
         X2 = (self.P0[tt] + np.tile(q[:, 0], T)[:, None] * (P[tt, 1] - P[tt, 0])
@@ -177,7 +184,13 @@ class Fem2DMode:
         lam = np.stack([1 - lam12[:, 0] - lam12[:, 1], lam12[:, 0], lam12[:, 1]], axis=1)   # (p,3)
         g = self.g[t]                                               # (p,3,2)
         e2 = np.zeros((len(t), 2), dtype=np.complex128)
-        if self.order == 2:
+        if self.order >= 3:
+            Nh, _ = self.ref.nd(lam12)                              # reference coordinates = (lambda_1, lambda_2)
+            _, gLh = self.ref.h1(lam12)
+            JiT = np.transpose(self.Jinv[t], (0, 2, 1))
+            e2 = np.einsum("pij,pj->pi", JiT, np.einsum("pn,pni->pi", self.ctp[t], Nh))
+            gz = np.einsum("pij,pj->pi", JiT, np.einsum("pl,pli->pi", self.czp[t], gLh))
+        elif self.order == 2:
             gz = np.zeros((len(t), 2), dtype=np.complex128)
             for i, (a, b) in enumerate(LP2):
                 W = lam[:, a:a + 1] * g[:, b] - lam[:, b:b + 1] * g[:, a]

@@ -54,7 +54,7 @@ def test_reference_projects_match_oracle(tmp_path, name):
 def test_loaded_project_2d_mode_ports_match_oracle(tmp_path):
     """The reference's slab-loaded WR90 project: its ports see air and teflon, so
     the reader drives them by their own 2D modes (solved per frequency on the
-    port faces split 16 x 16).  ND2 on the device, plain FP64 and the batched
+    port faces with 2D elements of the problem's order).  ND2 on the device, plain FP64 and the batched
     mixed sweep, against the oracle on the problem the same reader produced
     (|dS| <= 1e-8 plain with solver rtol 1e-12; <= 1e-6 mixed)."""
     from oracle import fem
@@ -125,8 +125,9 @@ def test_coax_project_impedance_definitions(tmp_path):
     """A rectangular coaxial line read from projects whose ports use the PI, VI
     and PV impedance definitions (current paths about the inner conductor): the
     device solve's port impedance equals the host 2D mode's under the same
-    definition (same faces, split 5 x 5, second-order 2D elements), the three
-    definitions agree to 0.5 % on this TEM line, and the line passes the wave
+    definition (the same faces unsplit, second-order 2D elements), the three
+    definitions agree to 1 % on this TEM line (0.75 % on these unsplit faces; the
+    spread shrinks as the port faces are refined), and the line passes the wave
     (|S21| > 0.99)."""
     import os
     from openparem_b200.fem3d import port_mode_faces_z
@@ -145,7 +146,7 @@ def test_coax_project_impedance_definitions(tmp_path):
         F.assemble()
         S, Zo, st = F.solve(fr[0], default_opts(rtol=1e-10, restart=200, maxits=6000))
         assert st["converged"] == 1 and abs(S[1, 0]) > 0.99, (zdef, S)
-        host = port_mode_faces_z(verts, fv, np.ones(len(fv), dtype=complex), mode, 5, fr[0], zdef, loop)["Z"]
+        host = port_mode_faces_z(verts, fv, np.ones(len(fv), dtype=complex), mode, 1, fr[0], zdef, loop)["Z"]
         assert abs(Zo[0] / host - 1) < 1e-8, (zdef, Zo, host)
         zo[zdef] = Zo[0]
-    assert abs(zo["PI"] / zo["PV"] - 1) < 5e-3 and abs(zo["VI"] / zo["PV"] - 1) < 5e-3
+    assert abs(zo["PI"] / zo["PV"] - 1) < 1e-2 and abs(zo["VI"] / zo["PV"] - 1) < 1e-2

@@ -86,10 +86,14 @@ def test_empty_guide_converges_to_analytic_te10():
 
 
 def test_reader_loaded_project_nd6_near_reference(tmp_path):
+    """The reader drives the reference's slab-loaded project's ports by order-6
+    modes on the unsplit port faces, the reference's own 2D problem; the oracle
+    then reproduces the reference's found arg S21 to 2e-7 deg and |S21| to 1e-10
+    dB (with second-order modes on faces split 10 x 10: 1.2e-6 deg)."""
     proj, rec = reference_project(str(tmp_path), "straight-loaded")
     prob, fr = project_problem(proj)
     assert [p["mode"]["kind"] for p in prob["ports"]] == ["FEM2D", "FEM2D"]
-    assert all(p["mode"]["nsub"] == 10 and p["mode"]["order2d"] == 2 for p in prob["ports"])
+    assert all(p["mode"]["nsub"] == 1 and p["mode"]["order2d"] == 6 for p in prob["ports"])
     assert np.allclose(fr, [8.3e9])
     S = fem.solve_frequency(fem.Operators(prob), 8.3e9)["S"]
     import json
@@ -99,6 +103,62 @@ def test_reader_loaded_project_nd6_near_reference(tmp_path):
              and v["portIn"] == 1][0]
     found_db = [v["found"] for v in cases.values() if v["variable"] == "magS(dB)" and v["portOut"] == 2
                 and v["portIn"] == 1][0]
-    assert abs(np.angle(S[1, 0], deg=True) - found) < 5e-6
-    assert abs(20 * np.log10(abs(S[1, 0])) - found_db) < 1e-8
+    assert abs(np.angle(S[1, 0], deg=True) - found) < 2e-7
+    assert abs(20 * np.log10(abs(S[1, 0])) - found_db) < 1e-10
     assert 20 * np.log10(abs(S[0, 0])) < -100
+
+
+@pytest.mark.parametrize("order,nsub", [(3, 1), (4, 1), (6, 1), (3, 2)])
+def test_library_order_p_mode_equals_oracle(order, nsub):
+    """Order-p port modes (the reference's 2D spaces at mesh.order p): the
+    library's gamma, Z, V and fields equal the oracle's restatement
+    (oracle/port2d_pp.py) on the slab-loaded guide's ports."""
+    prob = loaded(1)
+    ops = fem.Operators(prob)
+    topo = ops.topo
+    f = 8.3e9
+    rng = np.random.default_rng(5)
+    for k in range(2):
+        mode = dict(prob["ports"][k]["mode"], kind="FEM2D", nsub=nsub, order2d=order)
+        faces = ops.ports[k]["faces"]
+        om = Fem2DMode(prob, topo, faces, mode, f)
+        fv = np.array([topo.tets[topo.face_owner[x]][list(FACES[topo.face_lface[x]])] for x in faces])
+        reg = np.asarray(prob["tet_region"])[topo.face_owner[faces]]
+        eps = relative_eps(f, prob["eps_r"][reg], prob["tand"][reg], prob["sigma"][reg])
+        pf = rng.integers(0, len(faces), 150)
+        a = rng.random((150, 2))
+        a = np.where(a.sum(1, keepdims=True) > 1, 1 - a[:, ::-1], a)
+        met, E, Hy = port_mode_faces(prob["verts"], fv, eps, mode, nsub, f, pf, a, order=order)
+        V = np.asarray(prob["verts"])
+        X = V[fv[pf, 0]] + a[:, 0:1] * (V[fv[pf, 1]] - V[fv[pf, 0]]) + a[:, 1:2] * (V[fv[pf, 2]] - V[fv[pf, 0]])
+        Eo = np.concatenate([om.metrics()["Et"].at_face(pf[i], a[i:i + 1], X[i:i + 1]) for i in range(len(pf))])
+        Ho = np.concatenate([om.metrics()["Ht"].at_face(pf[i], a[i:i + 1], X[i:i + 1]) for i in range(len(pf))])
+        y = om.gamma / (1j * 2 * np.pi * f * 4e-7 * np.pi * om.mu_port)
+        c = np.vdot(E.ravel(), Eo.ravel()) / np.vdot(E.ravel(), E.ravel())
+        assert abs(met["gamma"] - om.gamma) <= 1e-10 * abs(om.gamma)
+        assert abs(met["Z"] - om.Z) <= 1e-10 * abs(om.Z)
+        assert abs(c * met["V"] - om.V) <= 1e-10 * abs(om.V)
+        assert np.abs(Eo - c * E).max() <= 1e-10 * np.abs(Eo).max()
+        assert np.abs(Ho - c * y * Hy).max() <= 1e-10 * np.abs(Ho).max()
+
+
+def test_order_p_modes_converge_to_analytic():
+    """The order-p 2D solve (oracle/port2d_pp.py) reproduces the order-1 and
+    order-2 solvers' spaces exactly and converges with p: TE10 of an empty guide
+    and the slab-loaded guide's dispersion relation."""
+    from oracle.port2d import rect_mesh, solve_mode, solve_mode_p2, slab_beta
+    from oracle.port2d_pp import solve_mode_pp
+    a, b = 22.86e-3, 10.16e-3
+    pts, tris = rect_mesh(a, b, 8, 4)
+    f = 10e9
+    assert abs(solve_mode_pp(pts, tris, f, 1.0, p=1)[0] - solve_mode(pts, tris, f, 1.0)[0]) < 1e-12 * 160
+    assert abs(solve_mode_pp(pts, tris, f, 1.0, p=2)[0] - solve_mode_p2(pts, tris, f, 1.0)[0]) < 1e-12 * 160
+    exact = np.sqrt((2 * np.pi * f / 299792458.0) ** 2 - (np.pi / a) ** 2)
+    errs = [abs(solve_mode_pp(pts, tris, f, 1.0, p=p)[0] - exact) / exact for p in (2, 3, 4)]
+    assert errs[0] < 1e-5 and errs[1] < 1e-8 and errs[2] < 1e-10
+    w = 4e-3
+    pts2, tris2 = rect_mesh(a, b, 8, 4, x_breaks=(-w / 2, w / 2))
+    cen = pts2[tris2].mean(1)
+    eps = np.where(np.abs(cen[:, 0]) < w / 2, 2.2, 1.0)
+    ex2 = slab_beta(a, w, 2.2, f)
+    assert abs(solve_mode_pp(pts2, tris2, f, eps, p=6)[0] - ex2) / ex2 < 1e-11

@@ -115,7 +115,7 @@ def test_library_equals_oracle_definitions(tmp_path):
     for zdef in ("PV", "VI", "PI"):
         m = dict(mode, zdef=zdef)
         om = Fem2DMode(prob, topo, faces, m, f)
-        lib = port_mode_faces_z(prob["verts"], fv, eps, m, m["nsub"], f, zdef, m["ipath"], order=2)
+        lib = port_mode_faces_z(prob["verts"], fv, eps, m, m["nsub"], f, zdef, m["ipath"], order=m["order2d"])
         assert abs(lib["Z"] - om.Z) <= 1e-10 * abs(om.Z), (zdef, lib["Z"], om.Z)
         # V and I scale with the mode's normalisation; their ratio does not
         assert abs(lib["V"] / lib["I"] - om.V / om.I) <= 1e-10 * abs(om.V / om.I)
