@@ -204,7 +204,7 @@ def read_material(paths, name):
         if "=" in ln:
             k, v = ln.split("=", 1)
             if k in ("er", "mur", "tand", "conductivity", "Rz"):
-                out[k] = float(v)
+                out[k] = float(v.split("//")[0])   # a trailing // comment is not part of the value
     return out
 
 
@@ -248,7 +248,8 @@ OTHER = {"partially-filled-lossless": ("partially_filled_rect_waveguide/partiall
          "partially-filled-lossy": ("partially_filled_rect_waveguide/partially_filled_rect_waveguide_lossy", "part"),
          "tee": ("WR90/tee", "tee"),
          "t-junction": ("WR75/T-Junction", "T-Junction"),
-         "permeability-straight": ("permeability/rectangular_waveguide", "straight")}
+         "permeability-straight": ("permeability/rectangular_waveguide", "straight"),
+         "permeability-partially-filled": ("permeability/partially_filled_rect_waveguide", "part")}
 
 PROJECTS = {"straight-flipped": "straight-flipped", "straight-rotated-xyz": "straight-rotated",
             "shorted": "shorted", "opened": "opened", "straight-loaded": "straight-loaded",
@@ -299,6 +300,10 @@ def main(ref):
     reg["permeability-straight"] = {
         "test_cases": read_test_cases(os.path.join(ref, "regression", "OpenParEM3D", "permeability",
                                                    "rectangular_waveguide", "straight_test_cases.csv")),
+        "evaluation": []}
+    reg["permeability-partially-filled"] = {
+        "test_cases": read_test_cases(os.path.join(ref, "regression", "OpenParEM3D", "permeability",
+                                                   "partially_filled_rect_waveguide", "part_test_cases.csv")),
         "evaluation": []}
     with open(os.path.join(HERE, "wr90_regression.json"), "w") as f:
         json.dump({"source": "regression/OpenParEM3D", "projects": reg}, f, indent=0)

@@ -132,3 +132,27 @@ def test_comparator_rejects_antenna_cases_and_missing_files(tmp_path):
     assert e.value.code == _lib.ERR_UNSUPPORTED
     with pytest.raises(OpemError):
         evaluate_test_cases(tmp_path / "missing.csv", res, tmp_path / "o.csv")
+
+
+def test_regression_flow_on_the_partially_filled_mu_r_guide(tmp_path):
+    """The same flow on the reference's permeability/partially_filled_rect_waveguide
+    project (a partial fill of eps_r 2.45, mu_r 2, ND6, no recorded run): its
+    ports see two materials, so the reader drives them by order-6 modes on the
+    unsplit port faces; every test case of the first frequency passes, |S21|
+    within +-1e-7 dB of 0 dB among them."""
+    from project_files import reference_project
+    from openparem_b200.fem3d import project_problem
+    from oracle import fem
+    proj, rec = reference_project(str(tmp_path), "permeability-partially-filled")
+    prob, fr = project_problem(proj)
+    assert [(p["mode"]["kind"], p["mode"]["nsub"], p["mode"]["order2d"]) for p in prob["ports"]] == [("FEM2D", 1, 6)] * 2
+    f0 = fr[0]
+    S = fem.solve_frequency(fem.Operators(prob), f0)["S"]
+    res = tmp_path / "part_results.csv"
+    write_results_csv(res, [f0], S[None], 0.0, "DB", "GHz")
+    cases = [r for r in _regression()["permeability-partially-filled"]["test_cases"] if float(r[1]) == f0]
+    tc = tmp_path / "cases.csv"
+    with open(tc, "w") as fh:
+        fh.write("# ResultDatabase::save_as_test\n" + "\n".join(",".join(r) for r in cases) + "\n")
+    n, npass = evaluate_test_cases(tc, res, tmp_path / "out.csv")
+    assert n == len(cases) >= 8 and npass == n
