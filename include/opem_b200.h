@@ -385,6 +385,12 @@ int  opem_server_info(opem_server srv, int64_t* info, int ninfo);
  * when the status word reported the timeout and the context still runs a
  * kernel afterwards, another status otherwise.                                   */
 int  opem_selftest_wait_timeout(opem_context ctx, int polls);
+/* Host check of the device Hessenberg least squares (no device needed): the
+ * column update and back substitution the solvers run on the GPU, compiled for
+ * the host, against the host Givens QR on seeded random problems of m columns,
+ * a fresh cycle and one started from a deflated (kd+1) x kd block.
+ * max_rel_diff: largest relative difference of residual estimates and y.     */
+int  opem_selftest_lsq(int m, int kd, int seed, double* max_rel_diff);
 
 /* ---- allocation-free assembly (no counterpart in the reference) -------------
  * For callers that cannot allocate device memory at the point of use: a

@@ -1,6 +1,10 @@
 // GMRES Hessenberg least squares on the device: kernels and launches (lsq.h).
 #include "lsq.h"
 
+#include <random>
+
+#include "dense.h"
+
 namespace opem {
 
 namespace {
@@ -86,3 +90,56 @@ void LsqWork::check(cudaStream_t s) {
 }
 
 }  // namespace opem
+
+// ---------------------------------------------------------------------------
+// host check: the device update (the same inline functions, compiled for the
+// host) against the host Givens QR (dense.cpp GivensLsq) on seeded problems
+// ---------------------------------------------------------------------------
+extern "C" int opem_selftest_lsq(int m, int kd, int seed, double* max_rel_diff) {
+    using namespace opem;
+    using cdd = std::complex<double>;
+    if (m < 2 || kd < 0 || kd > m - 2 || !max_rel_diff) return OPEM_ERR_ARG;
+    const int maxrot = kd * (kd + 1) / 2 + m + 1;
+    std::vector<double2> Hr((size_t)(m + 1) * m), g(m + 1), rs(maxrot);
+    std::vector<short2> ri(maxrot);
+    std::vector<double> rc(maxrot), est(1);
+    std::vector<int> nrot(1);
+    int err = 0;
+    const LsqState L{Hr.data(), g.data(), ri.data(), rc.data(), rs.data(), nrot.data(), est.data(), m, maxrot};
+    std::mt19937 gen((unsigned)seed);
+    std::normal_distribution<double> nd;
+    double worst = 0;
+    for (int start : {0, kd}) {
+        // H: a restart block (start+1) x start, then Hessenberg columns
+        std::vector<cdd> H((size_t)(m + 1) * m, 0.0), c(m + 1, 0.0);
+        for (int j = 0; j < m; ++j) {
+            const int top = j < start ? start : j + 1;
+            for (int i = 0; i <= top; ++i) H[i + (size_t)j * (m + 1)] = cdd(nd(gen), nd(gen));
+        }
+        if (start == 0) c[0] = 1.5;
+        else
+            for (int i = 0; i <= start; ++i) c[i] = cdd(nd(gen), nd(gen));
+        GivensLsq G;
+        G.reset(m, c);
+        for (int i = 0; i <= m; ++i) g[i] = make_double2(c[i].real(), c[i].imag());
+        nrot[0] = 0;
+        std::vector<double2> col(m + 1);
+        for (int j = 0; j < m; ++j) {
+            const int top = j < start ? start : j + 1;
+            for (int i = 0; i <= m; ++i) col[i] = make_double2(H[i + (size_t)j * (m + 1)].real(), H[i + (size_t)j * (m + 1)].imag());
+            const double e1 = G.add_column(j, &H[(size_t)j * (m + 1)], top);
+            const double e2 = lsq_add_column(L, 0, j, top, col.data(), &err);
+            worst = std::max(worst, std::fabs(e1 - e2) / std::max(1e-300, std::fabs(e1)));
+            if (j >= start) {
+                std::vector<cdd> y1;
+                G.solve(j + 1, y1);
+                std::vector<double2> y2(j + 1);
+                lsq_back_subst(L, 0, j + 1, y2.data());
+                for (int i = 0; i <= j; ++i)
+                    worst = std::max(worst, std::abs(y1[i] - cdd(y2[i].x, y2[i].y)) / std::max(1e-300, std::abs(y1[i])));
+            }
+        }
+    }
+    *max_rel_diff = worst;
+    return err ? OPEM_ERR_BREAKDOWN : OPEM_OK;
+}
