@@ -1,6 +1,7 @@
 // Reader of OpenParEM3D projects on the host: the .proj key/value file
 // (project.c), the gmsh 2.2 ASCII mesh with physical volumes named after
-// materials (mesh.cpp:449-588), the ports file (Path / Port / Boundary blocks,
+// materials (mesh.cpp:449-588) or MFEM's ASCII mesh with the regions file
+// materials_for_<mesh> (mesh.cpp:629-720), the ports file (Path / Port / Boundary blocks,
 // port.cpp:6369-7078) and the materials databases (OpenParEMmaterials.cpp),
 // turned into the inputs of opem_problem_create / set_regions / set_boundary /
 // set_port_te.  Supported subset: ports on any planar closed path; a rectangle
@@ -162,6 +163,93 @@ void read_gmsh22(const std::string& path, Project& P, std::vector<int>& phys) {
             P.region_names.push_back(it->second);
         }
     for (int t : phys) P.region.push_back(reg_of_tag[t]);
+}
+
+// MFEM's ASCII mesh format (v1.0 / v1.2: "dimension", "elements" with attribute,
+// geometry and vertex ids, "boundary", "vertices"), the other format the
+// reference loads (MeshMaterialList::loadMFEM, src/OpenParEMCommon/mesh.cpp:629-720):
+// the materials come from the regions file materials_for_<mesh file> beside it
+// ("OpenParEM Regions v1.0", lines "index name"), element attribute a taking the
+// name of index a - 1 (the material loop of OpenParEM3D.cpp:396-398).  Only the
+// tetrahedra are read; the boundary is marked from the ports file, as for gmsh.
+void read_mfem_mesh(const std::string& path, Project& P, std::vector<int>& phys) {
+    std::ifstream f(path);
+    if (!f) throw std::runtime_error("cannot read mesh " + path);
+    std::string tok;
+    std::getline(f, tok);
+    int dim = 0;
+    std::vector<std::array<int64_t, 4>> tets;
+    while (f >> tok) {
+        if (tok.empty() || tok[0] == '#') { std::getline(f, tok); continue; }
+        if (tok == "dimension") {
+            f >> dim;
+        } else if (tok == "elements") {
+            long n;
+            f >> n;
+            for (long i = 0; i < n; ++i) {
+                int attr, geom;
+                f >> attr >> geom;
+                const int nv = geom == 4 ? 4 : (geom == 2 ? 3 : (geom == 5 ? 8 : (geom == 6 ? 6 : (geom == 7 ? 5 : (geom == 3 ? 4 : 2)))));
+                std::array<int64_t, 8> v{};
+                for (int k = 0; k < nv; ++k) f >> v[k];
+                if (geom != 4) throw std::runtime_error("MFEM mesh: only tetrahedral volume elements are read");
+                tets.push_back({v[0], v[1], v[2], v[3]});
+                phys.push_back(attr);
+            }
+        } else if (tok == "boundary") {
+            long n;
+            f >> n;
+            std::getline(f, tok);
+            for (long i = 0; i < n; ++i) std::getline(f, tok);
+        } else if (tok == "vertices") {
+            long n;
+            int vdim;
+            f >> n >> vdim;
+            if (vdim != 3) throw std::runtime_error("MFEM mesh: vertices must have 3 coordinates");
+            for (long i = 0; i < n; ++i) {
+                double x, y, z;
+                f >> x >> y >> z;
+                P.verts.insert(P.verts.end(), {x, y, z});
+            }
+            break;
+        }
+        if (!f) break;
+    }
+    if (dim != 3) throw std::runtime_error("MFEM mesh: dimension must be 3");
+    if (tets.empty()) throw std::runtime_error("mesh has no tetrahedra");
+    const int64_t nvt = (int64_t)P.verts.size() / 3;
+    for (auto& t : tets)
+        for (int64_t v : t) {
+            if (v < 0 || v >= nvt) throw std::runtime_error("element refers to an unknown node");
+            P.tets.push_back(v);
+        }
+    // the regions file
+    const size_t sl = path.find_last_of('/');
+    const std::string dir = sl == std::string::npos ? std::string() : path.substr(0, sl + 1);
+    const std::string base = sl == std::string::npos ? path : path.substr(sl + 1);
+    std::vector<std::string> L;
+    if (!read_lines(dir + "materials_for_" + base, L) || L.empty() || L[0].rfind("OpenParEM Regions v", 0) != 0)
+        throw std::runtime_error("MFEM mesh: regions file materials_for_" + base + " missing or malformed");
+    std::map<int, std::string> names;
+    for (size_t i = 1; i < L.size(); ++i) {
+        std::string ln = trim(L[i].substr(0, L[i].find("//")));
+        if (ln.empty()) continue;
+        std::istringstream is(ln);
+        int idx;
+        std::string name;
+        if (!(is >> idx >> name)) throw std::runtime_error("MFEM mesh: bad line in the regions file");
+        if (name.size() >= 2 && name.front() == '"') name = name.substr(1, name.size() - 2);
+        names[idx] = name;
+    }
+    std::map<int, int> reg_of_attr;
+    for (int a : phys)
+        if (!reg_of_attr.count(a)) {
+            auto it = names.find(a - 1);
+            if (it == names.end()) throw std::runtime_error("MFEM mesh: element attribute without a region name");
+            reg_of_attr[a] = (int)P.region_names.size();
+            P.region_names.push_back(it->second);
+        }
+    for (int a : phys) P.region.push_back(reg_of_attr[a]);
 }
 
 void read_materials(const std::string& path, std::map<std::string, Mat>& db) {
@@ -342,7 +430,14 @@ void build(const std::string& proj_path, int order_override, Project& P) {
     P.order = std::atoi(kv1(P, "mesh.order", "1").c_str());
     if (order_override > 0) P.order = order_override;
     std::vector<int> phys;
-    read_gmsh22(join(P.dir, mesh), P, phys);
+    {
+        std::ifstream probe(join(P.dir, mesh));
+        std::string first;
+        std::getline(probe, first);
+        first = trim(first);
+        if (first == "MFEM mesh v1.0" || first == "MFEM mesh v1.2") read_mfem_mesh(join(P.dir, mesh), P, phys);
+        else read_gmsh22(join(P.dir, mesh), P, phys);
+    }
     // materials: global database, then the local one overrides
     std::map<std::string, Mat> db;
     read_materials(join(join(P.dir, kv1(P, "materials.global.path")), kv1(P, "materials.global.name")), db);

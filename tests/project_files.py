@@ -250,3 +250,25 @@ def write_coax_project(d, zdef="PI", with_current=True, freqs=(3e9,)):
                               "impedance_calculation": "line", "lines": [{"Sport": k, "integration": integ}]})
     return write_project(d, "coax", verts, tets, 1, {1: "air"}, spec,
                          {"air": {"er": 1.0, "mur": 1.0, "tand": 0.0, "Rz": 0.0}}, 1, list(freqs))
+
+
+def write_mfem_mesh(path, verts, tets, attr, names):
+    """A mesh in MFEM's ASCII format (v1.0) with the reference's regions file
+    materials_for_<name> beside it: attr (per tetrahedron, 1-based) and names
+    {attribute: material}; the boundary section lists no faces (the reader
+    marks the boundary from the ports file)."""
+    attr = np.broadcast_to(np.asarray(attr, dtype=np.int64), (len(tets),))
+    with open(path, "w") as f:
+        f.write("MFEM mesh v1.0\n\n#\n# written for the reader tests\n#\n\ndimension\n3\n\n")
+        f.write(f"elements\n{len(tets)}\n")
+        for a, t in zip(attr, tets):
+            f.write(f"{int(a)} 4 {t[0]} {t[1]} {t[2]} {t[3]}\n")
+        f.write("\nboundary\n0\n\n")
+        f.write(f"vertices\n{len(verts)}\n3\n")
+        for v in verts:
+            f.write(f"{float(v[0]):.17g} {float(v[1]):.17g} {float(v[2]):.17g}\n")
+    d, base = os.path.split(path)
+    with open(os.path.join(d, "materials_for_" + base), "w") as f:
+        f.write("OpenParEM Regions v1.0\n")
+        for a, nm in sorted(names.items()):
+            f.write(f"{int(a) - 1} {nm}\n")

@@ -120,3 +120,55 @@ def test_polygon_port_paths(tmp_path):
     assert np.allclose(modes[0]["normal"], [0, 0, -1]) and np.allclose(modes[1]["normal"], [0, 0, 1])
     assert np.allclose([modes[0]["a"], modes[0]["b"]], [24e-3, 16e-3])   # the outline's bounding box
     assert np.allclose(modes[1]["vpath"][0], [-6e-3, -8e-3, 40e-3])
+
+
+@pytest.mark.skipif(not _ROOT or not os.path.isdir(os.path.join(_ROOT, "regression", "OpenParEM3D")),
+                    reason="the reference tree is not mounted here")
+def test_reference_regression_projects_read():
+    """Every regression project of the reference reads (80 of 88, gmsh and MFEM
+    mesh formats), except those the reader declines with a reason:
+    multi-conductor ports (several Line / Mode blocks, or integration paths
+    summed from several paths) and a mesh file the tree does not hold."""
+    import glob
+    from openparem_b200.fem3d import project_info
+    paths = sorted(glob.glob(os.path.join(_ROOT, "regression", "OpenParEM3D", "*", "*", "*.proj")))
+    ok, declined = 0, 0
+    for p in paths:
+        try:
+            info, _ = project_info(p)
+            assert info["tets"] > 0 and info["ports"] >= 1
+            ok += 1
+        except OpemError as e:
+            msg = str(e)
+            assert ("multi-conductor" in msg or "summed from several paths" in msg or "no tetrahedra" in msg
+                    or "cannot read mesh" in msg), (p, msg)
+            declined += 1
+    assert ok >= 80 and ok + declined == len(paths)
+
+
+def test_mfem_format_mesh_reads_as_gmsh(tmp_path):
+    """A project whose mesh is in MFEM's format (with the reference's regions
+    file materials_for_<mesh>) reads to the same problem as the same mesh in
+    gmsh 2.2: vertices, tetrahedra, regions and materials, boundary
+    classification and ports."""
+    from openparem_b200 import meshgen
+    from openparem_b200.fem3d import project_problem
+    from project_files import write_mfem_mesh
+    proj = write_guide_project(str(tmp_path))
+    pg, fg = project_problem(proj)
+    verts, tets = meshgen.box_kuhn(meshgen.WR_A, meshgen.WR_B, 50e-3, 6, 3, 15)
+    d2 = tmp_path / "mfem"
+    os.makedirs(d2)
+    for fn in os.listdir(tmp_path):
+        if fn.endswith((".proj", ".txt")):
+            with open(tmp_path / fn) as a, open(d2 / fn, "w") as b:
+                b.write(a.read())
+    write_mfem_mesh(str(d2 / "guide.msh"), verts, tets, 1, {1: "air"})
+    pm, fm = project_problem(str(d2 / "guide.proj"))
+    for k in ("verts", "tets", "tet_region", "bdr_tris", "bdr_attr", "eps_r", "mu_r"):
+        assert np.array_equal(np.asarray(pg[k]), np.asarray(pm[k])), k
+    assert np.allclose(fg, fm) and len(pm["ports"]) == 2
+    os.remove(d2 / "materials_for_guide.msh")
+    with pytest.raises(OpemError) as e:
+        project_problem(str(d2 / "guide.proj"))
+    assert "regions file" in str(e.value)
