@@ -267,11 +267,14 @@ int  opem_port_mode_faces(int64_t nverts, const double* verts, int64_t nface, co
                           const double* eps_face, const double* mu_face, const double* desc, int nsub, int order,
                           double freq, double* metrics, int64_t npts, const int64_t* pt_face, const double* pt_s,
                           double* E_out, double* Hy_out);
-/* The same metrics under an impedance definition (as opem_problem_set_port_impedance):
- * metrics = {gamma, Z, V, Pz, I} (5 complex; I = 0 without a current path).     */
+/* The same metrics under an impedance definition (as opem_problem_set_port_impedance),
+ * of mode `mode` of the cross-section in decreasing beta^2 (0 = the fundamental
+ * mode; 1..15 by subspace iteration with order-`order` elements of the reference's
+ * 2D spaces): metrics = {gamma, Z, V, Pz, I} (5 complex; I = 0 without a current
+ * path).                                                                        */
 int  opem_port_mode_faces_z(int64_t nverts, const double* verts, int64_t nface, const int64_t* face_verts,
                             const double* eps_face, const double* mu_face, const double* desc, int nsub, int order,
-                            double freq, int definition, int npath, const double* path, int closed,
+                            double freq, int definition, int npath, const double* path, int closed, int mode,
                             double* metrics);
 
 /* ---- S-parameter post-processing (host only, no GPU needed) -----------------

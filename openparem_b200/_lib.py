@@ -87,7 +87,7 @@ SIGNATURES = [
     ("opem_project_port_impedance", C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                                C.POINTER(C.c_int), DP, C.c_int, C.c_char_p, C.c_int]),
     ("opem_port_mode_faces_z", C.c_int, [C.c_int64, DP, C.c_int64, I64P, DP, DP, DP, C.c_int, C.c_int, C.c_double,
-                                          C.c_int, C.c_int, DP, C.c_int, DP]),
+                                          C.c_int, C.c_int, DP, C.c_int, C.c_int, DP]),
     ("opem_s_renormalize", C.c_int, [C.c_int, DP, DP, C.c_double, C.c_double, DP]),
     ("opem_write_touchstone", C.c_int, [C.c_char_p, C.c_int, DP, C.c_int, DP, C.c_double, C.c_char_p, C.c_char_p]),
     ("opem_s_mixed_mode", C.c_int, [C.c_int, DP, C.c_int, C.POINTER(C.c_int), C.c_double, DP, DP]),

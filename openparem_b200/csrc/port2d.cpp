@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "../../include/opem_b200.h"
+#include "dense.h"
 #include "opem_internal.h"
 #include "portfem.h"
 
@@ -240,6 +241,107 @@ int solve_pencil(int n, const std::vector<Triplet>& A, const std::vector<Triplet
     if (!ok) return OPEM_ERR_NOT_CONVERGED;
     xout.assign(n, 0.0);
     for (int i = 0; i < n; ++i) xout[i] = x[pos[i]];
+    return OPEM_OK;
+}
+
+// The k eigenpairs of A x = -beta^2 B x with the largest beta^2 (the k eigenvalues
+// nearest the shift sigma, which lies below all of them) by subspace iteration on
+// (A - sigma B)^-1 B with k + 2 vectors (one banded LU, RCM order as above) and
+// Rayleigh-Ritz on the projected pencil: converged when the k Ritz values have
+// settled to 1e-14 and at least 40 iterations ran (the Ritz vectors trail the
+// values).  lam[i] = -beta_i^2 in increasing distance from sigma, X (n x k,
+// column-major) the Ritz vectors in the caller's numbering.
+int solve_pencil_k(int n, const std::vector<Triplet>& A, const std::vector<Triplet>& Bm, double sigma, int k,
+                   std::vector<cd>& lam, std::vector<cd>& X) {
+    const int q = std::min(n, k + 2);
+    if (k < 1 || k > n) return OPEM_ERR_ARG;
+    std::vector<std::vector<int>> adj(n);
+    for (auto* T : {&A, &Bm})
+        for (auto& x : *T)
+            if (x.r != x.c) adj[x.r].push_back(x.c);
+    for (auto& a : adj) { std::sort(a.begin(), a.end()); a.erase(std::unique(a.begin(), a.end()), a.end()); }
+    std::vector<int> ord = rcm(n, adj);
+    std::vector<int> pos(n);
+    for (int i = 0; i < n; ++i) pos[ord[i]] = i;
+    int bw = 0;
+    for (int i = 0; i < n; ++i)
+        for (int j : adj[i]) bw = std::max(bw, std::abs(pos[i] - pos[j]));
+    Banded M;
+    M.init(n, bw, bw);
+    for (auto& x : A) M.at(pos[x.r], pos[x.c]) += x.v;
+    for (auto& x : Bm) M.at(pos[x.r], pos[x.c]) -= sigma * x.v;
+    if (!M.factor()) return OPEM_ERR_BREAKDOWN;
+    auto mul = [&](const std::vector<Triplet>& T, const cd* x, cd* y) {   // permuted numbering
+        std::fill(y, y + n, cd(0.0));
+        for (auto& t : T) y[pos[t.r]] += t.v * x[pos[t.c]];
+    };
+    std::vector<cd> Y((size_t)n * q), AY((size_t)n * q), BY((size_t)n * q), tmp(n);
+    for (int c = 0; c < q; ++c)
+        for (int i = 0; i < n; ++i) Y[(size_t)c * n + i] = cd(1.0 + 0.001 * ((i * (c + 3)) % 11), 0.0007 * ((i + 5 * c) % 7));
+    std::vector<cd> prev(k, cd(0.0));
+    lam.assign(k, 0.0);
+    bool ok = false;
+    for (int it = 0; it < 2000 && !ok; ++it) {
+        // Y <- (A - sigma B)^-1 B Y, orthonormal columns
+        for (int c = 0; c < q; ++c) {
+            mul(Bm, &Y[(size_t)c * n], tmp.data());
+            M.solve(tmp);
+            std::copy(tmp.begin(), tmp.end(), &Y[(size_t)c * n]);
+        }
+        if (opem::orthonormalise(n, q, Y) != q) return OPEM_ERR_BREAKDOWN;
+        // projected pencil Ah z = lam Bh z -> C = Bh^-1 (Ah - sigma Bh), eigenvalues lam - sigma
+        for (int c = 0; c < q; ++c) {
+            mul(A, &Y[(size_t)c * n], &AY[(size_t)c * n]);
+            mul(Bm, &Y[(size_t)c * n], &BY[(size_t)c * n]);
+        }
+        std::vector<cd> Ah((size_t)q * q), Bh((size_t)q * q);
+        for (int i = 0; i < q; ++i)
+            for (int j = 0; j < q; ++j) {
+                cd a = 0, b = 0;
+                for (int r = 0; r < n; ++r) {
+                    a += std::conj(Y[(size_t)i * n + r]) * AY[(size_t)j * n + r];
+                    b += std::conj(Y[(size_t)i * n + r]) * BY[(size_t)j * n + r];
+                }
+                Ah[i + (size_t)j * q] = a;
+                Bh[i + (size_t)j * q] = b;
+            }
+        std::vector<cd> C((size_t)q * q);
+        for (int j = 0; j < q; ++j) {
+            std::vector<cd> col(q);
+            for (int i = 0; i < q; ++i) col[i] = Ah[i + (size_t)j * q] - sigma * Bh[i + (size_t)j * q];
+            if (!opem::lu_solve(q, Bh, col)) return OPEM_ERR_BREAKDOWN;
+            for (int i = 0; i < q; ++i) C[i + (size_t)j * q] = col[i];
+        }
+        std::vector<cd> th, Z;
+        if (!opem::eig_smallest(q, C, q, th, Z)) return OPEM_ERR_BREAKDOWN;
+        std::vector<int> idx(q);
+        for (int i = 0; i < q; ++i) idx[i] = i;
+        std::sort(idx.begin(), idx.end(), [&](int a, int b) { return std::abs(th[a]) < std::abs(th[b]); });
+        // Ritz vectors, nearest first
+        std::vector<cd> Yn((size_t)n * q, 0.0);
+        for (int c = 0; c < q; ++c)
+            for (int j = 0; j < q; ++j) {
+                const cd z = Z[j + (size_t)idx[c] * q];
+                if (z == 0.0) continue;
+                for (int r = 0; r < n; ++r) Yn[(size_t)c * n + r] += Y[(size_t)j * n + r] * z;
+            }
+        Y.swap(Yn);
+        bool settled = true;
+        for (int i = 0; i < k; ++i) {
+            lam[i] = sigma + th[idx[i]];
+            if (!(std::abs(lam[i] - prev[i]) <= 1e-14 * std::abs(lam[i]))) settled = false;
+            prev[i] = lam[i];
+        }
+        ok = settled && it >= 40;
+    }
+    if (!ok) return OPEM_ERR_NOT_CONVERGED;
+    X.assign((size_t)n * k, 0.0);
+    for (int c = 0; c < k; ++c) {
+        double nr = 0;
+        for (int r = 0; r < n; ++r) nr += std::norm(Y[(size_t)c * n + r]);
+        nr = std::sqrt(nr);
+        for (int i = 0; i < n; ++i) X[(size_t)c * n + i] = Y[(size_t)c * n + pos[i]] / nr;
+    }
     return OPEM_OK;
 }
 
@@ -756,8 +858,9 @@ namespace opem {
 
 int port_mode_2d_pp(int64_t nnodes, const double* xy, int64_t ntri, const int64_t* tris, const cd* eps_r,
                     const cd* mu_r, double freq, int p, cd& beta, std::vector<cd>& ct, std::vector<cd>& cz,
-                    std::vector<int64_t>& st) {
-    if (nnodes < 3 || !xy || ntri < 1 || !tris || !eps_r || !(freq > 0) || p < 1 || p > 8) return OPEM_ERR_ARG;
+                    std::vector<int64_t>& st, int mode) {
+    if (nnodes < 3 || !xy || ntri < 1 || !tris || !eps_r || !(freq > 0) || p < 1 || p > 8 || mode < 0 || mode > 15)
+        return OPEM_ERR_ARG;
     for (int64_t t = 0; t < 3 * ntri; ++t)
         if (tris[t] < 0 || tris[t] >= nnodes) return OPEM_ERR_ARG;
     const RefSpaces2D& R = ref_spaces_2d(p);
@@ -897,7 +1000,17 @@ int port_mode_2d_pp(int64_t nnodes, const double* xy, int64_t ntri, const int64_
     for (auto& x : Bnn) if (zmap[x.r] >= 0 && zmap[x.c] >= 0) Bm.push_back({zmap[x.r], zmap[x.c], x.v});
     cd lam = 0;
     std::vector<cd> xs;
-    int rc = solve_pencil(n, A, Bm, -k0 * k0 * emax, lam, xs);
+    int rc;
+    if (mode == 0) {
+        rc = solve_pencil(n, A, Bm, -k0 * k0 * emax, lam, xs);
+    } else {   // the mode-th mode in decreasing beta^2
+        std::vector<cd> lams, X;
+        rc = solve_pencil_k(n, A, Bm, -k0 * k0 * emax, mode + 1, lams, X);
+        if (rc == OPEM_OK) {
+            lam = lams[mode];
+            xs.assign(X.begin() + (size_t)mode * n, X.begin() + (size_t)(mode + 1) * n);
+        }
+    }
     if (rc != OPEM_OK) return rc;
     beta = std::sqrt(-lam);
     if (beta.real() < 0) beta = -beta;

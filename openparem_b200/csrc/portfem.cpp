@@ -63,7 +63,7 @@ void PortFem2D::eval_tri(int64_t t, const double X[3], cd E[3], cd Hy[3]) const 
     const double lam[3] = {1 - l1 - l2, l1, l2};
     const double* gg = &g[6 * t];
     cd ex = 0.0, ey = 0.0, zx, zy;
-    if (order >= 3) {
+    if (ref) {   // order >= 3, or a higher mode at any order
         // reference bases at (l1, l2), covariant map J^-T (J^-1 = Ji row-major)
         const int nf = ref->nf, nl = ref->nl;
         std::vector<double> N(2 * nf), cu(nf), L(nl), gL(2 * nl);
@@ -148,7 +148,7 @@ int64_t PortFem2D::locate(const double X[3]) const {
 
 int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* fv, const cd* eps_face, const cd* mu_face,
                      const double* desc, int nsub, int order, double freq, double mu_port, PortFem2D& M,
-                     std::string& err, int zdef, const double* ipath, int npath, bool closed) {
+                     std::string& err, int zdef, const double* ipath, int npath, bool closed, int mode) {
     if (zdef < 0 || zdef > 2 || (zdef != 0 && (!ipath || npath < 2))) {
         err = "impedance definition: VI and PI need a current path of at least two points";
         return OPEM_ERR_ARG;
@@ -243,13 +243,13 @@ int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* fv, cons
     int64_t ne = 0;
     std::vector<int64_t> edges;
     std::vector<double> et, ez;
-    if (order >= 2) {
+    if (order >= 2 || mode > 0) {
         std::vector<cd> epsc(T), muc(T);
         for (int64_t t = 0; t < T; ++t) { epsc[t] = cd(eps2[2 * t], eps2[2 * t + 1]); muc[t] = M.mu[t]; }
         cd b2;
         std::vector<int64_t> st2;
         int rc;
-        if (order == 2) {
+        if (order == 2 && mode == 0) {
             rc = port_mode_2d_p2(nn, M.xy.data(), T, tris.data(), epsc.data(), muc.data(), freq, b2, M.ct, M.cz, st2);
         } else {
             try {
@@ -259,7 +259,7 @@ int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* fv, cons
                 return OPEM_ERR_ARG;
             }
             rc = port_mode_2d_pp(nn, M.xy.data(), T, tris.data(), epsc.data(), muc.data(), freq, order, b2, M.ct,
-                                 M.cz, st2);
+                                 M.cz, st2, mode);
         }
         if (rc != OPEM_OK) { err = "port mode: 2D eigensolve failed"; return rc; }
         beta[0] = b2.real();
@@ -304,7 +304,7 @@ int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* fv, cons
             M.g[6 * t + 2 * k] = Ji[0] * r[k][0] + Ji[2] * r[k][1];
             M.g[6 * t + 2 * k + 1] = Ji[1] * r[k][0] + Ji[3] * r[k][1];
         }
-        if (order >= 2) continue;   // coefficients per triangle already (ct, cz)
+        if (order >= 2 || M.ref) continue;   // coefficients per triangle already (ct, cz)
         for (int i = 0; i < 3; ++i) {
             const int64_t e = eid.at({s[LP[i][0]], s[LP[i][1]]});
             M.ce[3 * t + i] = cd(et[2 * e], et[2 * e + 1]);
@@ -416,10 +416,10 @@ int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* fv, cons
 extern "C" int opem_port_mode_faces_z(int64_t nverts, const double* verts, int64_t nface, const int64_t* face_verts,
                                       const double* eps_face, const double* mu_face, const double* desc, int nsub,
                                       int order, double freq, int definition, int npath, const double* path,
-                                      int closed, double* metrics) {
+                                      int closed, int mode, double* metrics) {
     using cd = std::complex<double>;
     if (nverts < 3 || !verts || nface < 1 || !face_verts || !eps_face || !desc || !metrics) return OPEM_ERR_ARG;
-    if (npath < 0 || (npath > 0 && !path)) return OPEM_ERR_ARG;
+    if (npath < 0 || (npath > 0 && !path) || mode < 0 || mode > 15) return OPEM_ERR_ARG;
     for (int64_t i = 0; i < 3 * nface; ++i)
         if (face_verts[i] < 0 || face_verts[i] >= nverts) return OPEM_ERR_ARG;
     std::vector<cd> eps(nface), mu(nface, cd(1.0));
@@ -430,7 +430,7 @@ extern "C" int opem_port_mode_faces_z(int64_t nverts, const double* verts, int64
     opem::PortFem2D M;
     std::string err;
     int rc = opem::port_fem2d_solve(verts, nface, face_verts, eps.data(), mu.data(), desc, nsub, order, freq, mu[0].real(), M,
-                                    err, definition, npath > 0 ? path : nullptr, npath, closed != 0);
+                                    err, definition, npath > 0 ? path : nullptr, npath, closed != 0, mode);
     if (rc != OPEM_OK) return rc;
     const cd m5[5] = {M.gamma, M.Z, M.V, M.Pz, M.I};
     for (int i = 0; i < 5; ++i) { metrics[2 * i] = m5[i].real(); metrics[2 * i + 1] = m5[i].imag(); }

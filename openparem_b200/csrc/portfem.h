@@ -36,13 +36,15 @@ struct RefSpaces2D {
 };
 const RefSpaces2D& ref_spaces_2d(int p);   // cached; throws std::runtime_error for p < 1 or p > 8
 
-// The fundamental mode with order-p elements of RefSpaces2D (the spaces of the
-// reference's 2D solver at mesh.order p): per triangle nf e_t and nl e_z
-// coefficients on the reference bases, and the sorted vertex ids.
+// The fundamental mode (mode 0), or the mode-th mode in decreasing beta^2
+// (mode <= 15: subspace iteration over the mode + 1 leading modes), with
+// order-p elements of RefSpaces2D (the spaces of the reference's 2D solver at
+// mesh.order p): per triangle nf e_t and nl e_z coefficients on the reference
+// bases, and the sorted vertex ids.
 int port_mode_2d_pp(int64_t nnodes, const double* xy, int64_t ntri, const int64_t* tris,
                     const std::complex<double>* eps_r, const std::complex<double>* mu_r, double freq, int p,
                     std::complex<double>& beta, std::vector<std::complex<double>>& ct,
-                    std::vector<std::complex<double>>& cz, std::vector<int64_t>& st);
+                    std::vector<std::complex<double>>& cz, std::vector<int64_t>& st, int mode = 0);
 
 struct PortFem2D {
     using cd = std::complex<double>;
@@ -76,10 +78,11 @@ struct PortFem2D {
 // voltage path); order: 2D element order (1 or 2); mu_port: mu_r used to scale
 // H_t / y; zdef: OPEM_Z_PV / VI / PI; ipath: the current path's points (xyz,
 // npath of them, closed: with the segment back to the first).  Returns an
-// OPEM_* code.
+// OPEM_* code.  mode > 0: the mode-th mode in decreasing beta^2 instead of the
+// fundamental one (order-p elements of RefSpaces2D for every order).
 int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* face_verts,
                      const std::complex<double>* eps_face, const std::complex<double>* mu_face, const double* desc,
                      int nsub, int order, double freq, double mu_port, PortFem2D& out, std::string& err,
-                     int zdef = 0, const double* ipath = nullptr, int npath = 0, bool closed = true);
+                     int zdef = 0, const double* ipath = nullptr, int npath = 0, bool closed = true, int mode = 0);
 
 }  // namespace opem

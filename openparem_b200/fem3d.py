@@ -103,10 +103,11 @@ _ZDEF = {"PV": 0, "VI": 1, "PI": 2}
 
 
 def port_mode_faces_z(verts, face_verts, eps_face, mode, nsub, freq, zdef="PV", ipath=None, closed=True,
-                      mu_face=None, order=2):
+                      mu_face=None, order=2, mode_index=0):
     """The 2D mode's metrics under an impedance definition (opem_port_mode_faces_z,
-    host only): zdef "PV" | "VI" | "PI", ipath (k, 3) the current path's points
-    -> {gamma, Z, V, Pz, I}."""
+    host only): zdef "PV" | "VI" | "PI", ipath (k, 3) the current path's points,
+    mode_index the mode in decreasing beta^2 (0: the fundamental) ->
+    {gamma, Z, V, Pz, I}."""
     verts = np.ascontiguousarray(verts, dtype=np.float64)
     fv = np.ascontiguousarray(face_verts, dtype=np.int64)
     eps = np.ascontiguousarray(np.stack([np.real(eps_face), np.imag(eps_face)], axis=1), dtype=np.float64)
@@ -117,7 +118,7 @@ def port_mode_faces_z(verts, face_verts, eps_face, mode, nsub, freq, zdef="PV", 
     rc = _lib.lib().opem_port_mode_faces_z(len(verts), _dp(verts), len(fv), fv.ctypes.data_as(_lib.I64P), _dp(eps),
                                            None if mu is None else _dp(mu), _dp(d), int(nsub), int(order),
                                            float(freq), _ZDEF[zdef], 0 if ip is None else len(ip),
-                                           None if ip is None else _dp(ip), int(closed), _dp(m))
+                                           None if ip is None else _dp(ip), int(closed), int(mode_index), _dp(m))
     if rc != _lib.OK:
         raise OpemError(rc, "opem_port_mode_faces_z")
     c = m[0::2] + 1j * m[1::2]

@@ -128,11 +128,12 @@ def ref_spaces(p):
     return _REF[p]
 
 
-def solve_mode_pp(pts, tris, freq, eps_r, mu_r=None, p=1):
-    """Fundamental mode with order-p elements: (beta, ct (T, p(p+2)), cz (T, nl),
-    st (T,3) sorted vertex ids): per triangle the coefficients of e_t and e_z on
-    the reference nodal bases of ref_spaces(p), the triangle's local vertices in
-    increasing global order."""
+def solve_mode_pp(pts, tris, freq, eps_r, mu_r=None, p=1, mode=0):
+    """Fundamental mode (mode 0), or the mode-th mode in decreasing beta^2, with
+    order-p elements: (beta, ct (T, p(p+2)), cz (T, nl), st (T,3) sorted vertex
+    ids): per triangle the coefficients of e_t and e_z on the reference nodal
+    bases of ref_spaces(p), the triangle's local vertices in increasing global
+    order."""
     pts = np.asarray(pts, dtype=float)
     tris = np.asarray(tris, dtype=np.int64)
     nt = len(tris)
@@ -202,12 +203,13 @@ def solve_mode_pp(pts, tris, freq, eps_r, mu_r=None, p=1):
     sigma = -k0 ** 2 * np.max(np.real(eps_r * mu_r))
     lu = spla.splu((A - sigma * B).tocsc(), permc_spec="MMD_AT_PLUS_A")
     op = spla.LinearOperator(A.shape, matvec=lambda x: lu.solve(B @ x), dtype=complex)
-    mu, vec = spla.eigs(op, k=1, which="LM")
-    lam = sigma + 1.0 / mu[0]
+    mu, vec = spla.eigs(op, k=mode + 1, which="LM", tol=1e-14 if mode else 0)
+    order = np.argsort(-np.abs(mu))          # nearest the shift first: decreasing beta^2
+    lam = sigma + 1.0 / mu[order[mode]]
     beta = np.sqrt(-lam + 0j)
     if beta.real < 0:
         beta = -beta
-    x = vec[:, 0]
+    x = vec[:, order[mode]]
     et = np.zeros(net, dtype=complex)
     et[ke] = x[:len(ke)]
     psi = np.zeros(nz, dtype=complex)

@@ -101,12 +101,14 @@ class Fem2DMode:
                            np.asarray(prob["sigma"], dtype=np.float64)[reg])
         mu = np.asarray(prob["mu_r"], dtype=np.float64)[reg].astype(np.complex128)
         self.order = int(mode.get("order2d", 1))
-        if self.order >= 3:   # order-p edge / Lagrange elements (oracle.port2d_pp)
-            beta, ct, cz, _ = solve_mode_pp(xy, tris, freq, eps, mu, self.order)
+        mode_index = int(mode.get("mode_index", 0))   # 0: the fundamental mode; k: the k-th in decreasing beta^2
+        if self.order >= 3 or mode_index > 0:   # order-p edge / Lagrange elements (oracle.port2d_pp)
+            beta, ct, cz, _ = solve_mode_pp(xy, tris, freq, eps, mu, self.order, mode_index)
             e0 = ct[:, :3 * self.order].ravel()
             big = e0[np.argmax(np.abs(e0))]
             self.ctp, self.czp = ct / big, cz / big
             self.ref = ref_spaces(self.order)
+            self.pp = True
         elif self.order == 2:
             beta, ct, cz, _ = solve_mode_p2(xy, tris, freq, eps, mu)
             big = ct[:, :3].ravel()[np.argmax(np.abs(ct[:, :3]).ravel())]   # largest Whitney coefficient
@@ -128,7 +130,7 @@ class Fem2DMode:
         self.g = np.einsum("tji,kj->tki", Jinv, r)          # grad lambda_k = J^-T r_k : (T,3,2)
         self.area = 0.5 * np.abs(det)
         self.st, self.P0, self.Jinv = st, P[:, 0], Jinv
-        if self.order == 1:
+        if self.order == 1 and not getattr(self, "pp", False):
             eid = {(int(a), int(b)): e for e, (a, b) in enumerate(edges)}
             lp = [(0, 1), (0, 2), (1, 2)]
             self.ce = np.array([[et[eid[(int(t[a]), int(t[b]))]] for a, b in lp] for t in st])   # (T,3)
@@ -184,7 +186,7 @@ class Fem2DMode:
         lam = np.stack([1 - lam12[:, 0] - lam12[:, 1], lam12[:, 0], lam12[:, 1]], axis=1)   # (p,3)
         g = self.g[t]                                               # (p,3,2)
         e2 = np.zeros((len(t), 2), dtype=np.complex128)
-        if self.order >= 3:
+        if getattr(self, "pp", False):
             Nh, _ = self.ref.nd(lam12)                              # reference coordinates = (lambda_1, lambda_2)
             _, gLh = self.ref.h1(lam12)
             JiT = np.transpose(self.Jinv[t], (0, 2, 1))

@@ -162,3 +162,32 @@ def test_order_p_modes_converge_to_analytic():
     eps = np.where(np.abs(cen[:, 0]) < w / 2, 2.2, 1.0)
     ex2 = slab_beta(a, w, 2.2, f)
     assert abs(solve_mode_pp(pts2, tris2, f, eps, p=6)[0] - ex2) / ex2 < 1e-11
+
+
+def test_higher_modes_library_equals_oracle_and_analytic():
+    """Modes beyond the fundamental (subspace iteration in the library, shifted
+    Arnoldi in the oracle): on an empty WR90 cross-section at 16 GHz the three
+    leading modes TE10, TE20 and TE01 come out in decreasing beta with the
+    analytic propagation constants (order-4 elements on the unsplit port faces:
+    2e-8 and better), and the library's gamma and Z equal the oracle's."""
+    from openparem_b200 import meshgen
+    from openparem_b200.fem3d import port_mode_faces_z
+    from project_files import faces_at_z
+    a, b = meshgen.WR_A, meshgen.WR_B
+    prob = meshgen.waveguide_problem(a, b, 20e-3, 6, 3, 4, 1)
+    ops = fem.Operators(prob)
+    topo = ops.topo
+    faces = ops.ports[0]["faces"]
+    fv = np.array([topo.tets[topo.face_owner[x]][list(FACES[topo.face_lface[x]])] for x in faces])
+    f = 16e9
+    k0 = 2 * np.pi * f / 299792458.0
+    kc = sorted([np.pi / a, 2 * np.pi / a, np.pi / b])
+    base = dict(prob["ports"][0]["mode"], kind="FEM2D", nsub=1, order2d=4)
+    eps = np.ones(len(fv), dtype=complex)
+    for mi in range(3):
+        lib = port_mode_faces_z(prob["verts"], fv, eps, base, 1, f, order=4, mode_index=mi)
+        om = Fem2DMode(prob, topo, faces, dict(base, mode_index=mi), f)
+        exact = np.sqrt(k0 ** 2 - kc[mi] ** 2)
+        assert abs(lib["gamma"].imag - exact) <= 3e-8 * exact, (mi, lib["gamma"], exact)
+        assert abs(lib["gamma"] - om.gamma) <= 1e-9 * abs(om.gamma)
+        assert abs(lib["Z"] - om.Z) <= 1e-7 * abs(om.Z) + 1e-9
