@@ -307,6 +307,19 @@ int  opem_s_mixed_mode(int nports, const double* S, int npairs, const int* pairs
  * OPEM_ERR_BREAKDOWN if Tv, Ti or Ms + Mc S is singular.                         */
 int  opem_s_single_ended(int nports, const double* S, const double* Zmode, const double* Tv, const double* Ti,
                          double zref, double* S_out, double* Zo_out);
+/* Line-to-modal maps of one port with n lines and n modes, the reference's "line"
+ * calculation (Mode::calculateModalCurrent / calculateModalVoltage,
+ * OpenParEM2D fem2D.cpp:1591-1790): I and V (n x n complex, row = mode, column =
+ * line) the modes' currents on the lines' current paths and voltages on their
+ * voltage paths (V may be NULL).  Ti[i][k] = sign(Re I[i][k]) scaled by
+ * 0.5 (|sum sign I| + |sum I|) / |sum sign I|; a mode whose Ti[i][0] is negative is
+ * flipped (flipped[i] = 1: its field, currents and voltages change sign) and its
+ * row negated; Tv = (conj(Ti)^-1)^T.  Im and Vm (n complex each, may be NULL) get
+ * the mode currents sum_k Ti[i][k] I[i][k] and voltages sum_k Tv[i][k] V[i][k]
+ * after the flips.  flipped may be NULL.  OPEM_ERR_BREAKDOWN if a mode carries no
+ * net signed current or Ti is singular.                                          */
+int  opem_port_line_maps(int n, const double* I, const double* V, double* Ti, double* Tv, int* flipped, double* Im,
+                         double* Vm);
 /* Touchstone 2.0 (the reference's mixed-mode writer, results.cpp:1210-1372): as
  * opem_write_touchstone plus the 2.0 keywords and, with pairs, [Mixed-Mode Order]. */
 int  opem_write_touchstone2(const char* path, int nfreq, const double* freqs, int nports, const double* S,

@@ -23,15 +23,19 @@ namespace {
 
 using cd = std::complex<double>;
 
-// inverse of an n x n complex matrix (row-major) by Gauss-Jordan with partial pivoting
-bool invert(int n, std::vector<cd>& a) {
+// inverse of an n x n complex matrix (row-major) by Gauss-Jordan with partial
+// pivoting; false when a pivot is not above rel_tol times the largest entry
+bool invert(int n, std::vector<cd>& a, double rel_tol = 0.0) {
+    double amax = 0.0;
+    for (const cd& v : a) amax = std::max(amax, std::abs(v));
+    const double tiny = rel_tol * amax;
     std::vector<cd> inv((size_t)n * n, 0.0);
     for (int i = 0; i < n; ++i) inv[(size_t)i * n + i] = 1.0;
     for (int c = 0; c < n; ++c) {
         int p = c;
         for (int r = c + 1; r < n; ++r)
             if (std::abs(a[(size_t)r * n + c]) > std::abs(a[(size_t)p * n + c])) p = r;
-        if (!(std::abs(a[(size_t)p * n + c]) > 0)) return false;
+        if (!(std::abs(a[(size_t)p * n + c]) > tiny)) return false;
         if (p != c)
             for (int k = 0; k < n; ++k) {
                 std::swap(a[(size_t)p * n + k], a[(size_t)c * n + k]);
@@ -155,6 +159,69 @@ int opem_s_mixed_mode(int nports, const double* S, int npairs, const int* pairs,
     for (int i = 0; i < n * n; ++i) { S_out[2 * i] = Sb[i].real(); S_out[2 * i + 1] = Sb[i].imag(); }
     if (Zo_out)
         for (int i = 0; i < n; ++i) { Zo_out[2 * i] = zb[i]; Zo_out[2 * i + 1] = 0.0; }
+    return OPEM_OK;
+}
+
+// Line-to-modal maps of a port with n conductors carrying n modes, the
+// reference's "line" calculation (OpenParEM2D Mode::calculateModalCurrent /
+// calculateModalVoltage, src/OpenParEM2D/fem2D.cpp:1591-1790): for mode i with
+// currents I[i][k] on the lines' current paths, Ti[i][k] = sign(Re I[i][k]) times
+// 0.5 (|sum_k sign I| + |sum_k I|) / |sum_k sign I| (the return current); a mode
+// whose Ti[i][0] comes out negative has its field, currents and voltages flipped
+// and its row negated; the mode current is sum_k Ti[i][k] I[i][k]; then
+// Tv = (conj(Ti)^-1)^T and the mode voltage sum_k Tv[i][k] V[i][k].
+int opem_port_line_maps(int n, const double* I, const double* V, double* Ti, double* Tv, int* flipped, double* Im,
+                        double* Vm) {
+    if (n < 1 || !I || !Ti || !Tv) return OPEM_ERR_ARG;
+    std::vector<cd> cur((size_t)n * n), vol((size_t)n * n, 0.0), T((size_t)n * n), K((size_t)n * n);
+    for (int i = 0; i < n * n; ++i) {
+        cur[i] = cd(I[2 * i], I[2 * i + 1]);
+        if (V) vol[i] = cd(V[2 * i], V[2 * i + 1]);
+    }
+    std::vector<cd> mcur(n), mvol(n, 0.0);
+    for (int i = 0; i < n; ++i) {
+        cd mode_current = 0.0, return_current = 0.0;
+        for (int k = 0; k < n; ++k) {
+            const double sg = cur[(size_t)i * n + k].real() >= 0 ? 1.0 : -1.0;
+            T[(size_t)i * n + k] = sg;
+            mode_current += sg * cur[(size_t)i * n + k];
+            return_current += cur[(size_t)i * n + k];
+        }
+        if (!(std::abs(mode_current) > 0)) return OPEM_ERR_BREAKDOWN;
+        const double scale = 0.5 * (std::abs(mode_current) + std::abs(return_current)) / std::abs(mode_current);
+        for (int k = 0; k < n; ++k) T[(size_t)i * n + k] *= scale;
+        int fl = 0;
+        if (T[(size_t)i * n].real() < 0) {
+            fl = 1;
+            for (int k = 0; k < n; ++k) {
+                T[(size_t)i * n + k] = -T[(size_t)i * n + k];
+                cur[(size_t)i * n + k] = -cur[(size_t)i * n + k];
+                vol[(size_t)i * n + k] = -vol[(size_t)i * n + k];
+            }
+        }
+        if (flipped) flipped[i] = fl;
+        cd s = 0.0;
+        for (int k = 0; k < n; ++k) s += T[(size_t)i * n + k] * cur[(size_t)i * n + k];
+        mcur[i] = s;
+    }
+    // Tv = (conj(Ti)^-1)^T = (conj(Ti)^T)^-1: invert the conjugate transpose; a
+    // sign pattern of +-1 rows can be singular, caught by a relative pivot bound
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < n; ++k) K[(size_t)k * n + i] = std::conj(T[(size_t)i * n + k]);
+    if (!invert(n, K, 1e-12)) return OPEM_ERR_BREAKDOWN;
+    for (int i = 0; i < n; ++i) {
+        cd s = 0.0;
+        for (int k = 0; k < n; ++k) s += K[(size_t)i * n + k] * vol[(size_t)i * n + k];
+        mvol[i] = s;
+    }
+    for (int i = 0; i < n * n; ++i) {
+        Ti[2 * i] = T[i].real(); Ti[2 * i + 1] = T[i].imag();
+        Tv[2 * i] = K[i].real(); Tv[2 * i + 1] = K[i].imag();
+    }
+    for (int i = 0; i < n; ++i) {
+        if (Im) { Im[2 * i] = mcur[i].real(); Im[2 * i + 1] = mcur[i].imag(); }
+        if (Vm) { Vm[2 * i] = mvol[i].real(); Vm[2 * i + 1] = mvol[i].imag(); }
+    }
     return OPEM_OK;
 }
 

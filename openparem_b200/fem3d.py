@@ -514,6 +514,34 @@ def single_ended(S, Zmode, Tv, Ti, zref=50.0):
     return out
 
 
+def port_line_maps(I, V=None):
+    """Line-to-modal maps of one multi-line port (opem_port_line_maps): I and V
+    (n, n) the modes' line currents and voltages (row = mode, column = line).
+    Returns {"Ti", "Tv", "flipped", "Im", "Vm"}; Im and Vm are the mode currents and
+    voltages after the flips (Vm zero without V)."""
+    I = np.ascontiguousarray(I, dtype=np.complex128)
+    n = I.shape[0]
+    if I.shape != (n, n) or n < 1:
+        raise OpemError(_lib.ERR_ARG, "port_line_maps: shapes")
+    vp = None
+    if V is not None:
+        V = np.ascontiguousarray(V, dtype=np.complex128)
+        if V.shape != (n, n):
+            raise OpemError(_lib.ERR_ARG, "port_line_maps: shapes")
+        vp = _dp(V.view(np.float64).ravel())
+    ti = np.zeros((n, n), dtype=np.complex128)
+    tv = np.zeros((n, n), dtype=np.complex128)
+    fl = np.zeros(n, dtype=np.int32)
+    im = np.zeros(n, dtype=np.complex128)
+    vm = np.zeros(n, dtype=np.complex128)
+    rc = _lib.lib().opem_port_line_maps(n, _dp(I.view(np.float64).ravel()), vp, _dp(ti.view(np.float64).ravel()),
+                                        _dp(tv.view(np.float64).ravel()), fl.ctypes.data_as(C.POINTER(C.c_int)),
+                                        _dp(im.view(np.float64).ravel()), _dp(vm.view(np.float64).ravel()))
+    if rc != _lib.OK:
+        raise OpemError(rc, "opem_port_line_maps")
+    return {"Ti": ti, "Tv": tv, "flipped": fl.astype(bool), "Im": im, "Vm": vm}
+
+
 def write_touchstone2(path, freqs, S, zref=50.0, fmt="RI", unit="GHz", pairs=()):
     """Touchstone 2.0 file (opem_write_touchstone2); pairs mark mixed-mode S-ports."""
     freqs = np.ascontiguousarray(freqs, dtype=np.float64)

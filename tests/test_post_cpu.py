@@ -209,3 +209,66 @@ def test_touchstone2_layout(tmp_path):
     write_touchstone2(tmp_path / "a.s2p", fr, S[:, :2, :2], 50.0, "MA", "GHz")
     l2 = open(tmp_path / "a.s2p").read().splitlines()
     assert "[Two-Port Data Order] 21_12" in l2 and not any(x.startswith("[Mixed-Mode") for x in l2)
+
+
+def _ref_line_maps(I, V):
+    """The reference's line calculation (OpenParEM2D fem2D.cpp:1591-1790) restated
+    in numpy: per mode, signs of the line currents scaled by the return-current
+    rule, a flip when the first entry is negative, Tv = (conj(Ti)^-1)^T."""
+    I, V = np.array(I, dtype=complex), np.array(V, dtype=complex)
+    n = I.shape[0]
+    Ti = np.zeros((n, n), dtype=complex)
+    fl = np.zeros(n, dtype=bool)
+    for i in range(n):
+        sg = np.where(I[i].real >= 0, 1.0, -1.0)
+        mc, rc = np.sum(sg * I[i]), np.sum(I[i])
+        Ti[i] = sg * 0.5 * (abs(mc) + abs(rc)) / abs(mc)
+        if Ti[i, 0].real < 0:
+            fl[i] = True
+            Ti[i], I[i], V[i] = -Ti[i], -I[i], -V[i]
+    Tv = np.linalg.inv(Ti.conj()).T
+    return Ti, Tv, fl, np.sum(Ti * I, axis=1), np.sum(Tv * V, axis=1)
+
+
+def test_port_line_maps_even_odd_pair():
+    """Symmetric coupled lines: the even mode (equal line currents c) maps with
+    Ti row [1, 1] and the odd mode (c, -c) with [1/2, -1/2]; the odd mode given
+    with its first current negative is flipped; the mode currents are 2c and c."""
+    from openparem_b200.fem3d import port_line_maps
+    c = 0.02 - 0.001j
+    I = np.array([[c, c], [-c, c]])
+    V = np.array([[3.0 + 0.1j, 3.0 + 0.1j], [-1.2, 1.2]])
+    r = port_line_maps(I, V)
+    assert np.abs(r["Ti"] - np.array([[1, 1], [0.5, -0.5]])).max() < 1e-15
+    assert list(r["flipped"]) == [False, True]
+    assert np.abs(r["Im"] - np.array([2 * c, c])).max() < 1e-15
+    # Tv = (conj(Ti)^-1)^T: even-mode voltage is the line mean, odd the difference
+    assert np.abs(r["Tv"] - np.array([[0.5, 0.5], [1.0, -1.0]])).max() < 1e-15
+    assert np.abs(r["Vm"] - np.array([3.0 + 0.1j, 2.4])).max() < 1e-15
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4])
+def test_port_line_maps_match_reference_rule_and_conserve_power(n):
+    """Random mode currents and voltages on n lines: the library's maps equal the
+    restated rule, and V_m . conj(I_m) summed over the modes equals the same sum
+    over the lines (Tv^T conj(Ti) = I), which the single-ended conversion needs."""
+    from openparem_b200.fem3d import port_line_maps
+    rng = np.random.default_rng(40 + n)
+    while True:   # sign patterns of +-1 can be singular: those raise, tested below
+        I = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n)) + 2 * np.eye(n)
+        if abs(np.linalg.det(np.where(I.real >= 0, 1.0, -1.0))) > 0.5:
+            break
+        with pytest.raises(OpemError):
+            port_line_maps(I)
+    V = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+    r = port_line_maps(I, V)
+    Ti, Tv, fl, Im, Vm = _ref_line_maps(I, V)
+    for k, ref in (("Ti", Ti), ("Tv", Tv), ("Im", Im), ("Vm", Vm)):
+        assert np.abs(r[k] - ref).max() < 1e-12 * max(1.0, np.abs(ref).max()), k
+    assert (r["flipped"] == fl).all()
+    assert np.abs(r["Tv"].T @ r["Ti"].conj() - np.eye(n)).max() < 1e-12
+    # powers of line voltage/current pairs on the mode basis
+    vl, il = rng.normal(size=n) + 1j * rng.normal(size=n), rng.normal(size=n) + 1j * rng.normal(size=n)
+    assert abs(np.sum((r["Tv"] @ vl) * np.conj(r["Ti"] @ il)) - np.sum(vl * np.conj(il))) < 1e-12
+    with pytest.raises(OpemError):
+        port_line_maps(np.zeros((n, n)))   # no net current
