@@ -407,6 +407,14 @@ int  opem_selftest_wait_timeout(opem_context ctx, int polls);
  * a fresh cycle and one started from a deflated (kd+1) x kd block.
  * max_rel_diff: largest relative difference of residual estimates and y.     */
 int  opem_selftest_lsq(int m, int kd, int seed, double* max_rel_diff);
+/* Host copy of the face tables the boundary assembly uploads (no device
+ * needed): for the order-p reference tetrahedron and each local face f = 0..3,
+ * the tangential mass tables (t1 t1, t2 t2, t1 t2 + t2 t1; ldf x ldf each, ldf =
+ * p (p + 2)) integrated exactly (nodal = 0) or with the port integrals' nodal
+ * rule (nodal = 1: the rule of MFEM's order-p L2 triangle, which the overlaps of
+ * ports driven by their own 2D modes use).  out: 4 * 3 * ldf * ldf doubles;
+ * OPEM_ERR_ARG when nout is smaller or p is outside 1..8.                       */
+int  opem_selftest_face_tables(int p, int nodal, double* out, int64_t nout);
 
 /* ---- allocation-free assembly (no counterpart in the reference) -------------
  * For callers that cannot allocate device memory at the point of use: a

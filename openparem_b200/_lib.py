@@ -76,6 +76,7 @@ SIGNATURES = [
     ("opem_server_cancel", C.c_int, [P, C.c_int64]),
     ("opem_selftest_wait_timeout", C.c_int, [P, C.c_int]),
     ("opem_selftest_lsq", C.c_int, [C.c_int, C.c_int, C.c_int, DP]),
+    ("opem_selftest_face_tables", C.c_int, [C.c_int, C.c_int, DP, C.c_int64]),
     ("opem_project_load", C.c_int, [P, C.c_char_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_int), DP, C.c_int]),
     ("opem_project_info", C.c_int, [C.c_char_p, C.c_int, I64P, C.c_int, DP, C.c_int, C.c_char_p, C.c_int]),
     ("opem_project_value", C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int]),

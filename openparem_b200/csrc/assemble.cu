@@ -281,6 +281,23 @@ void assemble_boundary(Problem& P) {
     }
     DBuf<double> d_ftab;
     d_ftab.upload(ftab, s);
+    // A port driven by its own 2D mode on unsplit faces carries the mode exactly
+    // in its trace space; its overlap block (R_one, used by no system matrix of a
+    // port group) takes the reference's nodal rule (tangentialInnerProduct,
+    // src/OpenParEM3D/port.cpp:3463-3490): the same reduction over tables built
+    // with that rule.  The Robin blocks keep exact integration.
+    auto nodal_port = [&](const BGroup& G) {
+        return G.type == OPEM_BDR_PORT && G.port >= 0 && G.port < (int)P.modes.size() && P.modes[G.port].kind == 1 &&
+               P.modes[G.port].nsub == 1;
+    };
+    DBuf<double> d_wtab;
+    bool any_nodal = false;
+    for (const BGroup& G : P.groups) any_nodal = any_nodal || nodal_port(G);
+    if (any_nodal) {
+        std::vector<double> wtab = ftab;
+        for (int f = 0; f < 4; ++f) std::copy(R.Wh[f].begin(), R.Wh[f].end(), wtab.begin() + (size_t)f * 4 * L2);
+        d_wtab.upload(wtab, s);
+    }
     DBuf<int32_t> d_owner, d_lface;
     d_owner.upload(T.face_owner, s);
     d_lface.upload(T.face_lface, s);
@@ -346,6 +363,17 @@ void assemble_boundary(Problem& P) {
         boundary_reduce_kernel<<<(unsigned)((G.nu + 127) / 128), 128, 0, s>>>(G.nu, ldf, d_uptr.p, d_uent.p, d_fg.p,
                                                                              d_ftab.p, G.R.p); ++P.ctx->launches;
         OPEM_CUDA(cudaGetLastError());
+        if (nodal_port(G)) {
+            DBuf<double> Rn;
+            Rn.alloc(5 * G.nu);
+            boundary_reduce_kernel<<<(unsigned)((G.nu + 127) / 128), 128, 0, s>>>(G.nu, ldf, d_uptr.p, d_uent.p,
+                                                                                 d_fg.p, d_wtab.p, Rn.p);
+            ++P.ctx->launches;
+            OPEM_CUDA(cudaGetLastError());
+            OPEM_CUDA(cudaMemcpyAsync(G.R.p + 4 * G.nu, Rn.p + 4 * G.nu, G.nu * sizeof(double),
+                                      cudaMemcpyDeviceToDevice, s));
+            OPEM_CUDA(cudaStreamSynchronize(s));
+        }
         OPEM_CUDA(cudaStreamSynchronize(s));
     }
 }

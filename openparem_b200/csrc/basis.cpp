@@ -13,7 +13,9 @@
 // parameterised from its lowest global vertex by every element touching it,
 // so the assembled space is H(curl)-conforming with no sign flips.
 #include "opem_internal.h"
+#include "../../include/opem_b200.h"
 
+#include <algorithm>
 #include <cmath>
 #include <map>
 #include <memory>
@@ -83,6 +85,54 @@ void tri_rule(int deg, std::vector<double>& s1, std::vector<double>& s2, std::ve
             s2.push_back((1.0 - x[i]) * x[j]);
             w.push_back(wx[i] * wx[j] * (1.0 - x[i]));
         }
+}
+
+// The rule the reference's port integrals amount to: a product of fields
+// interpolated at the nodes of MFEM 4.8's order-p L2 triangle (Gauss-Legendre
+// basis: the nodes (o_i, o_j) / (o_i + o_j + o_{p-i-j}), i + j <= p, o the p + 1
+// Gauss-Legendre points on [0, 1]) and the interpolant integrated exactly; the
+// weights are the integrals of the degree-p Lagrange polynomials on the nodes
+// (tangentialInnerProduct, src/OpenParEM3D/port.cpp:3463-3490; Fields::calculatePz,
+// src/OpenParEM2D/fem2D.cpp:395-480, at order p - 1).  Weights sum to 1/2.
+void l2_nodal_rule(int p, std::vector<double>& s1, std::vector<double>& s2, std::vector<double>& w) {
+    std::vector<double> o, ow;
+    gauss_legendre01(p + 1, o, ow);
+    std::sort(o.begin(), o.end());
+    s1.clear(); s2.clear();
+    for (int j = 0; j <= p; ++j)
+        for (int i = 0; i + j <= p; ++i) {
+            const double d = o[i] + o[j] + o[p - i - j];
+            s1.push_back(o[i] / d);
+            s2.push_back(o[j] / d);
+        }
+    // V^T w = moments, V[node][monomial s1^a s2^b], moments a! b! / (a + b + 2)!
+    const int n = (int)s1.size();
+    std::vector<int> ma, mb;
+    for (int a = 0; a <= p; ++a)
+        for (int b = 0; a + b <= p; ++b) { ma.push_back(a); mb.push_back(b); }
+    auto fact = [](int k) { double f = 1; for (int i = 2; i <= k; ++i) f *= i; return f; };
+    std::vector<double> A((size_t)n * (n + 1));   // row m: V[.][m] | moment m
+    for (int m = 0; m < n; ++m) {
+        for (int q = 0; q < n; ++q) A[(size_t)m * (n + 1) + q] = std::pow(s1[q], ma[m]) * std::pow(s2[q], mb[m]);
+        A[(size_t)m * (n + 1) + n] = fact(ma[m]) * fact(mb[m]) / fact(ma[m] + mb[m] + 2);
+    }
+    for (int c = 0; c < n; ++c) {   // Gaussian elimination, partial pivoting
+        int pr = c;
+        for (int r = c + 1; r < n; ++r)
+            if (std::fabs(A[(size_t)r * (n + 1) + c]) > std::fabs(A[(size_t)pr * (n + 1) + c])) pr = r;
+        if (pr != c)
+            for (int k = 0; k <= n; ++k) std::swap(A[(size_t)pr * (n + 1) + k], A[(size_t)c * (n + 1) + k]);
+        for (int r = c + 1; r < n; ++r) {
+            const double f = A[(size_t)r * (n + 1) + c] / A[(size_t)c * (n + 1) + c];
+            for (int k = c; k <= n; ++k) A[(size_t)r * (n + 1) + k] -= f * A[(size_t)c * (n + 1) + k];
+        }
+    }
+    w.assign(n, 0.0);
+    for (int r = n - 1; r >= 0; --r) {
+        double s = A[(size_t)r * (n + 1) + n];
+        for (int k = r + 1; k < n; ++k) s -= A[(size_t)r * (n + 1) + k] * w[k];
+        w[r] = s / A[(size_t)r * (n + 1) + r];
+    }
 }
 
 static void tet_rule(int deg, std::vector<double>& X, std::vector<double>& w) {
@@ -457,10 +507,11 @@ static std::unique_ptr<NDRef> build_ref(int p) {
             R->Qh[(size_t)i * ld + j] = qv;
         }
 
-    // ---- face tables
+    // ---- face tables (exact, and with the port integrals' nodal rule: Wh)
     int ldf = R->ldf;
-    std::vector<double> s1, s2, wt;
+    std::vector<double> s1, s2, wt, n1, n2, nw;
     tri_rule(2 * p + 1, s1, s2, wt);
+    l2_nodal_rule(p, n1, n2, nw);
     static const int FE[4][3] = {{0, 1, 3}, {0, 2, 4}, {1, 2, 5}, {3, 4, 5}};   // (ab, ac, bc) edges
     for (int f = 0; f < 4; ++f) {
         std::vector<int>& fd = R->face_dofs[f];
@@ -510,6 +561,36 @@ static std::unique_ptr<NDRef> build_ref(int p) {
                 R->Fh[f][((size_t)2 * ldf + i) * ldf + j] = f12;
                 R->Ch[f][(size_t)i * ldf + j] = cc;
             }
+        // the same tangential tables with the nodal rule
+        const int nqn = (int)nw.size();
+        std::vector<double> W1((size_t)ldf * nqn), W2((size_t)ldf * nqn);
+        for (int q = 0; q < nqn; ++q) {
+            double x[3];
+            for (int d = 0; d < 3; ++d) x[d] = va[d] + n1[q] * t1[d] + n2[q] * t2[d];
+            C.vander(x, V.data());
+            for (int a2 = 0; a2 < ldf; ++a2) {
+                double u[3];
+                evalv(&R->coef[(size_t)fd[a2] * dim], V.data(), nm, u);
+                W1[(size_t)a2 * nqn + q] = u[0] * t1[0] + u[1] * t1[1] + u[2] * t1[2];
+                W2[(size_t)a2 * nqn + q] = u[0] * t2[0] + u[1] * t2[1] + u[2] * t2[2];
+            }
+        }
+        R->Wh[f].assign((size_t)3 * ldf * ldf, 0.0);
+        for (int i = 0; i < ldf; ++i)
+            for (int j = 0; j < ldf; ++j) {
+                double f11 = 0, f22 = 0, f12 = 0;
+                for (int q = 0; q < nqn; ++q) {
+                    const double w = nw[q];
+                    const double a1 = W1[(size_t)i * nqn + q], a2 = W2[(size_t)i * nqn + q];
+                    const double b1 = W1[(size_t)j * nqn + q], b2 = W2[(size_t)j * nqn + q];
+                    f11 += w * a1 * b1;
+                    f22 += w * a2 * b2;
+                    f12 += w * (a1 * b2 + a2 * b1);
+                }
+                R->Wh[f][((size_t)0 * ldf + i) * ldf + j] = f11;
+                R->Wh[f][((size_t)1 * ldf + i) * ldf + j] = f22;
+                R->Wh[f][((size_t)2 * ldf + i) * ldf + j] = f12;
+            }
     }
     return R;
 }
@@ -527,3 +608,19 @@ const NDRef& nd_reference(int p) {
 }
 
 }  // namespace opem
+
+extern "C" int opem_selftest_face_tables(int p, int nodal, double* out, int64_t nout) {
+    if (p < 1 || p > 8 || !out) return OPEM_ERR_ARG;
+    try {
+        const opem::NDRef& R = opem::nd_reference(p);
+        const size_t L = (size_t)3 * R.ldf * R.ldf;
+        if (nout < (int64_t)(4 * L)) return OPEM_ERR_ARG;
+        for (int f = 0; f < 4; ++f) {
+            const std::vector<double>& src = nodal ? R.Wh[f] : R.Fh[f];
+            std::copy(src.begin(), src.end(), out + f * L);
+        }
+    } catch (const std::exception&) {
+        return OPEM_ERR_ARG;
+    }
+    return OPEM_OK;
+}

@@ -30,6 +30,9 @@ struct NDRef {
     std::vector<double> Qh;       // ld*ld : int phi_i . curl phi_j
     // per local face f: Fh[f] = 3*ldf*ldf in (t1t1, t2t2, t1t2+t2t1); Ch[f] = ldf*ldf
     std::vector<double> Fh[4], Ch[4];
+    // Fh with the port integrals' nodal rule (l2_nodal_rule(p)) in place of exact
+    // integration: the overlaps of ports driven by their own 2D modes
+    std::vector<double> Wh[4];
     std::vector<int> face_dofs[4];   // ldf local dof ids per face
     std::vector<double> coef;        // ld*3*nmon basis coefficients
     std::vector<int> mon;            // nmon*3 exponents
@@ -46,6 +49,9 @@ const NDRef& nd_reference(int p);
 void gauss_legendre01(int n, std::vector<double>& x, std::vector<double>& w);
 // Collapsed rules exact to total degree `deg` (Gauss-Legendre in each direction).
 void tri_rule(int deg, std::vector<double>& s1, std::vector<double>& s2, std::vector<double>& w);
+// The nodal rule of MFEM's order-p L2 triangle (Gauss-Legendre nodes) that the
+// reference's port integrals amount to; weights sum to 1/2.
+void l2_nodal_rule(int p, std::vector<double>& s1, std::vector<double>& s2, std::vector<double>& w);
 // Orthonormal test polynomials on the unit triangle: coefficients T (n x n) over
 // monomials s1^i s2^j of degree <= P ordered by degree, i descending.
 std::vector<double> tri_test_polys(int P, std::vector<int>& mon2);

@@ -1033,4 +1033,87 @@ int port_mode_2d_pp(int64_t nnodes, const double* xy, int64_t ntri, const int64_
     return OPEM_OK;
 }
 
+int project_nd_2d(int64_t nnodes, const double* xy, int64_t ntri, const int64_t* st, int p, const cd* weight,
+                  const std::function<void(int64_t, double, double, cd&, cd&)>& field, std::vector<cd>& ch) {
+    if (nnodes < 3 || !xy || ntri < 1 || !st || p < 1 || p > 8 || !weight) return OPEM_ERR_ARG;
+    const RefSpaces2D& R = ref_spaces_2d(p);
+    static const int LP[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+    // numbering: p moments per edge (edges of sorted vertex pairs), p (p-1) per triangle
+    std::map<std::pair<int64_t, int64_t>, int> eid;
+    for (int64_t t = 0; t < ntri; ++t)
+        for (auto& lp : LP) eid[{st[3 * t + lp[0]], st[3 * t + lp[1]]}] = 0;
+    int ne = 0;
+    for (auto& kv : eid) kv.second = ne++;
+    const int nf = R.nf, nint = p * (p - 1);
+    const int64_t n = (int64_t)ne * p + ntri * nint;
+    if (n > INT32_MAX / 2) return OPEM_ERR_ARG;
+    std::vector<int> tdof((size_t)nf * ntri);
+    for (int64_t t = 0; t < ntri; ++t) {
+        for (int i = 0; i < 3; ++i) {
+            const int e = eid[{st[3 * t + LP[i][0]], st[3 * t + LP[i][1]]}];
+            for (int k = 0; k < p; ++k) tdof[(size_t)nf * t + p * i + k] = e * p + k;
+        }
+        for (int j = 0; j < nint; ++j) tdof[(size_t)nf * t + 3 * p + j] = (int)(ne * p + t * nint + j);
+    }
+    std::vector<double> q1, q2, qw;
+    tri_rule(2 * p + 2, q1, q2, qw);
+    const int nq = (int)qw.size();
+    std::vector<double> Nh((size_t)nq * nf * 2), Ch((size_t)nf);
+    for (int q = 0; q < nq; ++q) R.nd(q1[q], q2[q], &Nh[(size_t)q * nf * 2], Ch.data());
+    std::vector<Triplet> Mt;
+    Mt.reserve((size_t)ntri * nf * nf);
+    std::vector<cd> rhs(n, 0.0), Ml((size_t)nf * nf);
+    std::vector<double> Np((size_t)nf * 2);
+    for (int64_t t = 0; t < ntri; ++t) {
+        const double* p0 = xy + 2 * st[3 * t];
+        const double* p1 = xy + 2 * st[3 * t + 1];
+        const double* p2 = xy + 2 * st[3 * t + 2];
+        const double J00 = p1[0] - p0[0], J01 = p2[0] - p0[0], J10 = p1[1] - p0[1], J11 = p2[1] - p0[1];
+        const double det = J00 * J11 - J01 * J10;
+        if (!(std::fabs(det) > 0)) return OPEM_ERR_ARG;
+        const double a00 = J11 / det, a01 = -J10 / det, a10 = -J01 / det, a11 = J00 / det;   // J^-T
+        std::fill(Ml.begin(), Ml.end(), 0.0);
+        const int* td = &tdof[(size_t)nf * t];
+        for (int q = 0; q < nq; ++q) {
+            const cd w = qw[q] * std::fabs(det) * weight[t];
+            const double* nh = &Nh[(size_t)q * nf * 2];
+            for (int i = 0; i < nf; ++i) {
+                Np[2 * i] = a00 * nh[2 * i] + a01 * nh[2 * i + 1];
+                Np[2 * i + 1] = a10 * nh[2 * i] + a11 * nh[2 * i + 1];
+            }
+            cd fx, fy;
+            field(t, p0[0] + q1[q] * J00 + q2[q] * J01, p0[1] + q1[q] * J10 + q2[q] * J11, fx, fy);
+            for (int i = 0; i < nf; ++i) {
+                rhs[td[i]] += w * (Np[2 * i] * fx + Np[2 * i + 1] * fy);
+                for (int j = 0; j < nf; ++j)
+                    Ml[(size_t)i * nf + j] += w * (Np[2 * i] * Np[2 * j] + Np[2 * i + 1] * Np[2 * j + 1]);
+            }
+        }
+        for (int i = 0; i < nf; ++i)
+            for (int j = 0; j < nf; ++j) Mt.push_back({td[i], td[j], Ml[(size_t)i * nf + j]});
+    }
+    // banded LU in reverse Cuthill-McKee order
+    std::vector<std::vector<int>> adj(n);
+    for (auto& x : Mt)
+        if (x.r != x.c) adj[x.r].push_back(x.c);
+    for (auto& a : adj) { std::sort(a.begin(), a.end()); a.erase(std::unique(a.begin(), a.end()), a.end()); }
+    const std::vector<int> ord = rcm((int)n, adj);
+    std::vector<int> pos(n);
+    for (int64_t i = 0; i < n; ++i) pos[ord[i]] = (int)i;
+    int bw = 0;
+    for (int64_t i = 0; i < n; ++i)
+        for (int j : adj[i]) bw = std::max(bw, std::abs(pos[i] - pos[j]));
+    Banded B;
+    B.init((int)n, bw, bw);
+    for (auto& x : Mt) B.at(pos[x.r], pos[x.c]) += x.v;
+    if (!B.factor()) return OPEM_ERR_BREAKDOWN;
+    std::vector<cd> b(n);
+    for (int64_t i = 0; i < n; ++i) b[pos[i]] = rhs[i];
+    B.solve(b);
+    ch.assign((size_t)nf * ntri, 0.0);
+    for (int64_t t = 0; t < ntri; ++t)
+        for (int i = 0; i < nf; ++i) ch[(size_t)nf * t + i] = b[pos[tdof[(size_t)nf * t + i]]];
+    return OPEM_OK;
+}
+
 }  // namespace opem

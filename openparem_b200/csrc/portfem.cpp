@@ -20,6 +20,13 @@
 //     is given, I = int H . dl (the same Gauss rule per segment);
 //   * Z by the port's impedance definition (OpenParEM2D Mode::calculateImpedance,
 //     fem2D.cpp:1803-1824): PV V V* / (2 Pz*), VI V / I, PI 2 Pz / (I I*).
+// On unsplit port faces (and at orders above 2, and for higher modes) the mode
+// is solved with the order-p elements of RefSpaces2D, so it lies in the 3D trace
+// space, and the chain follows the reference's 2D solver further: H_t is the
+// mu-weighted L2 projection of the expression above onto the edge space (Hsolve,
+// src/OpenParEM2D/Hsolve.c:454-560) and Pz integrates E_t x H_t* interpolated on
+// the order-(p-1) L2 triangle (Fields::calculatePz, fem2D.cpp:395-480); the 3D
+// overlaps of such a port use the order-p nodal rule (assemble.cu).
 // The 3D port trace is then the moment interpolation of this field on each
 // port face (engine.cu port_traces), as for the analytic modes.
 #include "portfem.h"
@@ -63,7 +70,7 @@ void PortFem2D::eval_tri(int64_t t, const double X[3], cd E[3], cd Hy[3]) const 
     const double lam[3] = {1 - l1 - l2, l1, l2};
     const double* gg = &g[6 * t];
     cd ex = 0.0, ey = 0.0, zx, zy;
-    if (ref) {   // order >= 3, or a higher mode at any order
+    if (ref) {   // order-p path: unsplit faces, order >= 3, or a higher mode
         // reference bases at (l1, l2), covariant map J^-T (J^-1 = Ji row-major)
         const int nf = ref->nf, nl = ref->nl;
         std::vector<double> N(2 * nf), cu(nf), L(nl), gL(2 * nl);
@@ -72,6 +79,19 @@ void PortFem2D::eval_tri(int64_t t, const double X[3], cd E[3], cd Hy[3]) const 
         cd rx = 0.0, ry = 0.0, gx = 0.0, gy = 0.0;
         const cd* c = &ct[(size_t)nf * t];
         for (int i = 0; i < nf; ++i) { rx += c[i] * N[2 * i]; ry += c[i] * N[2 * i + 1]; }
+        if (!ch.empty()) {   // H_t / y from its projection onto the edge space
+            cd hx = 0.0, hy = 0.0;
+            const cd* h = &ch[(size_t)nf * t];
+            for (int i = 0; i < nf; ++i) { hx += h[i] * N[2 * i]; hy += h[i] * N[2 * i + 1]; }
+            ex = Ji[0] * rx + Ji[2] * ry;
+            ey = Ji[1] * rx + Ji[3] * ry;
+            const cd px = Ji[0] * hx + Ji[2] * hy, py = Ji[1] * hx + Ji[3] * hy;
+            for (int i = 0; i < 3; ++i) {
+                E[i] = ex * u[i] + ey * v[i];
+                Hy[i] = px * u[i] + py * v[i];
+            }
+            return;
+        }
         const cd* z = &cz[(size_t)nl * t];
         for (int i = 0; i < nl; ++i) { gx += z[i] * gL[2 * i]; gy += z[i] * gL[2 * i + 1]; }
         ex = Ji[0] * rx + Ji[2] * ry;
@@ -243,13 +263,17 @@ int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* fv, cons
     int64_t ne = 0;
     std::vector<int64_t> edges;
     std::vector<double> et, ez;
-    if (order >= 2 || mode > 0) {
+    // order-p elements of RefSpaces2D on unsplit faces (the mode then lies in the
+    // 3D trace space), at orders above 2 and for higher modes; the split faces
+    // keep the earlier first- and second-order solvers
+    const bool use_ref = order >= 3 || mode > 0 || nsub == 1;
+    if (order >= 2 || use_ref) {
         std::vector<cd> epsc(T), muc(T);
         for (int64_t t = 0; t < T; ++t) { epsc[t] = cd(eps2[2 * t], eps2[2 * t + 1]); muc[t] = M.mu[t]; }
         cd b2;
         std::vector<int64_t> st2;
         int rc;
-        if (order == 2 && mode == 0) {
+        if (!use_ref) {
             rc = port_mode_2d_p2(nn, M.xy.data(), T, tris.data(), epsc.data(), muc.data(), freq, b2, M.ct, M.cz, st2);
         } else {
             try {
@@ -318,6 +342,23 @@ int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* fv, cons
         M.gz[2 * t] = gx;
         M.gz[2 * t + 1] = gy;
     }
+    // order-p path: H_t as the reference's 2D solver forms it, the mu-weighted L2
+    // projection of n x (gamma e_t + grad e_z) / (j w mu) onto the edge space
+    // (projected here divided by y)
+    if (M.ref) {
+        auto hfield = [&](int64_t t, double x, double y, cd& fx, cd& fy) {
+            double X[3];
+            for (int c = 0; c < 3; ++c) X[c] = M.o[c] + x * M.u[c] + y * M.v[c];
+            cd E[3], Hy[3];
+            M.eval_tri(t, X, E, Hy);
+            fx = Hy[0] * M.u[0] + Hy[1] * M.u[1] + Hy[2] * M.u[2];
+            fy = Hy[0] * M.v[0] + Hy[1] * M.v[1] + Hy[2] * M.v[2];
+        };
+        std::vector<cd> chp;
+        const int rc = project_nd_2d(nn, M.xy.data(), T, M.st.data(), order, M.mu.data(), hfield, chp);
+        if (rc != OPEM_OK) { err = "port mode: H projection failed"; return rc; }
+        M.ch.swap(chp);
+    }
     // V = -int E . dl along the voltage path
     {
         const double* p0 = desc + 16;
@@ -344,7 +385,12 @@ int port_fem2d_solve(const double* verts, int64_t nface, const int64_t* fv, cons
         // edge-midpoint rule (exact for the quadratic integrand of order 1), or
         // the degree-2p triangle rule (order p >= 2: integrand of degree 2p)
         std::vector<double> r1, r2, rw;
-        if (order >= 2) {
+        if (M.ref) {
+            // the reference's Pz (Fields::calculatePz, src/OpenParEM2D/fem2D.cpp:395-480):
+            // E_t x H_t* interpolated on the order-(p-1) L2 triangle and integrated
+            l2_nodal_rule(order - 1, r1, r2, rw);
+            for (double& x : rw) x *= 6.0;
+        } else if (order >= 2) {
             tri_rule(2 * order, r1, r2, rw);
             for (double& x : rw) x *= 6.0;   // weights of the midpoint form: area/3 * sum -> sum_q 2 w_q area
         } else {

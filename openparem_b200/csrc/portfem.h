@@ -2,6 +2,7 @@
 #pragma once
 #include <complex>
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -46,6 +47,18 @@ int port_mode_2d_pp(int64_t nnodes, const double* xy, int64_t ntri, const int64_
                     std::complex<double>& beta, std::vector<std::complex<double>>& ct,
                     std::vector<std::complex<double>>& cz, std::vector<int64_t>& st, int mode = 0);
 
+// Weighted L2 projection of a tangential field onto the order-p edge space of
+// RefSpaces2D on the triangles (st: 3 sorted vertex ids per triangle; weight: one
+// complex factor per triangle; no boundary condition), as the reference's 2D
+// solver forms H_t (Hsolve, src/OpenParEM2D/Hsolve.c:454-560, with the mass
+// matrix weighted by omega mu, fem2D.cpp:2297-2303).  field(t, x, y, fx, fy)
+// gives the field at the point (x, y) of triangle t.  ch: nf coefficients per
+// triangle on the reference bases.  Returns an OPEM_* code.
+int project_nd_2d(int64_t nnodes, const double* xy, int64_t ntri, const int64_t* st, int p,
+                  const std::complex<double>* weight,
+                  const std::function<void(int64_t, double, double, std::complex<double>&, std::complex<double>&)>& field,
+                  std::vector<std::complex<double>>& ch);
+
 struct PortFem2D {
     using cd = std::complex<double>;
     int nsub = 0;
@@ -59,7 +72,8 @@ struct PortFem2D {
     std::vector<double> P0, Jinv, g;  // per sub-triangle: first node (2), J^-1 (4), grad lambda (3x2)
     std::vector<cd> ce, gz, mu;       // order 1: edge coefficients (3), grad e_z (2); mu_r (1)
     std::vector<cd> ct, cz;           // order 2: e_t (8) and e_z (6) coefficients; order >= 3: nf and nl
-    const RefSpaces2D* ref = nullptr; // order >= 3: the reference bases
+    const RefSpaces2D* ref = nullptr; // order-p path (unsplit faces, order >= 3, higher modes): the reference bases
+    std::vector<cd> ch;               // order-p path: H_t / y projected onto the edge space (nf per triangle)
     std::vector<int64_t> sub;         // per face: (i, j, upper) -> sub-triangle
 
     // E_t and H_t / y (y = gamma / (j w mu0 mu_port)) at the 3D point X of

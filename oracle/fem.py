@@ -17,7 +17,7 @@ import scipy.sparse as sp
 import scipy.sparse.linalg as spla
 
 from .nd_basis import NDBasis, EDGES, FACES, ndofs
-from .quadrature import line_rule, tri_rule
+from .quadrature import line_rule, tri_rule, l2_nodal_rule
 from . import materials, modes
 
 EPS0 = materials.EPS0
@@ -129,9 +129,23 @@ def element_matrices(prob, topo):
     return Me, Ke, Qe
 
 
-def face_matrices(prob, topo, faces):
-    """(dofs, Bm, Bcc) for boundary faces: tangential mass and surface curl-curl."""
+def nodal_face_tables(p):
+    """Face tables of basis(p) with the port integrals' nodal rule
+    (quadrature.l2_nodal_rule(p)) in place of exact integration."""
+    key = ("nodal", p)
+    if key not in _BASIS_CACHE:
+        B = basis(p)[0]
+        rule = l2_nodal_rule(p)
+        _BASIS_CACHE[key] = [B.face_tensors(f, rule) for f in range(4)]
+    return _BASIS_CACHE[key]
+
+
+def face_matrices(prob, topo, faces, nodal=False):
+    """(dofs, Bm, Bcc) for boundary faces: tangential mass and surface curl-curl
+    (Bm with the port integrals' nodal rule when nodal is set)."""
     B, _, _, _, ftabs = basis(topo.p)
+    if nodal:
+        ftabs = nodal_face_tables(topo.p)
     verts = np.asarray(prob["verts"], dtype=np.float64)
     dofs, Bm, Bcc = [], [], []
     for f in faces:
@@ -197,6 +211,7 @@ class Operators:
         for k in range(len(prob["ports"])):
             faces = np.array(sorted(self.port_faces.get(k, [])), dtype=np.int64)
             fd, Bm, Bcc = face_matrices(prob, topo, faces)
+            _, Bmn, _ = face_matrices(prob, topo, faces, nodal=True)
             rf = reg_of_face[faces]
             w_mu = 1.0 / np.asarray(prob["mu_r"], dtype=np.float64)[rf]
             w_eps = np.asarray(prob["eps_r"], dtype=np.float64)[rf]
@@ -210,6 +225,10 @@ class Operators:
                 "Bm_tand": _coo(n, fd, Bm, w_tand),
                 "Bm_sig": _coo(n, fd, Bm, w_sig),
                 "Bm1": _coo(n, fd, Bm),
+                # the reference's overlap integrals (tangentialInnerProduct,
+                # port.cpp:3463-3490): the product interpolated at the nodes of the
+                # order-p L2 triangle and integrated, i.e. the nodal rule
+                "Bm1n": _coo(n, fd, Bmn),
                 "region": int(reg_of_face[faces[0]]) if len(faces) else 0,
             })
         self.pec_dofs = np.unique(topo.face_global_dofs(self.pec_faces)) if len(self.pec_faces) else np.zeros(0, np.int64)
@@ -370,7 +389,10 @@ def solve_frequency(ops, freq, return_fields=False, reciprocal=True):
         qe = (ops.Q_mu @ e) / (w * MU0)
         h = 1j * (Plu.solve(qe.real) + 1j * Plu.solve(qe.imag))
         for k in range(N):
-            Bm = ops.ports[k]["Bm1"]
+            # ports driven by their own 2D mode carry it exactly in the trace space:
+            # their overlaps follow the reference's rule; analytic modes are
+            # integrated exactly
+            Bm = ops.ports[k]["Bm1n" if mm[k].get("nodal") else "Bm1"]
             e0 = np.vdot(Et[k], Bm @ e)
             e2 = np.vdot(Et[k], Bm @ Et[k])
             h0 = np.vdot(Ht[k], Bm @ h)

@@ -206,16 +206,17 @@ class NDBasis:
         Qh = np.einsum("q,iqa,jqa->ij", w, P, C)
         return Mh, Kh, Qh
 
-    def face_tensors(self, f):
+    def face_tensors(self, f, rule=None):
         """For local face f: (dofs, Fhat[k,l] (2,2,nf,nf), Chat (nf,nf)).
 
         Fhat[k,l]_ij = int_unit-tri (phi_i . t_k)(phi_j . t_l) ds,
-        Chat_ij      = int_unit-tri (curl phi_i . N)(curl phi_j . N) ds, N = t1 x t2.
+        Chat_ij      = int_unit-tri (curl phi_i . N)(curl phi_j . N) ds, N = t1 x t2;
+        exactly, or with rule = (points, weights) on the unit triangle.
         """
         a, b, c = FACES[f]
         t1 = VERTS[b] - VERTS[a]; t2 = VERTS[c] - VERTS[a]
         N = np.cross(t1, t2)
-        st, wt = tri_rule(2 * self.p + 1)
+        st, wt = tri_rule(2 * self.p + 1) if rule is None else rule
         X = VERTS[a][None, :] + st[:, 0:1] * t1[None, :] + st[:, 1:2] * t2[None, :]
         dofs = self.face_dofs(f)
         P = self.eval(X)[dofs]

@@ -128,6 +128,50 @@ def ref_spaces(p):
     return _REF[p]
 
 
+def _nd_numbering(st, p):
+    """Global ND_p DOFs of each triangle (T, p(p+2)): p per edge (edges of the
+    sorted vertex pairs), p(p-1) per triangle; returns (tdofs, net, edges, einv)."""
+    nt = len(st)
+    ekey = np.concatenate([st[:, [a, b]] for a, b in LP])
+    edges, einv = np.unique(ekey, axis=0, return_inverse=True)
+    tedge = einv.reshape(3, nt).T
+    ne = len(edges)
+    nint = p * (p - 1)
+    net = ne * p + nt * nint
+    tdofs = np.concatenate([(tedge[:, :, None] * p + np.arange(p)[None, None, :]).reshape(nt, 3 * p),
+                            ne * p + nint * np.arange(nt)[:, None] + np.arange(nint)[None, :]], axis=1)
+    return tdofs, net, edges, einv
+
+
+def project_nd(pts, tris, p, weight, field):
+    """Weighted L2 projection of a tangential field onto ND_p of the triangles,
+    as the reference's 2D solver forms H_t (Hsolve, src/OpenParEM2D/Hsolve.c:454-560:
+    Mt H_t = gamma Zt E_t + Cz E_z with Mt the mass matrix weighted by omega mu,
+    src/OpenParEM2D/fem2D.cpp:2297-2326; no boundary condition).  field(t, X2)
+    -> (q, 2) values at points X2 of triangle t; weight (T,) per triangle.
+    Returns per-triangle coefficients (T, p(p+2)) on the bases of ref_spaces(p)."""
+    pts = np.asarray(pts, dtype=float)
+    st = np.sort(np.asarray(tris, dtype=np.int64), axis=1)
+    nt = len(st)
+    tdofs, net, _, _ = _nd_numbering(st, p)
+    X, w = tri_rule(2 * p + 2)
+    Nh, _ = ref_spaces(p).nd(X)
+    rows, cols, vals = [], [], []
+    rhs = np.zeros(net, dtype=complex)
+    for t in range(nt):
+        P = pts[st[t]]
+        J = np.array([P[1] - P[0], P[2] - P[0]]).T
+        det = np.linalg.det(J)
+        N = np.einsum("ij,qnj->qni", np.linalg.inv(J).T, Nh)
+        wq = w * abs(det) * weight[t]
+        td = tdofs[t]
+        rows.append(np.repeat(td, len(td))); cols.append(np.tile(td, len(td)))
+        vals.append(np.einsum("q,qai,qbi->ab", wq, N, N).ravel())
+        np.add.at(rhs, td, np.einsum("q,qai,qi->a", wq, N, field(t, P[0] + X @ J.T)))
+    M = sp.csc_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(net, net))
+    return spla.spsolve(M, rhs)[tdofs]
+
+
 def solve_mode_pp(pts, tris, freq, eps_r, mu_r=None, p=1, mode=0):
     """Fundamental mode (mode 0), or the mode-th mode in decreasing beta^2, with
     order-p elements: (beta, ct (T, p(p+2)), cz (T, nl), st (T,3) sorted vertex
@@ -142,14 +186,9 @@ def solve_mode_pp(pts, tris, freq, eps_r, mu_r=None, p=1, mode=0):
     k0 = 2 * np.pi * freq * np.sqrt(MU0 * EPS0)
     R = ref_spaces(p)
     st = np.sort(tris, axis=1)
-    ekey = np.concatenate([st[:, [a, b]] for a, b in LP])
-    edges, einv = np.unique(ekey, axis=0, return_inverse=True)
+    tdofs, net, edges, einv = _nd_numbering(st, p)
     tedge = einv.reshape(3, nt).T
     ne, nn = len(edges), len(pts)
-    nint = p * (p - 1)
-    net = ne * p + nt * nint
-    tdofs = np.concatenate([(tedge[:, :, None] * p + np.arange(p)[None, None, :]).reshape(nt, 3 * p),
-                            ne * p + nint * np.arange(nt)[:, None] + np.arange(nint)[None, :]], axis=1)
     nle, nli = p - 1, (p - 1) * (p - 2) // 2
     nz = nn + ne * nle + nt * nli
     zdofs = np.concatenate([st, (nn + tedge[:, :, None] * nle + np.arange(nle)[None, None, :]).reshape(nt, 3 * nle),

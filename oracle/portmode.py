@@ -23,6 +23,13 @@ that chain for one mode per port:
 * Z by the mode's impedance definition ("zdef", OpenParEM2D
   Mode::calculateImpedance, src/OpenParEM2D/fem2D.cpp:1803-1824): PV
   V V* / (2 Pz*) (the default), VI V / I, PI 2 Pz / (I I*).
+
+On unsplit port faces (nsub = 1) the mode is solved with the order-p elements
+of oracle.port2d_pp, so it lies in the 3D trace space, and it follows the
+reference's 2D solver further: H_t is the mu-weighted L2 projection of the
+expression above onto ND_p (Hsolve), Pz integrates E_t x H_t* interpolated on
+the order-(p-1) L2 triangle (Fields::calculatePz), and the 3D overlaps use the
+order-p nodal rule (oracle.fem, quadrature.l2_nodal_rule).
 """
 import numpy as np
 
@@ -30,8 +37,8 @@ from .materials import MU0, EPS0, relative_eps
 from .modes import _frame
 from .nd_basis import FACES
 from .port2d import solve_mode, solve_mode_p2, LP2
-from .port2d_pp import solve_mode_pp, ref_spaces
-from .quadrature import tri_rule
+from .port2d_pp import solve_mode_pp, ref_spaces, project_nd
+from .quadrature import tri_rule, l2_nodal_rule
 
 
 def port_submesh(verts, face_verts, nsub, origin, uh, vh):
@@ -102,7 +109,10 @@ class Fem2DMode:
         mu = np.asarray(prob["mu_r"], dtype=np.float64)[reg].astype(np.complex128)
         self.order = int(mode.get("order2d", 1))
         mode_index = int(mode.get("mode_index", 0))   # 0: the fundamental mode; k: the k-th in decreasing beta^2
-        if self.order >= 3 or mode_index > 0:   # order-p edge / Lagrange elements (oracle.port2d_pp)
+        # order-p edge / Lagrange elements (oracle.port2d_pp): on unsplit port faces
+        # (the mode then lies in the 3D trace space), at orders above 2 and for
+        # higher modes; the split faces of the earlier path keep its solvers
+        if self.order >= 3 or mode_index > 0 or self.nsub == 1:
             beta, ct, cz, _ = solve_mode_pp(xy, tris, freq, eps, mu, self.order, mode_index)
             e0 = ct[:, :3 * self.order].ravel()
             big = e0[np.argmax(np.abs(e0))]
@@ -137,6 +147,14 @@ class Fem2DMode:
             self.cz = ez[st]                                     # (T,3)
             self.gz = np.einsum("tk,tki->ti", self.cz, self.g)   # grad e_z (T,2)
         self.w = 2 * np.pi * freq
+        self.chp = None
+        if getattr(self, "pp", False):
+            # H_t as the reference's 2D solver forms it: the mu-weighted L2
+            # projection of n x (gamma e_t + grad e_z) / (j w mu) onto ND_p
+            def h2d(t, X2):
+                _, H = self._eval(np.full(len(X2), t), X2)
+                return np.stack([H @ self.uh, H @ self.vh], axis=1)
+            self.chp = project_nd(xy, tris, self.order, mu, h2d)
         # metrics
         p0 = np.asarray(mode["vpath"][0], dtype=np.float64)
         p1 = np.asarray(mode["vpath"][1], dtype=np.float64)
@@ -146,7 +164,12 @@ class Fem2DMode:
         ws = np.tile(0.5 * wg / K, K)
         Xp = p0[None, :] + s[:, None] * (p1 - p0)[None, :]
         self.V = -np.sum(ws * (self.Et(Xp) @ (p1 - p0)))
-        q, wq = tri_rule(max(4, 2 * self.order))   # exact for the degree-2p integrand
+        if self.chp is not None:
+            # the reference's Pz (Fields::calculatePz, src/OpenParEM2D/fem2D.cpp:395-480):
+            # E_t x H_t* interpolated on the order-(p-1) L2 triangle and integrated
+            q, wq = l2_nodal_rule(self.order - 1)
+        else:
+            q, wq = tri_rule(max(4, 2 * self.order))   # exact for the degree-2p integrand
         T, nq = len(st), len(wq)
         tt = np.repeat(np.arange(T), nq)
         X2 = (self.P0[tt] + np.tile(q[:, 0], T)[:, None] * (P[tt, 1] - P[tt, 0])
@@ -192,6 +215,10 @@ class Fem2DMode:
             JiT = np.transpose(self.Jinv[t], (0, 2, 1))
             e2 = np.einsum("pij,pj->pi", JiT, np.einsum("pn,pni->pi", self.ctp[t], Nh))
             gz = np.einsum("pij,pj->pi", JiT, np.einsum("pl,pli->pi", self.czp[t], gLh))
+            if self.chp is not None:
+                h2 = np.einsum("pij,pj->pi", JiT, np.einsum("pn,pni->pi", self.chp[t], Nh))
+                E = e2[:, 0:1] * self.uh[None, :] + e2[:, 1:2] * self.vh[None, :]
+                return E, h2[:, 0:1] * self.uh[None, :] + h2[:, 1:2] * self.vh[None, :]
         elif self.order == 2:
             gz = np.zeros((len(t), 2), dtype=np.complex128)
             for i, (a, b) in enumerate(LP2):
@@ -253,5 +280,7 @@ class Fem2DMode:
             def at_face(self, f, S12, X):
                 return mode._eval(mode.face_tri(f, S12), mode._xy(X))[self.which]
 
+        # unsplit faces: the mode lies in the 3D trace space and the overlaps follow
+        # the reference's nodal rule (oracle.fem)
         return {"gamma": self.gamma, "Z": self.Z, "V": self.V, "Pz": self.Pz, "I": self.I, "Et": _Field(0),
-                "Ht": _Field(1)}
+                "Ht": _Field(1), "nodal": self.chp is not None and self.nsub == 1}

@@ -249,7 +249,10 @@ OTHER = {"partially-filled-lossless": ("partially_filled_rect_waveguide/partiall
          "tee": ("WR90/tee", "tee"),
          "t-junction": ("WR75/T-Junction", "T-Junction"),
          "permeability-straight": ("permeability/rectangular_waveguide", "straight"),
-         "permeability-partially-filled": ("permeability/partially_filled_rect_waveguide", "part")}
+         "permeability-partially-filled": ("permeability/partially_filled_rect_waveguide", "part"),
+         # a microstrip line over a GaAs substrate crossing a dielectric bridge: the
+         # strip is a hole in the port faces (conductor inside the cross-section)
+         "bridge-3p78": ("microstrip/bridge", "bridge_3p78")}
 
 PROJECTS = {"straight-flipped": "straight-flipped", "straight-rotated-xyz": "straight-rotated",
             "shorted": "shorted", "opened": "opened", "straight-loaded": "straight-loaded",

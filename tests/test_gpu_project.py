@@ -126,9 +126,10 @@ def test_coax_project_impedance_definitions(tmp_path):
     and PV impedance definitions (current paths about the inner conductor): the
     device solve's port impedance equals the host 2D mode's under the same
     definition (the same faces unsplit, second-order 2D elements), the three
-    definitions agree to 1 % on this TEM line (0.75 % on these unsplit faces; the
-    spread shrinks as the port faces are refined), and the line passes the wave
-    (|S21| > 0.99)."""
+    definitions agree to 5 % on this TEM line (with H_t projected onto the edge
+    space and Pz by the order-(p-1) nodal rule, as the reference forms them, PI
+    and VI sit 3.0 % and 1.5 % from PV on these 4 mm cells, 0.33 % and 0.16 % on
+    1 mm cells), and the line passes the wave (|S21| > 0.99)."""
     import os
     from openparem_b200.fem3d import port_mode_faces_z
     from project_files import write_coax_project, coax_mesh, faces_at_z
@@ -149,4 +150,4 @@ def test_coax_project_impedance_definitions(tmp_path):
         host = port_mode_faces_z(verts, fv, np.ones(len(fv), dtype=complex), mode, 1, fr[0], zdef, loop)["Z"]
         assert abs(Zo[0] / host - 1) < 1e-8, (zdef, Zo, host)
         zo[zdef] = Zo[0]
-    assert abs(zo["PI"] / zo["PV"] - 1) < 1e-2 and abs(zo["VI"] / zo["PV"] - 1) < 1e-2
+    assert abs(zo["PI"] / zo["PV"] - 1) < 5e-2 and abs(zo["VI"] / zo["PV"] - 1) < 5e-2

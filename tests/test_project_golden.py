@@ -139,3 +139,34 @@ def test_more_reference_projects(tmp_path, name, tol_deg, tol_db):
             assert abs(20 * np.log10(abs(s)) - v["found"]) < tol, v
         n += 1
     assert n >= 6
+
+
+def test_microstrip_bridge_pin(tmp_path):
+    """The reference's microstrip/bridge_3p78 project (ND5): a strip over a GaAs
+    substrate crossing a 3.78 dielectric bridge, the strip a hole in the port
+    faces, both ports driven by their quasi-TEM 2D modes (PV).  Read by the C++
+    reader and solved by the oracle with the reference's port rules (H_t
+    projected onto the edge space, overlaps by the order-p nodal rule), every
+    value the reference recorded at 25 GHz is reproduced: measured 5.2e-8 deg
+    and 2.5e-9 dB (with exact overlap integrals and the unprojected H_t the
+    phases were 0.05 deg off)."""
+    proj, rec = reference_project(str(tmp_path), "bridge-3p78")
+    prob, fr = project_problem(proj)
+    assert [(p["mode"]["kind"], p["mode"]["nsub"], p["mode"]["order2d"]) for p in prob["ports"]] == \
+        [("FEM2D", 1, 5)] * 2
+    with open(os.path.join(HERE, "golden", "wr90_expected.json")) as f:
+        rows = json.load(f)["cases"][rec["results_key"]]
+    f0 = min(v["frequency"] for v in rows.values())
+    assert f0 == fr[0] == 25e9
+    S = fem.solve_frequency(fem.Operators(prob), f0)["S"]
+    n = 0
+    for v in rows.values():
+        if v["frequency"] != f0:
+            continue
+        s = S[v["portOut"] - 1, v["portIn"] - 1]
+        if v["variable"] == "argS(deg)":
+            assert abs(np.angle(s, deg=True) - v["found"]) < 5e-7, v
+        else:
+            assert abs(20 * np.log10(abs(s)) - v["found"]) < 5e-8, v
+        n += 1
+    assert n == 8
