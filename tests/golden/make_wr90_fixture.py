@@ -256,7 +256,9 @@ OTHER = {"partially-filled-lossless": ("partially_filled_rect_waveguide/partiall
 
 PROJECTS = {"straight-flipped": "straight-flipped", "straight-rotated-xyz": "straight-rotated",
             "shorted": "shorted", "opened": "opened", "straight-loaded": "straight-loaded",
-            "straight-lossy": "straight", "straight-loaded-lossy": "straight-loaded"}
+            "straight-lossy": "straight", "straight-loaded-lossy": "straight-loaded",
+            "straight-rotated-x": "straight-rotated", "straight-rotated-y": "straight-rotated",
+            "straight-asymmetric": "straight-asymmetric"}
 
 
 def main(ref):

@@ -6,6 +6,8 @@ read by the C++ reader, and solved by the oracle at their own mesh order (6):
   straight-flipped       the guide with its ports swapped in the ports file
   straight-rotated-xyz   the guide rotated about x, y and z: port planes, mode
                          frames and voltage paths off every axis
+  straight-rotated-x/-y  the guide rotated about one axis
+  straight-asymmetric    the guide on an asymmetric mesh
   shorted                one port, the far end PEC
   opened                 one port, the far end a perfect_magnetic_conductor
                          boundary
@@ -64,7 +66,10 @@ def test_reference_projects_read(tmp_path):
 
 
 @pytest.mark.parametrize("name,stem", [("straight-flipped", "straight-flipped"),
-                                       ("straight-rotated-xyz", "straight-rotated")])
+                                       ("straight-rotated-xyz", "straight-rotated"),
+                                       ("straight-rotated-x", "straight-rotated"),
+                                       ("straight-rotated-y", "straight-rotated"),
+                                       ("straight-asymmetric", "straight-asymmetric")])
 def test_two_port_nd6_pin(tmp_path, name, stem):
     proj, _ = reference_project(str(tmp_path), name)
     prob, _ = project_problem(proj)
