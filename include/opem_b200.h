@@ -127,17 +127,32 @@ int  opem_problem_set_port_fem2d(opem_problem prob, int port, const double* desc
  * port driven by an analytic TE mode.                                          */
 int  opem_problem_set_port_impedance(opem_problem prob, int port, int definition, int npath, const double* path,
                                      int closed);
+/* A further mode of a port driven by its own 2D mode (after
+ * opem_problem_set_port_fem2d; the reference's ports with several Mode blocks):
+ * mode = 1..15, the mode-th mode of the same 2D problem in decreasing beta^2,
+ * with its own voltage path (vpath: start xyz, end xyz) and impedance definition
+ * (definition, npath, path, closed as for opem_problem_set_port_impedance).  It
+ * adds one S-port and one driving set on the same faces: S-ports are every
+ * port's first mode in port order, then the added modes in the order added;
+ * *sport (may be NULL) receives its 0-based S-port index.  When another port
+ * drives, a port with several modes absorbs with the gamma of largest magnitude
+ * among them (Port::addPortIntegrators, port.cpp:5790-5806).  Such problems solve
+ * on the FP64 path: mixed precision returns OPEM_ERR_UNSUPPORTED.  Setting the
+ * port again (set_port_te / set_port_fem2d) removes its added modes.
+ * OPEM_ERR_STATE when the port is not driven by its own 2D mode.               */
+int  opem_problem_add_port_mode(opem_problem prob, int port, int mode, const double* vpath, int definition,
+                                int npath, const double* path, int closed, int* sport);
 /* Builds DOF numbering, CSR pattern, vertex patches, and assembles the frequency-
  * independent operators on the device.                                         */
 int  opem_problem_assemble(opem_problem prob);
-/* info[0]=ndofs, [1]=nnz, [2]=nports, [3]=npatches, [4]=max patch size, [5]=local dofs,
+/* info[0]=ndofs, [1]=nnz, [2]=S-ports (ports plus added modes), [3]=npatches, [4]=max patch size, [5]=local dofs,
  * [6]=device bytes held, [7]=sum of patch sizes, [8]=sum of squared patch sizes
  * (entries of the block-Jacobi blocks).                                         */
 int  opem_problem_info(opem_problem prob, int64_t* info, int ninfo);
 
 /* ---- the per-frequency solve (fem3D::solve + calculateSplits + calculateS) ----
- * S_out: nports*nports complex (interleaved re,im), row = portOut, col = portIn.
- * Zo_out: nports complex (may be NULL).  stats may be NULL.                     */
+ * S_out: N*N complex (interleaved re,im), N = S-ports (info[2]), row = portOut,
+ * col = portIn.  Zo_out: N complex (may be NULL).  stats may be NULL.           */
 int  opem_solve_frequency(opem_problem prob, double freq, const opem_solver_opts* opts,
                           double* S_out, double* Zo_out, opem_solve_stats* stats);
 /* A sweep: nfreq frequencies x all driving sets in one call (batched in mixed mode).

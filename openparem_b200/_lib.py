@@ -93,6 +93,8 @@ SIGNATURES = [
     ("opem_write_touchstone", C.c_int, [C.c_char_p, C.c_int, DP, C.c_int, DP, C.c_double, C.c_char_p, C.c_char_p]),
     ("opem_s_mixed_mode", C.c_int, [C.c_int, DP, C.c_int, C.POINTER(C.c_int), C.c_double, DP, DP]),
     ("opem_s_single_ended", C.c_int, [C.c_int, DP, DP, DP, DP, C.c_double, DP, DP]),
+    ("opem_problem_add_port_mode", C.c_int, [C.c_void_p, C.c_int, C.c_int, DP, C.c_int, C.c_int, DP, C.c_int,
+                                             C.POINTER(C.c_int)]),
     ("opem_port_line_maps", C.c_int, [C.c_int, DP, DP, DP, DP, C.POINTER(C.c_int), DP, DP]),
     ("opem_s_relative_change", C.c_int, [C.c_int, DP, DP, DP]),
     ("opem_refine_mesh", C.c_int, [C.c_int64, DP, C.c_int64, I64P, I32P, C.c_int64, I64P, I32P, C.c_int64, I64P,

@@ -31,7 +31,7 @@ int64_t Problem::device_bytes() const {
     b += d_rowptr.bytes() + d_cols.bytes() + d_d2e_ptr.bytes() + d_d2e_elem.bytes() + d_d2e_loc.bytes();
     b += d_K.bytes() + d_Meps.bytes() + d_Mtand.bytes() + d_Msig.bytes() + d_M1.bytes() + d_Q.bytes();
     b += f_K.bytes() + f_Meps.bytes() + f_Mtand.bytes() + f_Msig.bytes();
-    b += d_elemcoef.bytes() + d_pec.bytes() + d_portmask.bytes() + d_et.bytes() + d_nxe.bytes();
+    b += d_elemcoef.bytes() + d_pec.bytes() + d_portmask.bytes() + d_et.bytes() + d_nxe.bytes() + d_et_x.bytes() + d_nxe_x.bytes();
     b += d_patch_ptr.bytes() + d_patch_dofs.bytes() + d_d2p_ptr.bytes() + d_d2p_idx.bytes() + d_patch_off.bytes();
     for (auto& g : groups) b += g.uslot.bytes() + g.urow.bytes() + g.ucol.bytes() + g.R.bytes() + g.brow.bytes() + g.bptr.bytes();
     return b;
@@ -79,10 +79,10 @@ bool has_fem2d_ports(const Problem& P) {
     return false;
 }
 
-// The 2D mode of port k at freq, from the cache or solved now.  The port faces
-// are taken in the order port_traces visits them.
-static std::shared_ptr<const PortFem2D> port_fem2d(const Problem& P, int k, double freq) {
-    const PortMode& pm = P.modes[k];
+// The 2D mode pm (P.modes[k] or an extra mode of port k) of port k's faces at
+// freq, from the mode's cache or solved now.  The port faces are taken in the
+// order port_traces visits them.
+static std::shared_ptr<const PortFem2D> port_fem2d_pm(const Problem& P, int k, const PortMode& pm, double freq) {
     std::lock_guard<std::mutex> lk(pm.fem->mu);
     for (auto& e : pm.fem->sols)
         if (e.first == freq) return e.second;
@@ -106,11 +106,41 @@ static std::shared_ptr<const PortFem2D> port_fem2d(const Problem& P, int k, doub
     int rc = port_fem2d_solve(T.verts.data(), (int64_t)fv.size() / 3, fv.data(), eps.data(), mu.data(), pm.desc,
                               pm.nsub, pm.order2d, freq, mu[0].real(), *sol, err, pm.zdef,
                               pm.ipath.empty() ? nullptr : pm.ipath.data(), (int)(pm.ipath.size() / 3),
-                              pm.ipath_closed);
+                              pm.ipath_closed, pm.mode);
     if (rc != OPEM_OK) throw OpemError(rc, err);
     pm.fem->sols.emplace_back(freq, sol);
     if (pm.fem->sols.size() > 8) pm.fem->sols.erase(pm.fem->sols.begin());
     return sol;
+}
+
+static std::shared_ptr<const PortFem2D> port_fem2d(const Problem& P, int k, double freq) {
+    return port_fem2d_pm(P, k, P.modes[k], freq);
+}
+
+void sport_gamma_Z_V(const Problem& P, int s, double freq, cd& gamma, cd& Z, cd& V) {
+    if (s < P.nports) {
+        port_gamma_Z_V(P, s, freq, gamma, Z, V);
+        return;
+    }
+    const ExtraMode& x = P.extra[s - P.nports];
+    auto sol = port_fem2d_pm(P, x.port, x.m, freq);
+    gamma = sol->gamma;
+    Z = sol->Z;
+    V = sol->V;
+}
+
+// Port::addPortIntegrators (src/OpenParEM3D/port.cpp:5790-5806): a port with
+// several modes absorbs with the gamma of largest magnitude among them
+cd robin_gamma(const Problem& P, int k, double freq) {
+    cd g, Z, V;
+    port_gamma_Z_V(P, k, freq, g, Z, V);
+    for (int i = 0; i < (int)P.extra.size(); ++i) {
+        if (P.extra[i].port != k) continue;
+        cd gx;
+        sport_gamma_Z_V(P, P.nports + i, freq, gx, Z, V);
+        if (std::abs(gx) > std::abs(g)) g = gx;
+    }
+    return g;
 }
 
 void port_gamma_Z_V(const Problem& P, int k, double freq, cd& gamma, cd& Z, cd& V) {
@@ -154,7 +184,8 @@ void port_gamma_Z_V(const Problem& P, int k, double freq, cd& gamma, cd& Z, cd& 
 
 // Trace DOFs of a tangential field on one port (Mode::fillX's data, port.cpp:3234-3341):
 // the edge and face moment functionals applied to E_t and n x E_t.
-static void port_traces_fem2d(Problem& P, int k, std::vector<double>& et, std::vector<double>& nxe, double freq);
+static void port_traces_fem2d(Problem& P, int k, std::vector<double>& et, std::vector<double>& nxe, double freq,
+                              const PortMode* pm = nullptr);
 
 static void port_traces(Problem& P, int k, std::vector<double>& et, std::vector<double>& nxe, double freq) {
     if (P.modes[k].kind == 1) {
@@ -266,9 +297,10 @@ static void port_traces(Problem& P, int k, std::vector<double>& et, std::vector<
 // being traced.  An edge inside the port gets the mean of its two faces'
 // moments: E_t's tangential trace is the same from both sides, H_t's (a normal
 // component of the edge-element field) jumps between cells.
-static void port_traces_fem2d(Problem& P, int k, std::vector<double>& et, std::vector<double>& nxe, double freq) {
+static void port_traces_fem2d(Problem& P, int k, std::vector<double>& et, std::vector<double>& nxe, double freq,
+                              const PortMode* pm) {
     const Topology& T = P.topo;
-    std::shared_ptr<const PortFem2D> fem = port_fem2d(P, k, freq);
+    std::shared_ptr<const PortFem2D> fem = port_fem2d_pm(P, k, pm ? *pm : P.modes[k], freq);
     const NDRef& R = nd_reference(T.p);
     const int p = T.p, N = fem->nsub;
     et.assign(2 * T.n, 0.0);
@@ -381,6 +413,15 @@ void refresh_port_traces(Problem& P, double freq) {
                                   cudaMemcpyHostToDevice, s));
         OPEM_CUDA(cudaMemcpyAsync(P.d_nxe.p + (size_t)2 * n * k, nx.data(), nx.size() * sizeof(double),
                                   cudaMemcpyHostToDevice, s));
+        // (pageable sources: each copy has read its buffer when it returns)
+    }
+    for (size_t i = 0; i < P.extra.size(); ++i) {
+        std::vector<double> et, nx;
+        port_traces_fem2d(P, P.extra[i].port, et, nx, freq, &P.extra[i].m);
+        OPEM_CUDA(cudaMemcpyAsync(P.d_et_x.p + (size_t)2 * n * i, et.data(), et.size() * sizeof(double),
+                                  cudaMemcpyHostToDevice, s));
+        OPEM_CUDA(cudaMemcpyAsync(P.d_nxe_x.p + (size_t)2 * n * i, nx.data(), nx.size() * sizeof(double),
+                                  cudaMemcpyHostToDevice, s));
     }
     OPEM_CUDA(cudaStreamSynchronize(s));
     P.trace_freq = freq;
@@ -397,8 +438,7 @@ void system_coefficients(const Problem& P, double freq, int d, VolCoef& vc, std:
         BCoef c;
         std::memset(&c, 0, sizeof(c));
         if (G.type == OPEM_BDR_PORT && G.port != d) {
-            cd gamma, Z, V;
-            port_gamma_Z_V(P, G.port, freq, gamma, Z, V);
+            const cd gamma = robin_gamma(P, G.port, freq);
             cd ig = 1.0 / gamma;
             cd ce = -k02 * ig, ct = cd(0, k02) * ig, cs = cd(0, w * MU0) * ig;
             c.c_cc = make_double2(ig.real(), ig.imag());
@@ -506,7 +546,8 @@ static void solve_frequency_plain(Problem& P, double freq, const opem_solver_opt
                                   bool keep_fields) {
     cudaStream_t s = P.ctx->stream;
     const int64_t n = P.topo.n, nnz = (int64_t)P.topo.cols.size();
-    const int N = P.nports;
+    // S-ports: every port's first mode, then the extra modes (one driving set each)
+    const int N = P.nsports();
     unsigned vg = (unsigned)(P.ctx->sm_count * 8);
     cudaEvent_t e0, e1;
     OPEM_CUDA(cudaEventCreate(&e0));
@@ -517,17 +558,27 @@ static void solve_frequency_plain(Problem& P, double freq, const opem_solver_opt
     std::vector<cd> Cp(N * N), Cm(N * N), gam(N), Z(N), V(N);
     double w = 2 * M_PI * freq;
     refresh_port_traces(P, freq);
-    for (int k = 0; k < N; ++k) port_gamma_Z_V(P, k, freq, gam[k], Z[k], V[k]);
+    for (int k = 0; k < N; ++k) sport_gamma_Z_V(P, k, freq, gam[k], Z[k], V[k]);
+    // trace vectors of S-port k
+    auto et_of = [&](int k) {
+        return k < P.nports ? reinterpret_cast<const double2*>(P.d_et.p) + (size_t)k * n
+                            : reinterpret_cast<const double2*>(P.d_et_x.p) + (size_t)(k - P.nports) * n;
+    };
+    auto nxe_of = [&](int k) {
+        return k < P.nports ? reinterpret_cast<const double2*>(P.d_nxe.p) + (size_t)k * n
+                            : reinterpret_cast<const double2*>(P.d_nxe_x.p) + (size_t)(k - P.nports) * n;
+    };
     out.st = opem_solve_stats{};
     out.st.converged = 1;
     if (keep_fields) { P.last_e.assign(N, {}); P.last_h.assign(N, {}); }
     for (int d = 0; d < N; ++d) {
+        const int pd = sport_port(P, d);   // the port this driving set drives
         VolCoef vc;
         std::vector<BCoef> bc;
-        system_coefficients(P, freq, d, vc, bc);
+        system_coefficients(P, freq, pd, vc, bc);
         form_system_matrix(P, vc, bc, A.p);
-        dmask_kernel<<<vg, 256, 0, s>>>(n, P.d_pec.p, P.d_portmask.p, d, dm.p); ++P.ctx->launches;
-        const double2* et = reinterpret_cast<const double2*>(P.d_et.p) + (size_t)d * n;
+        dmask_kernel<<<vg, 256, 0, s>>>(n, P.d_pec.p, P.d_portmask.p, pd, dm.p); ++P.ctx->launches;
+        const double2* et = et_of(d);
         lift_kernel<<<vg, 256, 0, s>>>(n, et, P.d_pec.p, x0.p); ++P.ctx->launches;
         // b_F = -(A x0'')_F
         spmv_complex(P, A.p, x0.p, b.p, dm.p);
@@ -546,13 +597,14 @@ static void solve_frequency_plain(Problem& P, double freq, const opem_solver_opt
         out.st.h_iterations += rh.its;
         // overlaps
         for (int k = 0; k < N; ++k) {
-            const double2* etk = reinterpret_cast<const double2*>(P.d_et.p) + (size_t)k * n;
-            const double2* nxk = reinterpret_cast<const double2*>(P.d_nxe.p) + (size_t)k * n;
+            const double2* etk = et_of(k);
+            const double2* nxk = nxe_of(k);
+            const int pk = sport_port(P, k);
             double2* o4 = ov.p + 4 * (d * N + k);
-            port_overlap(P, k, etk, x.p, o4 + 0);   // e0 = <Em, E>
-            port_overlap(P, k, etk, etk, o4 + 1);   // e2
-            port_overlap(P, k, nxk, h.p, o4 + 2);   // <n x Em, H>   (scaled below)
-            port_overlap(P, k, nxk, nxk, o4 + 3);   // <n x Em, n x Em>
+            port_overlap(P, pk, etk, x.p, o4 + 0);   // e0 = <Em, E>
+            port_overlap(P, pk, etk, etk, o4 + 1);   // e2
+            port_overlap(P, pk, nxk, h.p, o4 + 2);   // <n x Em, H>   (scaled below)
+            port_overlap(P, pk, nxk, nxk, o4 + 3);   // <n x Em, n x Em>
         }
         if (keep_fields) {
             P.last_e[d].resize(2 * n);
@@ -569,7 +621,7 @@ static void solve_frequency_plain(Problem& P, double freq, const opem_solver_opt
         for (int k = 0; k < N; ++k) {
             const double2* o4 = &hov[4 * (d * N + k)];
             // mode H_t = y n x E_t, y = gamma / (j w mu):  h0 = conj(y) <nxE, H>, h2 = |y|^2 <nxE, nxE>
-            int r = port_region(P, k);
+            int r = port_region(P, sport_port(P, k));
             cd y = gam[k] / cd(0, w * P.mu_r[r] * MU0);
             cd e0(o4[0].x, o4[0].y), e2(o4[1].x, o4[1].y);
             cd h0 = std::conj(y) * cd(o4[2].x, o4[2].y), h2 = std::norm(y) * cd(o4[3].x, o4[3].y);
@@ -641,6 +693,9 @@ static void assemble_problem(Problem& P) {
     for (int k = 0; k < P.nports; ++k)
         if (!P.modes.size() || k >= (int)P.modes.size() || !P.modes[k].set)
             throw OpemError(OPEM_ERR_STATE, "port mode not set for port " + std::to_string(k));
+    for (const ExtraMode& x : P.extra)
+        if (x.port < 0 || x.port >= P.nports || P.modes[x.port].kind != 1)
+            throw OpemError(OPEM_ERR_STATE, "an extra mode needs a port driven by its own 2D mode");
     // dirichlet masks
     const NDRef& R = nd_reference(T.p);
     P.h_pec.assign(T.n, 0);
@@ -695,9 +750,16 @@ static void assemble_problem(Problem& P) {
     }
     P.d_et.upload(et_all, s);
     P.d_nxe.upload(nx_all, s);
+    if (!P.extra.empty()) {   // extra modes: traced per frequency as well
+        std::vector<double> zx((size_t)2 * T.n * P.extra.size(), 0.0);
+        P.d_et_x.upload(zx, s);
+        P.d_nxe_x.upload(zx, s);
+        OPEM_CUDA(cudaStreamSynchronize(s));
+    }
     P.trace_freq = -1;
     for (int k = 0; k < P.nports; ++k)
         if (P.modes[k].kind == 1) P.modes[k].fem = std::make_shared<PortFemCache>();   // geometry may have changed
+    for (ExtraMode& x : P.extra) x.m.fem = std::make_shared<PortFemCache>();
     OPEM_CUDA(cudaStreamSynchronize(s));
     P.assembled = true;
 }
@@ -747,8 +809,7 @@ static int coefficients_fixed(const Problem& P, double freq, int d, VolCoef& vc,
         BCoef c;
         std::memset(&c, 0, sizeof(c));
         if (G.type == OPEM_BDR_PORT && G.port != d) {
-            cd gamma, Z, V;
-            port_gamma_Z_V(P, G.port, freq, gamma, Z, V);
+            const cd gamma = robin_gamma(P, G.port, freq);
             cd ig = 1.0 / gamma;
             cd ce = -k02 * ig, ct = cd(0, k02) * ig, cs = cd(0, w * MU0) * ig;
             c.c_cc = make_double2(ig.real(), ig.imag());
@@ -918,6 +979,9 @@ int opem_problem_set_port_te(opem_problem prob, int port, const double* desc) {
     P.modes[port].ipath.clear();
     P.modes[port].fem.reset();
     std::memcpy(P.modes[port].desc, desc, 22 * sizeof(double));
+    // the port's further modes belonged to its earlier definition
+    P.extra.erase(std::remove_if(P.extra.begin(), P.extra.end(), [&](const ExtraMode& x) { return x.port == port; }),
+                  P.extra.end());
     P.assembled = false;
     return OPEM_OK;
 }
@@ -935,8 +999,38 @@ int opem_problem_set_port_fem2d(opem_problem prob, int port, const double* desc,
     m.order2d = order;
     m.zdef = OPEM_Z_PV;
     m.ipath.clear();
+    m.mode = 0;
     m.fem = std::make_shared<PortFemCache>();
     std::memcpy(m.desc, desc, 22 * sizeof(double));
+    P.extra.erase(std::remove_if(P.extra.begin(), P.extra.end(), [&](const ExtraMode& x) { return x.port == port; }),
+                  P.extra.end());
+    P.assembled = false;
+    return OPEM_OK;
+}
+
+int opem_problem_add_port_mode(opem_problem prob, int port, int mode, const double* vpath, int definition, int npath,
+                               const double* path, int closed, int* sport) {
+    if (!prob || !vpath || port < 0 || mode < 1 || mode > 15 || definition < OPEM_Z_PV || definition > OPEM_Z_PI ||
+        npath < 0 || (npath > 0 && !path) || (definition != OPEM_Z_PV && npath < 2))
+        return OPEM_ERR_ARG;
+    for (int i = 0; i < 6; ++i)
+        if (!std::isfinite(vpath[i])) return OPEM_ERR_ARG;
+    for (int i = 0; i < 3 * npath; ++i)
+        if (!std::isfinite(path[i])) return OPEM_ERR_ARG;
+    Problem& P = prob->p;
+    if ((int)P.modes.size() <= port || !P.modes[port].set || P.modes[port].kind != 1) return OPEM_ERR_STATE;
+    if ((int)P.modes.size() + (int)P.extra.size() >= 16) return OPEM_ERR_UNSUPPORTED;
+    ExtraMode x;
+    x.port = port;
+    x.m = P.modes[port];   // frame, split and element order of the port
+    x.m.mode = mode;
+    std::memcpy(x.m.desc + 16, vpath, 6 * sizeof(double));
+    x.m.zdef = definition;
+    x.m.ipath.assign(path ? path : nullptr, path ? path + 3 * npath : nullptr);
+    x.m.ipath_closed = closed != 0;
+    x.m.fem = std::make_shared<PortFemCache>();
+    P.extra.push_back(std::move(x));
+    if (sport) *sport = (int)P.modes.size() + (int)P.extra.size() - 1;
     P.assembled = false;
     return OPEM_OK;
 }
@@ -974,7 +1068,7 @@ int opem_problem_info(opem_problem prob, int64_t* info, int ninfo) {
     const Problem& P = prob->p;
     const int64_t sum_s = (int64_t)P.topo.patch_dofs.size();
     const int64_t sum_s2 = P.topo.patch_off.empty() ? 0 : P.topo.patch_off.back();
-    int64_t v[9] = {P.topo.n, (int64_t)P.topo.cols.size(), P.nports, P.npatch, P.topo.max_patch, P.topo.ld,
+    int64_t v[9] = {P.topo.n, (int64_t)P.topo.cols.size(), P.nsports(), P.npatch, P.topo.max_patch, P.topo.ld,
                     P.device_bytes(), sum_s, sum_s2};
     for (int i = 0; i < ninfo && i < 9; ++i) info[i] = v[i];
     return OPEM_OK;
@@ -994,6 +1088,10 @@ int opem_solve_frequency(opem_problem prob, double freq, const opem_solver_opts*
     if (!opts_ok(&o)) return OPEM_ERR_ARG;
     Problem& P = prob->p;
     if (!P.assembled) { P.ctx->last_error = "problem not assembled"; return OPEM_ERR_STATE; }
+    if (o.precision == OPEM_PREC_MIXED && !P.extra.empty()) {
+        P.ctx->last_error = "ports with several modes run on the FP64 path";
+        return OPEM_ERR_UNSUPPORTED;
+    }
     FreqResult fr;
     int rc = guarded(P.ctx, [&] {
         OPEM_CUDA(cudaSetDevice(P.ctx->device));
@@ -1013,7 +1111,7 @@ int opem_solve_frequency(opem_problem prob, double freq, const opem_solver_opts*
         }
     });
     if (rc) return rc;
-    int N = P.nports;
+    int N = P.nsports();
     for (int i = 0; i < N * N; ++i) { S_out[2 * i] = fr.S[i].real(); S_out[2 * i + 1] = fr.S[i].imag(); }
     if (Zo_out)
         for (int i = 0; i < N; ++i) { Zo_out[2 * i] = fr.Zo[i].real(); Zo_out[2 * i + 1] = fr.Zo[i].imag(); }
@@ -1024,9 +1122,13 @@ int opem_solve_frequency(opem_problem prob, double freq, const opem_solver_opts*
 int opem_solve_sweep(opem_problem prob, int nfreq, const double* freqs, const opem_solver_opts* opts, double* S_out,
                      opem_solve_stats* stats) {
     if (!prob || nfreq <= 0 || !freqs || !S_out) return OPEM_ERR_ARG;
-    int N = prob->p.nports, worst = OPEM_OK;
+    int N = prob->p.nsports(), worst = OPEM_OK;
     if (opts && opts->precision == OPEM_PREC_MIXED) {
         Problem& P = prob->p;
+        if (!P.extra.empty()) {
+            P.ctx->last_error = "ports with several modes run on the FP64 path";
+            return OPEM_ERR_UNSUPPORTED;
+        }
         if (!opts_ok(opts)) return OPEM_ERR_ARG;
         if (!P.assembled) { P.ctx->last_error = "problem not assembled"; return OPEM_ERR_STATE; }
         for (int f = 0; f < nfreq; ++f)

@@ -92,7 +92,18 @@ struct PortMode {
     int zdef = 0;    // kind 1: OPEM_Z_PV / VI / PI
     std::vector<double> ipath;   // kind 1: current path points (xyz)
     bool ipath_closed = true;
+    int mode = 0;    // kind 1: which mode of the 2D problem, in decreasing beta^2
     std::shared_ptr<PortFemCache> fem;
+};
+
+// A further mode of a port driven by its own 2D modes: one more S-port (and
+// driving set) on the same faces, as the reference's ports with several modes.
+// S-ports are numbered: every port's first mode in port order, then these in
+// the order they were added.
+struct ExtraMode {
+    int port = -1;
+    PortMode m;      // kind 1, the port's frame and element order; its own mode
+                     // number, voltage path (desc[16..21]) and impedance definition
 };
 
 struct Problem {
@@ -104,6 +115,8 @@ struct Problem {
     std::vector<std::pair<int, Bdr>> bdr;           // attr -> type
     int nports = 0;
     std::vector<PortMode> modes;
+    std::vector<ExtraMode> extra;   // further modes of ports driven by their 2D modes
+    int nsports() const { return nports + (int)extra.size(); }
     double trace_freq = -1;     // frequency of the device traces of ports driven by their 2D mode
     bool assembled = false;
     int64_t ws_cap = 0;         // device bytes a batched sweep may take for its workspace (0: half of free)
@@ -129,6 +142,7 @@ struct Problem {
     std::vector<std::vector<double>> et_trace;     // per port: n complex (only port dofs nonzero)
     std::vector<std::vector<double>> nxe_trace;    // per port: trace of n x Et
     DBuf<double> d_et, d_nxe;                      // nports * n complex
+    DBuf<double> d_et_x, d_nxe_x;                  // the same for the extra modes
     // vertex patches
     DBuf<int32_t> d_patch_ptr, d_patch_dofs, d_d2p_ptr, d_d2p_idx;
     DBuf<int64_t> d_patch_off;
@@ -151,6 +165,12 @@ void form_system_matrix_n(Problem& P, const VolCoef& vc, const BCoef* bc, size_t
 // host: coefficients of A(freq) for driving set d
 void system_coefficients(const Problem& P, double freq, int d, VolCoef& vc, std::vector<BCoef>& bc);
 void port_gamma_Z_V(const Problem& P, int port, double freq, cd& gamma, cd& Z, cd& V);
+// gamma, Z, V of S-port s (port modes, then the extra modes)
+void sport_gamma_Z_V(const Problem& P, int s, double freq, cd& gamma, cd& Z, cd& V);
+// the physical port of S-port s
+inline int sport_port(const Problem& P, int s) { return s < P.nports ? s : P.extra[s - P.nports].port; }
+// gamma of port k's absorbing condition: of its largest-|gamma| mode
+cd robin_gamma(const Problem& P, int k, double freq);
 // Re-computes the device traces of the ports driven by their own 2D mode for
 // freq (no-op when there are none or they are current); synchronises the stream.
 void refresh_port_traces(Problem& P, double freq);

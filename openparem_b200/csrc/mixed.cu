@@ -2177,6 +2177,7 @@ static void solve_batch(Problem& P, const std::vector<System>& systems, const op
 // x N driving sets <= RMAX systems.
 void solve_sweep_mixed(Problem& P, int nfreq, const double* freqs, const opem_solver_opts& o,
                        std::vector<std::vector<cd>>& S, std::vector<opem_solve_stats>& st) {
+    if (!P.extra.empty()) throw OpemError(OPEM_ERR_UNSUPPORTED, "ports with several modes run on the FP64 path");
     const int N = P.nports;
     int F = std::max(1, RMAX / std::max(1, N));
     if (o.poly_degree > 1) ensure_f32_operators(P, P.ctx->stream);

@@ -95,11 +95,11 @@ void run_request(Request& rq, opem_context_s* slot) {
     const int64_t cap = P.ws_cap;
     P.ctx = &slot->c;   // the request runs on the slot's stream
     P.ws_cap = (int64_t)rq.bytes;
-    const int N0 = std::max(1, P.nports);
+    const int N0 = std::max(1, P.nsports());
     int rc = OPEM_OK;
     if (!P.assembled) rc = opem_problem_assemble(rq.prob);
     if (rc == OPEM_OK) {
-        const int N = std::max(1, P.nports);
+        const int N = std::max(1, P.nsports());
         rq.S.assign((size_t)2 * N * N * rq.freqs.size(), 0.0);
         rq.stats.assign(rq.freqs.size(), opem_solve_stats{});
         rc = opem_solve_sweep(rq.prob, (int)rq.freqs.size(), rq.freqs.data(), &rq.opts, rq.S.data(), rq.stats.data());

@@ -263,7 +263,20 @@ class Fem3D:
                         int(port["mode"].get("ipath_closed", True))), "set_port_impedance")
             else:
                 _chk(self.ctx.h, L.opem_problem_set_port_te(self.h, k, _dp(d)), "set_port_te")
-        self.nports = len(prob["ports"])
+        # further modes of ports driven by their own 2D modes: one S-port each, after
+        # every port's first mode (the oracle's order)
+        nextra = 0
+        for k, port in enumerate(prob["ports"]):
+            for x in port["mode"].get("extra_modes", ()):
+                vp = np.ascontiguousarray(np.concatenate([np.ravel(x["vpath"][0]), np.ravel(x["vpath"][1])]),
+                                          dtype=np.float64)
+                ip = x.get("ipath")
+                ip = None if ip is None else np.ascontiguousarray(ip, dtype=np.float64).reshape(-1, 3)
+                _chk(self.ctx.h, L.opem_problem_add_port_mode(
+                    self.h, k, int(x["index"]), _dp(vp), _ZDEF[x.get("zdef", "PV")], 0 if ip is None else len(ip),
+                    None if ip is None else _dp(ip), int(x.get("ipath_closed", True)), None), "add_port_mode")
+                nextra += 1
+        self.nports = len(prob["ports"]) + nextra
         self._assembled = False
 
     @classmethod

@@ -329,7 +329,7 @@ def assemble_A(ops, freq, driven):
     for k, port in enumerate(ops.ports):
         if k == driven:
             continue
-        g = port_mode(ops, k, freq)["gamma"]
+        g = robin_gamma(ops, k, freq)
         A = A + (1.0 / g) * port["Bcc"] + (1.0 / g) * (-k0 ** 2 * port["Bm_eps"] + 1j * k0 ** 2 * port["Bm_tand"]
                                                       + 1j * w * MU0 * port["Bm_sig"])
     for spec, Bm in ops.imp:
@@ -357,16 +357,62 @@ def port_mode(ops, k, freq):
     return modes.mode_metrics(prob["ports"][k]["mode"], freq, eps_c, prob["mu_r"][r])
 
 
+def sports(prob):
+    """The S-ports: (port, extra) pairs, every port's first mode in port order,
+    then the further modes of ports driven by their own 2D modes ("extra_modes"
+    of the port's mode: dicts with "index" (mode number in decreasing beta^2),
+    "vpath" and optionally "zdef", "ipath", "ipath_closed"), in port order."""
+    out = [(k, None) for k in range(len(prob["ports"]))]
+    for k, p in enumerate(prob["ports"]):
+        for x in p["mode"].get("extra_modes", ()):
+            out.append((k, x))
+    return out
+
+
+def sport_mode(ops, s, freq):
+    """Metrics of S-port s (sports order) at freq."""
+    k, x = sports(ops.prob)[s]
+    if x is None:
+        return port_mode(ops, k, freq)
+    cache = ops.__dict__.setdefault("_fem2d_x", {})
+    if (s, freq) not in cache:
+        from .portmode import Fem2DMode
+        mode = dict(ops.prob["ports"][k]["mode"])
+        mode.pop("extra_modes", None)
+        mode.update(mode_index=int(x["index"]), vpath=x["vpath"], zdef=x.get("zdef", "PV"))
+        mode.pop("ipath", None)
+        if x.get("ipath") is not None:
+            mode.update(ipath=x["ipath"], ipath_closed=x.get("ipath_closed", True))
+        cache[(s, freq)] = Fem2DMode(ops.prob, ops.topo, ops.ports[k]["faces"], mode, freq).metrics()
+    return cache[(s, freq)]
+
+
+def robin_gamma(ops, k, freq):
+    """gamma of port k's absorbing condition when another port drives: with
+    several modes on the port, the one of largest |gamma| (Port::addPortIntegrators,
+    src/OpenParEM3D/port.cpp:5790-5806, "to avoid passivity violations")."""
+    g = port_mode(ops, k, freq)["gamma"]
+    for s, (q, x) in enumerate(sports(ops.prob)):
+        if x is not None and q == k:
+            gx = sport_mode(ops, s, freq)["gamma"]
+            if abs(gx) > abs(g):
+                g = gx
+    return g
+
+
 def solve_frequency(ops, freq, return_fields=False, reciprocal=True):
     """One frequency point: every driving set, E and H, overlaps, S.
-    Mirrors the driving-set loop src/OpenParEM3D/OpenParEM3D.cpp:497-566."""
+    Mirrors the driving-set loop src/OpenParEM3D/OpenParEM3D.cpp:497-566; a port
+    with several modes contributes one S-port (and one driving set) per mode."""
     topo = ops.topo
     prob = ops.prob
     w = 2 * np.pi * freq
-    N = len(ops.ports)
-    mm = [port_mode(ops, k, freq) for k in range(N)]
-    Et = [ops.port_trace(k, mm[k]["Et"]) for k in range(N)]
-    Ht = [ops.port_trace(k, mm[k]["Ht"]) for k in range(N)]
+    sp_ = sports(prob)
+    N = len(sp_)
+    pk = [k for k, _ in sp_]
+    mm = [sport_mode(ops, s, freq) for s in range(N)]
+    Et = [ops.port_trace(pk[s], mm[s]["Et"]) for s in range(N)]
+    Ht = [ops.port_trace(pk[s], mm[s]["Ht"]) for s in range(N)]
     Cp = np.zeros((N, N), dtype=np.complex128)   # [driving set, S-port]
     Cm = np.zeros((N, N), dtype=np.complex128)
     fields = []
@@ -375,10 +421,10 @@ def solve_frequency(ops, freq, return_fields=False, reciprocal=True):
     # mass matrix is symmetric positive definite, so no pivoting is needed
     Plu = spla.splu(P, permc_spec="MMD_AT_PLUS_A", options=dict(SymmetricMode=True, DiagPivotThresh=0.0))
     for d in range(N):
-        A = assemble_A(ops, freq, d)
+        A = assemble_A(ops, freq, pk[d])
         A = eliminate(A, ops.pec_dofs)
         x0 = np.zeros(topo.n, dtype=np.complex128)
-        pd = ops.ports[d]["dofs"]
+        pd = ops.ports[pk[d]]["dofs"]
         x0[pd] = Et[d][pd]
         b = -(A @ x0)
         b[pd] = x0[pd]
@@ -392,7 +438,7 @@ def solve_frequency(ops, freq, return_fields=False, reciprocal=True):
             # ports driven by their own 2D mode carry it exactly in the trace space:
             # their overlaps follow the reference's rule; analytic modes are
             # integrated exactly
-            Bm = ops.ports[k]["Bm1n" if mm[k].get("nodal") else "Bm1"]
+            Bm = ops.ports[pk[k]]["Bm1n" if mm[k].get("nodal") else "Bm1"]
             e0 = np.vdot(Et[k], Bm @ e)
             e2 = np.vdot(Et[k], Bm @ Et[k])
             h0 = np.vdot(Ht[k], Bm @ h)
