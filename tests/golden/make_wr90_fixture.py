@@ -310,6 +310,10 @@ def main(ref):
         "test_cases": read_test_cases(os.path.join(ref, "regression", "OpenParEM3D", "permeability",
                                                    "partially_filled_rect_waveguide", "part_test_cases.csv")),
         "evaluation": []}
+    reg["bridge-3p78"] = {
+        "test_cases": read_test_cases(os.path.join(ref, "regression", "OpenParEM3D", "microstrip", "bridge",
+                                                   "bridge_3p78_test_cases.csv")),
+        "evaluation": []}
     with open(os.path.join(HERE, "wr90_regression.json"), "w") as f:
         json.dump({"source": "regression/OpenParEM3D", "projects": reg}, f, indent=0)
     with open(os.path.join(HERE, "wr90_projects.json"), "w") as f:

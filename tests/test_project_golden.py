@@ -154,7 +154,10 @@ def test_microstrip_bridge_pin(tmp_path):
     projected onto the edge space, overlaps by the order-p nodal rule), every
     value the reference recorded at 25 GHz is reproduced: measured 5.2e-8 deg
     and 2.5e-9 dB (with exact overlap integrals and the unprojected H_t the
-    phases were 0.05 deg off)."""
+    phases were 0.05 deg off).  The reference's regression flow then passes the
+    project's own test cases of that frequency (opem_write_results_csv ->
+    opem_evaluate_test_cases, tolerances down to 1e-10 relative)."""
+    from openparem_b200.fem3d import write_results_csv, evaluate_test_cases
     proj, rec = reference_project(str(tmp_path), "bridge-3p78")
     prob, fr = project_problem(proj)
     assert [(p["mode"]["kind"], p["mode"]["nsub"], p["mode"]["order2d"]) for p in prob["ports"]] == \
@@ -175,3 +178,12 @@ def test_microstrip_bridge_pin(tmp_path):
             assert abs(20 * np.log10(abs(s)) - v["found"]) < 5e-8, v
         n += 1
     assert n == 8
+    res = tmp_path / "bridge_3p78_results.csv"
+    write_results_csv(res, [f0], S[None], 0.0, "DB", "GHz")
+    with open(os.path.join(HERE, "golden", "wr90_regression.json")) as f:
+        cases = [r for r in json.load(f)["projects"]["bridge-3p78"]["test_cases"] if float(r[1]) == f0]
+    tc = tmp_path / "cases.csv"
+    with open(tc, "w") as fh:
+        fh.write("# ResultDatabase::save_as_test\n" + "\n".join(",".join(r) for r in cases) + "\n")
+    ncase, npass = evaluate_test_cases(tc, res, tmp_path / "out.csv")
+    assert ncase == len(cases) == 8 and npass == ncase
