@@ -247,14 +247,20 @@ int solve_pencil(int n, const std::vector<Triplet>& A, const std::vector<Triplet
 // The k eigenpairs of A x = -beta^2 B x with the largest beta^2 (the k eigenvalues
 // nearest the shift sigma, which lies below all of them) by subspace iteration on
 // (A - sigma B)^-1 B with k + 2 vectors (one banded LU, RCM order as above) and
-// Rayleigh-Ritz on the projected pencil: converged when the k Ritz values have
-// settled to 1e-14 and at least 40 iterations ran (the Ritz vectors trail the
-// values).  lam[i] = -beta_i^2 in increasing distance from sigma, X (n x k,
+// Rayleigh-Ritz on the projected pencil: converged when every wanted Ritz pair's
+// residual is below 1e-11 relative and its value has settled to 1e-13.  lam[i] = -beta_i^2 in increasing distance from sigma, X (n x k,
 // column-major) the Ritz vectors in the caller's numbering.
+// The pencil's A has no e_z block, so every (0, psi) is an eigenvector with
+// lam = 0: a null space as large as the e_z space, which lies between the
+// propagating modes (lam < 0) and the cut-off ones (lam > 0) and would capture
+// the iteration.  The unknowns from nut on are psi; after every step psi is set
+// to the solution of the e_z rows of B x = 0 (psi = -B_zz^-1 B_zt e_t), which
+// every eigenvector of a nonzero lam satisfies and which removes any null-space
+// component, so cut-off modes are found too.
 int solve_pencil_k(int n, const std::vector<Triplet>& A, const std::vector<Triplet>& Bm, double sigma, int k,
-                   std::vector<cd>& lam, std::vector<cd>& X) {
+                   std::vector<cd>& lam, std::vector<cd>& X, int nut) {
     const int q = std::min(n, k + 2);
-    if (k < 1 || k > n) return OPEM_ERR_ARG;
+    if (k < 1 || k > n || nut < 1 || nut > n) return OPEM_ERR_ARG;
     std::vector<std::vector<int>> adj(n);
     for (auto* T : {&A, &Bm})
         for (auto& x : *T)
@@ -275,9 +281,42 @@ int solve_pencil_k(int n, const std::vector<Triplet>& A, const std::vector<Tripl
         std::fill(y, y + n, cd(0.0));
         for (auto& t : T) y[pos[t.r]] += t.v * x[pos[t.c]];
     };
+    // B_zz (banded LU, RCM order of its own pattern) and B_zt for the psi constraint
+    const int nz = n - nut;
+    std::vector<Triplet> Bzt;
+    Banded Mz;
+    std::vector<int> zpos(std::max(nz, 0));
+    if (nz > 0) {
+        std::vector<std::vector<int>> zadj(nz);
+        for (auto& t : Bm) {
+            if (t.r < nut) continue;
+            if (t.c < nut) Bzt.push_back(t);
+            else if (t.r != t.c) zadj[t.r - nut].push_back(t.c - nut);
+        }
+        for (auto& a : zadj) { std::sort(a.begin(), a.end()); a.erase(std::unique(a.begin(), a.end()), a.end()); }
+        std::vector<int> zord = rcm(nz, zadj);
+        for (int i = 0; i < nz; ++i) zpos[zord[i]] = i;
+        int zbw = 0;
+        for (int i = 0; i < nz; ++i)
+            for (int j : zadj[i]) zbw = std::max(zbw, std::abs(zpos[i] - zpos[j]));
+        Mz.init(nz, zbw, zbw);
+        for (auto& t : Bm)
+            if (t.r >= nut && t.c >= nut) Mz.at(zpos[t.r - nut], zpos[t.c - nut]) += t.v;
+        if (!Mz.factor()) return OPEM_ERR_BREAKDOWN;
+    }
+    std::vector<cd> zr(std::max(nz, 0));
+    auto constrain = [&](cd* y) {   // y in the permuted numbering
+        if (nz == 0) return;
+        std::fill(zr.begin(), zr.end(), cd(0.0));
+        for (auto& t : Bzt) zr[zpos[t.r - nut]] -= t.v * y[pos[t.c]];
+        Mz.solve(zr);
+        for (int i = 0; i < nz; ++i) y[pos[nut + i]] = zr[zpos[i]];
+    };
     std::vector<cd> Y((size_t)n * q), AY((size_t)n * q), BY((size_t)n * q), tmp(n);
-    for (int c = 0; c < q; ++c)
+    for (int c = 0; c < q; ++c) {
         for (int i = 0; i < n; ++i) Y[(size_t)c * n + i] = cd(1.0 + 0.001 * ((i * (c + 3)) % 11), 0.0007 * ((i + 5 * c) % 7));
+        constrain(&Y[(size_t)c * n]);
+    }
     std::vector<cd> prev(k, cd(0.0));
     lam.assign(k, 0.0);
     bool ok = false;
@@ -286,6 +325,7 @@ int solve_pencil_k(int n, const std::vector<Triplet>& A, const std::vector<Tripl
         for (int c = 0; c < q; ++c) {
             mul(Bm, &Y[(size_t)c * n], tmp.data());
             M.solve(tmp);
+            constrain(tmp.data());
             std::copy(tmp.begin(), tmp.end(), &Y[(size_t)c * n]);
         }
         if (opem::orthonormalise(n, q, Y) != q) return OPEM_ERR_BREAKDOWN;
@@ -317,22 +357,37 @@ int solve_pencil_k(int n, const std::vector<Triplet>& A, const std::vector<Tripl
         std::vector<int> idx(q);
         for (int i = 0; i < q; ++i) idx[i] = i;
         std::sort(idx.begin(), idx.end(), [&](int a, int b) { return std::abs(th[a]) < std::abs(th[b]); });
-        // Ritz vectors, nearest first
-        std::vector<cd> Yn((size_t)n * q, 0.0);
+        // Ritz vectors, nearest first, and their products with A and B (the same
+        // combinations of AY and BY)
+        std::vector<cd> Yn((size_t)n * q, 0.0), AYn((size_t)n * k, 0.0), BYn((size_t)n * k, 0.0);
         for (int c = 0; c < q; ++c)
             for (int j = 0; j < q; ++j) {
                 const cd z = Z[j + (size_t)idx[c] * q];
                 if (z == 0.0) continue;
                 for (int r = 0; r < n; ++r) Yn[(size_t)c * n + r] += Y[(size_t)j * n + r] * z;
+                if (c < k)
+                    for (int r = 0; r < n; ++r) {
+                        AYn[(size_t)c * n + r] += AY[(size_t)j * n + r] * z;
+                        BYn[(size_t)c * n + r] += BY[(size_t)j * n + r] * z;
+                    }
             }
         Y.swap(Yn);
+        // converged when every wanted pair's residual |A y - lam B y| is below
+        // 1e-11 of |A y| + |lam| |B y| and its value has settled to 1e-13
         bool settled = true;
         for (int i = 0; i < k; ++i) {
             lam[i] = sigma + th[idx[i]];
-            if (!(std::abs(lam[i] - prev[i]) <= 1e-14 * std::abs(lam[i]))) settled = false;
+            double rr = 0, na = 0, nb = 0;
+            for (int r = 0; r < n; ++r) {
+                rr += std::norm(AYn[(size_t)i * n + r] - lam[i] * BYn[(size_t)i * n + r]);
+                na += std::norm(AYn[(size_t)i * n + r]);
+                nb += std::norm(BYn[(size_t)i * n + r]);
+            }
+            if (!(std::sqrt(rr) <= 1e-11 * (std::sqrt(na) + std::abs(lam[i]) * std::sqrt(nb)))) settled = false;
+            if (!(std::abs(lam[i] - prev[i]) <= 1e-13 * std::abs(lam[i]))) settled = false;
             prev[i] = lam[i];
         }
-        ok = settled && it >= 40;
+        ok = settled && it >= 3;
     }
     if (!ok) return OPEM_ERR_NOT_CONVERGED;
     X.assign((size_t)n * k, 0.0);
@@ -1005,7 +1060,7 @@ int port_mode_2d_pp(int64_t nnodes, const double* xy, int64_t ntri, const int64_
         rc = solve_pencil(n, A, Bm, -k0 * k0 * emax, lam, xs);
     } else {   // the mode-th mode in decreasing beta^2
         std::vector<cd> lams, X;
-        rc = solve_pencil_k(n, A, Bm, -k0 * k0 * emax, mode + 1, lams, X);
+        rc = solve_pencil_k(n, A, Bm, -k0 * k0 * emax, mode + 1, lams, X, nut);
         if (rc == OPEM_OK) {
             lam = lams[mode];
             xs.assign(X.begin() + (size_t)mode * n, X.begin() + (size_t)(mode + 1) * n);

@@ -241,7 +241,20 @@ def solve_mode_pp(pts, tris, freq, eps_r, mu_r=None, p=1, mode=0):
     B = B[keep][:, keep].tocsc()
     sigma = -k0 ** 2 * np.max(np.real(eps_r * mu_r))
     lu = spla.splu((A - sigma * B).tocsc(), permc_spec="MMD_AT_PLUS_A")
-    op = spla.LinearOperator(A.shape, matvec=lambda x: lu.solve(B @ x), dtype=complex)
+    # every (0, psi) solves A x = 0 B x: a null space between the propagating
+    # (lam < 0) and the cut-off (lam > 0) modes.  Setting psi from the e_z rows of
+    # B x = 0, which every eigenvector of a nonzero lam satisfies, removes it.
+    nt_ = len(ke)
+    Bz = B[nt_:, nt_:].tocsc()
+    Bzt = B[nt_:, :nt_].tocsr()
+    luz = spla.splu(Bz, permc_spec="MMD_AT_PLUS_A") if Bz.shape[0] else None
+
+    def op_mv(x):
+        y = lu.solve(B @ x)
+        if luz is not None:
+            y[nt_:] = luz.solve(-(Bzt @ y[:nt_]))
+        return y
+    op = spla.LinearOperator(A.shape, matvec=op_mv, dtype=complex)
     mu, vec = spla.eigs(op, k=mode + 1, which="LM", tol=1e-14 if mode else 0)
     order = np.argsort(-np.abs(mu))          # nearest the shift first: decreasing beta^2
     lam = sigma + 1.0 / mu[order[mode]]
