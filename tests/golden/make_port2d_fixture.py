@@ -23,6 +23,12 @@ CASES = {
     "PartFilled_order_4": ("partially_filled_rect_waveguide/PartFilled_order_4_norefinement", "PartFilled.proj"),
     "PartFilled_order_5": ("partially_filled_rect_waveguide/PartFilled_order_5_norefinement", "PartFilled.proj"),
     "PartFilled_order_6": ("partially_filled_rect_waveguide/PartFilled_order_6_norefinement", "PartFilled.proj"),
+    # meshes refined uniformly (mesh.uniform_refinement.count) before the solve
+    "WR90_order_3_refined3": ("WR90_rectangular_waveguide/WR90/WR90_order_3_no_refinement_no_mesh_reuse", "WR90.proj"),
+    "PartFilled_order_3_refined1": ("partially_filled_rect_waveguide/PartFilled_order_3_norefinement",
+                                    "PartFilled.proj"),
+    "PartFilled_order_4_refined1_wide": ("partially_filled_rect_waveguide/PartFilled_order_4_norefinement_widebandwidth",
+                                         "PartFilled.proj"),
 }
 
 
@@ -98,7 +104,7 @@ def main(ref):
     for case, (rel, pf) in CASES.items():
         d = os.path.join(root, rel)
         kv = read_proj2d(os.path.join(d, pf))
-        assert kv.get("refinement.frequency") == "none" and kv.get("mesh.uniform_refinement.count", "0") == "0"
+        assert kv.get("refinement.frequency") == "none"
         xy, tris, phys, names = read_mesh2d(os.path.join(d, kv["mesh.file"]))
         mdb = [os.path.join(d, kv.get("materials.local.path", "./"), kv.get("materials.local.name") or "-"),
                os.path.join(d, kv.get("materials.global.path", "./"), kv.get("materials.global.name") or "-")]
@@ -110,6 +116,7 @@ def main(ref):
         tc = [f for f in os.listdir(d) if f.endswith("_exact_test_cases.csv")][0]
         cases = [r for r in read_test_cases(os.path.join(d, tc)) if "_result_" in r[0]]
         out[case] = {"project": f"regression/OpenParEM2D/{rel}/{pf}", "order": int(kv["mesh.order"]),
+                     "uniform_refinement": int(kv.get("mesh.uniform_refinement.count", "0") or 0),
                      "modes": int(kv["solution.modes"]), "impedance": kv.get("solution.impedance.definition", "none"),
                      "freqs": freqs, "xy": xy, "tris": tris, "material": [names[p] for p in phys],
                      "materials": mats, "vpaths": {str(k): v for k, v in vpaths.items()}, "cases": cases}

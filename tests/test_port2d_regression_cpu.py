@@ -30,16 +30,41 @@ def _cases():
         return json.load(f)["cases"]
 
 
-# (the order-5 and order-6 partially filled cases of the fixture pass as well and
-# take minutes: the suite runs order 4 at its first frequency)
-@pytest.mark.parametrize("name,nfreq", [("WR90_order_6", 2), ("PartFilled_order_4", 1)])
+def refine_uniform(xy, tris, material):
+    """One uniform refinement (mesh.uniform_refinement.count): every triangle
+    into four by its edge midpoints.  The discrete modes depend on the refined
+    mesh only, not on how its nodes and triangles are numbered."""
+    xy = [tuple(p) for p in xy]
+    mid = {}
+
+    def m(a, b):
+        k = (min(a, b), max(a, b))
+        if k not in mid:
+            mid[k] = len(xy)
+            xy.append(tuple(0.5 * (np.asarray(xy[a]) + np.asarray(xy[b]))))
+        return mid[k]
+    out, mat = [], []
+    for (a, b, c), mt in zip(tris, material):
+        ab, bc, ca = m(a, b), m(b, c), m(c, a)
+        out += [(a, ab, ca), (ab, b, bc), (ca, bc, c), (ab, bc, ca)]
+        mat += [mt] * 4
+    return np.asarray(xy), np.asarray(out, dtype=np.int64), mat
+
+
+# (the order-5 and order-6 partially filled cases and the refined order-3 one of
+# the fixture pass as well and take minutes: the suite runs the others at their
+# first frequency, WR90 at order 6 at both)
+@pytest.mark.parametrize("name,nfreq", [("WR90_order_6", 2), ("PartFilled_order_4", 1),
+                                        ("WR90_order_3_refined3", 1)])
 def test_reference_2d_regression_cases(name, nfreq):
     c = _cases()[name]
     c["freqs"] = c["freqs"][:nfreq]
     c["cases"] = [r for r in c["cases"] if float(r[1]) in c["freqs"]]
     xy = np.asarray(c["xy"], dtype=float)
-    verts = np.column_stack([xy, np.zeros(len(xy))])
     tris = np.asarray(c["tris"], dtype=np.int64)
+    for _ in range(c["uniform_refinement"]):
+        xy, tris, c["material"] = refine_uniform(xy, tris, c["material"])
+    verts = np.column_stack([xy, np.zeros(len(xy))])
     eps = np.array([c["materials"][m]["er"] for m in c["material"]], dtype=complex)
     mu = np.array([c["materials"][m]["mur"] for m in c["material"]], dtype=complex)
     lo, hi = xy.min(axis=0), xy.max(axis=0)
