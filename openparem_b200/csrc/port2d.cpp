@@ -133,12 +133,58 @@ std::vector<int> rcm(int n, const std::vector<std::vector<int>>& adj, int start 
 }
 
 // Fundamental eigenpair of the pencil A x = -beta^2 B x (largest beta^2) by
+// The pencil's A has no e_z block, so every (0, psi) is an eigenvector with
+// lam = 0: a null space as large as the e_z space, which lies between the
+// propagating modes (lam < 0) and the cut-off ones (lam > 0) and captures an
+// iteration about a shift below them once the wanted mode is cut off.  With the
+// unknowns from nut on being psi, PsiConstraint sets psi to the solution of the
+// e_z rows of B x = 0 (psi = -B_zz^-1 B_zt e_t), which every eigenvector of a
+// nonzero lam satisfies; applied after every step it removes any null-space
+// component.  pos: the iteration's permuted numbering.
+struct PsiConstraint {
+    int n = 0, nut = 0, nz = 0;
+    std::vector<Triplet> Bzt;
+    Banded Mz;
+    std::vector<int> zpos;
+    std::vector<cd> zr;
+    bool init(int n_, int nut_, const std::vector<Triplet>& Bm) {
+        n = n_; nut = nut_; nz = n - nut;
+        if (nz <= 0) return true;
+        std::vector<std::vector<int>> zadj(nz);
+        for (auto& t : Bm) {
+            if (t.r < nut) continue;
+            if (t.c < nut) Bzt.push_back(t);
+            else if (t.r != t.c) zadj[t.r - nut].push_back(t.c - nut);
+        }
+        for (auto& a : zadj) { std::sort(a.begin(), a.end()); a.erase(std::unique(a.begin(), a.end()), a.end()); }
+        std::vector<int> zord = rcm(nz, zadj);
+        zpos.assign(nz, 0);
+        for (int i = 0; i < nz; ++i) zpos[zord[i]] = i;
+        int zbw = 0;
+        for (int i = 0; i < nz; ++i)
+            for (int j : zadj[i]) zbw = std::max(zbw, std::abs(zpos[i] - zpos[j]));
+        Mz.init(nz, zbw, zbw);
+        for (auto& t : Bm)
+            if (t.r >= nut && t.c >= nut) Mz.at(zpos[t.r - nut], zpos[t.c - nut]) += t.v;
+        zr.assign(nz, 0.0);
+        return Mz.factor();
+    }
+    void apply(cd* y, const std::vector<int>& pos) {
+        if (nz <= 0) return;
+        std::fill(zr.begin(), zr.end(), cd(0.0));
+        for (auto& t : Bzt) zr[zpos[t.r - nut]] -= t.v * y[pos[t.c]];
+        Mz.solve(zr);
+        for (int i = 0; i < nz; ++i) y[pos[nut + i]] = zr[zpos[i]];
+    }
+};
+
 // inverse iteration with the shift sigma: RCM ordering, banded LU of A - sigma B,
 // converged when the eigenvalue has settled and the unit eigenvector stops
 // moving (up to phase).  Returns an OPEM_* code; lam = -beta^2, xout unit norm
-// in the caller's numbering.
+// in the caller's numbering.  nut < n: the unknowns from nut on are psi, held to
+// PsiConstraint.
 int solve_pencil(int n, const std::vector<Triplet>& A, const std::vector<Triplet>& Bm, double sigma, cd& lam,
-                 std::vector<cd>& xout) {
+                 std::vector<cd>& xout, int nut = -1) {
     // ordering and band
     std::vector<std::vector<int>> adj(n);
     for (auto* T : {&A, &Bm})
@@ -182,6 +228,8 @@ int solve_pencil(int n, const std::vector<Triplet>& A, const std::vector<Triplet
     };
     cd shift = sigma;
     if (!factor_at(shift)) return OPEM_ERR_BREAKDOWN;
+    PsiConstraint psi;
+    if (nut > 0 && nut < n && !psi.init(n, nut, Bm)) return OPEM_ERR_BREAKDOWN;
     bool refreshed = false;
     // inverse iteration: y = (A - sigma B)^-1 B x; its dominant eigenvalue mu gives lambda = sigma + 1/mu
     auto Bmul = [&](const std::vector<cd>& x, std::vector<cd>& y) {
@@ -190,6 +238,7 @@ int solve_pencil(int n, const std::vector<Triplet>& A, const std::vector<Triplet
     };
     std::vector<cd> x(n), y(n), bx(n), xold(n);
     for (int i = 0; i < n; ++i) x[i] = cd(1.0 + 0.001 * (i % 7), 0.0005 * (i % 5));
+    psi.apply(x.data(), pos);
     cd lam_prev = 0;
     lam = 0;
     bool ok = false;
@@ -199,6 +248,7 @@ int solve_pencil(int n, const std::vector<Triplet>& A, const std::vector<Triplet
         Bmul(x, bx);
         y = bx;
         M.solve(y);
+        psi.apply(y.data(), pos);
         // Rayleigh-type estimate mu = (x^H B y) / (x^H B x), B symmetric
         std::vector<cd> by(n);
         Bmul(y, by);
@@ -250,13 +300,8 @@ int solve_pencil(int n, const std::vector<Triplet>& A, const std::vector<Triplet
 // Rayleigh-Ritz on the projected pencil: converged when every wanted Ritz pair's
 // residual is below 1e-11 relative and its value has settled to 1e-13.  lam[i] = -beta_i^2 in increasing distance from sigma, X (n x k,
 // column-major) the Ritz vectors in the caller's numbering.
-// The pencil's A has no e_z block, so every (0, psi) is an eigenvector with
-// lam = 0: a null space as large as the e_z space, which lies between the
-// propagating modes (lam < 0) and the cut-off ones (lam > 0) and would capture
-// the iteration.  The unknowns from nut on are psi; after every step psi is set
-// to the solution of the e_z rows of B x = 0 (psi = -B_zz^-1 B_zt e_t), which
-// every eigenvector of a nonzero lam satisfies and which removes any null-space
-// component, so cut-off modes are found too.
+// The unknowns from nut on are psi, held to PsiConstraint after every step, so
+// cut-off modes are found too.
 int solve_pencil_k(int n, const std::vector<Triplet>& A, const std::vector<Triplet>& Bm, double sigma, int k,
                    std::vector<cd>& lam, std::vector<cd>& X, int nut) {
     const int q = std::min(n, k + 2);
@@ -281,37 +326,9 @@ int solve_pencil_k(int n, const std::vector<Triplet>& A, const std::vector<Tripl
         std::fill(y, y + n, cd(0.0));
         for (auto& t : T) y[pos[t.r]] += t.v * x[pos[t.c]];
     };
-    // B_zz (banded LU, RCM order of its own pattern) and B_zt for the psi constraint
-    const int nz = n - nut;
-    std::vector<Triplet> Bzt;
-    Banded Mz;
-    std::vector<int> zpos(std::max(nz, 0));
-    if (nz > 0) {
-        std::vector<std::vector<int>> zadj(nz);
-        for (auto& t : Bm) {
-            if (t.r < nut) continue;
-            if (t.c < nut) Bzt.push_back(t);
-            else if (t.r != t.c) zadj[t.r - nut].push_back(t.c - nut);
-        }
-        for (auto& a : zadj) { std::sort(a.begin(), a.end()); a.erase(std::unique(a.begin(), a.end()), a.end()); }
-        std::vector<int> zord = rcm(nz, zadj);
-        for (int i = 0; i < nz; ++i) zpos[zord[i]] = i;
-        int zbw = 0;
-        for (int i = 0; i < nz; ++i)
-            for (int j : zadj[i]) zbw = std::max(zbw, std::abs(zpos[i] - zpos[j]));
-        Mz.init(nz, zbw, zbw);
-        for (auto& t : Bm)
-            if (t.r >= nut && t.c >= nut) Mz.at(zpos[t.r - nut], zpos[t.c - nut]) += t.v;
-        if (!Mz.factor()) return OPEM_ERR_BREAKDOWN;
-    }
-    std::vector<cd> zr(std::max(nz, 0));
-    auto constrain = [&](cd* y) {   // y in the permuted numbering
-        if (nz == 0) return;
-        std::fill(zr.begin(), zr.end(), cd(0.0));
-        for (auto& t : Bzt) zr[zpos[t.r - nut]] -= t.v * y[pos[t.c]];
-        Mz.solve(zr);
-        for (int i = 0; i < nz; ++i) y[pos[nut + i]] = zr[zpos[i]];
-    };
+    PsiConstraint psi;
+    if (!psi.init(n, nut, Bm)) return OPEM_ERR_BREAKDOWN;
+    auto constrain = [&](cd* y) { psi.apply(y, pos); };   // y in the permuted numbering
     std::vector<cd> Y((size_t)n * q), AY((size_t)n * q), BY((size_t)n * q), tmp(n);
     for (int c = 0; c < q; ++c) {
         for (int i = 0; i < n; ++i) Y[(size_t)c * n + i] = cd(1.0 + 0.001 * ((i * (c + 3)) % 11), 0.0007 * ((i + 5 * c) % 7));
@@ -1057,7 +1074,7 @@ int port_mode_2d_pp(int64_t nnodes, const double* xy, int64_t ntri, const int64_
     std::vector<cd> xs;
     int rc;
     if (mode == 0) {
-        rc = solve_pencil(n, A, Bm, -k0 * k0 * emax, lam, xs);
+        rc = solve_pencil(n, A, Bm, -k0 * k0 * emax, lam, xs, nut);
     } else {   // the mode-th mode in decreasing beta^2
         std::vector<cd> lams, X;
         rc = solve_pencil_k(n, A, Bm, -k0 * k0 * emax, mode + 1, lams, X, nut);
