@@ -107,13 +107,16 @@ int  opem_problem_set_port_te(opem_problem prob, int port, const double* desc);
 /* Port driven by the fundamental mode of its own cross-section, solved at every
  * frequency on the port faces split nsub x nsub (1..64) with the materials of
  * the tetrahedra behind them (the 2D solve the reference spawns per frequency,
- * port.cpp:5081-5176).  order 1: lowest-order edge elements for e_t and linear
- * nodal e_z (opem_port_mode_2d's solve); order 2: degree-2 edge elements and
- * quadratic nodal e_z (beta converges at fourth order in the split); order p up
- * to 8: first-kind edge elements of order p and degree-p nodal e_z, the spaces of
- * the reference's 2D solver at mesh.order p (with nsub 1 and p the 3D order the
- * mode lies in the 3D port trace space).  desc as for opem_problem_set_port_te;
- * its a, b, m, n are not used.                                                 */
+ * port.cpp:5081-5176).  On split faces (nsub > 1) order 1: lowest-order edge
+ * elements for e_t and linear nodal e_z (opem_port_mode_2d's solve); order 2:
+ * degree-2 edge elements and quadratic nodal e_z (beta converges at fourth order
+ * in the split).  With nsub 1, or order 3 to 8: first-kind edge elements of order
+ * p and degree-p nodal e_z, the spaces of the reference's 2D solver at
+ * mesh.order p; with nsub 1 and p the 3D order the mode lies in the 3D port trace
+ * space, and the port follows the reference's 2D solver further: H_t projected
+ * onto the edge space, Pz and the port's overlap integrals by the nodal rules of
+ * MFEM's L2 triangle.  desc as for opem_problem_set_port_te; its a, b, m, n are
+ * not used.                                                                    */
 int  opem_problem_set_port_fem2d(opem_problem prob, int port, const double* desc, int nsub, int order);
 /* Impedance definition of a port driven by its own 2D mode (after
  * opem_problem_set_port_fem2d; the reference's impedance_definition and current
